@@ -1,0 +1,359 @@
+"""Benchmark of the B200 room solver.
+
+Default workload (N=1): the large thermal room, 10x8x3 m on a 320x256x96
+MAC grid (7.86 M cells), two facing 3 m/s fans, Boussinesq buoyancy, heated
+floor / cooled ceiling patches, four seeded boxes, dt = 0.005 s, pressure to
+1e-8.  A step is one projection time step of that room; inputs are larger
+than L2 (u, v, w, p, T alone are 315 MB), so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload large_thermal|lbm_room|basic_room]
+                    [--precision fp64|mixed]
+
+Under torchrun every rank runs its own replica of the room on its GPU (rooms
+are independent: weak scaling, no collective on the data path); the time is
+the max over ranks.  The reference arm times the reference's own CPU solver
+(oracle/_ref, compiled from the reference sources) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ff-room_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "cell-steps/s & room-solves/s, mixed-prec batched vs plain FP64 on B200; p50/p99"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+# Algorithmic bytes per cell (FP64 fields, 2-byte stencil code, 1-byte
+# masks/codes); see DESIGN.md for the derivation.
+CG_INIT_B = 50.0       # read u*,v*,w* + code, write r, d, x
+CG_ITER_B = 74.0       # phase A (r, d_old, x, code -> d, Ad, x) + phase B (r, Ad -> r)
+CG_FINAL_B = 24.0      # x += alpha d
+LBM_STEP_B = {"fp64": 2 * 19 * 8 + 1 + 4 * 8, "fp32": 2 * 19 * 4 + 1 + 4 * 8, "fp16": 2 * 19 * 2 + 1 + 4 * 8}
+
+
+def measured_peak():
+    try:
+        with open(PEAKS) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def load_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh).get(kernel)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------- workloads
+
+def make_workload(name: str, precision: str):
+    from ffrb import workloads
+    from ffrb.params import params_from_scene
+    from ffrb.scene import build_room
+    if name == "large_thermal":
+        cfg, params = workloads.large_thermal()
+        if precision == "fp64":
+            params = params.with_(precision="fp64", poisson="cg")
+        return "fluid", cfg, build_room(cfg), params
+    if name == "basic_room":
+        cfg = workloads.basic_room()
+        return "fluid", cfg, build_room(cfg), params_from_scene(cfg)
+    if name == "lbm_room":
+        cfg, tau, dt = workloads.lbm_room()
+        return "lbm", cfg, build_room(cfg), {"tau": tau, "dt": dt, "storage": "fp64" if precision == "fp64"
+                                            else ("fp16" if precision == "fp16" else "fp32")}
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ---------------------------------------------------------- our arm
+
+def run_ours(args, rank: int, world: int, dist):
+    import torch
+    from ffrb import capi
+    kind, cfg, room, params = make_workload(args.workload, args.precision)
+    dev = torch.cuda.current_device()
+    cells = room.n_cells
+    if kind == "fluid":
+        h = capi.FluidHandle(room, params)
+    else:
+        h = capi.LbmHandle(room, params["tau"], args.steps + args.warmup, 0.0, params["dt"], params["storage"])
+    h.advance(args.warmup)
+    h.synchronize()
+    stream = torch.cuda.ExternalStream(h.stream())
+    h.profile(True)
+    l0 = capi.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        ev0.record(stream)
+        recs = h.advance(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = capi.launch_count() - l0
+    ms = ev0.elapsed_time(ev1)
+    prof = h.profile_read()
+    h.profile(False)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    steps_done = len(recs)
+    value = world * cells * steps_done / (ms / 1e3)
+    peak, peak_kind = measured_peak()
+    if kind == "fluid":
+        iters = [r["cg_iterations"] for r in recs]
+        bytes_cg = sum(cells * (CG_INIT_B + CG_ITER_B * it + CG_FINAL_B) for it in iters)
+        t_cg = prof["pressure"][0] / 1e3
+        achieved = bytes_cg / t_cg / 1e9
+        launches_cg = max(1, prof["pressure"][1])
+        roof = {"bound": "hbm", "kernel": "k_cg (persistent pressure CG)", "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "traffic": load_traffic("k_cg_per_cell_iter"),
+                "algorithmic_bytes_per_launch": bytes_cg / launches_cg,
+                "share_of_step": round(prof["pressure"][0] / ms, 4),
+                "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}
+        extra = {"cg_iterations_mean": float(np.mean(iters)), "velocity_change_last": recs[-1]["velocity_change"]}
+    else:
+        b = LBM_STEP_B[params["storage"]] * cells * steps_done
+        t_k = prof["stream_collide"][0] / 1e3
+        achieved = b / t_k / 1e9
+        roof = {"bound": "hbm", "kernel": "k_lbm_step (fused pull-stream/collide)", "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": load_traffic("k_lbm_step_per_cell"),
+                "algorithmic_bytes_per_launch": b / max(1, steps_done),
+                "share_of_step": round(prof["stream_collide"][0] / ms, 4),
+                "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}
+        extra = {"storage": params["storage"]}
+    h.close()
+    e2e = run_e2e(args, kind, room, params) if rank == 0 else None
+    return {"value": value, "ms": ms, "steps": steps_done, "launches": launches, "roofline": roof,
+            "clocks": clk.summary(), "extra": extra, "e2e": e2e, "cells": cells, "kind": kind}
+
+
+def run_e2e(args, kind, room, params):
+    """The same metric through the public C ABI from host buffers: upload the
+    room and the initial fields, run the steps, read every field back."""
+    from ffrb import capi
+    n = room.n_cells
+    shapes = room.shapes()
+    init = {k: np.zeros(int(np.prod(shapes[k]))) for k in ("u", "v", "w", "p")}
+    h2d = sum(a.nbytes for a in init.values()) + n + 3 * 8 * (room.nx + room.ny + room.nz)
+    t0 = time.perf_counter()
+    if kind == "fluid":
+        h = capi.FluidHandle(room, params, init)
+        recs = h.advance(args.steps)
+        out = {k: h.get(k) for k in "uvwpT"}
+    else:
+        h = capi.LbmHandle(room, params["tau"], args.steps, 0.0, params["dt"], params["storage"], init)
+        recs = h.advance(args.steps)
+        out = {k: h.get(k) for k in "uvwp"}
+    h.close()
+    t = time.perf_counter() - t0
+    d2h = sum(a.nbytes for a in out.values()) + 48 * len(recs)
+    steps = len(recs)
+    return {"value": n * steps / t, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps, "wall_s": t,
+            "includes": "room upload + solver setup + steps + all fields read back"}
+
+
+# ------------------------------------------------- CPU reference timing
+
+def cpu_reference(args, kind, room, params, gpu_iters=None, max_seconds=30.0):
+    """The reference solver (oracle/_ref driver, OpenMP on all host threads)
+    on a bounded sample of the workload."""
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    cells = room.n_cells
+    if not orc.ref_available():
+        return None
+    drv = orc.RefDriver()
+    if kind == "lbm":
+        t0 = time.perf_counter()
+        drv.lbm_run(room, params["tau"], params["dt"], 0.0, 2)
+        t = time.perf_counter() - t0
+        return {"value": cells * 2 / t, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
+                "sample": f"2 LBM steps of the {room.nx}x{room.ny}x{room.nz} lattice (the reference LBM has no OpenMP)"}
+    # projection: time one step at two CG caps, fit the per-iteration cost,
+    # extrapolate to the iteration count the same CG needs per step
+    caps = (20, 60)
+    ts = []
+    for cap in caps:
+        p = params.with_(poisson_max_iter=cap, precision="fp64", poisson="cg")
+        t0 = time.perf_counter()
+        drv.fluid_run(room, p, 1, use_openmp=True)
+        ts.append(time.perf_counter() - t0)
+    per_it = max(1e-9, (ts[1] - ts[0]) / (caps[1] - caps[0]))
+    base = max(0.0, ts[0] - caps[0] * per_it)
+    n_it = gpu_iters if gpu_iters else caps[1]
+    t_step = base + per_it * n_it
+    return {"value": cells / t_step, "unit": "cell-steps/s", "cores": threads, "kind": "reference",
+            "sample": (f"1 step of the {room.nx}x{room.ny}x{room.nz} room through the reference FluidSolver "
+                       f"(OpenMP, {threads} threads) at CG caps {caps[0]} and {caps[1]}; fixed cost "
+                       f"{base:.3f} s + {per_it * 1e3:.2f} ms/CG iteration, extrapolated to {n_it:.0f} "
+                       "iterations per step (the plain FP64 CG count of this room)")}
+
+
+def reference_arm(args):
+    """bench.py --impl reference: the reference's CPU solver, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    kind, cfg, room, params = make_workload(args.workload, args.precision)
+    import oracle as orc
+    if not orc.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}))
+        return
+    gpu_iters = args.ref_cg_iters
+    samples = []
+    for _ in range(max(1, args.steps)):
+        cb = cpu_reference(args, kind, room, params, gpu_iters)
+        samples.append(cb["value"])
+    v = statistics.median(samples)
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": room.n_cells / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_of(args, room, kind, params),
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def config_of(args, room, kind, params):
+    c = {"workload": args.workload, "grid": [room.nx, room.ny, room.nz], "cells": room.n_cells,
+         "l2": "inputs larger than L2 (no flush)" if room.n_cells * 8 * 5 > 126e6 else "L2 flush not applied",
+         "parallelism": f"replicas x{args.gpus}"}
+    if kind == "fluid":
+        c.update({"precision": params.precision, "poisson": params.poisson, "poisson_tol": params.poisson_tol,
+                  "dt": params.dt, "advection": params.advection, "thermal": params.thermal,
+                  "buoyancy": params.buoyancy})
+    else:
+        c.update(params)
+    return c
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="large_thermal")
+    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--ref-cg-iters", type=float, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = td
+    else:
+        torch.cuda.set_device(0)
+    res = run_ours(args, rank, world, dist)
+    if rank == 0:
+        kind, cfg, room, params = make_workload(args.workload, args.precision)
+        cb = None
+        if not args.no_cpu_baseline:
+            gi = res["extra"].get("cg_iterations_mean")
+            if kind == "fluid" and params.precision != "fp64":
+                gi = None
+            cb = cpu_reference(args, kind, room, params, gi)
+        dtype = {"fp64": "f64", "mixed": "f32/f64", "fp32": "f32", "fp16": "f16/f32"}.get(args.precision, args.precision)
+        line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
+                "steps": res["steps"], "warmup": args.warmup, "ms_per_step": res["ms"] / max(1, res["steps"]),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+                "data": "synthetic", "config": config_of(args, room, kind, params),
+                "roofline": res["roofline"], "cpu_baseline": cb, "e2e": res["e2e"],
+                "gpu_launches": res["launches"], "clocks": res["clocks"], "detail": res["extra"]}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,299 @@
+// common.cuh — shared device/host helpers of libffroom_cuda.so (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "ffroom.h"
+
+namespace ffr {
+
+// ------------------------------------------------------------ errors
+
+void set_error(const std::string &msg);
+int fail(int status, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+void count_launch(unsigned n = 1);
+
+#define FFR_CUDA(call)                                                        \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return ::ffr::cuda_fail(e_, #call);            \
+    } while (0)
+
+#define FFR_LAUNCHED(n)                                                       \
+    do {                                                                      \
+        cudaError_t e_ = cudaGetLastError();                                  \
+        if (e_ != cudaSuccess) return ::ffr::cuda_fail(e_, "kernel launch");  \
+        ::ffr::count_launch(n);                                               \
+    } while (0)
+
+// Cell types (Grid.hpp:9-14).
+enum : uint8_t { CT_FLUID = 0, CT_SOLID = 1, CT_INFLOW = 2, CT_OUTFLOW = 3 };
+
+// Face override codes, one byte per face: the low 7 bits say what the
+// no-slip + inflow appliers leave on the face (0 keep, 1 zero, 2+f the
+// velocity of fan f); bit 7 marks a zero-gradient outflow destination.
+enum : uint8_t { FC_KEEP = 0, FC_ZERO = 1, FC_FAN0 = 2, FC_OUTCOPY = 0x80 };
+constexpr int kMaxFans = 120;
+
+// Pressure-stencil code, one uint16 per cell: 2 bits per neighbour in the
+// order x-, x+, y-, y+, z-, z+ (0 no term, 1 interior, 2 Dirichlet ghost of
+// an OUTFLOW neighbour) and bit 12 for a SOLID (identity) row.
+enum : uint16_t { SC_NONE = 0, SC_IN = 1, SC_DIR = 2, SC_SOLID = 1u << 12 };
+
+// --------------------------------------------------------- room setup
+
+struct RoomGeom {
+    int nx, ny, nz;
+    long long n, nu, nv, nw;
+    double lx, ly, lz;
+};
+
+// Host-side, fully validated copy of an ffr_room_desc.
+struct HostRoom {
+    RoomGeom g;
+    std::vector<double> dxv, dyv, dzv;
+    std::vector<uint8_t> ct;
+    std::vector<ffr_fan> fans;
+    std::vector<ffr_patch> patches;
+    std::vector<ffr_heat_patch> heats;
+    long long n_fluid = 0;
+};
+
+int load_room(const ffr_room_desc *d, HostRoom &out);
+
+// Face codes (fc_u/v/w) from the reference BC appliers, replayed on codes.
+void build_face_codes(const HostRoom &r, std::vector<uint8_t> &fu,
+                      std::vector<uint8_t> &fv, std::vector<uint8_t> &fw);
+// Pressure stencil codes and per-axis stencil scales (PoissonSolver.cpp:33-49).
+void build_stencil(const HostRoom &r, std::vector<uint16_t> &sc,
+                   std::vector<double> &scale /* 2*(nx+ny+nz): l,r per index */);
+
+// ------------------------------------------------------ device memory
+
+// One cudaMalloc per handle, carved into 256-byte aligned slices.
+struct Arena {
+    char *base = nullptr;
+    size_t size = 0, used = 0;
+    int alloc(size_t bytes);
+    template <class T> T *take(size_t count) {
+        size_t b = (count * sizeof(T) + 255) & ~size_t(255);
+        if (used + b > size) return nullptr;
+        T *p = reinterpret_cast<T *>(base + used);
+        used += b;
+        return p;
+    }
+    void release();
+};
+
+// ------------------------------------------------ grid-wide barrier
+
+// Counter barrier for a cooperative launch (all blocks co-resident).  Every
+// wait is bounded by `kBarrierTimeoutNs`; a block that gives up sets `err`
+// and returns false so that the kernel can unwind.
+struct GridSync {
+    unsigned int count;
+    unsigned int gen;
+    int err;
+    int pad;
+};
+constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;  // 4 s
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Deterministic block sum (fixed shuffle tree, fixed warp order).  All
+// threads get the total.  `sh` holds >= 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double t = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+    if (wid == 0) t = warp_sum(t);
+    if (threadIdx.x == 0) sh[0] = t;
+    __syncthreads();
+    t = sh[0];
+    __syncthreads();
+    return t;
+}
+
+__device__ __forceinline__ double block_max(double v, double *sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    v = warp_max(v);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double t = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+    if (wid == 0) t = warp_max(t);
+    if (threadIdx.x == 0) sh[0] = t;
+    __syncthreads();
+    t = sh[0];
+    __syncthreads();
+    return t;
+}
+
+// Grid-wide sum of NV values: block partials go to partials[b*NV+v]; the
+// last block to arrive adds them in block order (so the result does not
+// depend on arrival order), publishes out[v] and releases the others.
+// Returns false when the wait timed out.
+template <int NV>
+__device__ bool grid_allreduce(GridSync *gs, double *partials, double *out, double (&vals)[NV],
+                               double *sh)
+{
+    __shared__ int s_last, s_ok;
+    for (int v = 0; v < NV; v++) {
+        double t = block_sum(vals[v], sh);
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NV + v] = t;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned g = ld_acquire(&gs->gen);
+        const unsigned arrived = atomicAdd(&gs->count, 1u);
+        s_last = (arrived == gridDim.x - 1);
+        s_ok = 1;
+        if (!s_last) {
+            const unsigned long long t0 = global_ns();
+            while (ld_acquire(&gs->gen) == g) {
+                __nanosleep(64);
+                if (global_ns() - t0 > kBarrierTimeoutNs || *(volatile int *)&gs->err) {
+                    atomicExch(&gs->err, 1);
+                    s_ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int v = 0; v < NV; v++) {
+            double t = 0.0;
+            for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+                t += __ldcg(&partials[(size_t)b * NV + v]);
+            t = block_sum(t, sh);
+            if (threadIdx.x == 0) __stcg(&out[v], t);
+        }
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicExch(&gs->count, 0u);
+            __threadfence();
+            atomicAdd(&gs->gen, 1u);
+        }
+    }
+    __syncthreads();
+    const bool ok = s_ok;
+    for (int v = 0; v < NV; v++) vals[v] = __ldcg(&out[v]);
+    __syncthreads();
+    return ok;
+}
+
+// Max of non-negative doubles through their bit patterns (monotone for
+// x >= 0).  NaN never reaches it: callers fold with fmax, which drops NaN
+// the way std::max(acc, x) does (FluidSolver.cpp:527-534).
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *slot, double v)
+{
+    if (v > 0.0) atomicMax(slot, (unsigned long long)__double_as_longlong(v));
+}
+
+inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+// Event-pair timing of kernel groups on one stream (host side).
+struct GroupTimer {
+    bool on = false;
+    int ngroups = 0;
+    std::vector<cudaEvent_t> pool;
+    struct Pending { int group; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<double> ms;
+    std::vector<long long> launches;
+    cudaEvent_t open_ev = nullptr;
+    int open_group = -1;
+
+    void reset(int groups)
+    {
+        ngroups = groups;
+        ms.assign(groups, 0.0);
+        launches.assign(groups, 0);
+    }
+    cudaEvent_t take()
+    {
+        if (pool.empty()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    // Opens group g at the current point of stream s.
+    void begin(int g, cudaStream_t s)
+    {
+        if (!on) return;
+        open_ev = take();
+        open_group = g;
+        cudaEventRecord(open_ev, s);
+    }
+    void end(cudaStream_t s, int nlaunch)
+    {
+        if (!on || open_group < 0) return;
+        cudaEvent_t b = take();
+        cudaEventRecord(b, s);
+        pending.push_back({open_group, open_ev, b});
+        launches[open_group] += nlaunch;
+        open_group = -1;
+    }
+    // Call after the stream has been synchronised.
+    void collect()
+    {
+        for (const Pending &p : pending) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ms[p.group] += t;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void destroy()
+    {
+        collect();
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+        pool.clear();
+    }
+};
+
+}  // namespace ffr

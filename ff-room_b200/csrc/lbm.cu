@@ -1,0 +1,687 @@
+// lbm.cu — D3Q19 BGK lattice Boltzmann, fused pull-stream/collide (sm_100a).
+//
+// The reference step (LBMSolver::step, cpp/src/core/LBMSolver.cpp:402-440)
+// is inflow BC -> collision -> push streaming with halfway bounce-back into
+// a zeroed buffer -> outflow copy -> macroscopic extraction.  Here the state
+// kept between steps is the post-collision population f* of every cell, in
+// two A/B buffers.  One kernel per step
+//   1. pulls, for every non-SOLID cell x and direction q, f*_q(x - e_q) when
+//      that cell is in the domain and not SOLID, else f*_opp(q)(x): exactly
+//      the one value the reference's push delivers into slot q of x;
+//   2. for OUTFLOW cells first redirects x to the cell whose post-stream
+//      populations the reference's outflow copies leave there (the chain of
+//      copies is resolved on the host, in the reference's patch order);
+//   3. takes the moments (the reference's extract_macroscopic input) and
+//      writes the cell velocity and p = rho*cs^2;
+//   4. applies the next step's inflow BC / BGK collision and stores f*.
+// A second kernel forms the face velocities, max |du| and max |div|.
+//
+// Storage modes: FP64 (the reference arithmetic), FP32 and FP16.  The
+// narrow modes store the shifted populations g_q = f_q - w_q (the "DDF
+// shifting" of Lehmann, Krause, Amati, Sega, Harting & Gekle, Phys. Rev. E
+// 106, 015308 (2022)) and collide in FP32.
+#include "common.cuh"
+
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <type_traits>
+
+namespace ffr {
+
+__constant__ int c_ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+__constant__ int c_ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+__constant__ int c_ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+__constant__ int c_opp[19] = {0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17};
+
+// D3Q19 weights (LBMSolver.cpp:19-25).
+__host__ __device__ __forceinline__ double lbm_w(int q)
+{
+    return q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
+}
+
+// LBMSolver::feq (LBMSolver.hpp:89-93), cs2 = 1/3, in the reference's
+// operation order.
+__device__ __forceinline__ double feq64(int q, double rho, double ux, double uy, double uz)
+{
+    const double cs2 = 1.0 / 3.0;
+    const double eu = c_ex[q] * ux + c_ey[q] * uy + c_ez[q] * uz;
+    const double usq = ux * ux + uy * uy + uz * uz;
+    return lbm_w(q) * rho * (1.0 + eu / cs2 + eu * eu / (2.0 * cs2 * cs2) - usq / (2.0 * cs2));
+}
+
+// Shifted equilibrium feq_q - w_q in FP32 for rho = 1 + drho.
+__device__ __forceinline__ float geq32(int q, float drho, float ux, float uy, float uz)
+{
+    const float eu = c_ex[q] * ux + c_ey[q] * uy + c_ez[q] * uz;
+    const float usq = ux * ux + uy * uy + uz * uz;
+    const float rho = 1.0f + drho;
+    return (float)lbm_w(q) * (drho + rho * (3.0f * eu + 4.5f * eu * eu - 1.5f * usq));
+}
+
+template <int MODE> struct Store;
+template <> struct Store<0> {
+    using T = double;
+    __device__ static double ld(const double *p) { return *p; }
+    __device__ static void st(double *p, double v) { *p = v; }
+};
+template <> struct Store<1> {
+    using T = float;
+    __device__ static float ld(const float *p) { return *p; }
+    __device__ static void st(float *p, float v) { *p = v; }
+};
+template <> struct Store<2> {
+    using T = __half;
+    __device__ static float ld(const __half *p) { return __half2float(*p); }
+    __device__ static void st(__half *p, float v) { *p = __float2half_rn(v); }
+};
+
+struct LbmDev {
+    int nx, ny, nz, n, nu, nv, nw;
+    const uint8_t *ct;          // cell types
+    const uint8_t *fan_of;      // fan index of each INFLOW cell (255: none)
+    const double *fan_lat;      // lattice fan velocity, 3 per fan
+    const int *remap_dst;       // sorted OUTFLOW destinations
+    const int *remap_src;       // their resolved source cells
+    int nremap;
+    const double *dxv, *dyv, *dzv;
+    double tau, l2p;
+};
+
+struct LbmState {
+    int step, halt, stop_on_converge, par;
+    unsigned long long dmax_bits, div_bits;
+    int ring_slot, flags;
+};
+
+__device__ __forceinline__ int find_src(const LbmDev &L, int c)
+{
+    int lo = 0, hi = L.nremap - 1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int d = L.remap_dst[mid];
+        if (d == c) return L.remap_src[mid];
+        if (d < c) lo = mid + 1; else hi = mid - 1;
+    }
+    return c;
+}
+
+// One fused step; see the file comment.  fa = f* of this step, fb = f* of
+// the next, cu/cv/cw = cell-centred velocity (m/s), p = rho*cs^2.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_lbm_step(LbmDev L, const typename Store<MODE>::T *f0,
+                                                  typename Store<MODE>::T *f1, double *cu, double *cv,
+                                                  double *cw, double *p, const LbmState *st)
+{
+    using S = Store<MODE>;
+    using T = typename S::T;
+    if (st->halt) return;
+    const T *fa = st->par ? f1 : f0;
+    T *fb = st->par ? (T *)f0 : f1;
+    const int nx = L.nx, ny = L.ny, nz = L.nz, n = L.n, plane = ny * nz;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const uint8_t t = L.ct[c];
+        if (t == CT_SOLID) {
+            cu[c] = 0.0; cv[c] = 0.0; cw[c] = 0.0;
+            continue;
+        }
+        const int o = (t == CT_OUTFLOW && L.nremap) ? find_src(L, c) : c;
+        using C = typename std::conditional<MODE == 0, double, float>::type;
+        C fq[19];
+        if (L.ct[o] == CT_SOLID) {
+#pragma unroll
+            for (int q = 0; q < 19; q++) fq[q] = MODE == 0 ? C(0) : C(-lbm_w(q));
+        } else {
+            const int oi = o / plane, orem = o - oi * plane, oj = orem / nz, ok = orem - oj * nz;
+#pragma unroll
+            for (int q = 0; q < 19; q++) {
+                const int si = oi - c_ex[q], sj = oj - c_ey[q], sk = ok - c_ez[q];
+                const int s = o - c_ex[q] * plane - c_ey[q] * nz - c_ez[q];
+                const bool in = si >= 0 && si < nx && sj >= 0 && sj < ny && sk >= 0 && sk < nz;
+                if (in && L.ct[s] != CT_SOLID) fq[q] = S::ld(fa + (size_t)q * n + s);
+                else fq[q] = S::ld(fa + (size_t)c_opp[q] * n + o);
+            }
+        }
+        // moments (LBMSolver.cpp:306-318) and next-step collision
+        if (MODE == 0) {
+            double rho = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+#pragma unroll
+            for (int q = 0; q < 19; q++) {
+                rho += fq[q];
+                ux += fq[q] * c_ex[q];
+                uy += fq[q] * c_ey[q];
+                uz += fq[q] * c_ez[q];
+            }
+            if (rho > 1e-14) { ux /= rho; uy /= rho; uz /= rho; }
+            cu[c] = ux * L.l2p; cv[c] = uy * L.l2p; cw[c] = uz * L.l2p;
+            p[c] = rho * (1.0 / 3.0);
+            if (t == CT_INFLOW && L.fan_of[c] != 255) {
+                const double *fv = L.fan_lat + 3 * L.fan_of[c];
+#pragma unroll
+                for (int q = 0; q < 19; q++) S::st(fb + (size_t)q * n + c, feq64(q, 1.0, fv[0], fv[1], fv[2]));
+            } else if (t == CT_INFLOW) {
+#pragma unroll
+                for (int q = 0; q < 19; q++) S::st(fb + (size_t)q * n + c, fq[q]);
+            } else {
+                const double itau = 1.0 / L.tau;
+#pragma unroll
+                for (int q = 0; q < 19; q++) {
+                    const double fe = feq64(q, rho, ux, uy, uz);
+                    S::st(fb + (size_t)q * n + c, fq[q] + itau * (fe - fq[q]));
+                }
+            }
+        } else {
+            float drho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 19; q++) {
+                drho += fq[q];
+                jx += fq[q] * c_ex[q];
+                jy += fq[q] * c_ey[q];
+                jz += fq[q] * c_ez[q];
+            }
+            const float rho = 1.0f + drho;
+            float ux = jx, uy = jy, uz = jz;
+            if (rho > 1e-14f) { ux /= rho; uy /= rho; uz /= rho; }
+            cu[c] = (double)ux * L.l2p; cv[c] = (double)uy * L.l2p; cw[c] = (double)uz * L.l2p;
+            p[c] = (double)rho * (1.0 / 3.0);
+            if (t == CT_INFLOW && L.fan_of[c] != 255) {
+                const double *fv = L.fan_lat + 3 * L.fan_of[c];
+#pragma unroll
+                for (int q = 0; q < 19; q++)
+                    S::st(fb + (size_t)q * n + c, geq32(q, 0.0f, (float)fv[0], (float)fv[1], (float)fv[2]));
+            } else if (t == CT_INFLOW) {
+#pragma unroll
+                for (int q = 0; q < 19; q++) S::st(fb + (size_t)q * n + c, fq[q]);
+            } else {
+                const float itau = (float)(1.0 / L.tau);
+#pragma unroll
+                for (int q = 0; q < 19; q++) {
+                    const float ge = geq32(q, drho, ux, uy, uz);
+                    S::st(fb + (size_t)q * n + c, fq[q] + itau * (ge - fq[q]));
+                }
+            }
+        }
+    }
+}
+
+// Initial f* : f = w_q (LBMSolver.cpp:65-74), INFLOW cells feq(1, u_fan)
+// (apply_inflow_bc, LBMSolver.cpp:80-99), then the first collision.
+template <int MODE>
+__global__ void k_lbm_init(LbmDev L, typename Store<MODE>::T *f)
+{
+    using S = Store<MODE>;
+    const int n = L.n;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const uint8_t t = L.ct[c];
+        if (MODE == 0) {
+            double fq[19];
+            const bool fan = t == CT_INFLOW && L.fan_of[c] != 255;
+            const double *fv = fan ? L.fan_lat + 3 * L.fan_of[c] : nullptr;
+#pragma unroll
+            for (int q = 0; q < 19; q++) fq[q] = fan ? feq64(q, 1.0, fv[0], fv[1], fv[2]) : lbm_w(q);
+            if (t == CT_FLUID || t == CT_OUTFLOW) {
+                double rho = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
+                for (int q = 0; q < 19; q++) {
+                    rho += fq[q]; ux += fq[q] * c_ex[q]; uy += fq[q] * c_ey[q]; uz += fq[q] * c_ez[q];
+                }
+                if (rho > 1e-14) { ux /= rho; uy /= rho; uz /= rho; }
+                const double itau = 1.0 / L.tau;
+                for (int q = 0; q < 19; q++) fq[q] += itau * (feq64(q, rho, ux, uy, uz) - fq[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 19; q++) S::st(f + (size_t)q * n + c, fq[q]);
+        } else {
+            float g[19];
+            const bool fan = t == CT_INFLOW && L.fan_of[c] != 255;
+            const double *fv = fan ? L.fan_lat + 3 * L.fan_of[c] : nullptr;
+#pragma unroll
+            for (int q = 0; q < 19; q++)
+                g[q] = fan ? geq32(q, 0.0f, (float)fv[0], (float)fv[1], (float)fv[2]) : 0.0f;
+            if (t == CT_FLUID || t == CT_OUTFLOW) {
+                float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+                for (int q = 0; q < 19; q++) {
+                    drho += g[q]; jx += g[q] * c_ex[q]; jy += g[q] * c_ey[q]; jz += g[q] * c_ez[q];
+                }
+                const float rho = 1.0f + drho;
+                const float itau = (float)(1.0 / L.tau);
+                for (int q = 0; q < 19; q++) g[q] += itau * (geq32(q, drho, jx / rho, jy / rho, jz / rho) - g[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 19; q++) S::st(f + (size_t)q * n + c, g[q]);
+        }
+    }
+}
+
+// Face velocities of extract_macroscopic (LBMSolver.cpp:333-375), max
+// |du| against the previous faces (LBMSolver.cpp:423-433) and max |div|
+// over FLUID cells (LBMSolver.cpp:382-396), cell-centric like k_correct.
+__global__ void __launch_bounds__(256) k_lbm_faces(LbmDev L, const double *cu, const double *cv,
+                                                   const double *cw, double *u, double *v, double *w,
+                                                   LbmState *st)
+{
+    __shared__ double sh[32];
+    if (st->halt) return;
+    const int nx = L.nx, ny = L.ny, nz = L.nz, plane = ny * nz;
+    double dmax = 0.0, divmax = 0.0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.n; c += gridDim.x * blockDim.x) {
+        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+        const double ulo = (i == 0) ? cu[c] : 0.5 * (cu[c - plane] + cu[c]);
+        const double uhi = (i == nx - 1) ? cu[c] : 0.5 * (cu[c] + cu[c + plane]);
+        const double vlo = (j == 0) ? cv[c] : 0.5 * (cv[c - nz] + cv[c]);
+        const double vhi = (j == ny - 1) ? cv[c] : 0.5 * (cv[c] + cv[c + nz]);
+        const double wlo = (k == 0) ? cw[c] : 0.5 * (cw[c - 1] + cw[c]);
+        const double whi = (k == nz - 1) ? cw[c] : 0.5 * (cw[c] + cw[c + 1]);
+        const int uf = c, vf = (i * (ny + 1) + j) * nz + k, wf = (i * ny + j) * (nz + 1) + k;
+        dmax = fmax(dmax, fabs(ulo - u[uf])); u[uf] = ulo;
+        dmax = fmax(dmax, fabs(vlo - v[vf])); v[vf] = vlo;
+        dmax = fmax(dmax, fabs(wlo - w[wf])); w[wf] = wlo;
+        if (i == nx - 1) { dmax = fmax(dmax, fabs(uhi - u[uf + plane])); u[uf + plane] = uhi; }
+        if (j == ny - 1) { dmax = fmax(dmax, fabs(vhi - v[vf + nz])); v[vf + nz] = vhi; }
+        if (k == nz - 1) { dmax = fmax(dmax, fabs(whi - w[wf + 1])); w[wf + 1] = whi; }
+        if (L.ct[c] == CT_FLUID)
+            divmax = fmax(divmax, fabs((uhi - ulo) / L.dxv[i] + (vhi - vlo) / L.dyv[j] + (whi - wlo) / L.dzv[k]));
+    }
+    dmax = block_max(dmax, sh);
+    divmax = block_max(divmax, sh);
+    if (threadIdx.x == 0) {
+        atomic_max_nonneg(&st->dmax_bits, dmax);
+        atomic_max_nonneg(&st->div_bits, divmax);
+    }
+}
+
+__global__ void k_lbm_finalize(double dt, double tol, LbmState *st, ffr_step_result *ring)
+{
+    if (st->halt || threadIdx.x != 0) return;
+    const double vc = __longlong_as_double((long long)st->dmax_bits) / dt;
+    ffr_step_result r;
+    r.step = st->step + 1;
+    r.velocity_change = vc;
+    r.pressure_residual = 0.0;
+    r.divergence_max = __longlong_as_double((long long)st->div_bits);
+    r.converged = vc < tol;
+    r.T_mean = 0.0;
+    r.cg_iterations = 0;
+    r.flags = st->flags;
+    ring[st->ring_slot] = r;
+    st->ring_slot += 1;
+    st->step += 1;
+    st->par ^= 1;
+    st->dmax_bits = 0;
+    st->div_bits = 0;
+    st->flags = 0;
+    if (r.converged && st->stop_on_converge) st->halt = 1;
+}
+
+__global__ void k_lbm_divergence(LbmDev L, const double *u, const double *v, const double *w,
+                                 unsigned long long *out)
+{
+    __shared__ double sh[32];
+    const int ny = L.ny, nz = L.nz, plane = ny * nz;
+    double m = 0.0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.n; c += gridDim.x * blockDim.x) {
+        if (L.ct[c] != CT_FLUID) continue;
+        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+        const int vf = (i * (ny + 1) + j) * nz + k, wf = (i * ny + j) * (nz + 1) + k;
+        m = fmax(m, fabs((u[c + plane] - u[c]) / L.dxv[i] + (v[vf + nz] - v[vf]) / L.dyv[j] +
+                         (w[wf + 1] - w[wf]) / L.dzv[k]));
+    }
+    m = block_max(m, sh);
+    if (threadIdx.x == 0) atomic_max_nonneg(out, m);
+}
+
+}  // namespace ffr
+
+using namespace ffr;
+
+namespace {
+constexpr int kRingL = 1024;
+constexpr int kThr = 256;
+
+unsigned blocks_for(long long n)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return (unsigned)std::max<long long>(1, std::min<long long>((long long)sms * 8, (n + kThr - 1) / kThr));
+}
+}  // namespace
+
+struct ffr_lbm {
+    HostRoom room;
+    int storage;
+    double tau, dt, tol;
+    int max_steps;
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    LbmDev L;
+    void *f0, *f1;
+    double *cu, *cv, *cw, *u, *v, *w, *p;
+    LbmState *st, *st_host;
+    ffr_step_result *ring, *ring_host;
+    unsigned long long *div_slot;
+    unsigned blocks;
+    GroupTimer prof;
+};
+
+namespace {
+
+int lbm_enqueue(ffr_lbm *s)
+{
+    cudaStream_t st = s->stream;
+    s->prof.begin(FFR_LPROF_STREAM_COLLIDE, st);
+    switch (s->storage) {
+    case FFR_LBM_FP64:
+        k_lbm_step<0><<<s->blocks, kThr, 0, st>>>(s->L, (const double *)s->f0, (double *)s->f1, s->cu, s->cv,
+                                                    s->cw, s->p, s->st);
+        break;
+    case FFR_LBM_FP32:
+        k_lbm_step<1><<<s->blocks, kThr, 0, st>>>(s->L, (const float *)s->f0, (float *)s->f1, s->cu, s->cv,
+                                                    s->cw, s->p, s->st);
+        break;
+    default:
+        k_lbm_step<2><<<s->blocks, kThr, 0, st>>>(s->L, (const __half *)s->f0, (__half *)s->f1, s->cu, s->cv,
+                                                    s->cw, s->p, s->st);
+    }
+    FFR_LAUNCHED(1);
+    s->prof.end(st, 1);
+    s->prof.begin(FFR_LPROF_FACES, st);
+    k_lbm_faces<<<s->blocks, kThr, 0, st>>>(s->L, s->cu, s->cv, s->cw, s->u, s->v, s->w, s->st);
+    FFR_LAUNCHED(1);
+    k_lbm_finalize<<<1, 32, 0, st>>>(s->dt, s->tol, s->st, s->ring);
+    FFR_LAUNCHED(1);
+    s->prof.end(st, 2);
+    return FFR_OK;
+}
+
+int lbm_pull(ffr_lbm *s)
+{
+    FFR_CUDA(cudaMemcpyAsync(s->st_host, s->st, sizeof(LbmState), cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    s->prof.collect();
+    return FFR_OK;
+}
+
+// Sequential outflow copies of LBMSolver::apply_outflow_bc (LBMSolver.cpp:
+// 196-282) resolved to one source per destination: the outflow list (which
+// holds the openings too) and then the opening list again.
+void resolve_remap(const HostRoom &h, std::vector<int> &dst, std::vector<int> &src)
+{
+    const int nx = h.g.nx, ny = h.g.ny, nz = h.g.nz;
+    std::vector<int> map(h.g.n);
+    for (long long c = 0; c < h.g.n; c++) map[c] = (int)c;
+    auto CI = [&](int i, int j, int k) { return (i * ny + j) * nz + k; };
+    auto pass = [&](const ffr_patch &p) {
+        const int N[3] = {nx, ny, nz};
+        const int wall = p.side == 0 ? 0 : N[p.axis] - 1, s = p.side == 0 ? 1 : N[p.axis] - 2;
+        if (s < 0 || s >= N[p.axis]) return;
+        const int la = p.axis == 0 ? ny : nx, lb = p.axis == 2 ? ny : nz;
+        for (int a = p.a_min; a <= p.a_max; a++)
+            for (int b = p.b_min; b <= p.b_max; b++) {
+                if (a < 0 || a >= la || b < 0 || b >= lb) continue;
+                int cd, cs;
+                if (p.axis == 0) { cd = CI(wall, a, b); cs = CI(s, a, b); }
+                else if (p.axis == 1) { cd = CI(a, wall, b); cs = CI(a, s, b); }
+                else { cd = CI(a, b, wall); cs = CI(a, b, s); }
+                if (h.ct[cd] != CT_OUTFLOW) continue;
+                map[cd] = map[cs];
+            }
+    };
+    for (const ffr_patch &p : h.patches) pass(p);
+    for (const ffr_patch &p : h.patches) if (p.is_opening) pass(p);
+    dst.clear(); src.clear();
+    for (long long c = 0; c < h.g.n; c++)
+        if (map[c] != (int)c) { dst.push_back((int)c); src.push_back(map[c]); }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double convergence_tol,
+                   double dt, int storage, const ffr_fields *init, ffr_lbm **out)
+{
+    if (!out) return fail(FFR_EINVAL, "NULL out");
+    *out = nullptr;
+    if (storage < FFR_LBM_FP64 || storage > FFR_LBM_FP16) return fail(FFR_EINVAL, "bad LBM storage mode");
+    if (!(dt > 0) || !(tau > 0)) return fail(FFR_EINVAL, "tau and dt must be positive");
+    ffr_lbm *s = new (std::nothrow) ffr_lbm();
+    if (!s) return fail(FFR_ENOMEM, "host allocation");
+    int rc = load_room(room, s->room);
+    if (rc) { delete s; return rc; }
+    const RoomGeom &g = s->room.g;
+    if (19ll * g.n >= (1ll << 31)) { delete s; return fail(FFR_ERANGE, "lattice too large (19*N >= 2^31)"); }
+    s->storage = storage; s->tau = tau; s->dt = dt; s->tol = convergence_tol; s->max_steps = max_steps;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete s;
+        return fail(FFR_ECUDA, "cudaStreamCreate");
+    }
+    // per-cell fan index: the last fan whose box holds an INFLOW cell
+    std::vector<uint8_t> fan_of(g.n, 255);
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    for (size_t f = 0; f < s->room.fans.size(); f++) {
+        const ffr_fan &fn = s->room.fans[f];
+        for (int i = fn.i_min; i <= fn.i_max; i++)
+            for (int j = fn.j_min; j <= fn.j_max; j++)
+                for (int k = fn.k_min; k <= fn.k_max; k++) {
+                    if (i < 0 || i >= nx || j < 0 || j >= ny || k < 0 || k >= nz) continue;
+                    const int c = (i * ny + j) * nz + k;
+                    if (s->room.ct[c] == CT_INFLOW) fan_of[c] = (uint8_t)f;
+                }
+    }
+    const double p2l = dt / (g.lx / g.nx);   // phys_to_lat = dt / grid.dx (LBMSolver.cpp:42-44)
+    std::vector<double> fan_lat(3 * std::max<size_t>(1, s->room.fans.size()), 0.0);
+    for (size_t f = 0; f < s->room.fans.size(); f++)
+        for (int c = 0; c < 3; c++) fan_lat[3 * f + c] = s->room.fans[f].vel[c] * p2l;
+    std::vector<int> rd, rs;
+    resolve_remap(s->room, rd, rs);
+    const size_t es = storage == FFR_LBM_FP64 ? 8 : (storage == FFR_LBM_FP32 ? 4 : 2);
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t bytes = 2 * al(es * 19 * g.n) + 4 * al(8 * g.n) + al(8 * g.nu) + al(8 * g.nv) +
+                         al(8 * g.nw) + 2 * al(g.n) + al(8 * fan_lat.size()) + 2 * al(4 * (rd.size() + 1)) +
+                         al(8 * (g.nx + g.ny + g.nz)) + al(sizeof(LbmState)) +
+                         al(sizeof(ffr_step_result) * kRingL) + 3 * 256;
+    rc = s->arena.alloc(bytes);
+    if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
+    Arena &a = s->arena;
+    s->f0 = a.take<char>(es * 19 * g.n);
+    s->f1 = a.take<char>(es * 19 * g.n);
+    s->cu = a.take<double>(g.n); s->cv = a.take<double>(g.n); s->cw = a.take<double>(g.n);
+    s->p = a.take<double>(g.n);
+    s->u = a.take<double>(g.nu); s->v = a.take<double>(g.nv); s->w = a.take<double>(g.nw);
+    uint8_t *ct = a.take<uint8_t>(g.n), *fo = a.take<uint8_t>(g.n);
+    double *fl = a.take<double>(fan_lat.size());
+    int *rdd = a.take<int>(rd.size() + 1), *rsd = a.take<int>(rd.size() + 1);
+    double *dxv = a.take<double>(g.nx), *dyv = a.take<double>(g.ny), *dzv = a.take<double>(g.nz);
+    s->st = a.take<LbmState>(1);
+    s->ring = a.take<ffr_step_result>(kRingL);
+    s->div_slot = a.take<unsigned long long>(1);
+    if (!s->div_slot || cudaMallocHost(&s->st_host, sizeof(LbmState)) != cudaSuccess ||
+        cudaMallocHost(&s->ring_host, sizeof(ffr_step_result) * kRingL) != cudaSuccess) {
+        ffr_lbm_destroy(s);
+        return fail(FFR_ENOMEM, "LBM allocation");
+    }
+    cudaStream_t st = s->stream;
+    FFR_CUDA(cudaMemcpyAsync(ct, s->room.ct.data(), g.n, cudaMemcpyHostToDevice, st));
+    FFR_CUDA(cudaMemcpyAsync(fo, fan_of.data(), g.n, cudaMemcpyHostToDevice, st));
+    FFR_CUDA(cudaMemcpyAsync(fl, fan_lat.data(), 8 * fan_lat.size(), cudaMemcpyHostToDevice, st));
+    if (!rd.empty()) {
+        FFR_CUDA(cudaMemcpyAsync(rdd, rd.data(), 4 * rd.size(), cudaMemcpyHostToDevice, st));
+        FFR_CUDA(cudaMemcpyAsync(rsd, rs.data(), 4 * rs.size(), cudaMemcpyHostToDevice, st));
+    }
+    FFR_CUDA(cudaMemcpyAsync(dxv, s->room.dxv.data(), 8 * g.nx, cudaMemcpyHostToDevice, st));
+    FFR_CUDA(cudaMemcpyAsync(dyv, s->room.dyv.data(), 8 * g.ny, cudaMemcpyHostToDevice, st));
+    FFR_CUDA(cudaMemcpyAsync(dzv, s->room.dzv.data(), 8 * g.nz, cudaMemcpyHostToDevice, st));
+    auto up = [&](double *d, const double *h, long long cnt) -> int {
+        if (h) FFR_CUDA(cudaMemcpyAsync(d, h, 8 * cnt, cudaMemcpyHostToDevice, st));
+        else FFR_CUDA(cudaMemsetAsync(d, 0, 8 * cnt, st));
+        return FFR_OK;
+    };
+    if ((rc = up(s->u, init ? init->u : nullptr, g.nu)) || (rc = up(s->v, init ? init->v : nullptr, g.nv)) ||
+        (rc = up(s->w, init ? init->w : nullptr, g.nw)) || (rc = up(s->p, init ? init->p : nullptr, g.n))) {
+        ffr_lbm_destroy(s);
+        return rc;
+    }
+    FFR_CUDA(cudaMemsetAsync(s->st, 0, sizeof(LbmState), st));
+    s->L = LbmDev{nx, ny, nz, (int)g.n, (int)g.nu, (int)g.nv, (int)g.nw, ct, fo, fl, rdd, rsd,
+                  (int)rd.size(), dxv, dyv, dzv, tau, (g.lx / g.nx) / dt};
+    s->blocks = blocks_for(g.n);
+    switch (storage) {
+    case FFR_LBM_FP64: k_lbm_init<0><<<s->blocks, kThr, 0, st>>>(s->L, (double *)s->f0); break;
+    case FFR_LBM_FP32: k_lbm_init<1><<<s->blocks, kThr, 0, st>>>(s->L, (float *)s->f0); break;
+    default: k_lbm_init<2><<<s->blocks, kThr, 0, st>>>(s->L, (__half *)s->f0);
+    }
+    FFR_LAUNCHED(1);
+    FFR_CUDA(cudaStreamSynchronize(st));
+    memset(s->st_host, 0, sizeof(LbmState));
+    s->prof.reset(FFR_LPROF_N);
+    *out = s;
+    return FFR_OK;
+}
+
+int ffr_lbm_destroy(ffr_lbm *s)
+{
+    if (!s) return FFR_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    s->prof.destroy();
+    s->arena.release();
+    if (s->st_host) cudaFreeHost(s->st_host);
+    if (s->ring_host) cudaFreeHost(s->ring_host);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return FFR_OK;
+}
+
+int ffr_lbm_advance(ffr_lbm *s, int nsteps, int stop_on_converge, ffr_step_result *results, int *steps_done)
+{
+    if (!s || nsteps < 0) return fail(FFR_EINVAL, "bad handle or nsteps");
+    int total = 0;
+    while (total < nsteps) {
+        const int chunk = std::min(kRingL, nsteps - total);
+        int rc = lbm_pull(s);
+        if (rc) return rc;
+        LbmState hs = *s->st_host;
+        hs.ring_slot = 0;
+        hs.halt = 0;
+        hs.stop_on_converge = stop_on_converge ? 1 : 0;
+        FFR_CUDA(cudaMemcpyAsync(s->st, &hs, sizeof(LbmState), cudaMemcpyHostToDevice, s->stream));
+        for (int k = 0; k < chunk; k++)
+            if ((rc = lbm_enqueue(s))) return rc;
+        FFR_CUDA(cudaMemcpyAsync(s->ring_host, s->ring, sizeof(ffr_step_result) * chunk, cudaMemcpyDeviceToHost,
+                                 s->stream));
+        if ((rc = lbm_pull(s))) return rc;
+        const int got = s->st_host->ring_slot;
+        if (results) memcpy(results + total, s->ring_host, sizeof(ffr_step_result) * got);
+        total += got;
+        if (got < chunk) break;
+    }
+    if (steps_done) *steps_done = total;
+    return FFR_OK;
+}
+
+int ffr_lbm_step(ffr_lbm *s, ffr_step_result *out)
+{
+    ffr_step_result tmp;
+    int done = 0;
+    int rc = ffr_lbm_advance(s, 1, 0, out ? out : &tmp, &done);
+    if (rc) return rc;
+    return done == 1 ? FFR_OK : fail(FFR_ECUDA, "step did not execute");
+}
+
+int ffr_lbm_divergence_max(ffr_lbm *s, double *out)
+{
+    if (!s || !out) return fail(FFR_EINVAL, "NULL argument");
+    FFR_CUDA(cudaMemsetAsync(s->div_slot, 0, 8, s->stream));
+    k_lbm_divergence<<<s->blocks, kThr, 0, s->stream>>>(s->L, s->u, s->v, s->w, s->div_slot);
+    FFR_LAUNCHED(1);
+    unsigned long long bits = 0;
+    FFR_CUDA(cudaMemcpyAsync(&bits, s->div_slot, 8, cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    memcpy(out, &bits, 8);
+    return FFR_OK;
+}
+
+int ffr_lbm_current_step(ffr_lbm *s, int *out)
+{
+    if (!s || !out) return fail(FFR_EINVAL, "NULL argument");
+    int rc = lbm_pull(s);
+    if (rc) return rc;
+    *out = s->st_host->step;
+    return FFR_OK;
+}
+
+static double *lbm_field(ffr_lbm *s, int field, long long *len)
+{
+    const RoomGeom &g = s->room.g;
+    switch (field) {
+    case FFR_FIELD_U: *len = g.nu; return s->u;
+    case FFR_FIELD_V: *len = g.nv; return s->v;
+    case FFR_FIELD_W: *len = g.nw; return s->w;
+    case FFR_FIELD_P: *len = g.n; return s->p;
+    default: return nullptr;
+    }
+}
+
+int ffr_lbm_get_field(ffr_lbm *s, int field, double *host)
+{
+    long long len = 0;
+    double *d = s && host ? lbm_field(s, field, &len) : nullptr;
+    if (!d) return fail(FFR_EINVAL, "bad LBM get_field arguments");
+    FFR_CUDA(cudaMemcpyAsync(host, d, 8 * len, cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    return FFR_OK;
+}
+
+int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host)
+{
+    long long len = 0;
+    double *d = s && host ? lbm_field(s, field, &len) : nullptr;
+    if (!d) return fail(FFR_EINVAL, "bad LBM set_field arguments");
+    FFR_CUDA(cudaMemcpyAsync(d, host, 8 * len, cudaMemcpyHostToDevice, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    return FFR_OK;
+}
+
+int ffr_lbm_synchronize(ffr_lbm *s)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    s->prof.collect();
+    return FFR_OK;
+}
+
+int ffr_lbm_stream(ffr_lbm *s, void **stream)
+{
+    if (!s || !stream) return fail(FFR_EINVAL, "NULL argument");
+    *stream = (void *)s->stream;
+    return FFR_OK;
+}
+
+int ffr_lbm_profile(ffr_lbm *s, int enable)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    s->prof.collect();
+    s->prof.reset(FFR_LPROF_N);
+    s->prof.on = enable != 0;
+    return FFR_OK;
+}
+
+int ffr_lbm_profile_read(ffr_lbm *s, double *ms, long long *launches)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    s->prof.collect();
+    for (int g = 0; g < FFR_LPROF_N; g++) {
+        if (ms) ms[g] = s->prof.ms[g];
+        if (launches) launches[g] = s->prof.launches[g];
+    }
+    return FFR_OK;
+}
+
+}  // extern "C"

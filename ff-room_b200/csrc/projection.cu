@@ -1,0 +1,1315 @@
+// projection.cu — Chorin projection step on the MAC grid, FP64 (sm_100a).
+//
+// One step (FluidSolver::step, cpp/src/core/FluidSolver.cpp:486-550) is
+//   k_predict        advection + diffusion + buoyancy + no-slip/inflow codes
+//   k_cg             persistent cooperative CG: rhs, x0 = 0, iterations
+//   k_correct        pressure correction + BC codes + outflow copy,
+//                    max |du| and max |div| in the same pass (cell-centric)
+//   k_opening_T,     thermal: opening BC, advection-diffusion of T with the
+//   k_advect_T,      block partial sums of T over FLUID cells, opening BC,
+//   k_heat           fixed-T patches
+//   k_finalize       StepResult, convergence, halt flag, T buffer swap
+// All kernels return at once when the room's halt flag is set, so a run of
+// queued steps can stop on convergence without a host round trip.
+#include "projection.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+namespace ffr {
+
+#define UIX(i, j, k) (((i) * ny + (j)) * nz + (k))
+#define VIX(i, j, k) (((i) * (ny + 1) + (j)) * nz + (k))
+#define WIX(i, j, k) (((i) * ny + (j)) * (nz + 1) + (k))
+
+// ------------------------------------------------- advection formulas
+
+// upwind1, FluidSolver.cpp:47-50.
+__device__ __forceinline__ double adv_up(double pm, double pc, double pp, double a, double h)
+{
+    return (a > 0.0) ? a * (pc - pm) / h : a * (pp - pc) / h;
+}
+
+// quick_adv, FluidSolver.cpp:56-72 (phi_mm on the negative branch, >= 0).
+__device__ __forceinline__ double adv_quick(double pmm, double pm, double pc, double pp, double a,
+                                            double h)
+{
+    double fr, fl;
+    if (a >= 0.0) {
+        fr = (6.0 * pc + 3.0 * pp - pm) / 8.0;
+        fl = (6.0 * pm + 3.0 * pc - pmm) / 8.0;
+    } else {
+        fr = (6.0 * pp + 3.0 * pc - pmm) / 8.0;
+        fl = (6.0 * pc + 3.0 * pp - pm) / 8.0;
+    }
+    return a * (fr - fl) / h;
+}
+
+// lax_wendroff_adv, FluidSolver.cpp:75-81.
+__device__ __forceinline__ double adv_lw(double pm, double pc, double pp, double a, double dt,
+                                         double h)
+{
+    const double cr = a * dt / h;
+    const double flr = a * (0.5 * (pc + pp) - 0.5 * cr * (pp - pc));
+    const double fll = a * (0.5 * (pm + pc) - 0.5 * cr * (pc - pm));
+    return (flr - fll) / h;
+}
+
+__device__ __forceinline__ double face_code(uint8_t code, double val, const double *fanvel, int comp)
+{
+    const int c = code & 0x7f;
+    if (c == FC_KEEP) return val;
+    if (c == FC_ZERO) return 0.0;
+    return fanvel[(c - FC_FAN0) * 3 + comp];
+}
+
+struct PredArgs {
+    double dt, nu;
+    int scheme;          // 0 upwind, 1 QUICK, 2 Lax-Wendroff
+    int buoyancy;
+    double bcoeff;       // g * beta * dt
+    double T_ref;
+};
+
+// Predictor for every face of u, v and w (one thread per face, flat over
+// the three arrays): FluidSolver::compute_intermediate (FluidSolver.cpp:
+// 83-309), then apply_buoyancy on interior w faces (FluidSolver.cpp:373-386),
+// then the no-slip / inflow codes (BoundaryManager.cpp:60-130).
+__global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const double *__restrict__ u,
+                                                 const double *__restrict__ v,
+                                                 const double *__restrict__ w,
+                                                 const double *__restrict__ T0,
+                                                 const double *__restrict__ T1,
+                                                 double *__restrict__ us, double *__restrict__ vs,
+                                                 double *__restrict__ ws, const StepState *st)
+{
+    if (st->halt) return;
+    const int nx = R.nx, ny = R.ny, nz = R.nz;
+    const int total = R.nu + R.nv + R.nw;
+    const int quick = A.scheme == 1, lw = A.scheme == 2;
+    const double dt = A.dt, nu = A.nu;
+    const double *T = st->tpar ? T1 : T0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        if (t < R.nu) {
+            const int i = t / (ny * nz), rem = t - i * ny * nz, j = rem / nz, k = rem - j * nz;
+            double val = u[t];
+            if (i > 0 && i < nx) {
+                const double hx = R.dxv[i], hy = R.dyv[j], hz = R.dzv[k];
+                const double cx = 1.0 / (hx * hx), cy = 1.0 / (hy * hy), cz = 1.0 / (hz * hz);
+                const double uc = val;
+                const double xm = (i > 1) ? u[t - ny * nz] : 0.0;
+                const double xp = (i < nx - 1) ? u[t + ny * nz] : 0.0;
+                const double av = (j > 0 && j < ny) ? 0.5 * (v[VIX(i - 1, j, k)] + v[VIX(i, j, k)]) : 0.0;
+                const double ym = (j > 0) ? u[t - nz] : 0.0;
+                const double yp = (j < ny - 1) ? u[t + nz] : 0.0;
+                const double aw = (k > 0 && k < nz) ? 0.5 * (w[WIX(i - 1, j, k)] + w[WIX(i, j, k)]) : 0.0;
+                const double zm = (k > 0) ? u[t - 1] : 0.0;
+                const double zp = (k < nz - 1) ? u[t + 1] : 0.0;
+                double adv;
+                if (quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+                    // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1
+                    // (k=1) they fall into the previous row of the flat array
+                    adv = adv_quick(u[t - 2 * ny * nz], xm, uc, xp, uc, hx)
+                        + adv_quick(u[t - 2 * nz], ym, uc, yp, av, hy)
+                        + adv_quick(u[t - 2], zm, uc, zp, aw, hz);
+                } else if (lw) {
+                    adv = adv_lw(xm, uc, xp, uc, dt, hx) + adv_lw(ym, uc, yp, av, dt, hy)
+                        + adv_lw(zm, uc, zp, aw, dt, hz);
+                } else {
+                    adv = adv_up(xm, uc, xp, uc, hx) + adv_up(ym, uc, yp, av, hy)
+                        + adv_up(zm, uc, zp, aw, hz);
+                }
+                const double dif = nu * (cx * (xm - 2 * uc + xp) + cy * (ym - 2 * uc + yp)
+                                         + cz * (zm - 2 * uc + zp));
+                val = uc + dt * (-adv + dif);
+            }
+            us[t] = face_code(R.fcu[t], val, R.fanvel, 0);
+        } else if (t < R.nu + R.nv) {
+            const int f = t - R.nu;
+            const int i = f / ((ny + 1) * nz), rem = f - i * (ny + 1) * nz, j = rem / nz,
+                      k = rem - j * nz;
+            double val = v[f];
+            if (j > 0 && j < ny) {
+                const double hx = R.dxv[i], hy = R.dyv[j], hz = R.dzv[k];
+                const double cx = 1.0 / (hx * hx), cy = 1.0 / (hy * hy), cz = 1.0 / (hz * hz);
+                const double vc = val;
+                const double au = (i > 0) ? 0.5 * (u[UIX(i, j - 1, k)] + u[UIX(i, j, k)]) : 0.0;
+                const double xm = (i > 0) ? v[f - (ny + 1) * nz] : 0.0;
+                const double xp = (i < nx - 1) ? v[f + (ny + 1) * nz] : 0.0;
+                const double ym = (j > 1) ? v[f - nz] : 0.0;
+                const double yp = (j < ny - 1) ? v[f + nz] : 0.0;
+                const double aw = (k > 0 && k < nz) ? 0.5 * (w[WIX(i, j - 1, k)] + w[WIX(i, j, k)]) : 0.0;
+                const double zm = (k > 0) ? v[f - 1] : 0.0;
+                const double zp = (k < nz - 1) ? v[f + 1] : 0.0;
+                double adv;
+                if (quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+                    // v's x and z "far" neighbours are the near ones
+                    // (FluidSolver.cpp:208,211)
+                    adv = adv_quick(xm, xm, vc, xp, au, hx) + adv_quick(v[f - 2 * nz], ym, vc, yp, vc, hy)
+                        + adv_quick(zm, zm, vc, zp, aw, hz);
+                } else if (lw) {
+                    adv = adv_lw(xm, vc, xp, au, dt, hx) + adv_lw(ym, vc, yp, vc, dt, hy)
+                        + adv_lw(zm, vc, zp, aw, dt, hz);
+                } else {
+                    adv = adv_up(xm, vc, xp, au, hx) + adv_up(ym, vc, yp, vc, hy)
+                        + adv_up(zm, vc, zp, aw, hz);
+                }
+                const double dif = nu * (cx * (xm - 2 * vc + xp) + cy * (ym - 2 * vc + yp)
+                                         + cz * (zm - 2 * vc + zp));
+                val = vc + dt * (-adv + dif);
+            }
+            vs[f] = face_code(R.fcv[f], val, R.fanvel, 1);
+        } else {
+            const int f = t - R.nu - R.nv;
+            const int i = f / (ny * (nz + 1)), rem = f - i * ny * (nz + 1), j = rem / (nz + 1),
+                      k = rem - j * (nz + 1);
+            double val = w[f];
+            if (k > 0 && k < nz) {
+                const double hx = R.dxv[i], hy = R.dyv[j], hz = R.dzv[k];
+                const double cx = 1.0 / (hx * hx), cy = 1.0 / (hy * hy), cz = 1.0 / (hz * hz);
+                const double wc = val;
+                const double au = (i > 0) ? 0.5 * (u[UIX(i, j, k - 1)] + u[UIX(i, j, k)]) : 0.0;
+                const double xm = (i > 0) ? w[f - ny * (nz + 1)] : 0.0;
+                const double xp = (i < nx - 1) ? w[f + ny * (nz + 1)] : 0.0;
+                const double av = (j > 0) ? 0.5 * (v[VIX(i, j, k - 1)] + v[VIX(i, j, k)]) : 0.0;
+                const double ym = (j > 0) ? w[f - (nz + 1)] : 0.0;
+                const double yp = (j < ny - 1) ? w[f + (nz + 1)] : 0.0;
+                const double zm = (k > 1) ? w[f - 1] : 0.0;
+                const double zp = (k < nz - 1) ? w[f + 1] : 0.0;
+                double adv;
+                if (quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2) {
+                    // w's x and y "far" neighbours are the near ones
+                    // (FluidSolver.cpp:275-276)
+                    adv = adv_quick(xm, xm, wc, xp, au, hx) + adv_quick(ym, ym, wc, yp, av, hy)
+                        + adv_quick(w[f - 2], zm, wc, zp, wc, hz);
+                } else if (lw) {
+                    adv = adv_lw(xm, wc, xp, au, dt, hx) + adv_lw(ym, wc, yp, av, dt, hy)
+                        + adv_lw(zm, wc, zp, wc, dt, hz);
+                } else {
+                    adv = adv_up(xm, wc, xp, au, hx) + adv_up(ym, wc, yp, av, hy)
+                        + adv_up(zm, wc, zp, wc, hz);
+                }
+                const double dif = nu * (cx * (xm - 2 * wc + xp) + cy * (ym - 2 * wc + yp)
+                                         + cz * (zm - 2 * wc + zp));
+                val = wc + dt * (-adv + dif);
+                if (A.buoyancy) {
+                    const int c = UIX(i, j, k);
+                    val += A.bcoeff * (0.5 * (T[c - 1] + T[c]) - A.T_ref);
+                }
+            }
+            ws[f] = face_code(R.fcw[f], val, R.fanvel, 2);
+        }
+    }
+}
+
+// ------------------------------------------------------------ pressure
+
+struct CGArgs {
+    RoomDev R;
+    const double *us, *vs, *ws;    // rhs from predicted faces when from_faces
+    double rhs_factor;             // -(rho / dt), FluidSolver.cpp:315
+    int from_faces;
+    const double *rhs;             // explicit right-hand side otherwise
+    double *x;
+    double *r, *da, *db, *ad;
+    double *partials;
+    GridSync *gs;
+    CGScalars *sc;
+    int max_iter;
+    double tol;
+    StepState *st;                 // may be null
+    double *out_res;
+    int *out_iters;
+    int *out_flags;
+};
+
+__device__ __forceinline__ void stencil_term(unsigned cls, double s, double xn, double &diag,
+                                             double &off)
+{
+    if (cls == SC_IN) {
+        diag += s;
+        off += s * xn;
+    } else if (cls == SC_DIR) {
+        diag += 2.0 * s;
+    }
+}
+
+// PoissonSolver::solve (PoissonSolver.cpp:93-158) as one cooperative launch.
+// Per iteration: phase A forms the direction d = r + beta*d_old (the first
+// iteration uses d = r), applies the deferred x += alpha_old*d_old, computes
+// Ad with the mask stencil of apply_laplacian (PoissonSolver.cpp:22-91) and
+// the block partials of d.Ad; phase B does r -= alpha*Ad and ||r||^2.  Each
+// phase ends in a deterministic grid-wide sum.  Stopping rules, the
+// |d.Ad| < 1e-30 break and the returned residual follow the reference.
+__global__ void __launch_bounds__(256) k_cg(CGArgs A)
+{
+    __shared__ double sh[32];
+    if (A.st && A.st->halt) return;
+    const RoomDev &R = A.R;
+    const int nx = R.nx, ny = R.ny, nz = R.nz, n = R.n, plane = ny * nz;
+    const double *sxl = R.scale, *sxr = sxl + nx, *syl = sxr + nx, *syr = syl + ny, *szl = syr + ny,
+                 *szr = szl + nz;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    double *x = A.x, *r = A.r, *ad = A.ad;
+
+    // Phase 0: r = rhs (0 in SOLID rows), d = r, x = 0, ||r||^2.
+    double acc[1] = {0.0};
+    for (int c = t0; c < n; c += nth) {
+        double rv = 0.0;
+        if (!(R.sc[c] & SC_SOLID)) {
+            if (A.from_faces) {
+                const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+                const double div = (A.us[UIX(i + 1, j, k)] - A.us[UIX(i, j, k)]) / R.dxv[i]
+                                 + (A.vs[VIX(i, j + 1, k)] - A.vs[VIX(i, j, k)]) / R.dyv[j]
+                                 + (A.ws[WIX(i, j, k + 1)] - A.ws[WIX(i, j, k)]) / R.dzv[k];
+                rv = A.rhs_factor * div;
+            } else {
+                rv = A.rhs[c];
+            }
+        }
+        r[c] = rv;
+        A.da[c] = rv;
+        x[c] = 0.0;
+        acc[0] += rv * rv;
+    }
+    bool ok = grid_allreduce<1>(A.gs, A.partials, A.sc->red, acc, sh);
+    double rr = acc[0];
+    const double bnorm = sqrt(rr);
+    int flags = 0, iters = 0;
+    double res = 0.0;
+    if (!ok) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+    if (bnorm < 1e-15) goto finish;
+    {
+        double *dold = A.da, *dnew = A.db;
+        double beta = 0.0, alpha_prev = 0.0, alpha = 0.0;
+        bool first = true, pending = false;
+        int it = 0;
+        for (; it < A.max_iter; it++) {
+            double dacc[1] = {0.0};
+            for (int c = t0; c < n; c += nth) {
+                const unsigned code = R.sc[c];
+                double dc;
+                if (first) {
+                    dc = dold[c];
+                } else {
+                    const double dp = dold[c];
+                    dc = fma(beta, dp, r[c]);
+                    x[c] = fma(alpha_prev, dp, x[c]);
+                    dnew[c] = dc;
+                }
+                double a;
+                if (code & SC_SOLID) {
+                    a = dc;
+                } else {
+                    const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+                    double diag = 0.0, off = 0.0;
+#define DIRN(o) (first ? dold[c + (o)] : fma(beta, dold[c + (o)], r[c + (o)]))
+                    if ((code >> 0) & 3) stencil_term((code >> 0) & 3, sxl[i], ((code >> 0) & 3) == SC_IN ? DIRN(-plane) : 0.0, diag, off);
+                    if ((code >> 2) & 3) stencil_term((code >> 2) & 3, sxr[i], ((code >> 2) & 3) == SC_IN ? DIRN(plane) : 0.0, diag, off);
+                    if ((code >> 4) & 3) stencil_term((code >> 4) & 3, syl[j], ((code >> 4) & 3) == SC_IN ? DIRN(-nz) : 0.0, diag, off);
+                    if ((code >> 6) & 3) stencil_term((code >> 6) & 3, syr[j], ((code >> 6) & 3) == SC_IN ? DIRN(nz) : 0.0, diag, off);
+                    if ((code >> 8) & 3) stencil_term((code >> 8) & 3, szl[k], ((code >> 8) & 3) == SC_IN ? DIRN(-1) : 0.0, diag, off);
+                    if ((code >> 10) & 3) stencil_term((code >> 10) & 3, szr[k], ((code >> 10) & 3) == SC_IN ? DIRN(1) : 0.0, diag, off);
+#undef DIRN
+                    if (diag < 1e-30) diag = 1.0;
+                    a = diag * dc - off;
+                }
+                ad[c] = a;
+                dacc[0] += dc * a;
+            }
+            if (!grid_allreduce<1>(A.gs, A.partials, A.sc->red, dacc, sh)) {
+                flags = FFR_FLAG_TIMEOUT;
+                goto finish;
+            }
+            const double dad = dacc[0];
+            if (!first) {
+                double *tmp = dold; dold = dnew; dnew = tmp;
+            }
+            first = false;
+            pending = false;
+            if (fabs(dad) < 1e-30) {
+                flags |= FFR_FLAG_CG_BREAKDOWN;
+                break;
+            }
+            alpha = rr / dad;
+            double racc[1] = {0.0};
+            for (int c = t0; c < n; c += nth) {
+                const double rv = r[c] - alpha * ad[c];
+                r[c] = rv;
+                racc[0] += rv * rv;
+            }
+            if (!grid_allreduce<1>(A.gs, A.partials, A.sc->red, racc, sh)) {
+                flags = FFR_FLAG_TIMEOUT;
+                goto finish;
+            }
+            pending = true;
+            const double rr1 = racc[0];
+            res = sqrt(rr1) / bnorm;
+            if (res < A.tol) {
+                iters = it + 1;
+                break;
+            }
+            beta = rr1 / rr;
+            rr = rr1;
+            alpha_prev = alpha;
+        }
+        if (it >= A.max_iter || (flags & FFR_FLAG_CG_BREAKDOWN)) {
+            iters = A.max_iter;
+            res = sqrt(rr) / bnorm;
+            if (!(flags & FFR_FLAG_CG_BREAKDOWN)) flags |= FFR_FLAG_CG_MAXITER;
+        }
+        // dold now holds the direction of the last completed iteration.
+        if (pending) {
+            const double a_last = (iters == A.max_iter && !(flags & FFR_FLAG_CG_BREAKDOWN) && res >= A.tol)
+                                      ? alpha_prev : alpha;
+            for (int c = t0; c < n; c += nth) x[c] = fma(a_last, dold[c], x[c]);
+        }
+    }
+finish:
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (A.out_res) *A.out_res = res;
+        if (A.out_iters) *A.out_iters = iters;
+        if (A.out_flags) *A.out_flags = flags;
+        if (A.st) {
+            A.st->pres = res;
+            A.st->iters = iters;
+            atomicOr(&A.st->flags, flags);
+        }
+    }
+}
+
+// --------------------------------------------------------- correction
+
+struct CorrArgs {
+    double c0;        // dt / rho
+};
+
+// Cell-centric pressure correction (FluidSolver::apply_correction,
+// FluidSolver.cpp:332-371) followed by the BC appliers (FluidSolver.cpp:
+// 512-515) expressed through the face codes.  A thread owns the three low
+// faces of its cell (and the high boundary faces of the last cells) and
+// recomputes the three high faces, so it can also fold max |u_new - u_old|
+// (FluidSolver.cpp:527-534) and, for FLUID cells, |div u|
+// (compute_divergence_max, FluidSolver.cpp:470-484) in the same pass.
+__global__ void __launch_bounds__(256) k_correct(RoomDev R, CorrArgs A, double *__restrict__ u,
+                                                 double *__restrict__ v, double *__restrict__ w,
+                                                 const double *__restrict__ us,
+                                                 const double *__restrict__ vs,
+                                                 const double *__restrict__ ws,
+                                                 const double *__restrict__ p, StepState *st)
+{
+    __shared__ double sh[32];
+    if (st->halt) return;
+    const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
+    const double c0 = A.c0;
+    double dmax = 0.0, divmax = 0.0;
+    int nan = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.n; c += gridDim.x * blockDim.x) {
+        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+        const double pc = p[c];
+        // x faces
+        const int ul = c, uh = c + plane;
+        double lo = us[ul], hi = us[uh];
+        if (i >= 1) lo = lo - c0 * ((pc - p[c - plane]) / (0.5 * (R.dxv[i - 1] + R.dxv[i])));
+        if (i + 1 <= nx - 1) hi = hi - c0 * ((p[c + plane] - pc) / (0.5 * (R.dxv[i] + R.dxv[i + 1])));
+        uint8_t cl = R.fcu[ul], ch = R.fcu[uh];
+        lo = face_code(cl, lo, R.fanvel, 0);
+        hi = face_code(ch, hi, R.fanvel, 0);
+        if (cl & FC_OUTCOPY) lo = hi;
+        if (ch & FC_OUTCOPY) hi = lo;
+        const double ulo = lo, uhi = hi;
+        dmax = fmax(dmax, fabs(lo - u[ul]));
+        u[ul] = lo;
+        if (i == nx - 1) {
+            dmax = fmax(dmax, fabs(hi - u[uh]));
+            u[uh] = hi;
+        }
+        // y faces
+        const int vl = VIX(i, j, k), vh = vl + nz;
+        lo = vs[vl]; hi = vs[vh];
+        if (j >= 1) lo = lo - c0 * ((pc - p[c - nz]) / (0.5 * (R.dyv[j - 1] + R.dyv[j])));
+        if (j + 1 <= ny - 1) hi = hi - c0 * ((p[c + nz] - pc) / (0.5 * (R.dyv[j] + R.dyv[j + 1])));
+        cl = R.fcv[vl]; ch = R.fcv[vh];
+        lo = face_code(cl, lo, R.fanvel, 1);
+        hi = face_code(ch, hi, R.fanvel, 1);
+        if (cl & FC_OUTCOPY) lo = hi;
+        if (ch & FC_OUTCOPY) hi = lo;
+        const double vlo = lo, vhi = hi;
+        dmax = fmax(dmax, fabs(lo - v[vl]));
+        v[vl] = lo;
+        if (j == ny - 1) {
+            dmax = fmax(dmax, fabs(hi - v[vh]));
+            v[vh] = hi;
+        }
+        // z faces
+        const int wl = WIX(i, j, k), wh = wl + 1;
+        lo = ws[wl]; hi = ws[wh];
+        if (k >= 1) lo = lo - c0 * ((pc - p[c - 1]) / (0.5 * (R.dzv[k - 1] + R.dzv[k])));
+        if (k + 1 <= nz - 1) hi = hi - c0 * ((p[c + 1] - pc) / (0.5 * (R.dzv[k] + R.dzv[k + 1])));
+        cl = R.fcw[wl]; ch = R.fcw[wh];
+        lo = face_code(cl, lo, R.fanvel, 2);
+        hi = face_code(ch, hi, R.fanvel, 2);
+        if (cl & FC_OUTCOPY) lo = hi;
+        if (ch & FC_OUTCOPY) hi = lo;
+        const double wlo = lo, whi = hi;
+        dmax = fmax(dmax, fabs(lo - w[wl]));
+        w[wl] = lo;
+        if (k == nz - 1) {
+            dmax = fmax(dmax, fabs(hi - w[wh]));
+            w[wh] = hi;
+        }
+        if (isnan(ulo) || isnan(uhi) || isnan(vlo) || isnan(vhi) || isnan(wlo) || isnan(whi)) nan = 1;
+        if (R.ct[c] == CT_FLUID) {
+            const double d = fabs((uhi - ulo) / R.dxv[i] + (vhi - vlo) / R.dyv[j] + (whi - wlo) / R.dzv[k]);
+            divmax = fmax(divmax, d);
+        }
+    }
+    dmax = block_max(dmax, sh);
+    divmax = block_max(divmax, sh);
+    nan = __syncthreads_or(nan);
+    if (threadIdx.x == 0) {
+        atomic_max_nonneg(&st->dmax_bits, dmax);
+        atomic_max_nonneg(&st->div_bits, divmax);
+        if (nan) atomicOr(&st->flags, FFR_FLAG_NAN);
+    }
+}
+
+// compute_divergence_max (FluidSolver.cpp:470-484) on demand.
+__global__ void k_divergence(RoomDev R, const double *u, const double *v, const double *w,
+                             unsigned long long *out)
+{
+    __shared__ double sh[32];
+    const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
+    (void)nx;
+    double m = 0.0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.n; c += gridDim.x * blockDim.x) {
+        if (R.ct[c] != CT_FLUID) continue;
+        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+        const double d = fabs((u[c + plane] - u[c]) / R.dxv[i]
+                              + (v[VIX(i, j + 1, k)] - v[VIX(i, j, k)]) / R.dyv[j]
+                              + (w[WIX(i, j, k + 1)] - w[WIX(i, j, k)]) / R.dzv[k]);
+        m = fmax(m, d);
+    }
+    m = block_max(m, sh);
+    if (threadIdx.x == 0) atomic_max_nonneg(out, m);
+}
+
+// ------------------------------------------------------------ thermal
+
+// BoundaryManager::apply_opening_temperature (BoundaryManager.cpp:137-178)
+// for one opening patch; `next` picks the T buffer the step is writing.
+__global__ void k_opening_T(RoomDev R, ffr_patch P, const double *u, const double *v,
+                            const double *w, double *T0, double *T1, const StepState *st, int next)
+{
+    if (st && st->halt) return;
+    const int nx = R.nx, ny = R.ny, nz = R.nz;
+    double *T = ((st ? st->tpar : 0) ^ next) ? T1 : T0;
+    const int na = P.a_max - P.a_min + 1, nb = P.b_max - P.b_min + 1;
+    const int sd = P.side;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na * nb; t += gridDim.x * blockDim.x) {
+        const int a = P.a_min + t / nb, b = P.b_min + t % nb;
+        double vf;
+        int cw, cin;
+        if (P.axis == 0) {
+            vf = u[UIX(sd ? nx : 0, a, b)];
+            cw = UIX(sd ? nx - 1 : 0, a, b);
+            cin = UIX(sd ? nx - 2 : 1, a, b);
+        } else if (P.axis == 1) {
+            vf = v[VIX(a, sd ? ny : 0, b)];
+            cw = UIX(a, sd ? ny - 1 : 0, b);
+            cin = UIX(a, sd ? ny - 2 : 1, b);
+        } else {
+            vf = w[WIX(a, b, sd ? nz : 0)];
+            cw = UIX(a, b, sd ? nz - 1 : 0);
+            cin = UIX(a, b, sd ? nz - 2 : 1);
+        }
+        const bool incoming = sd ? (vf <= 0.0) : (vf >= 0.0);
+        T[cw] = incoming ? P.T_outside : T[cin];
+    }
+}
+
+struct ThermArgs {
+    double dt, alpha;
+    int scheme;
+};
+
+// FluidSolver::advect_temperature (FluidSolver.cpp:388-456) with the block
+// partial sums of the new T over FLUID cells for compute_T_mean
+// (FluidSolver.cpp:458-468).
+__global__ void __launch_bounds__(256) k_advect_T(RoomDev R, ThermArgs A, const double *__restrict__ u,
+                                                  const double *__restrict__ v,
+                                                  const double *__restrict__ w, double *T0,
+                                                  double *T1, double *tpart, const StepState *st)
+{
+    __shared__ double sh[32];
+    if (st->halt) return;
+    const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
+    const double *T = st->tpar ? T1 : T0;
+    double *Tn = st->tpar ? T0 : T1;
+    const int quick = A.scheme == 1, lw = A.scheme == 2;
+    const double dt = A.dt;
+    double sum = 0.0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.n; c += gridDim.x * blockDim.x) {
+        if (R.ct[c] != CT_FLUID) {
+            Tn[c] = T[c];
+            continue;
+        }
+        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+        const double hx = R.dxv[i], hy = R.dyv[j], hz = R.dzv[k];
+        const double tc = T[c];
+        const double ac = 0.5 * (u[c] + u[c + plane]);
+        const double bc = 0.5 * (v[VIX(i, j, k)] + v[VIX(i, j + 1, k)]);
+        const double cc = 0.5 * (w[WIX(i, j, k)] + w[WIX(i, j, k + 1)]);
+        // Neumann at the domain edge and at SOLID cells (FluidSolver.cpp:417-422)
+        auto tat = [&](int ii, int jj, int kk) -> double {
+            if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) return tc;
+            const int q = UIX(ii, jj, kk);
+            return R.ct[q] == CT_SOLID ? tc : T[q];
+        };
+        const double xm = tat(i - 1, j, k), xp = tat(i + 1, j, k);
+        const double ym = tat(i, j - 1, k), yp = tat(i, j + 1, k);
+        const double zm = tat(i, j, k - 1), zp = tat(i, j, k + 1);
+        double adv;
+        if (quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+            adv = adv_quick(tat(i - 2, j, k), xm, tc, xp, ac, hx)
+                + adv_quick(tat(i, j - 2, k), ym, tc, yp, bc, hy)
+                + adv_quick(tat(i, j, k - 2), zm, tc, zp, cc, hz);
+        } else if (lw) {
+            adv = adv_lw(xm, tc, xp, ac, dt, hx) + adv_lw(ym, tc, yp, bc, dt, hy)
+                + adv_lw(zm, tc, zp, cc, dt, hz);
+        } else {
+            adv = adv_up(xm, tc, xp, ac, hx) + adv_up(ym, tc, yp, bc, hy) + adv_up(zm, tc, zp, cc, hz);
+        }
+        const double dif = A.alpha * ((xm - 2 * tc + xp) / (hx * hx) + (ym - 2 * tc + yp) / (hy * hy)
+                                      + (zm - 2 * tc + zp) / (hz * hz));
+        const double tn = tc + dt * (-adv + dif);
+        Tn[c] = tn;
+        sum += tn;
+    }
+    sum = block_sum(sum, sh);
+    if (threadIdx.x == 0) tpart[blockIdx.x] = sum;
+}
+
+// Fixed-temperature box (heat-patch extension) on the buffer that is
+// current once the step completes.
+__global__ void k_heat(RoomDev R, ffr_heat_patch H, double *T0, double *T1, const StepState *st,
+                       int next)
+{
+    if (st->halt) return;
+    const int ny = R.ny, nz = R.nz;
+    double *T = (st->tpar ^ next) ? T1 : T0;
+    const int i0 = max(0, H.i_min), i1 = min(R.nx - 1, H.i_max);
+    const int j0 = max(0, H.j_min), j1 = min(ny - 1, H.j_max);
+    const int k0 = max(0, H.k_min), k1 = min(nz - 1, H.k_max);
+    if (i0 > i1 || j0 > j1 || k0 > k1) return;
+    const int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ni * nj * nk; t += gridDim.x * blockDim.x) {
+        const int a = t / (nj * nk), rem = t - a * nj * nk, b = rem / nk, e = rem - b * nk;
+        T[UIX(i0 + a, j0 + b, k0 + e)] = H.T;
+    }
+}
+
+// T := T_initial on every cell (FluidSolver ctor, FluidSolver.cpp:28).
+__global__ void k_fill(double *x, int n, double val)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) x[c] = val;
+}
+
+struct FinArgs {
+    double dt, convergence_tol, T_initial, T_target;
+    int thermal;
+    long long n_fluid;
+    int tblocks;
+};
+
+// StepResult and convergence test of FluidSolver::step (FluidSolver.cpp:
+// 526-549); the velocity change max and divergence max were folded by
+// k_correct, the pressure residual by k_cg, the T partials by k_advect_T.
+__global__ void k_finalize(FinArgs A, const double *tpart, StepState *st, ffr_step_result *ring)
+{
+    __shared__ double sh[32];
+    if (st->halt) return;
+    double tmean = A.T_initial;
+    if (A.thermal) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < A.tblocks; b += blockDim.x) s += tpart[b];
+        s = block_sum(s, sh);
+        tmean = A.n_fluid > 0 ? s / (double)A.n_fluid : A.T_initial;
+    }
+    if (threadIdx.x != 0) return;
+    const double vc = __longlong_as_double((long long)st->dmax_bits) / A.dt;
+    const double dv = __longlong_as_double((long long)st->div_bits);
+    int conv;
+    if (A.thermal && A.T_target < 1e29)
+        conv = (A.T_target >= A.T_initial) ? (tmean >= A.T_target) : (tmean <= A.T_target);
+    else
+        conv = vc < A.convergence_tol;
+    ffr_step_result r;
+    r.step = st->step + 1;
+    r.velocity_change = vc;
+    r.pressure_residual = st->pres;
+    r.divergence_max = dv;
+    r.converged = conv;
+    r.T_mean = tmean;
+    r.cg_iterations = st->iters;
+    r.flags = st->flags;
+    ring[st->ring_slot] = r;
+    st->ring_slot += 1;
+    st->step += 1;
+    if (A.thermal) st->tpar ^= 1;
+    st->dmax_bits = 0;
+    st->div_bits = 0;
+    st->flags = 0;
+    if (conv && st->stop_on_converge) st->halt = 1;
+}
+
+#undef UIX
+#undef VIX
+#undef WIX
+
+}  // namespace ffr
+
+// =================================================================== host
+
+using namespace ffr;
+
+namespace {
+
+constexpr int kRing = 1024;
+constexpr int kThreads = 256;
+
+int sm_count()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+unsigned stream_blocks(long long work)
+{
+    const long long cap = (long long)sm_count() * 8;
+    return (unsigned)std::max<long long>(1, std::min<long long>(cap, (work + kThreads - 1) / kThreads));
+}
+
+// Device copy of the room-derived tables shared by a solver and its CG.
+struct RoomTables {
+    double *dxv, *dyv, *dzv, *scale, *fanvel;
+    uint8_t *ct, *fcu, *fcv, *fcw;
+    uint16_t *sc;
+};
+
+size_t tables_bytes(const HostRoom &h)
+{
+    const RoomGeom &g = h.g;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    return al(8 * g.nx) + al(8 * g.ny) + al(8 * g.nz) + al(8 * 2 * (g.nx + g.ny + g.nz)) +
+           al(8 * 3 * kMaxFans) + al(g.n) + al(g.nu) + al(g.nv) + al(g.nw) + al(2 * g.n);
+}
+
+int upload_tables(const HostRoom &h, Arena &ar, cudaStream_t s, RoomTables &t, RoomDev &R)
+{
+    const RoomGeom &g = h.g;
+    std::vector<uint8_t> fu, fv, fw;
+    std::vector<uint16_t> sc;
+    std::vector<double> scale;
+    build_face_codes(h, fu, fv, fw);
+    build_stencil(h, sc, scale);
+    std::vector<double> fan(3 * kMaxFans, 0.0);
+    for (size_t f = 0; f < h.fans.size(); f++)
+        for (int c = 0; c < 3; c++) fan[3 * f + c] = h.fans[f].vel[c];
+    t.dxv = ar.take<double>(g.nx);
+    t.dyv = ar.take<double>(g.ny);
+    t.dzv = ar.take<double>(g.nz);
+    t.scale = ar.take<double>(scale.size());
+    t.fanvel = ar.take<double>(fan.size());
+    t.ct = ar.take<uint8_t>(g.n);
+    t.fcu = ar.take<uint8_t>(g.nu);
+    t.fcv = ar.take<uint8_t>(g.nv);
+    t.fcw = ar.take<uint8_t>(g.nw);
+    t.sc = ar.take<uint16_t>(g.n);
+    if (!t.sc) return fail(FFR_ENOMEM, "arena exhausted (tables)");
+    FFR_CUDA(cudaMemcpyAsync(t.dxv, h.dxv.data(), 8 * g.nx, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.dyv, h.dyv.data(), 8 * g.ny, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.dzv, h.dzv.data(), 8 * g.nz, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.scale, scale.data(), 8 * scale.size(), cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.fanvel, fan.data(), 8 * fan.size(), cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.ct, h.ct.data(), g.n, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.fcu, fu.data(), g.nu, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.fcv, fv.data(), g.nv, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.fcw, fw.data(), g.nw, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(t.sc, sc.data(), 2 * g.n, cudaMemcpyHostToDevice, s));
+    // The host vectors die at return: wait for the copies.
+    FFR_CUDA(cudaStreamSynchronize(s));
+    R.nx = g.nx; R.ny = g.ny; R.nz = g.nz;
+    R.n = (int)g.n; R.nu = (int)g.nu; R.nv = (int)g.nv; R.nw = (int)g.nw;
+    R.dxv = t.dxv; R.dyv = t.dyv; R.dzv = t.dzv;
+    R.ct = t.ct; R.fcu = t.fcu; R.fcv = t.fcv; R.fcw = t.fcw;
+    R.sc = t.sc; R.scale = t.scale; R.fanvel = t.fanvel;
+    return FFR_OK;
+}
+
+// CG launch geometry: as many co-resident blocks as the room can use.
+struct CGLaunch {
+    unsigned blocks;
+    double *partials;
+    GridSync *gs;
+    CGScalars *sc;
+};
+
+unsigned cg_max_blocks()
+{
+    static unsigned cap = 0;
+    if (!cap) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg, kThreads, 0);
+        if (per_sm <= 0) per_sm = 1;
+        cap = (unsigned)(per_sm * sm_count());
+    }
+    return cap;
+}
+
+int launch_cg(const CGArgs &a, unsigned blocks, cudaStream_t s)
+{
+    FFR_CUDA(cudaMemsetAsync(a.gs, 0, sizeof(GridSync), s));
+    void *args[] = {(void *)&a};
+    FFR_CUDA(cudaLaunchCooperativeKernel((void *)k_cg, dim3(blocks), dim3(kThreads), args, 0, s));
+    count_launch(1);
+    return FFR_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------- fluid handle
+
+struct ffr_fluid {
+    HostRoom room;
+    ffr_fluid_params prm;
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    RoomTables tab;
+    RoomDev R;
+    double *u, *v, *w, *us, *vs, *ws, *p, *T0, *T1;
+    double *r, *da, *db, *ad, *partials, *tpart, *cg_res;
+    int *cg_iters, *cg_flags;
+    GridSync *gs;
+    CGScalars *sc;
+    StepState *st;
+    ffr_step_result *ring;
+    ffr_step_result *ring_host;
+    StepState *st_host;
+    unsigned long long *div_slot;
+    unsigned cg_blocks, blocks_faces, blocks_cells;
+    GroupTimer prof;
+};
+
+namespace {
+
+int fluid_enqueue_step(ffr_fluid *s)
+{
+    const ffr_fluid_params &P = s->prm;
+    cudaStream_t st = s->stream;
+    const RoomGeom &g = s->room.g;
+    PredArgs pa{P.dt, P.nu, P.advection, P.buoyancy ? 1 : 0, P.g_accel * P.beta * P.dt, P.T_initial};
+    s->prof.begin(FFR_PROF_PREDICT, st);
+    k_predict<<<s->blocks_faces, kThreads, 0, st>>>(s->R, pa, s->u, s->v, s->w, s->T0, s->T1, s->us,
+                                                     s->vs, s->ws, s->st);
+    FFR_LAUNCHED(1);
+    s->prof.end(st, 1);
+    CGArgs ca{};
+    ca.R = s->R;
+    ca.us = s->us; ca.vs = s->vs; ca.ws = s->ws;
+    ca.rhs_factor = -(P.rho / P.dt);
+    ca.from_faces = 1;
+    ca.x = s->p; ca.r = s->r; ca.da = s->da; ca.db = s->db; ca.ad = s->ad;
+    ca.partials = s->partials; ca.gs = s->gs; ca.sc = s->sc;
+    ca.max_iter = P.poisson_max_iter; ca.tol = P.poisson_tol;
+    ca.st = s->st;
+    s->prof.begin(FFR_PROF_PRESSURE, st);
+    int rc = launch_cg(ca, s->cg_blocks, st);
+    if (rc) return rc;
+    s->prof.end(st, 1);
+    CorrArgs co{P.dt / P.rho};
+    s->prof.begin(FFR_PROF_CORRECT, st);
+    k_correct<<<s->blocks_cells, kThreads, 0, st>>>(s->R, co, s->u, s->v, s->w, s->us, s->vs, s->ws,
+                                                     s->p, s->st);
+    FFR_LAUNCHED(1);
+    s->prof.end(st, 1);
+    int nthermal = 1;
+    s->prof.begin(FFR_PROF_THERMAL, st);
+    if (P.thermal) {
+        for (const ffr_patch &op : s->room.patches) {
+            if (!op.is_opening) continue;
+            k_opening_T<<<stream_blocks((long long)(op.a_max - op.a_min + 1) * (op.b_max - op.b_min + 1)),
+                          kThreads, 0, st>>>(s->R, op, s->u, s->v, s->w, s->T0, s->T1, s->st, 0);
+            FFR_LAUNCHED(1);
+            nthermal++;
+        }
+        ThermArgs ta{P.dt, P.k_thermal / (P.rho * P.cp), P.advection};
+        k_advect_T<<<s->blocks_cells, kThreads, 0, st>>>(s->R, ta, s->u, s->v, s->w, s->T0, s->T1,
+                                                          s->tpart, s->st);
+        FFR_LAUNCHED(1);
+        nthermal++;
+        for (const ffr_patch &op : s->room.patches) {
+            if (!op.is_opening) continue;
+            k_opening_T<<<stream_blocks((long long)(op.a_max - op.a_min + 1) * (op.b_max - op.b_min + 1)),
+                          kThreads, 0, st>>>(s->R, op, s->u, s->v, s->w, s->T0, s->T1, s->st, 1);
+            FFR_LAUNCHED(1);
+            nthermal++;
+        }
+    }
+    for (const ffr_heat_patch &h : s->room.heats) {
+        k_heat<<<stream_blocks((long long)(h.i_max - h.i_min + 1) * (h.j_max - h.j_min + 1) *
+                               (h.k_max - h.k_min + 1)),
+                 kThreads, 0, st>>>(s->R, h, s->T0, s->T1, s->st, P.thermal ? 1 : 0);
+        FFR_LAUNCHED(1);
+        nthermal++;
+    }
+    FinArgs fa{P.dt, P.convergence_tol, P.T_initial, P.T_target, P.thermal ? 1 : 0,
+               s->room.n_fluid, (int)s->blocks_cells};
+    k_finalize<<<1, kThreads, 0, st>>>(fa, s->tpart, s->st, s->ring);
+    FFR_LAUNCHED(1);
+    s->prof.end(st, nthermal);
+    (void)g;
+    return FFR_OK;
+}
+
+double *field_ptr(ffr_fluid *s, int field)
+{
+    switch (field) {
+    case FFR_FIELD_U: return s->u;
+    case FFR_FIELD_V: return s->v;
+    case FFR_FIELD_W: return s->w;
+    case FFR_FIELD_P: return s->p;
+    case FFR_FIELD_T: return s->st_host->tpar ? s->T1 : s->T0;
+    default: return nullptr;
+    }
+}
+
+long long field_len(const ffr_fluid *s, int field)
+{
+    const RoomGeom &g = s->room.g;
+    switch (field) {
+    case FFR_FIELD_U: return g.nu;
+    case FFR_FIELD_V: return g.nv;
+    case FFR_FIELD_W: return g.nw;
+    default: return g.n;
+    }
+}
+
+int pull_state(ffr_fluid *s)
+{
+    FFR_CUDA(cudaMemcpyAsync(s->st_host, s->st, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    s->prof.collect();
+    return FFR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
+                     const ffr_fields *init, ffr_fluid **out)
+{
+    if (!params || !out) return fail(FFR_EINVAL, "NULL params or out");
+    *out = nullptr;
+    if (params->precision != FFR_PREC_FP64)
+        return fail(FFR_ENOTSUP, "only FFR_PREC_FP64 is built in this library");
+    if (params->poisson != FFR_POISSON_CG || params->use_multigrid)
+        return fail(FFR_ENOTSUP, "only the CG pressure solve is built in this library");
+    if (!(params->dt > 0) || !(params->rho > 0)) return fail(FFR_EINVAL, "dt and rho must be positive");
+    if (params->advection < 0 || params->advection > 2) return fail(FFR_EINVAL, "bad advection scheme");
+    if (params->poisson_max_iter < 0) return fail(FFR_EINVAL, "negative poisson_max_iter");
+    ffr_fluid *s = new (std::nothrow) ffr_fluid();
+    if (!s) return fail(FFR_ENOMEM, "host allocation");
+    int rc = load_room(room, s->room);
+    if (rc) { delete s; return rc; }
+    s->prm = *params;
+    const RoomGeom &g = s->room.g;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete s;
+        return fail(FFR_ECUDA, "cudaStreamCreate");
+    }
+    s->cg_blocks = std::max(1u, std::min(cg_max_blocks(), (unsigned)((g.n + kThreads - 1) / kThreads)));
+    s->blocks_faces = stream_blocks(g.nu + g.nv + g.nw);
+    s->blocks_cells = stream_blocks(g.n);
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t bytes = tables_bytes(s->room) + 2 * (al(8 * g.nu) + al(8 * g.nv) + al(8 * g.nw)) +
+                         7 * al(8 * g.n) + al(8 * s->cg_blocks * 4) + al(8 * s->blocks_cells) +
+                         al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
+                         al(sizeof(ffr_step_result) * kRing) + 4 * 256;
+    rc = s->arena.alloc(bytes);
+    if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
+    rc = upload_tables(s->room, s->arena, s->stream, s->tab, s->R);
+    Arena &a = s->arena;
+    s->u = a.take<double>(g.nu); s->v = a.take<double>(g.nv); s->w = a.take<double>(g.nw);
+    s->us = a.take<double>(g.nu); s->vs = a.take<double>(g.nv); s->ws = a.take<double>(g.nw);
+    s->p = a.take<double>(g.n); s->T0 = a.take<double>(g.n); s->T1 = a.take<double>(g.n);
+    s->r = a.take<double>(g.n); s->da = a.take<double>(g.n); s->db = a.take<double>(g.n);
+    s->ad = a.take<double>(g.n);
+    s->partials = a.take<double>(s->cg_blocks * 4);
+    s->tpart = a.take<double>(s->blocks_cells);
+    s->gs = a.take<GridSync>(1);
+    s->sc = a.take<CGScalars>(1);
+    s->st = a.take<StepState>(1);
+    s->ring = a.take<ffr_step_result>(kRing);
+    s->cg_res = a.take<double>(1);
+    s->cg_iters = a.take<int>(1);
+    s->cg_flags = a.take<int>(1);
+    s->div_slot = a.take<unsigned long long>(1);
+    if (rc || !s->div_slot) {
+        if (!rc) rc = fail(FFR_ENOMEM, "arena exhausted");
+        ffr_fluid_destroy(s);
+        return rc;
+    }
+    if (cudaMallocHost(&s->ring_host, sizeof(ffr_step_result) * kRing) != cudaSuccess ||
+        cudaMallocHost(&s->st_host, sizeof(StepState)) != cudaSuccess) {
+        ffr_fluid_destroy(s);
+        return fail(FFR_ENOMEM, "pinned host allocation");
+    }
+    memset(s->st_host, 0, sizeof(StepState));
+    s->prof.reset(FFR_PROF_N);
+    cudaStream_t st = s->stream;
+#define UP(dst, src, cnt)                                                                      \
+    do {                                                                                       \
+        if (src) FFR_CUDA(cudaMemcpyAsync(dst, src, 8 * (cnt), cudaMemcpyHostToDevice, st));   \
+        else FFR_CUDA(cudaMemsetAsync(dst, 0, 8 * (cnt), st));                                 \
+    } while (0)
+    UP(s->u, init ? init->u : nullptr, g.nu);
+    UP(s->v, init ? init->v : nullptr, g.nv);
+    UP(s->w, init ? init->w : nullptr, g.nw);
+    UP(s->p, init ? init->p : nullptr, g.n);
+#undef UP
+    FFR_CUDA(cudaMemsetAsync(s->st, 0, sizeof(StepState), st));
+    k_fill<<<stream_blocks(g.n), kThreads, 0, st>>>(s->T0, (int)g.n, params->T_initial);
+    FFR_LAUNCHED(1);
+    if (params->thermal) {
+        for (const ffr_patch &op : s->room.patches) {
+            if (!op.is_opening) continue;
+            k_opening_T<<<stream_blocks((long long)(op.a_max - op.a_min + 1) * (op.b_max - op.b_min + 1)),
+                          kThreads, 0, st>>>(s->R, op, s->u, s->v, s->w, s->T0, s->T1, s->st, 0);
+            FFR_LAUNCHED(1);
+        }
+    }
+    FFR_CUDA(cudaStreamSynchronize(st));
+    *out = s;
+    return FFR_OK;
+}
+
+int ffr_fluid_destroy(ffr_fluid *s)
+{
+    if (!s) return FFR_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    s->prof.destroy();
+    s->arena.release();
+    if (s->ring_host) cudaFreeHost(s->ring_host);
+    if (s->st_host) cudaFreeHost(s->st_host);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return FFR_OK;
+}
+
+int ffr_fluid_advance(ffr_fluid *s, int nsteps, int stop_on_converge, ffr_step_result *results,
+                      int *steps_done)
+{
+    if (!s || nsteps < 0) return fail(FFR_EINVAL, "bad handle or nsteps");
+    int done_total = 0;
+    while (done_total < nsteps) {
+        const int chunk = std::min(kRing, nsteps - done_total);
+        StepState hs;
+        FFR_CUDA(cudaMemcpyAsync(&hs, s->st, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
+        FFR_CUDA(cudaStreamSynchronize(s->stream));
+        hs.ring_slot = 0;
+        hs.halt = 0;
+        hs.stop_on_converge = stop_on_converge ? 1 : 0;
+        FFR_CUDA(cudaMemcpyAsync(s->st, &hs, sizeof(StepState), cudaMemcpyHostToDevice, s->stream));
+        for (int k = 0; k < chunk; k++) {
+            int rc = fluid_enqueue_step(s);
+            if (rc) return rc;
+        }
+        FFR_CUDA(cudaMemcpyAsync(s->ring_host, s->ring, sizeof(ffr_step_result) * chunk,
+                                 cudaMemcpyDeviceToHost, s->stream));
+        int rc = pull_state(s);
+        if (rc) return rc;
+        GridSync gsh;
+        FFR_CUDA(cudaMemcpy(&gsh, s->gs, sizeof(GridSync), cudaMemcpyDeviceToHost));
+        const int got = s->st_host->ring_slot;
+        if (results) memcpy(results + done_total, s->ring_host, sizeof(ffr_step_result) * got);
+        done_total += got;
+        if (gsh.err) {
+            if (steps_done) *steps_done = done_total;
+            return fail(FFR_ETIMEDOUT, "pressure-solve grid barrier timed out");
+        }
+        if (got < chunk) break;   // halted on convergence
+    }
+    if (steps_done) *steps_done = done_total;
+    return FFR_OK;
+}
+
+int ffr_fluid_step(ffr_fluid *s, ffr_step_result *out)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    if (!out) {
+        // no result wanted: queue one step without a host round trip
+        StepState hs;
+        FFR_CUDA(cudaMemcpyAsync(&hs, s->st, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
+        FFR_CUDA(cudaStreamSynchronize(s->stream));
+        if (hs.ring_slot >= kRing) {
+            hs.ring_slot = 0;
+            FFR_CUDA(cudaMemcpyAsync(s->st, &hs, sizeof(StepState), cudaMemcpyHostToDevice, s->stream));
+        }
+        return fluid_enqueue_step(s);
+    }
+    int done = 0;
+    int rc = ffr_fluid_advance(s, 1, 0, out, &done);
+    if (rc) return rc;
+    return done == 1 ? FFR_OK : fail(FFR_ECUDA, "step did not execute");
+}
+
+int ffr_fluid_divergence_max(ffr_fluid *s, double *out)
+{
+    if (!s || !out) return fail(FFR_EINVAL, "NULL argument");
+    FFR_CUDA(cudaMemsetAsync(s->div_slot, 0, 8, s->stream));
+    k_divergence<<<s->blocks_cells, kThreads, 0, s->stream>>>(s->R, s->u, s->v, s->w, s->div_slot);
+    FFR_LAUNCHED(1);
+    unsigned long long bits = 0;
+    FFR_CUDA(cudaMemcpyAsync(&bits, s->div_slot, 8, cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    memcpy(out, &bits, 8);
+    return FFR_OK;
+}
+
+int ffr_fluid_current_step(ffr_fluid *s, int *out)
+{
+    if (!s || !out) return fail(FFR_EINVAL, "NULL argument");
+    int rc = pull_state(s);
+    if (rc) return rc;
+    *out = s->st_host->step;
+    return FFR_OK;
+}
+
+int ffr_fluid_get_field(ffr_fluid *s, int field, double *host)
+{
+    if (!s || !host || field < 0 || field > 4) return fail(FFR_EINVAL, "bad get_field arguments");
+    int rc = pull_state(s);
+    if (rc) return rc;
+    FFR_CUDA(cudaMemcpyAsync(host, field_ptr(s, field), 8 * field_len(s, field), cudaMemcpyDeviceToHost,
+                             s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    return FFR_OK;
+}
+
+int ffr_fluid_set_field(ffr_fluid *s, int field, const double *host)
+{
+    if (!s || !host || field < 0 || field > 4) return fail(FFR_EINVAL, "bad set_field arguments");
+    int rc = pull_state(s);
+    if (rc) return rc;
+    FFR_CUDA(cudaMemcpyAsync(field_ptr(s, field), host, 8 * field_len(s, field), cudaMemcpyHostToDevice,
+                             s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    return FFR_OK;
+}
+
+int ffr_fluid_field_dev(ffr_fluid *s, int field, double **dev)
+{
+    if (!s || !dev || field < 0 || field > 4) return fail(FFR_EINVAL, "bad field_dev arguments");
+    int rc = pull_state(s);
+    if (rc) return rc;
+    *dev = field_ptr(s, field);
+    return FFR_OK;
+}
+
+int ffr_fluid_synchronize(ffr_fluid *s)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    s->prof.collect();
+    return FFR_OK;
+}
+
+int ffr_fluid_stream(ffr_fluid *s, void **stream)
+{
+    if (!s || !stream) return fail(FFR_EINVAL, "NULL argument");
+    *stream = (void *)s->stream;
+    return FFR_OK;
+}
+
+int ffr_fluid_profile(ffr_fluid *s, int enable)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    s->prof.collect();
+    s->prof.reset(FFR_PROF_N);
+    s->prof.on = enable != 0;
+    return FFR_OK;
+}
+
+int ffr_fluid_profile_read(ffr_fluid *s, double *ms, long long *launches)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    s->prof.collect();
+    for (int g = 0; g < FFR_PROF_N; g++) {
+        if (ms) ms[g] = s->prof.ms[g];
+        if (launches) launches[g] = s->prof.launches[g];
+    }
+    return FFR_OK;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------- poisson handle
+
+struct ffr_poisson {
+    HostRoom room;
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    RoomTables tab;
+    RoomDev R;
+    int max_iter;
+    double tol;
+    double *r, *da, *db, *ad, *partials, *res, *x_tmp, *b_tmp;
+    int *iters, *flags;
+    GridSync *gs;
+    CGScalars *sc;
+    unsigned blocks;
+};
+
+extern "C" {
+
+int ffr_poisson_create(const ffr_room_desc *room, int max_iter, double tol, ffr_poisson **out)
+{
+    if (!out) return fail(FFR_EINVAL, "NULL out");
+    *out = nullptr;
+    if (max_iter < 0) return fail(FFR_EINVAL, "negative max_iter");
+    ffr_poisson *s = new (std::nothrow) ffr_poisson();
+    if (!s) return fail(FFR_ENOMEM, "host allocation");
+    int rc = load_room(room, s->room);
+    if (rc) { delete s; return rc; }
+    s->max_iter = max_iter;
+    s->tol = tol;
+    const RoomGeom &g = s->room.g;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete s;
+        return fail(FFR_ECUDA, "cudaStreamCreate");
+    }
+    s->blocks = std::max(1u, std::min(cg_max_blocks(), (unsigned)((g.n + kThreads - 1) / kThreads)));
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t bytes = tables_bytes(s->room) + 6 * al(8 * g.n) + al(8 * s->blocks * 4) +
+                         al(sizeof(GridSync)) + al(sizeof(CGScalars)) + 4 * 256;
+    rc = s->arena.alloc(bytes);
+    if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
+    rc = upload_tables(s->room, s->arena, s->stream, s->tab, s->R);
+    Arena &a = s->arena;
+    s->r = a.take<double>(g.n); s->da = a.take<double>(g.n); s->db = a.take<double>(g.n);
+    s->ad = a.take<double>(g.n); s->x_tmp = a.take<double>(g.n); s->b_tmp = a.take<double>(g.n);
+    s->partials = a.take<double>(s->blocks * 4);
+    s->gs = a.take<GridSync>(1);
+    s->sc = a.take<CGScalars>(1);
+    s->res = a.take<double>(1);
+    s->iters = a.take<int>(1);
+    s->flags = a.take<int>(1);
+    if (rc || !s->flags) {
+        if (!rc) rc = fail(FFR_ENOMEM, "arena exhausted");
+        ffr_poisson_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return FFR_OK;
+}
+
+int ffr_poisson_destroy(ffr_poisson *s)
+{
+    if (!s) return FFR_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    s->arena.release();
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return FFR_OK;
+}
+
+int ffr_poisson_solve_dev(ffr_poisson *s, const double *rhs_dev, double *p_dev, void *stream,
+                          double *residual, int *iterations)
+{
+    if (!s || !rhs_dev || !p_dev) return fail(FFR_EINVAL, "NULL argument");
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    CGArgs ca{};
+    ca.R = s->R;
+    ca.from_faces = 0;
+    ca.rhs = rhs_dev;
+    ca.x = p_dev; ca.r = s->r; ca.da = s->da; ca.db = s->db; ca.ad = s->ad;
+    ca.partials = s->partials; ca.gs = s->gs; ca.sc = s->sc;
+    ca.max_iter = s->max_iter; ca.tol = s->tol;
+    ca.st = nullptr;
+    ca.out_res = s->res; ca.out_iters = s->iters; ca.out_flags = s->flags;
+    int rc = launch_cg(ca, s->blocks, st);
+    if (rc) return rc;
+    double res = 0.0;
+    int it = 0, fl = 0;
+    FFR_CUDA(cudaMemcpyAsync(&res, s->res, 8, cudaMemcpyDeviceToHost, st));
+    FFR_CUDA(cudaMemcpyAsync(&it, s->iters, 4, cudaMemcpyDeviceToHost, st));
+    FFR_CUDA(cudaMemcpyAsync(&fl, s->flags, 4, cudaMemcpyDeviceToHost, st));
+    FFR_CUDA(cudaStreamSynchronize(st));
+    if (residual) *residual = res;
+    if (iterations) *iterations = it;
+    if (fl & FFR_FLAG_TIMEOUT) return fail(FFR_ETIMEDOUT, "pressure-solve grid barrier timed out");
+    return FFR_OK;
+}
+
+int ffr_poisson_solve(ffr_poisson *s, const double *rhs, double *p, double *residual,
+                      int *iterations)
+{
+    if (!s || !rhs || !p) return fail(FFR_EINVAL, "NULL argument");
+    const long long n = s->room.g.n;
+    FFR_CUDA(cudaMemcpyAsync(s->b_tmp, rhs, 8 * n, cudaMemcpyHostToDevice, s->stream));
+    int rc = ffr_poisson_solve_dev(s, s->b_tmp, s->x_tmp, nullptr, residual, iterations);
+    if (rc) return rc;
+    FFR_CUDA(cudaMemcpyAsync(p, s->x_tmp, 8 * n, cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    return FFR_OK;
+}
+
+}  // extern "C"
+
+namespace ffr {
+// y = L x with the CG stencil (used by ffr_poisson_apply).
+__global__ void k_apply_stencil(RoomDev R, const double *x, double *y)
+{
+    const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
+    const double *sxl = R.scale, *sxr = sxl + nx, *syl = sxr + nx, *syr = syl + ny, *szl = syr + ny,
+                 *szr = szl + nz;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.n; c += gridDim.x * blockDim.x) {
+        const unsigned code = R.sc[c];
+        if (code & SC_SOLID) { y[c] = x[c]; continue; }
+        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+        double diag = 0.0, off = 0.0;
+        if ((code >> 0) & 3) stencil_term((code >> 0) & 3, sxl[i], ((code >> 0) & 3) == SC_IN ? x[c - plane] : 0.0, diag, off);
+        if ((code >> 2) & 3) stencil_term((code >> 2) & 3, sxr[i], ((code >> 2) & 3) == SC_IN ? x[c + plane] : 0.0, diag, off);
+        if ((code >> 4) & 3) stencil_term((code >> 4) & 3, syl[j], ((code >> 4) & 3) == SC_IN ? x[c - nz] : 0.0, diag, off);
+        if ((code >> 6) & 3) stencil_term((code >> 6) & 3, syr[j], ((code >> 6) & 3) == SC_IN ? x[c + nz] : 0.0, diag, off);
+        if ((code >> 8) & 3) stencil_term((code >> 8) & 3, szl[k], ((code >> 8) & 3) == SC_IN ? x[c - 1] : 0.0, diag, off);
+        if ((code >> 10) & 3) stencil_term((code >> 10) & 3, szr[k], ((code >> 10) & 3) == SC_IN ? x[c + 1] : 0.0, diag, off);
+        if (diag < 1e-30) diag = 1.0;
+        y[c] = diag * x[c] - off;
+    }
+}
+}  // namespace ffr
+
+extern "C" int ffr_poisson_apply(ffr_poisson *s, const double *x, double *ax)
+{
+    if (!s || !x || !ax) return fail(FFR_EINVAL, "NULL argument");
+    const long long n = s->room.g.n;
+    FFR_CUDA(cudaMemcpyAsync(s->b_tmp, x, 8 * n, cudaMemcpyHostToDevice, s->stream));
+    k_apply_stencil<<<stream_blocks(n), kThreads, 0, s->stream>>>(s->R, s->b_tmp, s->x_tmp);
+    FFR_LAUNCHED(1);
+    FFR_CUDA(cudaMemcpyAsync(ax, s->x_tmp, 8 * n, cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    return FFR_OK;
+}

@@ -1,0 +1,386 @@
+"""ctypes binding of libffroom_cuda.so (include/ffroom.h).
+
+This is the reference-side binding a ctypes caller would add for the C ABI;
+``_ffroom_core`` (the pybind11 module) is the other front-end.  The library
+is loaded from this package directory and must exist: there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional
+
+import numpy as np
+
+from .params import FluidParams
+from .scene import RoomSpec
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "libffroom_cuda.so")
+
+FFR_OK, FFR_EINVAL, FFR_ENOMEM, FFR_ECUDA, FFR_ETIMEDOUT, FFR_ENOTSUP, FFR_ERANGE = range(7)
+FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "T": 4}
+PREC = {"fp64": 0, "mixed": 1}
+POISSON = {"cg": 0, "mgpcg": 1}
+LBM_STORAGE = {"fp64": 0, "fp32": 1, "fp16": 2}
+
+_dp = C.POINTER(C.c_double)
+
+
+class FfrError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class Fan(C.Structure):
+    _fields_ = [("i_min", C.c_int), ("i_max", C.c_int), ("j_min", C.c_int), ("j_max", C.c_int),
+                ("k_min", C.c_int), ("k_max", C.c_int), ("vel", C.c_double * 3)]
+
+
+class Patch(C.Structure):
+    _fields_ = [("axis", C.c_int), ("side", C.c_int), ("a_min", C.c_int), ("a_max", C.c_int),
+                ("b_min", C.c_int), ("b_max", C.c_int), ("is_opening", C.c_int),
+                ("T_outside", C.c_double)]
+
+
+class HeatPatch(C.Structure):
+    _fields_ = [("i_min", C.c_int), ("i_max", C.c_int), ("j_min", C.c_int), ("j_max", C.c_int),
+                ("k_min", C.c_int), ("k_max", C.c_int), ("T", C.c_double)]
+
+
+class RoomDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("dxv", _dp), ("dyv", _dp), ("dzv", _dp), ("cell_type", C.POINTER(C.c_uint8)),
+                ("nfans", C.c_int), ("fans", C.POINTER(Fan)),
+                ("npatches", C.c_int), ("patches", C.POINTER(Patch)),
+                ("nheat", C.c_int), ("heats", C.POINTER(HeatPatch))]
+
+
+class FluidParamsC(C.Structure):
+    _fields_ = [("rho", C.c_double), ("nu", C.c_double), ("dt", C.c_double),
+                ("max_steps", C.c_int), ("convergence_tol", C.c_double),
+                ("poisson_max_iter", C.c_int), ("poisson_tol", C.c_double),
+                ("advection", C.c_int), ("use_multigrid", C.c_int), ("thermal", C.c_int),
+                ("T_initial", C.c_double), ("T_target", C.c_double), ("buoyancy", C.c_int),
+                ("g_accel", C.c_double), ("beta", C.c_double), ("k_thermal", C.c_double),
+                ("cp", C.c_double), ("precision", C.c_int), ("poisson", C.c_int)]
+
+
+class StepResultC(C.Structure):
+    _fields_ = [("step", C.c_int), ("velocity_change", C.c_double),
+                ("pressure_residual", C.c_double), ("divergence_max", C.c_double),
+                ("converged", C.c_int), ("T_mean", C.c_double), ("cg_iterations", C.c_int),
+                ("flags", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Fields(C.Structure):
+    _fields_ = [("u", _dp), ("v", _dp), ("w", _dp), ("p", _dp)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads the library once; raises when it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run ff-room_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        sigs = {
+            "ffr_status_string": ([C.c_int], C.c_char_p),
+            "ffr_last_error": ([], C.c_char_p),
+            "ffr_version": ([], C.c_char_p),
+            "ffr_launch_count": ([], C.c_ulonglong),
+            "ffr_fluid_create": ([C.POINTER(RoomDesc), C.POINTER(FluidParamsC), C.POINTER(Fields), C.POINTER(vp)], C.c_int),
+            "ffr_fluid_destroy": ([vp], C.c_int),
+            "ffr_fluid_step": ([vp, C.POINTER(StepResultC)], C.c_int),
+            "ffr_fluid_advance": ([vp, C.c_int, C.c_int, C.POINTER(StepResultC), C.POINTER(C.c_int)], C.c_int),
+            "ffr_fluid_divergence_max": ([vp, _dp], C.c_int),
+            "ffr_fluid_current_step": ([vp, C.POINTER(C.c_int)], C.c_int),
+            "ffr_fluid_get_field": ([vp, C.c_int, _dp], C.c_int),
+            "ffr_fluid_set_field": ([vp, C.c_int, _dp], C.c_int),
+            "ffr_fluid_field_dev": ([vp, C.c_int, C.POINTER(vp)], C.c_int),
+            "ffr_fluid_synchronize": ([vp], C.c_int),
+            "ffr_poisson_create": ([C.POINTER(RoomDesc), C.c_int, C.c_double, C.POINTER(vp)], C.c_int),
+            "ffr_poisson_destroy": ([vp], C.c_int),
+            "ffr_poisson_solve_dev": ([vp, vp, vp, vp, _dp, C.POINTER(C.c_int)], C.c_int),
+            "ffr_poisson_solve": ([vp, _dp, _dp, _dp, C.POINTER(C.c_int)], C.c_int),
+            "ffr_poisson_apply": ([vp, _dp, _dp], C.c_int),
+            "ffr_lbm_create": ([C.POINTER(RoomDesc), C.c_double, C.c_int, C.c_double, C.c_double, C.c_int,
+                                C.POINTER(Fields), C.POINTER(vp)], C.c_int),
+            "ffr_lbm_destroy": ([vp], C.c_int),
+            "ffr_lbm_step": ([vp, C.POINTER(StepResultC)], C.c_int),
+            "ffr_lbm_advance": ([vp, C.c_int, C.c_int, C.POINTER(StepResultC), C.POINTER(C.c_int)], C.c_int),
+            "ffr_lbm_divergence_max": ([vp, _dp], C.c_int),
+            "ffr_lbm_current_step": ([vp, C.POINTER(C.c_int)], C.c_int),
+            "ffr_lbm_get_field": ([vp, C.c_int, _dp], C.c_int),
+            "ffr_lbm_set_field": ([vp, C.c_int, _dp], C.c_int),
+            "ffr_lbm_synchronize": ([vp], C.c_int),
+            "ffr_fluid_stream": ([vp, C.POINTER(vp)], C.c_int),
+            "ffr_fluid_profile": ([vp, C.c_int], C.c_int),
+            "ffr_fluid_profile_read": ([vp, _dp, C.POINTER(C.c_longlong)], C.c_int),
+            "ffr_lbm_stream": ([vp, C.POINTER(vp)], C.c_int),
+            "ffr_lbm_profile": ([vp, C.c_int], C.c_int),
+            "ffr_lbm_profile_read": ([vp, _dp, C.POINTER(C.c_longlong)], C.c_int),
+        }
+        for name, (args, res) in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != FFR_OK:
+        L = lib()
+        raise FfrError(status, f"{L.ffr_status_string(status).decode()}: {L.ffr_last_error().decode()}")
+
+
+def launch_count() -> int:
+    return int(lib().ffr_launch_count())
+
+
+class _RoomMarshal:
+    """Keeps the numpy/ctypes buffers of a RoomDesc alive."""
+
+    def __init__(self, room: RoomSpec):
+        self.dxv = np.ascontiguousarray(room.dxv, dtype=np.float64)
+        self.dyv = np.ascontiguousarray(room.dyv, dtype=np.float64)
+        self.dzv = np.ascontiguousarray(room.dzv, dtype=np.float64)
+        self.ct = np.ascontiguousarray(room.cell_type, dtype=np.uint8)
+        self.fans = (Fan * max(1, len(room.fans)))()
+        for i, f in enumerate(room.fans):
+            self.fans[i] = Fan(*f.box, (C.c_double * 3)(*f.vel))
+        self.patches = (Patch * max(1, len(room.outflows)))()
+        for i, p in enumerate(room.outflows):
+            self.patches[i] = Patch(p.axis, p.side, p.a_min, p.a_max, p.b_min, p.b_max,
+                                    int(p.is_opening), p.T_outside if p.is_opening else 0.0)
+        self.heats = (HeatPatch * max(1, len(room.heats)))()
+        for i, h in enumerate(room.heats):
+            self.heats[i] = HeatPatch(*h.box, h.T)
+        self.desc = RoomDesc(room.nx, room.ny, room.nz, room.lx, room.ly, room.lz,
+                             self.dxv.ctypes.data_as(_dp), self.dyv.ctypes.data_as(_dp),
+                             self.dzv.ctypes.data_as(_dp),
+                             self.ct.ctypes.data_as(C.POINTER(C.c_uint8)),
+                             len(room.fans), self.fans, len(room.outflows), self.patches,
+                             len(room.heats), self.heats)
+
+
+def _params(p: FluidParams) -> FluidParamsC:
+    return FluidParamsC(p.rho, p.nu, p.dt, p.max_steps, p.convergence_tol, p.poisson_max_iter,
+                        p.poisson_tol, p.advection, int(p.use_multigrid), int(p.thermal), p.T_initial,
+                        p.T_target, int(p.buoyancy), p.g_accel, p.beta, p.k_thermal, p.cp,
+                        PREC[p.precision], POISSON[p.poisson])
+
+
+def _fields(init: Optional[dict]):
+    keep = {}
+    if not init:
+        return None, keep
+    for k in ("u", "v", "w", "p"):
+        if init.get(k) is not None:
+            keep[k] = np.ascontiguousarray(init[k], dtype=np.float64).reshape(-1)
+    f = Fields(*[keep[k].ctypes.data_as(_dp) if k in keep else None for k in ("u", "v", "w", "p")])
+    return f, keep
+
+
+class FluidHandle:
+    """One projection solver (ffr_fluid)."""
+    _pfx = "ffr_fluid"
+    _groups = ("predict", "pressure", "correct", "thermal")
+    _ngroups = 4
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        check(getattr(lib(), self._pfx + "_stream")(self.h, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, enable: bool = True) -> None:
+        check(getattr(lib(), self._pfx + "_profile")(self.h, int(enable)))
+
+    def profile_read(self):
+        n = self._ngroups
+        ms = (C.c_double * n)()
+        la = (C.c_longlong * n)()
+        check(getattr(lib(), self._pfx + "_profile_read")(self.h, ms, la))
+        return {g: (ms[i], la[i]) for i, g in enumerate(self._groups)}
+
+    def __init__(self, room: RoomSpec, params: FluidParams, init: Optional[dict] = None):
+        self.room = room
+        self.params = params
+        self._m = _RoomMarshal(room)
+        pc = _params(params)
+        f, keep = _fields(init)
+        h = C.c_void_p()
+        check(lib().ffr_fluid_create(C.byref(self._m.desc), C.byref(pc), C.byref(f) if f else None,
+                                     C.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().ffr_fluid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self) -> dict:
+        r = StepResultC()
+        check(lib().ffr_fluid_step(self.h, C.byref(r)))
+        return r.as_dict()
+
+    def advance(self, nsteps: int, stop_on_converge: bool = False, want_results: bool = True) -> List[dict]:
+        res = (StepResultC * max(1, nsteps))() if want_results else None
+        done = C.c_int(0)
+        check(lib().ffr_fluid_advance(self.h, nsteps, int(stop_on_converge), res, C.byref(done)))
+        return [res[i].as_dict() for i in range(done.value)] if want_results else [None] * done.value
+
+    def get(self, field: str) -> np.ndarray:
+        shape = self.room.shapes()[field]
+        out = np.empty(int(np.prod(shape)), dtype=np.float64)
+        check(lib().ffr_fluid_get_field(self.h, FIELD[field], out.ctypes.data_as(_dp)))
+        return out
+
+    def set(self, field: str, arr) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        check(lib().ffr_fluid_set_field(self.h, FIELD[field], a.ctypes.data_as(_dp)))
+
+    def field_dev(self, field: str) -> int:
+        p = C.c_void_p()
+        check(lib().ffr_fluid_field_dev(self.h, FIELD[field], C.byref(p)))
+        return p.value
+
+    def divergence_max(self) -> float:
+        d = C.c_double()
+        check(lib().ffr_fluid_divergence_max(self.h, C.byref(d)))
+        return d.value
+
+    def current_step(self) -> int:
+        s = C.c_int()
+        check(lib().ffr_fluid_current_step(self.h, C.byref(s)))
+        return s.value
+
+    def synchronize(self) -> None:
+        check(lib().ffr_fluid_synchronize(self.h))
+
+
+class PoissonHandle:
+    """ffr_poisson: the pressure solve bound to one room."""
+
+    def __init__(self, room: RoomSpec, max_iter: int, tol: float):
+        self.room = room
+        self._m = _RoomMarshal(room)
+        h = C.c_void_p()
+        check(lib().ffr_poisson_create(C.byref(self._m.desc), max_iter, tol, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().ffr_poisson_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, rhs):
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        p = np.empty_like(rhs)
+        res, it = C.c_double(), C.c_int()
+        check(lib().ffr_poisson_solve(self.h, rhs.ctypes.data_as(_dp), p.ctypes.data_as(_dp),
+                                      C.byref(res), C.byref(it)))
+        return p, res.value, it.value
+
+    def solve_dev(self, rhs_ptr: int, p_ptr: int, stream: int = 0):
+        res, it = C.c_double(), C.c_int()
+        check(lib().ffr_poisson_solve_dev(self.h, C.c_void_p(rhs_ptr), C.c_void_p(p_ptr),
+                                          C.c_void_p(stream) if stream else None, C.byref(res),
+                                          C.byref(it)))
+        return res.value, it.value
+
+    def apply(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        check(lib().ffr_poisson_apply(self.h, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp)))
+        return y
+
+
+class LbmHandle:
+    """ffr_lbm: the D3Q19 solver."""
+    _pfx = "ffr_lbm"
+    _groups = ("stream_collide", "faces")
+    _ngroups = 2
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        check(getattr(lib(), self._pfx + "_stream")(self.h, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, enable: bool = True) -> None:
+        check(getattr(lib(), self._pfx + "_profile")(self.h, int(enable)))
+
+    def profile_read(self):
+        n = self._ngroups
+        ms = (C.c_double * n)()
+        la = (C.c_longlong * n)()
+        check(getattr(lib(), self._pfx + "_profile_read")(self.h, ms, la))
+        return {g: (ms[i], la[i]) for i, g in enumerate(self._groups)}
+
+    def __init__(self, room: RoomSpec, tau: float, max_steps: int, tol: float, dt: float,
+                 storage: str = "fp64", init: Optional[dict] = None):
+        self.room = room
+        self._m = _RoomMarshal(room)
+        f, keep = _fields(init)
+        h = C.c_void_p()
+        check(lib().ffr_lbm_create(C.byref(self._m.desc), tau, max_steps, tol, dt, LBM_STORAGE[storage],
+                                   C.byref(f) if f else None, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().ffr_lbm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self) -> dict:
+        r = StepResultC()
+        check(lib().ffr_lbm_step(self.h, C.byref(r)))
+        return r.as_dict()
+
+    def advance(self, nsteps: int, stop_on_converge: bool = False) -> List[dict]:
+        res = (StepResultC * max(1, nsteps))()
+        done = C.c_int(0)
+        check(lib().ffr_lbm_advance(self.h, nsteps, int(stop_on_converge), res, C.byref(done)))
+        return [res[i].as_dict() for i in range(done.value)]
+
+    def get(self, field: str) -> np.ndarray:
+        shape = self.room.shapes()[field]
+        out = np.empty(int(np.prod(shape)), dtype=np.float64)
+        check(lib().ffr_lbm_get_field(self.h, FIELD[field], out.ctypes.data_as(_dp)))
+        return out
+
+    def divergence_max(self) -> float:
+        d = C.c_double()
+        check(lib().ffr_lbm_divergence_max(self.h, C.byref(d)))
+        return d.value
+
+    def synchronize(self) -> None:
+        check(lib().ffr_lbm_synchronize(self.h))

@@ -1,0 +1,248 @@
+/*
+ * ffroom.h — C ABI of the B200 (sm_100a) room solver, libffroom_cuda.so.
+ *
+ * This is the drop-in boundary for ff-room's per-timestep solver: the
+ * pybind11 module `_ffroom_core` shipped next to the library (the same class
+ * surface as the reference's cpp/src/bindings/module.cpp) calls only these
+ * functions, and a C, ctypes or cgo caller can bind them directly.  Every
+ * entry point returns an ffr_status; no C++ exception crosses the ABI.
+ * Field arrays use the reference layout (cpp/src/core/Grid.hpp:59-65):
+ * flat, k fastest; u is (nx+1)*ny*nz, v nx*(ny+1)*nz, w nx*ny*(nz+1),
+ * p / T / cell_type nx*ny*nz.  Host pointers are plain `double *`; device
+ * pointers are marked `_dev`.
+ *
+ * Thread safety: a handle may be used by one host thread at a time; distinct
+ * handles are independent (each owns its CUDA stream and memory).
+ */
+#ifndef FFROOM_H
+#define FFROOM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status */
+typedef enum ffr_status {
+    FFR_OK = 0,
+    FFR_EINVAL = 1,      /* bad argument (the reference would throw or misbehave) */
+    FFR_ENOMEM = 2,      /* device or pinned-host allocation failed */
+    FFR_ECUDA = 3,       /* a CUDA runtime call failed */
+    FFR_ETIMEDOUT = 4,   /* a bounded device-side wait gave up */
+    FFR_ENOTSUP = 5,     /* valid for the reference, not supported here */
+    FFR_ERANGE = 6       /* a size exceeds a fixed capacity */
+} ffr_status;
+
+/* Step-result status bits (ffr_step_result.flags). */
+#define FFR_FLAG_NAN          1  /* a NaN reached the velocity field */
+#define FFR_FLAG_CG_MAXITER   2  /* the pressure solve hit poisson_max_iter */
+#define FFR_FLAG_CG_BREAKDOWN 4  /* |d.Ad| < 1e-30 ended the pressure solve */
+#define FFR_FLAG_TIMEOUT      8  /* a device barrier timed out */
+
+/* Static text for a status code. */
+const char *ffr_status_string(int status);
+/* Detail of the most recent failure on the calling thread ("" if none). */
+const char *ffr_last_error(void);
+/* Library version, e.g. "0.1.0 sm_100a". */
+const char *ffr_version(void);
+/* Kernels this library has launched since load (all handles). */
+unsigned long long ffr_launch_count(void);
+
+/* ------------------------------------------------------------- rooms */
+
+/* Cell types, cpp/src/core/Grid.hpp:9-14. */
+enum { FFR_FLUID = 0, FFR_SOLID = 1, FFR_INFLOW = 2, FFR_OUTFLOW = 3 };
+/* Advection schemes, cpp/src/core/FluidSolver.hpp:9. */
+enum { FFR_UPWIND1 = 0, FFR_QUICK = 1, FFR_LAX_WENDROFF = 2 };
+/* Field selectors. */
+enum { FFR_FIELD_U = 0, FFR_FIELD_V = 1, FFR_FIELD_W = 2, FFR_FIELD_P = 3, FFR_FIELD_T = 4 };
+/* Arithmetic of the projection step. */
+enum { FFR_PREC_FP64 = 0,   /* the reference method, FP64 throughout */
+       FFR_PREC_MIXED = 1 };/* FP32 predictor/thermal, FP64 Krylov outer loop */
+/* Pressure solver. */
+enum { FFR_POISSON_CG = 0,    /* the reference's unpreconditioned CG */
+       FFR_POISSON_MGPCG = 1 };/* multigrid-preconditioned CG */
+/* LBM population storage. */
+enum { FFR_LBM_FP64 = 0, FFR_LBM_FP32 = 1, FFR_LBM_FP16 = 2 };
+
+/* FanBC, cpp/src/core/BoundaryManager.hpp:8-13: an inclusive cell box
+ * (clamped to the grid) and the face velocity it imposes. */
+typedef struct ffr_fan {
+    int i_min, i_max, j_min, j_max, k_min, k_max;
+    double vel[3];
+} ffr_fan;
+
+/* OutflowBC / OpeningBC, cpp/src/core/BoundaryManager.hpp:15-29: a patch of
+ * boundary cells on wall (axis, side); openings also carry T_outside. */
+typedef struct ffr_patch {
+    int axis, side, a_min, a_max, b_min, b_max;
+    int is_opening;
+    double T_outside;
+} ffr_patch;
+
+/* Fixed-temperature cell box (no counterpart in the reference: the heated
+ * floor / cooled ceiling extension, re-imposed after every step). */
+typedef struct ffr_heat_patch {
+    int i_min, i_max, j_min, j_max, k_min, k_max;
+    double T;
+} ffr_heat_patch;
+
+/* One room: the state a reference Grid + BoundaryManager pair carries
+ * (Grid.hpp:26-69, BoundaryManager.hpp:31-72).  `patches` is the
+ * BoundaryManager outflow list in insertion order with openings included,
+ * exactly as add_outflow/add_opening build it (BoundaryManager.cpp:24-44,
+ * 132-135). */
+typedef struct ffr_room_desc {
+    int nx, ny, nz;
+    double lx, ly, lz;
+    const double *dxv, *dyv, *dzv;     /* cell spacings, sizes nx, ny, nz */
+    const uint8_t *cell_type;          /* nx*ny*nz */
+    int nfans;    const ffr_fan *fans;
+    int npatches; const ffr_patch *patches;
+    int nheat;    const ffr_heat_patch *heats;
+} ffr_room_desc;
+
+/* FluidSolverParams + PoissonSolverParams, cpp/src/core/FluidSolver.hpp:
+ * 11-38 and PoissonSolver.hpp:14-18, plus precision / poisson selectors. */
+typedef struct ffr_fluid_params {
+    double rho, nu, dt;
+    int max_steps;
+    double convergence_tol;
+    int poisson_max_iter;
+    double poisson_tol;
+    int advection;
+    int use_multigrid;     /* reference flag; selects FFR_POISSON_MGPCG here */
+    int thermal;
+    double T_initial, T_target;
+    int buoyancy;
+    double g_accel, beta, k_thermal, cp;
+    int precision;         /* FFR_PREC_* */
+    int poisson;           /* FFR_POISSON_* */
+} ffr_fluid_params;
+
+/* StepResult, cpp/src/core/FluidSolver.hpp:40-47, plus the pressure-solve
+ * iteration count and status flags (FFR_FLAG_*). */
+typedef struct ffr_step_result {
+    int step;
+    double velocity_change;
+    double pressure_residual;
+    double divergence_max;
+    int converged;
+    double T_mean;
+    int cg_iterations;
+    int flags;
+} ffr_step_result;
+
+/* Initial fields for a new solver; any pointer may be NULL (zeros). */
+typedef struct ffr_fields {
+    const double *u, *v, *w, *p;
+} ffr_fields;
+
+/* --------------------------------------------------- projection solver */
+typedef struct ffr_fluid ffr_fluid;
+
+/* FluidSolver::FluidSolver (cpp/src/core/FluidSolver.cpp:18-32): uploads the
+ * room and the initial fields, sets T := T_initial and, when thermal,
+ * applies the opening temperature BC. */
+int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
+                     const ffr_fields *init, ffr_fluid **out);
+int ffr_fluid_destroy(ffr_fluid *s);
+
+/* FluidSolver::step (FluidSolver.cpp:486-550): one projection step; `out`
+ * may be NULL (then no host synchronisation happens). */
+int ffr_fluid_step(ffr_fluid *s, ffr_step_result *out);
+
+/* FluidSolver::run (FluidSolver.cpp:552-560) without the per-step callback:
+ * up to `nsteps` steps queued on the device with no host synchronisation in
+ * between; with stop_on_converge the steps after the first converged one do
+ * no work.  `results` (nsteps entries, may be NULL) receives every executed
+ * step; `steps_done` the count. */
+int ffr_fluid_advance(ffr_fluid *s, int nsteps, int stop_on_converge,
+                      ffr_step_result *results, int *steps_done);
+
+/* FluidSolver::compute_divergence_max (FluidSolver.cpp:470-484). */
+int ffr_fluid_divergence_max(ffr_fluid *s, double *out);
+/* FluidSolver::current_step (FluidSolver.hpp:63). */
+int ffr_fluid_current_step(ffr_fluid *s, int *out);
+
+/* Host <-> device copies of one field (FFR_FIELD_*), reference layout.  They
+ * back the Grid's numpy views (module.cpp:45-80). */
+int ffr_fluid_get_field(ffr_fluid *s, int field, double *host);
+int ffr_fluid_set_field(ffr_fluid *s, int field, const double *host);
+/* Device pointer of one field (valid until destroy; the solver swaps its
+ * buffers between steps, so re-query after every step). */
+int ffr_fluid_field_dev(ffr_fluid *s, int field, double **dev);
+/* Blocks until all queued work of the handle is done. */
+int ffr_fluid_synchronize(ffr_fluid *s);
+/* The cudaStream_t all work of the handle runs on. */
+int ffr_fluid_stream(ffr_fluid *s, void **stream);
+
+/* Kernel-group timing: while enabled, every queued step records CUDA events
+ * on the handle's stream around each group (no counterpart in the
+ * reference; it backs the benchmark's per-kernel roofline).  _read returns
+ * the milliseconds and the launch count accumulated per group since the
+ * last enable. */
+enum { FFR_PROF_PREDICT = 0, FFR_PROF_PRESSURE = 1, FFR_PROF_CORRECT = 2, FFR_PROF_THERMAL = 3,
+       FFR_PROF_N = 4 };
+int ffr_fluid_profile(ffr_fluid *s, int enable);
+int ffr_fluid_profile_read(ffr_fluid *s, double *ms, long long *launches);
+
+/* ------------------------------------------------------ pressure solve */
+typedef struct ffr_poisson ffr_poisson;
+
+/* A PoissonSolver bound to one room's mask and spacing
+ * (cpp/src/core/PoissonSolver.hpp:20-38); allocates its CG scratch. */
+int ffr_poisson_create(const ffr_room_desc *room, int max_iter, double tol,
+                       ffr_poisson **out);
+int ffr_poisson_destroy(ffr_poisson *s);
+
+/* PoissonSolver::solve (PoissonSolver.cpp:93-158) on device buffers: CG
+ * from x0 = 0 on L = -lap with the mask-dependent stencil
+ * (PoissonSolver.cpp:22-91).  `stream` is a cudaStream_t (NULL = the
+ * handle's own stream).  Synchronises and returns the relative residual and
+ * the iteration count. */
+int ffr_poisson_solve_dev(ffr_poisson *s, const double *rhs_dev, double *p_dev,
+                          void *stream, double *residual, int *iterations);
+
+/* The same on host buffers (uploads rhs, downloads p). */
+int ffr_poisson_solve(ffr_poisson *s, const double *rhs, double *p,
+                      double *residual, int *iterations);
+
+/* PoissonSolver::apply_laplacian (PoissonSolver.cpp:22-91) on host buffers. */
+int ffr_poisson_apply(ffr_poisson *s, const double *x, double *ax);
+
+/* ------------------------------------------------------------------ LBM */
+typedef struct ffr_lbm ffr_lbm;
+
+/* LBMSolver::LBMSolver (cpp/src/core/LBMSolver.cpp:33-74): f := W_q, INFLOW
+ * cells := feq(1, u_fan*dt/dx).  `init` seeds the face velocities that the
+ * first step's velocity change is measured against (NULL = zeros). */
+int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps,
+                   double convergence_tol, double dt, int storage,
+                   const ffr_fields *init, ffr_lbm **out);
+int ffr_lbm_destroy(ffr_lbm *s);
+/* LBMSolver::step (LBMSolver.cpp:402-440). */
+int ffr_lbm_step(ffr_lbm *s, ffr_step_result *out);
+/* LBMSolver::run (LBMSolver.cpp:446-454) without the callback. */
+int ffr_lbm_advance(ffr_lbm *s, int nsteps, int stop_on_converge,
+                    ffr_step_result *results, int *steps_done);
+/* LBMSolver::compute_divergence_max (LBMSolver.cpp:382-396). */
+int ffr_lbm_divergence_max(ffr_lbm *s, double *out);
+int ffr_lbm_current_step(ffr_lbm *s, int *out);
+/* Fields as the reference writes them into the Grid each step
+ * (extract_macroscopic, LBMSolver.cpp:288-376): u, v, w faces and p. */
+int ffr_lbm_get_field(ffr_lbm *s, int field, double *host);
+int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host);
+int ffr_lbm_synchronize(ffr_lbm *s);
+int ffr_lbm_stream(ffr_lbm *s, void **stream);
+/* Kernel-group timing as for ffr_fluid_profile; groups FFR_LPROF_*. */
+enum { FFR_LPROF_STREAM_COLLIDE = 0, FFR_LPROF_FACES = 1, FFR_LPROF_N = 2 };
+int ffr_lbm_profile(ffr_lbm *s, int enable);
+int ffr_lbm_profile_read(ffr_lbm *s, double *ms, long long *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FFROOM_H */

@@ -1,0 +1,43 @@
+"""The CPU oracle (oracle/ffr_oracle.c) against the reference's own outputs.
+
+The golden fixtures come from the compiled reference (tests/golden/
+make_golden.py).  The oracle must reproduce every field and every step
+result, including the CG iteration counts, before it may judge the GPU.
+Tolerances: 1e-11 max-norm relative for short runs (only the FMA contraction
+of the reference's -O3 build differs), 1e-8 for the 500-step run.
+"""
+import numpy as np
+import pytest
+
+from conftest import Golden, golden_names, rel_err
+from oracle import new_fields
+
+CASES = golden_names()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference(name, oracle):
+    g = Golden(name)
+    assert np.array_equal(g.room.cell_type, g.cell_type), "scene builder mask differs from the reference Scene"
+    fl = new_fields(g.room)
+    if g.lbm:
+        f = oracle.lbm_init(g.room, g.lbm["tau"], g.lbm["dt"])
+        recs = oracle.lbm_run(g.room, g.lbm["tau"], g.lbm["dt"], g.lbm["tol"], f, fl, g.nsteps)
+        keys = "uvwp"
+    else:
+        oracle.fluid_init(g.room, g.params, fl)
+        recs = oracle.fluid_run(g.room, g.params, fl, g.nsteps)
+        keys = "uvwpT"
+    tol = 1e-8 if g.nsteps > 100 else 1e-11
+    assert len(recs) == g.nsteps
+    for k in keys:
+        assert rel_err(fl[k], g.fields[k]) <= tol, (k, rel_err(fl[k], g.fields[k]))
+    its = np.array([r.cg_iterations for r in recs])
+    if g.nsteps > 100:
+        assert np.max(np.abs(its - g.hist["cg_iterations"])) <= 1
+    else:
+        assert np.array_equal(its, g.hist["cg_iterations"])
+    for key in ("velocity_change", "divergence_max", "T_mean", "pressure_residual"):
+        got = np.array([getattr(r, key) for r in recs])
+        assert rel_err(got, g.hist[key]) <= max(tol, 1e-9), key
+    assert [r.converged for r in recs] == list(g.hist["converged"].astype(bool))
