@@ -5,9 +5,10 @@
 // a zeroed buffer -> outflow copy -> macroscopic extraction.  Here the state
 // kept between steps is the post-collision population f* of every cell, in
 // two A/B buffers.  One kernel per step
-//   1. pulls, for every non-SOLID cell x and direction q, f*_q(x - e_q) when
-//      that cell is in the domain and not SOLID, else f*_opp(q)(x): exactly
-//      the one value the reference's push delivers into slot q of x;
+//   1. pulls, for every non-SOLID cell x and direction q, what the
+//      reference's push delivers into slot q of x: f*_q(x - e_q) when that
+//      cell is in the domain and not SOLID, plus f*_OPP[q](x) when x's own
+//      direction OPP[q] is blocked (outside the domain or SOLID);
 //   2. for OUTFLOW cells first redirects x to the cell whose post-stream
 //      populations the reference's outflow copies leave there (the chain of
 //      copies is resolved on the host, in the reference's patch order);
@@ -137,11 +138,30 @@ __global__ void __launch_bounds__(256) k_lbm_step(LbmDev L, const typename Store
             const int oi = o / plane, orem = o - oi * plane, oj = orem / nz, ok = orem - oj * nz;
 #pragma unroll
             for (int q = 0; q < 19; q++) {
+                // (a) the neighbour x - e_q streams into slot q
                 const int si = oi - c_ex[q], sj = oj - c_ey[q], sk = ok - c_ez[q];
                 const int s = o - c_ex[q] * plane - c_ey[q] * nz - c_ez[q];
-                const bool in = si >= 0 && si < nx && sj >= 0 && sj < ny && sk >= 0 && sk < nz;
-                if (in && L.ct[s] != CT_SOLID) fq[q] = S::ld(fa + (size_t)q * n + s);
-                else fq[q] = S::ld(fa + (size_t)c_opp[q] * n + o);
+                const bool ina = si >= 0 && si < nx && sj >= 0 && sj < ny && sk >= 0 && sk < nz && L.ct[s] != CT_SOLID;
+                // (b) x's own direction OPP[q] is blocked and reflects into slot q.
+                // OPP of LBMSolver.cpp:27 pairs the diagonals as mirror images
+                // (7 <-> 8 is (1,1,0) <-> (-1,1,0)), so (a) and (b) are
+                // independent and a slot gets 0, 1 or 2 values.
+                const int qq = c_opp[q];
+                const int ti = oi + c_ex[qq], tj = oj + c_ey[qq], tk = ok + c_ez[qq];
+                const int tcell = o + c_ex[qq] * plane + c_ey[qq] * nz + c_ez[qq];
+                const bool inb = !(ti >= 0 && ti < nx && tj >= 0 && tj < ny && tk >= 0 && tk < nz) || L.ct[tcell] == CT_SOLID;
+                if (MODE == 0) {
+                    C v = C(0);
+                    if (ina) v = v + S::ld(fa + (size_t)q * n + s);
+                    if (inb) v = v + S::ld(fa + (size_t)qq * n + o);
+                    fq[q] = v;
+                } else {
+                    // shifted storage g = f - w (w_q == w_OPP[q]): g_post = sum g + (k-1) w_q
+                    C v = C(-lbm_w(q));
+                    if (ina) v += S::ld(fa + (size_t)q * n + s) + C(lbm_w(q));
+                    if (inb) v += S::ld(fa + (size_t)qq * n + o) + C(lbm_w(q));
+                    fq[q] = v;
+                }
             }
         }
         // moments (LBMSolver.cpp:306-318) and next-step collision
