@@ -115,12 +115,12 @@ def load_traffic(kernel: str):
 
 # ------------------------------------------------------------- workloads
 
-def make_workload(name: str, precision: str):
+def make_workload(name: str, precision: str, grid=None):
     from ffrb import workloads
     from ffrb.params import params_from_scene
     from ffrb.scene import build_room
     if name == "large_thermal":
-        cfg, params = workloads.large_thermal()
+        cfg, params = workloads.large_thermal(**({"grid": grid} if grid else {}))
         if precision == "fp64":
             params = params.with_(precision="fp64", poisson="cg")
         return "fluid", cfg, build_room(cfg), params
@@ -128,7 +128,7 @@ def make_workload(name: str, precision: str):
         cfg = workloads.basic_room()
         return "fluid", cfg, build_room(cfg), params_from_scene(cfg)
     if name == "lbm_room":
-        cfg, tau, dt = workloads.lbm_room()
+        cfg, tau, dt = workloads.lbm_room(**({"grid": grid} if grid else {}))
         return "lbm", cfg, build_room(cfg), {"tau": tau, "dt": dt, "storage": "fp64" if precision == "fp64"
                                             else ("fp16" if precision == "fp16" else "fp32")}
     raise SystemExit(f"unknown workload {name}")
@@ -139,7 +139,7 @@ def make_workload(name: str, precision: str):
 def run_ours(args, rank: int, world: int, dist):
     import torch
     from ffrb import capi
-    kind, cfg, room, params = make_workload(args.workload, args.precision)
+    kind, cfg, room, params = make_workload(args.workload, args.precision, args.grid)
     dev = torch.cuda.current_device()
     cells = room.n_cells
     if kind == "fluid":
@@ -272,7 +272,7 @@ def reference_arm(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    kind, cfg, room, params = make_workload(args.workload, args.precision)
+    kind, cfg, room, params = make_workload(args.workload, args.precision, args.grid)
     import oracle as orc
     if not orc.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}))
@@ -316,6 +316,8 @@ def main():
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--ref-cg-iters", type=float, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=lambda s: tuple(int(x) for x in s.split(",")), default=None,
+                    help="override the grid (profiling runs on a smaller case)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
@@ -335,7 +337,7 @@ def main():
         torch.cuda.set_device(0)
     res = run_ours(args, rank, world, dist)
     if rank == 0:
-        kind, cfg, room, params = make_workload(args.workload, args.precision)
+        kind, cfg, room, params = make_workload(args.workload, args.precision, args.grid)
         cb = None
         if not args.no_cpu_baseline:
             gi = res["extra"].get("cg_iterations_mean")

@@ -1,0 +1,650 @@
+// mgpcg.cu — mixed-precision multigrid-preconditioned CG (sm_100a).
+//
+// The pressure system of PoissonSolver::solve (PoissonSolver.cpp:22-91,
+// 93-158) restricted to its FLUID/INFLOW rows is closed: those rows see
+// OUTFLOW neighbours only as Dirichlet ghosts (diag += 2s).  Scaled by the
+// cell volume V = dx*dy*dz it is symmetric positive definite, also on
+// stretched grids (V*s across a face is area/distance).  So:
+//   1. FP64 preconditioned CG on M = V*A_ff with right-hand side V*b,
+//      stopping on the reference's measure ||b - A x||_2 / ||b||_2 (all
+//      non-SOLID rows; the OUTFLOW rows are satisfied exactly by step 2);
+//   2. the OUTFLOW unknowns by one back-substitution of their own rows,
+//      x_o = (b_o + sum_fluid s x_nb) / diag_o;
+//   3. preconditioner: one V-cycle in FP32 on 2x2x2 cell aggregates.  Coarse
+//      face coefficients are half the sum of the fine ones across the coarse
+//      face (the rediscretised volume-scaled Laplacian), restriction sums the
+//      children's residuals, prolongation injects.  Smoothing is red-black
+//      Gauss-Seidel: red then black before the coarse correction, black then
+//      red after it, so the V-cycle is a symmetric operator and CG applies.
+// The whole solve is one cooperative launch; levels larger than
+// kBlockLevelCells are swept by the whole grid between grid barriers, the
+// remaining small levels by block 0 alone.
+#include "mgpcg.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace ffr {
+
+// ---------------------------------------------------------------- host
+
+void build_mg_levels(const HostRoom &r, MGHost &out)
+{
+    out.nx.clear(); out.ny.clear(); out.nz.clear(); out.coef.clear();
+    int nx = r.g.nx, ny = r.g.ny, nz = r.g.nz;
+    out.nx.push_back(nx); out.ny.push_back(ny); out.nz.push_back(nz);
+    out.coef.emplace_back();
+    // fine faces in FP64: T to the + neighbour (0 unless both active) and
+    // the Dirichlet part of the diagonal
+    const size_t n0 = (size_t)nx * ny * nz;
+    std::vector<double> tx(n0, 0.0), ty(n0, 0.0), tz(n0, 0.0), dir(n0, 0.0);
+    std::vector<uint8_t> act(n0, 0);
+    auto C0 = [&](int i, int j, int k) { return ((size_t)i * ny + j) * nz + k; };
+    auto isact = [](uint8_t t) { return t == CT_FLUID || t == CT_INFLOW; };
+    for (size_t c = 0; c < n0; c++) act[c] = isact(r.ct[c]);
+    auto hc = [](const std::vector<double> &h, int a, int b) { return 0.5 * (h[a] + h[b]); };
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                const size_t c = C0(i, j, k);
+                if (!act[c]) continue;
+                const double ax = r.dyv[j] * r.dzv[k], ay = r.dxv[i] * r.dzv[k], az = r.dxv[i] * r.dyv[j];
+                // + neighbours
+                if (i + 1 < nx) {
+                    const double t = ax / hc(r.dxv, i, i + 1);
+                    const uint8_t nt = r.ct[C0(i + 1, j, k)];
+                    if (isact(nt)) tx[c] = t; else if (nt == CT_OUTFLOW) dir[c] += 2 * t;
+                }
+                if (j + 1 < ny) {
+                    const double t = ay / hc(r.dyv, j, j + 1);
+                    const uint8_t nt = r.ct[C0(i, j + 1, k)];
+                    if (isact(nt)) ty[c] = t; else if (nt == CT_OUTFLOW) dir[c] += 2 * t;
+                }
+                if (k + 1 < nz) {
+                    const double t = az / hc(r.dzv, k, k + 1);
+                    const uint8_t nt = r.ct[C0(i, j, k + 1)];
+                    if (isact(nt)) tz[c] = t; else if (nt == CT_OUTFLOW) dir[c] += 2 * t;
+                }
+                // - neighbours that are Dirichlet ghosts
+                if (i > 0 && r.ct[C0(i - 1, j, k)] == CT_OUTFLOW) dir[c] += 2 * ax / hc(r.dxv, i - 1, i);
+                if (j > 0 && r.ct[C0(i, j - 1, k)] == CT_OUTFLOW) dir[c] += 2 * ay / hc(r.dyv, j - 1, j);
+                if (k > 0 && r.ct[C0(i, j, k - 1)] == CT_OUTFLOW) dir[c] += 2 * az / hc(r.dzv, k - 1, k);
+            }
+    while ((size_t)nx * ny * nz > 512 && (int)out.nx.size() < kMaxLevels) {
+        const int mx = (nx + 1) / 2, my = (ny + 1) / 2, mz = (nz + 1) / 2;
+        const size_t m = (size_t)mx * my * mz;
+        std::vector<double> cx(m, 0.0), cy(m, 0.0), cz(m, 0.0), cd(m, 0.0);
+        std::vector<uint8_t> ca(m, 0);
+        auto CC = [&](int i, int j, int k) { return ((size_t)i * my + j) * mz + k; };
+        for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++)
+                for (int k = 0; k < nz; k++) {
+                    const size_t c = ((size_t)i * ny + j) * nz + k;
+                    if (!act[c]) continue;
+                    const size_t P = CC(i / 2, j / 2, k / 2);
+                    ca[P] = 1;
+                    cd[P] += dir[c];
+                    if (tx[c] > 0 && (i + 1) / 2 != i / 2) cx[P] += tx[c];
+                    if (ty[c] > 0 && (j + 1) / 2 != j / 2) cy[P] += ty[c];
+                    if (tz[c] > 0 && (k + 1) / 2 != k / 2) cz[P] += tz[c];
+                }
+        for (size_t P = 0; P < m; P++) { cx[P] *= 0.5; cy[P] *= 0.5; cz[P] *= 0.5; cd[P] *= 0.5; }
+        std::vector<float4> coef(m);
+        for (int i = 0; i < mx; i++)
+            for (int j = 0; j < my; j++)
+                for (int k = 0; k < mz; k++) {
+                    const size_t P = CC(i, j, k);
+                    double D = 0.0;
+                    if (ca[P]) {
+                        D = cx[P] + cy[P] + cz[P] + cd[P];
+                        if (i > 0) D += cx[CC(i - 1, j, k)];
+                        if (j > 0) D += cy[CC(i, j - 1, k)];
+                        if (k > 0) D += cz[CC(i, j, k - 1)];
+                        if (!(D > 0)) D = 1.0;
+                    }
+                    coef[P] = make_float4((float)cx[P], (float)cy[P], (float)cz[P], (float)D);
+                }
+        out.nx.push_back(mx); out.ny.push_back(my); out.nz.push_back(mz);
+        out.coef.push_back(std::move(coef));
+        nx = mx; ny = my; nz = mz;
+        tx.swap(cx); ty.swap(cy); tz.swap(cz); dir.swap(cd); act.swap(ca);
+    }
+}
+
+// -------------------------------------------------------------- device
+
+__device__ __forceinline__ bool active_ct(uint8_t t) { return t == CT_FLUID || t == CT_INFLOW; }
+
+// Grid barrier without a reduction (same protocol as grid_allreduce).
+__device__ bool grid_barrier(GridSync *gs)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned g = ld_acquire(&gs->gen);
+        const unsigned arrived = atomicAdd(&gs->count, 1u);
+        s_ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(&gs->count, 0u);
+            __threadfence();
+            atomicAdd(&gs->gen, 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            while (ld_acquire(&gs->gen) == g) {
+                __nanosleep(32);
+                if (global_ns() - t0 > kBarrierTimeoutNs || *(volatile int *)&gs->err) {
+                    atomicExch(&gs->err, 1);
+                    s_ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return s_ok;
+}
+
+// Level-0 (fine) FP32 coefficients of cell (i,j,k) from its stencil code:
+// t[6] in the order x-, x+, y-, y+, z-, z+ (0 unless the neighbour is an
+// unknown) and the diagonal (Dirichlet ghosts count twice).
+__device__ __forceinline__ void fine_coefs(const MGDev &M, unsigned code, int i, int j, int k, float (&t)[6],
+                                           float &D)
+{
+    const float dx = M.dx[i], dy = M.dy[j], dz = M.dz[k];
+    const float tt[6] = {dy * dz * M.ixl[i], dy * dz * M.ixr[i], dx * dz * M.iyl[j],
+                         dx * dz * M.iyr[j], dx * dy * M.izl[k], dx * dy * M.izr[k]};
+    D = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+        const unsigned cls = (code >> (2 * a)) & 3u;
+        t[a] = cls == SC_IN ? tt[a] : 0.0f;
+        D += cls == SC_IN ? tt[a] : (cls == SC_DIR ? 2.0f * tt[a] : 0.0f);
+    }
+    if (!(D > 0.0f)) D = dx * dy * dz;
+}
+
+// sum_nb T_nb * (x_nb [+ e_parent(nb)]) and the diagonal of cell c on
+// level L (L >= 1: explicit coefficients).
+template <bool CORR>
+__device__ __forceinline__ float coarse_nbsum(const MGLevel &L, const MGLevel &Lc, int c, int i, int j, int k,
+                                              float &D)
+{
+    const int plane = L.ny * L.nz;
+    const float4 cf = L.coef[c];
+    D = cf.w;
+    float s = 0.0f;
+    auto val = [&](int cn, int ii, int jj, int kk) -> float {
+        float v = L.x[cn];
+        if (CORR) v += Lc.x[((ii >> 1) * Lc.ny + (jj >> 1)) * Lc.nz + (kk >> 1)];
+        return v;
+    };
+    if (i > 0) { const float t = L.coef[c - plane].x; if (t != 0.0f) s += t * val(c - plane, i - 1, j, k); }
+    if (i < L.nx - 1 && cf.x != 0.0f) s += cf.x * val(c + plane, i + 1, j, k);
+    if (j > 0) { const float t = L.coef[c - L.nz].y; if (t != 0.0f) s += t * val(c - L.nz, i, j - 1, k); }
+    if (j < L.ny - 1 && cf.y != 0.0f) s += cf.y * val(c + L.nz, i, j + 1, k);
+    if (k > 0) { const float t = L.coef[c - 1].z; if (t != 0.0f) s += t * val(c - 1, i, j, k - 1); }
+    if (k < L.nz - 1 && cf.z != 0.0f) s += cf.z * val(c + 1, i, j, k + 1);
+    return s;
+}
+
+template <bool CORR>
+__device__ __forceinline__ float fine_nbsum(const RoomDev &R, const MGDev &M, const MGLevel &L0, const MGLevel &L1,
+                                            int c, int i, int j, int k, float &D)
+{
+    float t[6];
+    fine_coefs(M, R.sc[c], i, j, k, t, D);
+    const int plane = R.ny * R.nz, nz = R.nz;
+    const int off[6] = {-plane, plane, -nz, nz, -1, 1};
+    const int di[6] = {-1, 1, 0, 0, 0, 0}, dj[6] = {0, 0, -1, 1, 0, 0}, dk[6] = {0, 0, 0, 0, -1, 1};
+    float s = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+        if (t[a] == 0.0f) continue;
+        float v = L0.x[c + off[a]];
+        if (CORR) v += L1.x[(((i + di[a]) >> 1) * L1.ny + ((j + dj[a]) >> 1)) * L1.nz + ((k + dk[a]) >> 1)];
+        s += t[a] * v;
+    }
+    return s;
+}
+
+__device__ __forceinline__ void decode(int c, int ny, int nz, int &i, int &j, int &k)
+{
+    const int plane = ny * nz;
+    i = c / plane;
+    const int rem = c - i * plane;
+    j = rem / nz;
+    k = rem - j * nz;
+}
+
+// One Gauss-Seidel half sweep on `color` of level l.  CORR adds the coarse
+// correction of level l+1 to the neighbour values (the post-smoothing pass
+// right after prolongation).
+template <bool CORR>
+__device__ void smooth_color(const PCGArgs &A, int l, int color, int start, int stride)
+{
+    const MGDev &M = A.M;
+    const MGLevel &L = M.lv[l];
+    const MGLevel &Lc = M.lv[l + 1 < M.nlev ? l + 1 : l];
+    for (int c = start; c < L.n; c += stride) {
+        int i, j, k;
+        decode(c, L.ny, L.nz, i, j, k);
+        if (((i + j + k) & 1) != color) continue;
+        float D, s;
+        if (l == 0) {
+            if (!active_ct(A.R.ct[c])) continue;
+            s = fine_nbsum<CORR>(A.R, M, L, Lc, c, i, j, k, D);
+        } else {
+            if (L.coef[c].w == 0.0f) continue;
+            s = coarse_nbsum<CORR>(L, Lc, c, i, j, k, D);
+        }
+        L.x[c] = (L.b[c] + s) / D;
+    }
+}
+
+// Residual of the red cells of level l (the black ones are exact after a
+// black sweep), summed into the parent rhs on level l+1, and the red-only
+// first sweep of level l+1 from a zero guess.
+__device__ void restrict_level(const PCGArgs &A, int l, int start, int stride)
+{
+    const MGDev &M = A.M;
+    const MGLevel &L = M.lv[l];
+    const MGLevel &C = M.lv[l + 1];
+    for (int P = start; P < C.n; P += stride) {
+        int I, J, K;
+        decode(P, C.ny, C.nz, I, J, K);
+        float sum = 0.0f;
+        for (int a = 0; a < 2; a++) {
+            const int i = 2 * I + a;
+            if (i >= L.nx) break;
+            for (int b = 0; b < 2; b++) {
+                const int j = 2 * J + b;
+                if (j >= L.ny) break;
+                for (int e = 0; e < 2; e++) {
+                    const int k = 2 * K + e;
+                    if (k >= L.nz) break;
+                    if (((i + j + k) & 1) != 0) continue;
+                    const int c = (i * L.ny + j) * L.nz + k;
+                    float D, s;
+                    if (l == 0) {
+                        if (!active_ct(A.R.ct[c])) continue;
+                        s = fine_nbsum<false>(A.R, M, L, L, c, i, j, k, D);
+                    } else {
+                        if (L.coef[c].w == 0.0f) continue;
+                        s = coarse_nbsum<false>(L, L, c, i, j, k, D);
+                    }
+                    sum += L.b[c] - (D * L.x[c] - s);
+                }
+            }
+        }
+        C.b[P] = sum;
+        const float D = C.coef[P].w;
+        C.x[P] = (((I + J + K) & 1) == 0 && D != 0.0f) ? sum / D : 0.0f;
+    }
+}
+
+// Levels lo .. nlev-1 inside block 0 (__syncthreads only).
+__device__ void block_vcycle(const PCGArgs &A, int lo)
+{
+    const MGDev &M = A.M;
+    const int t = threadIdx.x, nt = blockDim.x;
+    for (int l = lo; l < M.nlev - 1; l++) {
+        smooth_color<false>(A, l, 1, t, nt);
+        __syncthreads();
+        restrict_level(A, l, t, nt);
+        __syncthreads();
+    }
+    const int last = M.nlev - 1;
+    for (int sweep = 0; sweep < 8; sweep++) {
+        smooth_color<false>(A, last, 1, t, nt);
+        __syncthreads();
+        smooth_color<false>(A, last, 0, t, nt);
+        __syncthreads();
+    }
+    for (int l = M.nlev - 2; l >= lo; l--) {
+        smooth_color<true>(A, l, 1, t, nt);
+        __syncthreads();
+        smooth_color<false>(A, l, 0, t, nt);
+        __syncthreads();
+    }
+}
+
+// The reference's FP64 operator row (PoissonSolver.cpp:22-91) of cell c
+// applied to a direction given by dir(offset).
+template <class F>
+__device__ __forceinline__ double ref_row(const RoomDev &R, unsigned code, int i, int j, int k, double xc, F dir)
+{
+    const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
+    const double *sxl = R.scale, *sxr = sxl + nx, *syl = sxr + nx, *syr = syl + ny, *szl = syr + ny,
+                 *szr = szl + nz;
+    const double s[6] = {sxl[i], sxr[i], syl[j], syr[j], szl[k], szr[k]};
+    const int off[6] = {-plane, plane, -nz, nz, -1, 1};
+    double diag = 0.0, o = 0.0;
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+        const unsigned cls = (code >> (2 * a)) & 3u;
+        if (cls == SC_IN) {
+            diag += s[a];
+            o += s[a] * dir(off[a]);
+        } else if (cls == SC_DIR) {
+            diag += 2.0 * s[a];
+        }
+    }
+    if (diag < 1e-30) diag = 1.0;
+    return diag * xc - o;
+}
+
+__device__ __forceinline__ double face_rhs(const PCGArgs &A, int c, int i, int j, int k)
+{
+    const RoomDev &R = A.R;
+    if (!A.from_faces) return A.rhs[c];
+    const int ny = R.ny, nz = R.nz;
+    const int u0 = c, u1 = c + ny * nz;
+    const int v0 = (i * (ny + 1) + j) * nz + k, w0 = (i * ny + j) * (nz + 1) + k;
+    const double div = (A.us[u1] - A.us[u0]) / R.dxv[i] + (A.vs[v0 + nz] - A.vs[v0]) / R.dyv[j]
+                     + (A.ws[w0 + 1] - A.ws[w0]) / R.dzv[k];
+    return A.rhs_factor * div;
+}
+
+__global__ void __launch_bounds__(256) k_pcg(PCGArgs A)
+{
+    __shared__ double sh[32];
+    if (A.st && A.st->halt) return;
+    const RoomDev &R = A.R;
+    const MGDev &M = A.M;
+    const int n = R.n, ny = R.ny, nz = R.nz;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    float *z = M.lv[0].x;
+    double *x = A.x, *r = A.r, *q = A.q;
+    int flags = 0, iters = 0;
+    double res = 0.0;
+
+    // phase 0: rhs, r = V*rhs on the unknowns, x = 0, z = red sweep from 0
+    {
+        double acc[2] = {0.0, 0.0};
+        for (int c = t0; c < n; c += nth) {
+            int i, j, k;
+            decode(c, ny, nz, i, j, k);
+            const uint8_t t = R.ct[c];
+            x[c] = 0.0;
+            A.da[c] = 0.0;
+            double rv = 0.0;
+            float zv = 0.0f;
+            if (t != CT_SOLID) {
+                const double b = face_rhs(A, c, i, j, k);
+                acc[0] += b * b;
+                if (active_ct(t)) {
+                    acc[1] += b * b;
+                    rv = b * (M.vol_x[i] * M.vol_y[j] * M.vol_z[k]);
+                    if (((i + j + k) & 1) == 0) {
+                        float tt[6], D;
+                        fine_coefs(M, R.sc[c], i, j, k, tt, D);
+                        zv = (float)rv / D;
+                    }
+                }
+            }
+            r[c] = rv;
+            M.r32[c] = (float)rv;
+            z[c] = zv;
+        }
+        const bool ok = grid_allreduce<2>(A.gs, A.partials, A.sc->red, acc, sh);
+        if (!ok) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+        const double bnorm = sqrt(acc[0]);
+        if (bnorm < 1e-15) goto finish;
+
+        double *dold = A.da, *dnew = A.db;
+        double rz_old = 0.0, alpha = 0.0, alpha_prev = 0.0;
+        bool pending = false, converged = false;
+        for (int it = 0;; it++) {
+            // ---- preconditioner: V-cycle from the red sweep already in z
+            for (int l = 0; l < M.nlev_grid && l < M.nlev - 1; l++) {
+                smooth_color<false>(A, l, 1, t0, nth);
+                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                restrict_level(A, l, t0, nth);
+                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            }
+            if (M.nlev_grid < M.nlev) {
+                if (blockIdx.x == 0) block_vcycle(A, M.nlev_grid);
+                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            }
+            for (int l = min(M.nlev_grid, M.nlev - 1) - 1; l >= 1; l--) {
+                smooth_color<true>(A, l, 1, t0, nth);
+                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                smooth_color<false>(A, l, 0, t0, nth);
+                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            }
+            if (M.nlev_grid >= 1 && M.nlev > 1) {
+                smooth_color<true>(A, 0, 1, t0, nth);
+                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            }
+            // final red sweep of level 0 fused with r.z
+            double acc1[1] = {0.0};
+            if (M.nlev_grid >= 1) {
+                const MGLevel &L0 = M.lv[0];
+                for (int c = t0; c < n; c += nth) {
+                    if (!active_ct(R.ct[c])) continue;
+                    int i, j, k;
+                    decode(c, ny, nz, i, j, k);
+                    float zc;
+                    if (((i + j + k) & 1) == 0) {
+                        float D;
+                        const float s = fine_nbsum<false>(R, M, L0, L0, c, i, j, k, D);
+                        zc = (M.r32[c] + s) / D;
+                        z[c] = zc;
+                    } else {
+                        zc = z[c];
+                    }
+                    acc1[0] += r[c] * (double)zc;
+                }
+            } else {
+                for (int c = t0; c < n; c += nth)
+                    if (active_ct(R.ct[c])) acc1[0] += r[c] * (double)z[c];
+            }
+            if (!grid_allreduce<1>(A.gs, A.partials, A.sc->red, acc1, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            const double rz = acc1[0];
+            const double beta = it == 0 ? 0.0 : rz / rz_old;
+            rz_old = rz;
+
+            // ---- phase A: d = z + beta d_old, deferred x update, q = M d
+            double acc2[1] = {0.0};
+            for (int c = t0; c < n; c += nth) {
+                const uint8_t t = R.ct[c];
+                if (!active_ct(t)) { dnew[c] = 0.0; q[c] = 0.0; continue; }
+                int i, j, k;
+                decode(c, ny, nz, i, j, k);
+                const double dp = dold[c];
+                const double dc = fma(beta, dp, (double)z[c]);
+                if (it > 0) x[c] = fma(alpha_prev, dp, x[c]);
+                dnew[c] = dc;
+                const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
+                const double row = ref_row(R, R.sc[c], i, j, k, dc,
+                                           [&](int o) { return fma(beta, dold[c + o], (double)z[c + o]); });
+                const double qc = vol * row;
+                q[c] = qc;
+                acc2[0] += dc * qc;
+            }
+            if (!grid_allreduce<1>(A.gs, A.partials, A.sc->red, acc2, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            { double *tmp = dold; dold = dnew; dnew = tmp; }   // dold = current direction
+            pending = false;
+            const double dq = acc2[0];
+            if (fabs(dq) < 1e-30) {
+                flags |= FFR_FLAG_CG_BREAKDOWN;
+                iters = it;
+                break;
+            }
+            alpha = rz / dq;
+
+            // ---- phase B: r -= alpha q, ||b - A x||^2, red sweep of the next z
+            double acc3[1] = {0.0};
+            for (int c = t0; c < n; c += nth) {
+                const uint8_t t = R.ct[c];
+                if (!active_ct(t)) continue;
+                int i, j, k;
+                decode(c, ny, nz, i, j, k);
+                const double rv = r[c] - alpha * q[c];
+                r[c] = rv;
+                const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
+                const double ru = rv / vol;
+                acc3[0] += ru * ru;
+                const float r32 = (float)rv;
+                M.r32[c] = r32;
+                float zv = 0.0f;
+                if (((i + j + k) & 1) == 0) {
+                    float tt[6], D;
+                    fine_coefs(M, R.sc[c], i, j, k, tt, D);
+                    zv = r32 / D;
+                }
+                z[c] = zv;
+            }
+            if (!grid_allreduce<1>(A.gs, A.partials, A.sc->red, acc3, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            pending = true;
+            res = sqrt(acc3[0]) / bnorm;
+            iters = it + 1;
+            if (res < A.tol) { converged = true; break; }
+            if (iters >= A.max_iter) { flags |= FFR_FLAG_CG_MAXITER; break; }
+            alpha_prev = alpha;
+        }
+        (void)converged;
+        if (pending)
+            for (int c = t0; c < n; c += nth)
+                if (active_ct(R.ct[c])) x[c] = fma(alpha, dold[c], x[c]);
+        if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+        // OUTFLOW rows by back-substitution in the reference's own row form
+        for (int c = t0; c < n; c += nth) {
+            if (R.ct[c] != CT_OUTFLOW) continue;
+            int i, j, k;
+            decode(c, ny, nz, i, j, k);
+            const double b = face_rhs(A, c, i, j, k);
+            const double nx_ = R.nx;
+            (void)nx_;
+            // row: diag*x_o - sum_in s*x_nb = b  ->  x_o = (b + sum) / diag
+            const double row0 = ref_row(R, R.sc[c], i, j, k, 0.0, [&](int o) { return x[c + o]; });
+            // ref_row(.., xc = 0) = -sum s*x_nb; the diagonal is ref_row at unit xc with zero neighbours
+            const double diag = ref_row(R, R.sc[c], i, j, k, 1.0, [&](int) { return 0.0; });
+            x[c] = (b - row0) / diag;
+        }
+    }
+finish:
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (A.out_res) *A.out_res = res;
+        if (A.out_iters) *A.out_iters = iters;
+        if (A.out_flags) *A.out_flags = flags;
+        if (A.st) {
+            A.st->pres = res;
+            A.st->iters = iters;
+            atomicOr(&A.st->flags, flags);
+        }
+    }
+}
+
+}  // namespace ffr
+
+// ---------------------------------------------------------------- host
+
+namespace ffr {
+
+size_t mg_bytes(const HostRoom &r, const MGHost &h)
+{
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const RoomGeom &g = r.g;
+    size_t b = 2 * al(4 * g.n) + 6 * al(4 * (g.nx + g.ny + g.nz));
+    for (size_t l = 1; l < h.nx.size(); l++) {
+        const size_t m = (size_t)h.nx[l] * h.ny[l] * h.nz[l];
+        b += al(16 * m) + 2 * al(4 * m);
+    }
+    return b + 256;
+}
+
+int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGDev &M)
+{
+    const RoomGeom &g = r.g;
+    M.nlev = (int)h.nx.size();
+    M.nlev_grid = 0;
+    for (int l = 0; l < M.nlev; l++)
+        if ((long long)h.nx[l] * h.ny[l] * h.nz[l] > kBlockLevelCells) M.nlev_grid = l + 1;
+    // fine-level factors in FP32 (PoissonSolver.cpp:33-49 centre distances)
+    auto axis = [](const std::vector<double> &hh, std::vector<float> &d, std::vector<float> &il,
+                   std::vector<float> &ir) {
+        const int m = (int)hh.size();
+        d.resize(m); il.resize(m); ir.resize(m);
+        for (int i = 0; i < m; i++) {
+            d[i] = (float)hh[i];
+            const double hl = (i > 0) ? 0.5 * (hh[i - 1] + hh[i]) : hh[i];
+            const double hr = (i < m - 1) ? 0.5 * (hh[i] + hh[i + 1]) : hh[i];
+            il[i] = (float)(1.0 / hl);
+            ir[i] = (float)(1.0 / hr);
+        }
+    };
+    std::vector<float> dx, ixl, ixr, dy, iyl, iyr, dz, izl, izr;
+    axis(r.dxv, dx, ixl, ixr);
+    axis(r.dyv, dy, iyl, iyr);
+    axis(r.dzv, dz, izl, izr);
+    float *fx = ar.take<float>(g.nx), *fxl = ar.take<float>(g.nx), *fxr = ar.take<float>(g.nx);
+    float *fy = ar.take<float>(g.ny), *fyl = ar.take<float>(g.ny), *fyr = ar.take<float>(g.ny);
+    float *fz = ar.take<float>(g.nz), *fzl = ar.take<float>(g.nz), *fzr = ar.take<float>(g.nz);
+    // (6 arrays were budgeted per axis set; dx/dy/dz reuse the same slots)
+    M.lv[0].nx = g.nx; M.lv[0].ny = g.ny; M.lv[0].nz = g.nz; M.lv[0].n = (int)g.n;
+    M.lv[0].coef = nullptr;
+    M.lv[0].x = ar.take<float>(g.n);
+    M.r32 = ar.take<float>(g.n);
+    M.lv[0].b = M.r32;
+    if (!M.r32 || !fzr) return fail(FFR_ENOMEM, "arena exhausted (multigrid)");
+    FFR_CUDA(cudaMemcpyAsync(fx, dx.data(), 4 * g.nx, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(fxl, ixl.data(), 4 * g.nx, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(fxr, ixr.data(), 4 * g.nx, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(fy, dy.data(), 4 * g.ny, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(fyl, iyl.data(), 4 * g.ny, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(fyr, iyr.data(), 4 * g.ny, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(fz, dz.data(), 4 * g.nz, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(fzl, izl.data(), 4 * g.nz, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemcpyAsync(fzr, izr.data(), 4 * g.nz, cudaMemcpyHostToDevice, s));
+    FFR_CUDA(cudaMemsetAsync(M.lv[0].x, 0, 4 * g.n, s));
+    FFR_CUDA(cudaMemsetAsync(M.r32, 0, 4 * g.n, s));
+    M.dx = fx; M.dy = fy; M.dz = fz;
+    M.ixl = fxl; M.ixr = fxr; M.iyl = fyl; M.iyr = fyr; M.izl = fzl; M.izr = fzr;
+    for (int l = 1; l < M.nlev; l++) {
+        const size_t m = (size_t)h.nx[l] * h.ny[l] * h.nz[l];
+        MGLevel &L = M.lv[l];
+        L.nx = h.nx[l]; L.ny = h.ny[l]; L.nz = h.nz[l]; L.n = (int)m;
+        float4 *cf = ar.take<float4>(m);
+        L.x = ar.take<float>(m);
+        L.b = ar.take<float>(m);
+        if (!L.b) return fail(FFR_ENOMEM, "arena exhausted (multigrid levels)");
+        FFR_CUDA(cudaMemcpyAsync(cf, h.coef[l].data(), 16 * m, cudaMemcpyHostToDevice, s));
+        FFR_CUDA(cudaMemsetAsync(L.x, 0, 4 * m, s));
+        FFR_CUDA(cudaMemsetAsync(L.b, 0, 4 * m, s));
+        L.coef = cf;
+    }
+    FFR_CUDA(cudaStreamSynchronize(s));   // the host vectors die at return
+    return FFR_OK;
+}
+
+unsigned pcg_max_blocks()
+{
+    static unsigned cap = 0;
+    if (!cap) {
+        int per_sm = 0, dev = 0, sms = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, 256, 0);
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (per_sm <= 0) per_sm = 1;
+        if (sms <= 0) sms = 148;
+        cap = (unsigned)(per_sm * sms);
+    }
+    return cap;
+}
+
+int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used)
+{
+    const unsigned want = (unsigned)std::max<long long>(1, (a.R.n + 255) / 256);
+    const unsigned blocks = std::max(1u, std::min(pcg_max_blocks(), want));
+    if (blocks_used) *blocks_used = blocks;
+    FFR_CUDA(cudaMemsetAsync(a.gs, 0, sizeof(GridSync), s));
+    void *args[] = {(void *)&a};
+    FFR_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg, dim3(blocks), dim3(256), args, 0, s));
+    count_launch(1);
+    return FFR_OK;
+}
+
+}  // namespace ffr

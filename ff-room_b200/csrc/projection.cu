@@ -12,6 +12,7 @@
 // All kernels return at once when the room's halt flag is set, so a run of
 // queued steps can stop on convergence without a host round trip.
 #include "projection.cuh"
+#include "mgpcg.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -27,34 +28,56 @@ namespace ffr {
 // ------------------------------------------------- advection formulas
 
 // upwind1, FluidSolver.cpp:47-50.
-__device__ __forceinline__ double adv_up(double pm, double pc, double pp, double a, double h)
+template <class F>
+__device__ __forceinline__ F adv_up(F pm, F pc, F pp, F a, F h)
 {
-    return (a > 0.0) ? a * (pc - pm) / h : a * (pp - pc) / h;
+    return (a > F(0)) ? a * (pc - pm) / h : a * (pp - pc) / h;
 }
 
 // quick_adv, FluidSolver.cpp:56-72 (phi_mm on the negative branch, >= 0).
-__device__ __forceinline__ double adv_quick(double pmm, double pm, double pc, double pp, double a,
-                                            double h)
+template <class F>
+__device__ __forceinline__ F adv_quick(F pmm, F pm, F pc, F pp, F a, F h)
 {
-    double fr, fl;
-    if (a >= 0.0) {
-        fr = (6.0 * pc + 3.0 * pp - pm) / 8.0;
-        fl = (6.0 * pm + 3.0 * pc - pmm) / 8.0;
+    F fr, fl;
+    if (a >= F(0)) {
+        fr = (F(6) * pc + F(3) * pp - pm) / F(8);
+        fl = (F(6) * pm + F(3) * pc - pmm) / F(8);
     } else {
-        fr = (6.0 * pp + 3.0 * pc - pmm) / 8.0;
-        fl = (6.0 * pc + 3.0 * pp - pm) / 8.0;
+        fr = (F(6) * pp + F(3) * pc - pmm) / F(8);
+        fl = (F(6) * pc + F(3) * pp - pm) / F(8);
     }
     return a * (fr - fl) / h;
 }
 
 // lax_wendroff_adv, FluidSolver.cpp:75-81.
-__device__ __forceinline__ double adv_lw(double pm, double pc, double pp, double a, double dt,
-                                         double h)
+template <class F>
+__device__ __forceinline__ F adv_lw(F pm, F pc, F pp, F a, F dt, F h)
 {
-    const double cr = a * dt / h;
-    const double flr = a * (0.5 * (pc + pp) - 0.5 * cr * (pp - pc));
-    const double fll = a * (0.5 * (pm + pc) - 0.5 * cr * (pc - pm));
+    const F cr = a * dt / h;
+    const F flr = a * (F(0.5) * (pc + pp) - F(0.5) * cr * (pp - pc));
+    const F fll = a * (F(0.5) * (pm + pc) - F(0.5) * cr * (pc - pm));
     return (flr - fll) / h;
+}
+
+// The predicted increment dt*(-adv + dif) of one face from its stencil
+// values (FluidSolver.cpp:132-162), in arithmetic F.  ax is the advecting
+// velocity along x for this face, etc.; scheme 1 = QUICK (the caller has
+// checked its activation range and passes the far neighbours), 2 = LW.
+template <class F>
+__device__ __forceinline__ F face_increment(int use_quick, int lw, F c, F xmm, F xm, F xp, F ymm, F ym, F yp,
+                                            F zmm, F zm, F zp, F ax, F ay, F az, F hx, F hy, F hz, F nu, F dt)
+{
+    F adv;
+    if (use_quick) {
+        adv = adv_quick(xmm, xm, c, xp, ax, hx) + adv_quick(ymm, ym, c, yp, ay, hy) + adv_quick(zmm, zm, c, zp, az, hz);
+    } else if (lw) {
+        adv = adv_lw(xm, c, xp, ax, dt, hx) + adv_lw(ym, c, yp, ay, dt, hy) + adv_lw(zm, c, zp, az, dt, hz);
+    } else {
+        adv = adv_up(xm, c, xp, ax, hx) + adv_up(ym, c, yp, ay, hy) + adv_up(zm, c, zp, az, hz);
+    }
+    const F cx = F(1) / (hx * hx), cy = F(1) / (hy * hy), cz = F(1) / (hz * hz);
+    const F dif = nu * (cx * (xm - F(2) * c + xp) + cy * (ym - F(2) * c + yp) + cz * (zm - F(2) * c + zp));
+    return dt * (-adv + dif);
 }
 
 __device__ __forceinline__ double face_code(uint8_t code, double val, const double *fanvel, int comp)
@@ -76,7 +99,10 @@ struct PredArgs {
 // Predictor for every face of u, v and w (one thread per face, flat over
 // the three arrays): FluidSolver::compute_intermediate (FluidSolver.cpp:
 // 83-309), then apply_buoyancy on interior w faces (FluidSolver.cpp:373-386),
-// then the no-slip / inflow codes (BoundaryManager.cpp:60-130).
+// then the no-slip / inflow codes (BoundaryManager.cpp:60-130).  F is the
+// arithmetic of the increment: double reproduces the reference; float is
+// the mixed-precision mode (FP32 increment added to the FP64 state).
+template <class F>
 __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const double *__restrict__ u,
                                                  const double *__restrict__ v,
                                                  const double *__restrict__ w,
@@ -89,15 +115,13 @@ __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const do
     const int nx = R.nx, ny = R.ny, nz = R.nz;
     const int total = R.nu + R.nv + R.nw;
     const int quick = A.scheme == 1, lw = A.scheme == 2;
-    const double dt = A.dt, nu = A.nu;
+    const F dt = F(A.dt), nu = F(A.nu);
     const double *T = st->tpar ? T1 : T0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         if (t < R.nu) {
             const int i = t / (ny * nz), rem = t - i * ny * nz, j = rem / nz, k = rem - j * nz;
             double val = u[t];
             if (i > 0 && i < nx) {
-                const double hx = R.dxv[i], hy = R.dyv[j], hz = R.dzv[k];
-                const double cx = 1.0 / (hx * hx), cy = 1.0 / (hy * hy), cz = 1.0 / (hz * hz);
                 const double uc = val;
                 const double xm = (i > 1) ? u[t - ny * nz] : 0.0;
                 const double xp = (i < nx - 1) ? u[t + ny * nz] : 0.0;
@@ -107,23 +131,14 @@ __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const do
                 const double aw = (k > 0 && k < nz) ? 0.5 * (w[WIX(i - 1, j, k)] + w[WIX(i, j, k)]) : 0.0;
                 const double zm = (k > 0) ? u[t - 1] : 0.0;
                 const double zp = (k < nz - 1) ? u[t + 1] : 0.0;
-                double adv;
-                if (quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
-                    // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1
-                    // (k=1) they fall into the previous row of the flat array
-                    adv = adv_quick(u[t - 2 * ny * nz], xm, uc, xp, uc, hx)
-                        + adv_quick(u[t - 2 * nz], ym, uc, yp, av, hy)
-                        + adv_quick(u[t - 2], zm, uc, zp, aw, hz);
-                } else if (lw) {
-                    adv = adv_lw(xm, uc, xp, uc, dt, hx) + adv_lw(ym, uc, yp, av, dt, hy)
-                        + adv_lw(zm, uc, zp, aw, dt, hz);
-                } else {
-                    adv = adv_up(xm, uc, xp, uc, hx) + adv_up(ym, uc, yp, av, hy)
-                        + adv_up(zm, uc, zp, aw, hz);
-                }
-                const double dif = nu * (cx * (xm - 2 * uc + xp) + cy * (ym - 2 * uc + yp)
-                                         + cz * (zm - 2 * uc + zp));
-                val = uc + dt * (-adv + dif);
+                const int q = quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+                // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1
+                // (k=1) they fall into the previous row of the flat array
+                const double xmm = q ? u[t - 2 * ny * nz] : 0.0, ymm = q ? u[t - 2 * nz] : 0.0,
+                             zmm = q ? u[t - 2] : 0.0;
+                val = uc + (double)face_increment<F>(q, lw, F(uc), F(xmm), F(xm), F(xp), F(ymm), F(ym), F(yp),
+                                                     F(zmm), F(zm), F(zp), F(uc), F(av), F(aw), F(R.dxv[i]),
+                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
             }
             us[t] = face_code(R.fcu[t], val, R.fanvel, 0);
         } else if (t < R.nu + R.nv) {
@@ -132,8 +147,6 @@ __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const do
                       k = rem - j * nz;
             double val = v[f];
             if (j > 0 && j < ny) {
-                const double hx = R.dxv[i], hy = R.dyv[j], hz = R.dzv[k];
-                const double cx = 1.0 / (hx * hx), cy = 1.0 / (hy * hy), cz = 1.0 / (hz * hz);
                 const double vc = val;
                 const double au = (i > 0) ? 0.5 * (u[UIX(i, j - 1, k)] + u[UIX(i, j, k)]) : 0.0;
                 const double xm = (i > 0) ? v[f - (ny + 1) * nz] : 0.0;
@@ -143,22 +156,13 @@ __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const do
                 const double aw = (k > 0 && k < nz) ? 0.5 * (w[WIX(i, j - 1, k)] + w[WIX(i, j, k)]) : 0.0;
                 const double zm = (k > 0) ? v[f - 1] : 0.0;
                 const double zp = (k < nz - 1) ? v[f + 1] : 0.0;
-                double adv;
-                if (quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
-                    // v's x and z "far" neighbours are the near ones
-                    // (FluidSolver.cpp:208,211)
-                    adv = adv_quick(xm, xm, vc, xp, au, hx) + adv_quick(v[f - 2 * nz], ym, vc, yp, vc, hy)
-                        + adv_quick(zm, zm, vc, zp, aw, hz);
-                } else if (lw) {
-                    adv = adv_lw(xm, vc, xp, au, dt, hx) + adv_lw(ym, vc, yp, vc, dt, hy)
-                        + adv_lw(zm, vc, zp, aw, dt, hz);
-                } else {
-                    adv = adv_up(xm, vc, xp, au, hx) + adv_up(ym, vc, yp, vc, hy)
-                        + adv_up(zm, vc, zp, aw, hz);
-                }
-                const double dif = nu * (cx * (xm - 2 * vc + xp) + cy * (ym - 2 * vc + yp)
-                                         + cz * (zm - 2 * vc + zp));
-                val = vc + dt * (-adv + dif);
+                const int q = quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+                // v's x and z "far" neighbours are the near ones
+                // (FluidSolver.cpp:208,211)
+                const double ymm = q ? v[f - 2 * nz] : 0.0;
+                val = vc + (double)face_increment<F>(q, lw, F(vc), F(xm), F(xm), F(xp), F(ymm), F(ym), F(yp),
+                                                     F(zm), F(zm), F(zp), F(au), F(vc), F(aw), F(R.dxv[i]),
+                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
             }
             vs[f] = face_code(R.fcv[f], val, R.fanvel, 1);
         } else {
@@ -167,8 +171,6 @@ __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const do
                       k = rem - j * (nz + 1);
             double val = w[f];
             if (k > 0 && k < nz) {
-                const double hx = R.dxv[i], hy = R.dyv[j], hz = R.dzv[k];
-                const double cx = 1.0 / (hx * hx), cy = 1.0 / (hy * hy), cz = 1.0 / (hz * hz);
                 const double wc = val;
                 const double au = (i > 0) ? 0.5 * (u[UIX(i, j, k - 1)] + u[UIX(i, j, k)]) : 0.0;
                 const double xm = (i > 0) ? w[f - ny * (nz + 1)] : 0.0;
@@ -178,25 +180,16 @@ __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const do
                 const double yp = (j < ny - 1) ? w[f + (nz + 1)] : 0.0;
                 const double zm = (k > 1) ? w[f - 1] : 0.0;
                 const double zp = (k < nz - 1) ? w[f + 1] : 0.0;
-                double adv;
-                if (quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2) {
-                    // w's x and y "far" neighbours are the near ones
-                    // (FluidSolver.cpp:275-276)
-                    adv = adv_quick(xm, xm, wc, xp, au, hx) + adv_quick(ym, ym, wc, yp, av, hy)
-                        + adv_quick(w[f - 2], zm, wc, zp, wc, hz);
-                } else if (lw) {
-                    adv = adv_lw(xm, wc, xp, au, dt, hx) + adv_lw(ym, wc, yp, av, dt, hy)
-                        + adv_lw(zm, wc, zp, wc, dt, hz);
-                } else {
-                    adv = adv_up(xm, wc, xp, au, hx) + adv_up(ym, wc, yp, av, hy)
-                        + adv_up(zm, wc, zp, wc, hz);
-                }
-                const double dif = nu * (cx * (xm - 2 * wc + xp) + cy * (ym - 2 * wc + yp)
-                                         + cz * (zm - 2 * wc + zp));
-                val = wc + dt * (-adv + dif);
+                const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2;
+                // w's x and y "far" neighbours are the near ones
+                // (FluidSolver.cpp:275-276)
+                const double zmm = q ? w[f - 2] : 0.0;
+                val = wc + (double)face_increment<F>(q, lw, F(wc), F(xm), F(xm), F(xp), F(ym), F(ym), F(yp),
+                                                     F(zmm), F(zm), F(zp), F(au), F(av), F(wc), F(R.dxv[i]),
+                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
                 if (A.buoyancy) {
                     const int c = UIX(i, j, k);
-                    val += A.bcoeff * (0.5 * (T[c - 1] + T[c]) - A.T_ref);
+                    val += (double)(F(A.bcoeff) * (F(0.5) * (F(T[c - 1]) + F(T[c])) - F(A.T_ref)));
                 }
             }
             ws[f] = face_code(R.fcw[f], val, R.fanvel, 2);
@@ -537,7 +530,8 @@ struct ThermArgs {
 
 // FluidSolver::advect_temperature (FluidSolver.cpp:388-456) with the block
 // partial sums of the new T over FLUID cells for compute_T_mean
-// (FluidSolver.cpp:458-468).
+// (FluidSolver.cpp:458-468).  F as for k_predict.
+template <class F>
 __global__ void __launch_bounds__(256) k_advect_T(RoomDev R, ThermArgs A, const double *__restrict__ u,
                                                   const double *__restrict__ v,
                                                   const double *__restrict__ w, double *T0,
@@ -549,7 +543,6 @@ __global__ void __launch_bounds__(256) k_advect_T(RoomDev R, ThermArgs A, const 
     const double *T = st->tpar ? T1 : T0;
     double *Tn = st->tpar ? T0 : T1;
     const int quick = A.scheme == 1, lw = A.scheme == 2;
-    const double dt = A.dt;
     double sum = 0.0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.n; c += gridDim.x * blockDim.x) {
         if (R.ct[c] != CT_FLUID) {
@@ -557,7 +550,6 @@ __global__ void __launch_bounds__(256) k_advect_T(RoomDev R, ThermArgs A, const 
             continue;
         }
         const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
-        const double hx = R.dxv[i], hy = R.dyv[j], hz = R.dzv[k];
         const double tc = T[c];
         const double ac = 0.5 * (u[c] + u[c + plane]);
         const double bc = 0.5 * (v[VIX(i, j, k)] + v[VIX(i, j + 1, k)]);
@@ -565,26 +557,31 @@ __global__ void __launch_bounds__(256) k_advect_T(RoomDev R, ThermArgs A, const 
         // Neumann at the domain edge and at SOLID cells (FluidSolver.cpp:417-422)
         auto tat = [&](int ii, int jj, int kk) -> double {
             if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) return tc;
-            const int q = UIX(ii, jj, kk);
-            return R.ct[q] == CT_SOLID ? tc : T[q];
+            const int qq = UIX(ii, jj, kk);
+            return R.ct[qq] == CT_SOLID ? tc : T[qq];
         };
         const double xm = tat(i - 1, j, k), xp = tat(i + 1, j, k);
         const double ym = tat(i, j - 1, k), yp = tat(i, j + 1, k);
         const double zm = tat(i, j, k - 1), zp = tat(i, j, k + 1);
-        double adv;
-        if (quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
-            adv = adv_quick(tat(i - 2, j, k), xm, tc, xp, ac, hx)
-                + adv_quick(tat(i, j - 2, k), ym, tc, yp, bc, hy)
-                + adv_quick(tat(i, j, k - 2), zm, tc, zp, cc, hz);
+        const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+        const double xmm = q ? tat(i - 2, j, k) : 0.0, ymm = q ? tat(i, j - 2, k) : 0.0,
+                     zmm = q ? tat(i, j, k - 2) : 0.0;
+        const F hx = F(R.dxv[i]), hy = F(R.dyv[j]), hz = F(R.dzv[k]), dt = F(A.dt);
+        F adv;
+        if (q) {
+            adv = adv_quick(F(xmm), F(xm), F(tc), F(xp), F(ac), hx) + adv_quick(F(ymm), F(ym), F(tc), F(yp), F(bc), hy)
+                + adv_quick(F(zmm), F(zm), F(tc), F(zp), F(cc), hz);
         } else if (lw) {
-            adv = adv_lw(xm, tc, xp, ac, dt, hx) + adv_lw(ym, tc, yp, bc, dt, hy)
-                + adv_lw(zm, tc, zp, cc, dt, hz);
+            adv = adv_lw(F(xm), F(tc), F(xp), F(ac), dt, hx) + adv_lw(F(ym), F(tc), F(yp), F(bc), dt, hy)
+                + adv_lw(F(zm), F(tc), F(zp), F(cc), dt, hz);
         } else {
-            adv = adv_up(xm, tc, xp, ac, hx) + adv_up(ym, tc, yp, bc, hy) + adv_up(zm, tc, zp, cc, hz);
+            adv = adv_up(F(xm), F(tc), F(xp), F(ac), hx) + adv_up(F(ym), F(tc), F(yp), F(bc), hy)
+                + adv_up(F(zm), F(tc), F(zp), F(cc), hz);
         }
-        const double dif = A.alpha * ((xm - 2 * tc + xp) / (hx * hx) + (ym - 2 * tc + yp) / (hy * hy)
-                                      + (zm - 2 * tc + zp) / (hz * hz));
-        const double tn = tc + dt * (-adv + dif);
+        const F ftc = F(tc);
+        const F dif = F(A.alpha) * ((F(xm) - F(2) * ftc + F(xp)) / (hx * hx) + (F(ym) - F(2) * ftc + F(yp)) / (hy * hy)
+                                    + (F(zm) - F(2) * ftc + F(zp)) / (hz * hz));
+        const double tn = tc + (double)(dt * (-adv + dif));
         Tn[c] = tn;
         sum += tn;
     }
@@ -807,6 +804,9 @@ struct ffr_fluid {
     unsigned long long *div_slot;
     unsigned cg_blocks, blocks_faces, blocks_cells;
     GroupTimer prof;
+    bool mg = false, mixed = false;
+    MGDev M;
+    MGHost mgh;
 };
 
 namespace {
@@ -818,8 +818,12 @@ int fluid_enqueue_step(ffr_fluid *s)
     const RoomGeom &g = s->room.g;
     PredArgs pa{P.dt, P.nu, P.advection, P.buoyancy ? 1 : 0, P.g_accel * P.beta * P.dt, P.T_initial};
     s->prof.begin(FFR_PROF_PREDICT, st);
-    k_predict<<<s->blocks_faces, kThreads, 0, st>>>(s->R, pa, s->u, s->v, s->w, s->T0, s->T1, s->us,
-                                                     s->vs, s->ws, s->st);
+    if (s->mixed)
+        k_predict<float><<<s->blocks_faces, kThreads, 0, st>>>(s->R, pa, s->u, s->v, s->w, s->T0, s->T1, s->us,
+                                                                s->vs, s->ws, s->st);
+    else
+        k_predict<double><<<s->blocks_faces, kThreads, 0, st>>>(s->R, pa, s->u, s->v, s->w, s->T0, s->T1, s->us,
+                                                                 s->vs, s->ws, s->st);
     FFR_LAUNCHED(1);
     s->prof.end(st, 1);
     CGArgs ca{};
@@ -832,7 +836,21 @@ int fluid_enqueue_step(ffr_fluid *s)
     ca.max_iter = P.poisson_max_iter; ca.tol = P.poisson_tol;
     ca.st = s->st;
     s->prof.begin(FFR_PROF_PRESSURE, st);
-    int rc = launch_cg(ca, s->cg_blocks, st);
+    int rc;
+    if (s->mg) {
+        PCGArgs pa2{};
+        pa2.R = s->R; pa2.M = s->M;
+        pa2.us = s->us; pa2.vs = s->vs; pa2.ws = s->ws;
+        pa2.rhs_factor = -(P.rho / P.dt);
+        pa2.from_faces = 1;
+        pa2.x = s->p; pa2.r = s->r; pa2.da = s->da; pa2.db = s->db; pa2.q = s->ad;
+        pa2.partials = s->partials; pa2.gs = s->gs; pa2.sc = s->sc;
+        pa2.max_iter = P.poisson_max_iter; pa2.tol = P.poisson_tol;
+        pa2.st = s->st;
+        rc = launch_pcg(pa2, st, nullptr);
+    } else {
+        rc = launch_cg(ca, s->cg_blocks, st);
+    }
     if (rc) return rc;
     s->prof.end(st, 1);
     CorrArgs co{P.dt / P.rho};
@@ -852,8 +870,12 @@ int fluid_enqueue_step(ffr_fluid *s)
             nthermal++;
         }
         ThermArgs ta{P.dt, P.k_thermal / (P.rho * P.cp), P.advection};
-        k_advect_T<<<s->blocks_cells, kThreads, 0, st>>>(s->R, ta, s->u, s->v, s->w, s->T0, s->T1,
-                                                          s->tpart, s->st);
+        if (s->mixed)
+            k_advect_T<float><<<s->blocks_cells, kThreads, 0, st>>>(s->R, ta, s->u, s->v, s->w, s->T0, s->T1,
+                                                                     s->tpart, s->st);
+        else
+            k_advect_T<double><<<s->blocks_cells, kThreads, 0, st>>>(s->R, ta, s->u, s->v, s->w, s->T0, s->T1,
+                                                                      s->tpart, s->st);
         FFR_LAUNCHED(1);
         nthermal++;
         for (const ffr_patch &op : s->room.patches) {
@@ -920,10 +942,10 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
 {
     if (!params || !out) return fail(FFR_EINVAL, "NULL params or out");
     *out = nullptr;
-    if (params->precision != FFR_PREC_FP64)
-        return fail(FFR_ENOTSUP, "only FFR_PREC_FP64 is built in this library");
-    if (params->poisson != FFR_POISSON_CG || params->use_multigrid)
-        return fail(FFR_ENOTSUP, "only the CG pressure solve is built in this library");
+    if (params->precision != FFR_PREC_FP64 && params->precision != FFR_PREC_MIXED)
+        return fail(FFR_EINVAL, "bad precision");
+    if (params->poisson != FFR_POISSON_CG && params->poisson != FFR_POISSON_MGPCG)
+        return fail(FFR_EINVAL, "bad pressure solver");
     if (!(params->dt > 0) || !(params->rho > 0)) return fail(FFR_EINVAL, "dt and rho must be positive");
     if (params->advection < 0 || params->advection > 2) return fail(FFR_EINVAL, "bad advection scheme");
     if (params->poisson_max_iter < 0) return fail(FFR_EINVAL, "negative poisson_max_iter");
@@ -932,22 +954,30 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     int rc = load_room(room, s->room);
     if (rc) { delete s; return rc; }
     s->prm = *params;
+    s->mixed = params->precision == FFR_PREC_MIXED;
+    s->mg = params->poisson == FFR_POISSON_MGPCG || params->use_multigrid;
+    if (s->mg) build_mg_levels(s->room, s->mgh);
     const RoomGeom &g = s->room.g;
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete s;
         return fail(FFR_ECUDA, "cudaStreamCreate");
     }
-    s->cg_blocks = std::max(1u, std::min(cg_max_blocks(), (unsigned)((g.n + kThreads - 1) / kThreads)));
+    s->cg_blocks = std::max(1u, std::min(std::max(cg_max_blocks(), pcg_max_blocks()),
+                                         (unsigned)((g.n + kThreads - 1) / kThreads)));
     s->blocks_faces = stream_blocks(g.nu + g.nv + g.nw);
     s->blocks_cells = stream_blocks(g.n);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = tables_bytes(s->room) + 2 * (al(8 * g.nu) + al(8 * g.nv) + al(8 * g.nw)) +
                          7 * al(8 * g.n) + al(8 * s->cg_blocks * 4) + al(8 * s->blocks_cells) +
                          al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
-                         al(sizeof(ffr_step_result) * kRing) + 4 * 256;
+                         al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (s->mg ? mg_bytes(s->room, s->mgh) : 0);
     rc = s->arena.alloc(bytes);
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
     rc = upload_tables(s->room, s->arena, s->stream, s->tab, s->R);
+    if (!rc && s->mg) {
+        rc = mg_upload(s->room, s->mgh, s->arena, s->stream, s->M);
+        s->M.vol_x = s->R.dxv; s->M.vol_y = s->R.dyv; s->M.vol_z = s->R.dzv;
+    }
     Arena &a = s->arena;
     s->u = a.take<double>(g.nu); s->v = a.take<double>(g.nv); s->w = a.take<double>(g.nw);
     s->us = a.take<double>(g.nu); s->vs = a.take<double>(g.nv); s->ws = a.take<double>(g.nw);

@@ -1,0 +1,74 @@
+"""Mixed precision (FP32 increments on FP64 state, FP32 multigrid
+preconditioner, FP64 outer CG) against the FP64 reference method.
+
+Tolerance (the stated bound for mixed precision): every field within 1e-4
+max-norm relative error of the FP64 result after the same number of steps,
+with the pressure solved to the same relative residual.  The MG-PCG solve
+itself must reach the residual the plain CG reaches.
+"""
+import numpy as np
+import pytest
+
+from conftest import Golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["c1_upwind_10", "c1_quick_10", "two_fans_10", "summer_cooling_10", "edge_odd_quick_10",
+         "oblique_stretch_10", "updraft_laxw_10", "vent_quick_10", "thermal_small_10"]
+
+
+@pytest.mark.parametrize("poisson,precision", [("mgpcg", "fp64"), ("mgpcg", "mixed"), ("cg", "mixed")])
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_tracks_reference(name, poisson, precision):
+    from ffrb import capi
+    g = Golden(name)
+    p = g.params.with_(poisson=poisson, precision=precision)
+    h = capi.FluidHandle(g.room, p)
+    recs = h.advance(g.nsteps)
+    assert len(recs) == g.nsteps
+    for k in "uvwpT":
+        err = rel_err(h.get(k), g.fields[k])
+        assert err <= 1e-4, (k, err)
+    assert all(r["pressure_residual"] < g.params.poisson_tol for r in recs if r["cg_iterations"] > 0)
+    if poisson == "mgpcg":
+        # far fewer iterations than the unpreconditioned CG
+        assert np.mean([r["cg_iterations"] for r in recs]) < 0.35 * np.mean(g.hist["cg_iterations"])
+    h.close()
+
+
+def test_mgpcg_long_run_tracks_reference():
+    """500 steps of the benchmark room: mixed MG-PCG stays within 1e-4."""
+    from ffrb import capi
+    g = Golden("c1_upwind_500")
+    h = capi.FluidHandle(g.room, g.params.with_(poisson="mgpcg", precision="mixed"))
+    recs = h.advance(g.nsteps)
+    for k in "uvwp":
+        assert rel_err(h.get(k), g.fields[k]) <= 1e-4, k
+    assert rel_err([recs[-1]["velocity_change"]], [g.hist["velocity_change"][-1]]) <= 1e-3
+
+
+def test_projected_divergence_is_small():
+    """The projected field (before the BC re-application that the reference
+    performs after the correction) is divergence-free to the solver
+    tolerance: measured on FLUID cells away from BC-overwritten faces."""
+    from ffrb import capi
+    from ffrb.scene import build_room
+    from ffrb import workloads
+    cfg, prm = workloads.large_thermal(grid=(80, 64, 24))
+    room = build_room(cfg)
+    h = capi.FluidHandle(room, prm.with_(poisson_tol=1e-10))
+    h.advance(3)
+    u, v, w = h.get("u"), h.get("v"), h.get("w")
+    nx, ny, nz = room.nx, room.ny, room.nz
+    U = u.reshape(nx + 1, ny, nz); V = v.reshape(nx, ny + 1, nz); W = w.reshape(nx, ny, nz + 1)
+    div = ((U[1:] - U[:-1]) / room.dxv[:, None, None] + (V[:, 1:] - V[:, :-1]) / room.dyv[None, :, None]
+           + (W[:, :, 1:] - W[:, :, :-1]) / room.dzv[None, None, :])
+    ct = room.cell_type.reshape(nx, ny, nz)
+    # FLUID cells whose 6 neighbours are FLUID (no BC-overwritten face)
+    inner = np.zeros_like(ct, dtype=bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    for ax in range(3):
+        for sh in (-1, 1):
+            inner &= np.roll(ct, sh, axis=ax) == 0
+    inner &= ct == 0
+    assert np.abs(div[inner]).max() <= 1e-6
