@@ -41,6 +41,13 @@ FALLBACK_HBM = 6650.0
 CG_INIT_B = 50.0       # read u*,v*,w* + code, write r, d, x
 CG_ITER_B = 74.0       # phase A (r, d_old, x, code -> d, Ad, x) + phase B (r, Ad -> r)
 CG_FINAL_B = 24.0      # x += alpha d
+# Multigrid-preconditioned CG (k_pcg), per fine cell.  Per iteration: the
+# level-0 passes (black pre-smooth 15, restriction 11, black post-smooth
+# 15.5, red post-smooth + r.z 23, direction/operator 47, residual update 35)
+# plus ~16 for the coarse levels (16-byte coefficients, 1/8 the cells per
+# level); once per solve: set-up 60 and the final x update 24.
+PCG_ITER_B = 163.0
+PCG_ONCE_B = 84.0
 LBM_STEP_B = {"fp64": 2 * 19 * 8 + 1 + 4 * 8, "fp32": 2 * 19 * 4 + 1 + 4 * 8, "fp16": 2 * 19 * 2 + 1 + 4 * 8}
 
 
@@ -173,14 +180,20 @@ def run_ours(args, rank: int, world: int, dist):
     peak, peak_kind = measured_peak()
     if kind == "fluid":
         iters = [r["cg_iterations"] for r in recs]
-        bytes_cg = sum(cells * (CG_INIT_B + CG_ITER_B * it + CG_FINAL_B) for it in iters)
+        mg = params.poisson == "mgpcg"
+        if mg:
+            bytes_cg = sum(cells * (PCG_ONCE_B + PCG_ITER_B * it) for it in iters)
+            kname = "k_pcg (persistent multigrid-preconditioned CG)"
+        else:
+            bytes_cg = sum(cells * (CG_INIT_B + CG_ITER_B * it + CG_FINAL_B) for it in iters)
+            kname = "k_cg (persistent pressure CG)"
         t_cg = prof["pressure"][0] / 1e3
         achieved = bytes_cg / t_cg / 1e9
         launches_cg = max(1, prof["pressure"][1])
-        roof = {"bound": "hbm", "kernel": "k_cg (persistent pressure CG)", "achieved": round(achieved, 1),
+        roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "traffic": load_traffic("k_cg_per_cell_iter"),
+                "traffic": load_traffic("k_pcg_per_launch" if mg else "k_cg_per_launch"),
                 "algorithmic_bytes_per_launch": bytes_cg / launches_cg,
                 "share_of_step": round(prof["pressure"][0] / ms, 4),
                 "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}

@@ -79,9 +79,14 @@ template <> struct Store<2> {
     __device__ static void st(__half *p, float v) { *p = __float2half_rn(v); }
 };
 
+// Per-cell flags of the step kernel (besides the cell type in bits 0-1).
+enum : uint8_t { LF_OPEN = 4,    // all 18 neighbours in the domain and not SOLID
+                 LF_REMAP = 8 }; // OUTFLOW cell whose populations come from another cell
+
 struct LbmDev {
     int nx, ny, nz, n, nu, nv, nw;
     const uint8_t *ct;          // cell types
+    const uint8_t *fl;          // cell type | LF_* flags
     const uint8_t *fan_of;      // fan index of each INFLOW cell (255: none)
     const double *fan_lat;      // lattice fan velocity, 3 per fan
     const int *remap_dst;       // sorted OUTFLOW destinations
@@ -112,25 +117,32 @@ __device__ __forceinline__ int find_src(const LbmDev &L, int c)
 // One fused step; see the file comment.  fa = f* of this step, fb = f* of
 // the next, cu/cv/cw = cell-centred velocity (m/s), p = rho*cs^2.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_lbm_step(LbmDev L, const typename Store<MODE>::T *f0,
-                                                  typename Store<MODE>::T *f1, double *cu, double *cv,
-                                                  double *cw, double *p, const LbmState *st)
+__global__ void __launch_bounds__(256, MODE == 0 ? 2 : 3)
+    k_lbm_step(LbmDev L, const typename Store<MODE>::T *f0, typename Store<MODE>::T *f1, double *__restrict__ cu,
+               double *__restrict__ cv, double *__restrict__ cw, double *__restrict__ p, const LbmState *st)
 {
     using S = Store<MODE>;
     using T = typename S::T;
     if (st->halt) return;
-    const T *fa = st->par ? f1 : f0;
-    T *fb = st->par ? (T *)f0 : f1;
+    const T *__restrict__ fa = st->par ? f1 : f0;
+    T *__restrict__ fb = st->par ? (T *)f0 : f1;
     const int nx = L.nx, ny = L.ny, nz = L.nz, n = L.n, plane = ny * nz;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const uint8_t t = L.ct[c];
+        const uint8_t fl = L.fl[c];
+        const uint8_t t = fl & 3;
         if (t == CT_SOLID) {
             cu[c] = 0.0; cv[c] = 0.0; cw[c] = 0.0;
             continue;
         }
-        const int o = (t == CT_OUTFLOW && L.nremap) ? find_src(L, c) : c;
         using C = typename std::conditional<MODE == 0, double, float>::type;
         C fq[19];
+        if (fl & LF_OPEN) {
+            // interior cell: every slot is streamed from its upwind neighbour
+#pragma unroll
+            for (int q = 0; q < 19; q++)
+                fq[q] = C(S::ld(fa + (q * n + c - (c_ex[q] * plane + c_ey[q] * nz + c_ez[q]))));
+        } else {
+        const int o = (fl & LF_REMAP) ? find_src(L, c) : c;
         if (L.ct[o] == CT_SOLID) {
 #pragma unroll
             for (int q = 0; q < 19; q++) fq[q] = MODE == 0 ? C(0) : C(-lbm_w(q));
@@ -152,17 +164,18 @@ __global__ void __launch_bounds__(256) k_lbm_step(LbmDev L, const typename Store
                 const bool inb = !(ti >= 0 && ti < nx && tj >= 0 && tj < ny && tk >= 0 && tk < nz) || L.ct[tcell] == CT_SOLID;
                 if (MODE == 0) {
                     C v = C(0);
-                    if (ina) v = v + S::ld(fa + (size_t)q * n + s);
-                    if (inb) v = v + S::ld(fa + (size_t)qq * n + o);
+                    if (ina) v = v + S::ld(fa + (q * n + s));
+                    if (inb) v = v + S::ld(fa + (qq * n + o));
                     fq[q] = v;
                 } else {
                     // shifted storage g = f - w (w_q == w_OPP[q]): g_post = sum g + (k-1) w_q
                     C v = C(-lbm_w(q));
-                    if (ina) v += S::ld(fa + (size_t)q * n + s) + C(lbm_w(q));
-                    if (inb) v += S::ld(fa + (size_t)qq * n + o) + C(lbm_w(q));
+                    if (ina) v += S::ld(fa + (q * n + s)) + C(lbm_w(q));
+                    if (inb) v += S::ld(fa + (qq * n + o)) + C(lbm_w(q));
                     fq[q] = v;
                 }
             }
+        }
         }
         // moments (LBMSolver.cpp:306-318) and next-step collision
         if (MODE == 0) {
@@ -180,16 +193,16 @@ __global__ void __launch_bounds__(256) k_lbm_step(LbmDev L, const typename Store
             if (t == CT_INFLOW && L.fan_of[c] != 255) {
                 const double *fv = L.fan_lat + 3 * L.fan_of[c];
 #pragma unroll
-                for (int q = 0; q < 19; q++) S::st(fb + (size_t)q * n + c, feq64(q, 1.0, fv[0], fv[1], fv[2]));
+                for (int q = 0; q < 19; q++) S::st(fb + (q * n + c), feq64(q, 1.0, fv[0], fv[1], fv[2]));
             } else if (t == CT_INFLOW) {
 #pragma unroll
-                for (int q = 0; q < 19; q++) S::st(fb + (size_t)q * n + c, fq[q]);
+                for (int q = 0; q < 19; q++) S::st(fb + (q * n + c), fq[q]);
             } else {
                 const double itau = 1.0 / L.tau;
 #pragma unroll
                 for (int q = 0; q < 19; q++) {
                     const double fe = feq64(q, rho, ux, uy, uz);
-                    S::st(fb + (size_t)q * n + c, fq[q] + itau * (fe - fq[q]));
+                    S::st(fb + (q * n + c), fq[q] + itau * (fe - fq[q]));
                 }
             }
         } else {
@@ -210,16 +223,16 @@ __global__ void __launch_bounds__(256) k_lbm_step(LbmDev L, const typename Store
                 const double *fv = L.fan_lat + 3 * L.fan_of[c];
 #pragma unroll
                 for (int q = 0; q < 19; q++)
-                    S::st(fb + (size_t)q * n + c, geq32(q, 0.0f, (float)fv[0], (float)fv[1], (float)fv[2]));
+                    S::st(fb + (q * n + c), geq32(q, 0.0f, (float)fv[0], (float)fv[1], (float)fv[2]));
             } else if (t == CT_INFLOW) {
 #pragma unroll
-                for (int q = 0; q < 19; q++) S::st(fb + (size_t)q * n + c, fq[q]);
+                for (int q = 0; q < 19; q++) S::st(fb + (q * n + c), fq[q]);
             } else {
                 const float itau = (float)(1.0 / L.tau);
 #pragma unroll
                 for (int q = 0; q < 19; q++) {
                     const float ge = geq32(q, drho, ux, uy, uz);
-                    S::st(fb + (size_t)q * n + c, fq[q] + itau * (ge - fq[q]));
+                    S::st(fb + (q * n + c), fq[q] + itau * (ge - fq[q]));
                 }
             }
         }
@@ -277,8 +290,10 @@ __global__ void k_lbm_init(LbmDev L, typename Store<MODE>::T *f)
 // Face velocities of extract_macroscopic (LBMSolver.cpp:333-375), max
 // |du| against the previous faces (LBMSolver.cpp:423-433) and max |div|
 // over FLUID cells (LBMSolver.cpp:382-396), cell-centric like k_correct.
-__global__ void __launch_bounds__(256) k_lbm_faces(LbmDev L, const double *cu, const double *cv,
-                                                   const double *cw, double *u, double *v, double *w,
+__global__ void __launch_bounds__(256) k_lbm_faces(LbmDev L, const double *__restrict__ cu,
+                                                   const double *__restrict__ cv,
+                                                   const double *__restrict__ cw, double *__restrict__ u,
+                                                   double *__restrict__ v, double *__restrict__ w,
                                                    LbmState *st)
 {
     __shared__ double sh[32];
@@ -287,21 +302,37 @@ __global__ void __launch_bounds__(256) k_lbm_faces(LbmDev L, const double *cu, c
     double dmax = 0.0, divmax = 0.0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.n; c += gridDim.x * blockDim.x) {
         const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
-        const double ulo = (i == 0) ? cu[c] : 0.5 * (cu[c - plane] + cu[c]);
-        const double uhi = (i == nx - 1) ? cu[c] : 0.5 * (cu[c] + cu[c + plane]);
-        const double vlo = (j == 0) ? cv[c] : 0.5 * (cv[c - nz] + cv[c]);
-        const double vhi = (j == ny - 1) ? cv[c] : 0.5 * (cv[c] + cv[c + nz]);
-        const double wlo = (k == 0) ? cw[c] : 0.5 * (cw[c - 1] + cw[c]);
-        const double whi = (k == nz - 1) ? cw[c] : 0.5 * (cw[c] + cw[c + 1]);
         const int uf = c, vf = (i * (ny + 1) + j) * nz + k, wf = (i * ny + j) * (nz + 1) + k;
-        dmax = fmax(dmax, fabs(ulo - u[uf])); u[uf] = ulo;
-        dmax = fmax(dmax, fabs(vlo - v[vf])); v[vf] = vlo;
-        dmax = fmax(dmax, fabs(wlo - w[wf])); w[wf] = wlo;
-        if (i == nx - 1) { dmax = fmax(dmax, fabs(uhi - u[uf + plane])); u[uf + plane] = uhi; }
-        if (j == ny - 1) { dmax = fmax(dmax, fabs(vhi - v[vf + nz])); v[vf + nz] = vhi; }
-        if (k == nz - 1) { dmax = fmax(dmax, fabs(whi - w[wf + 1])); w[wf + 1] = whi; }
-        if (L.ct[c] == CT_FLUID)
+        // every load first, then the arithmetic, then the stores
+        const double cuc = cu[c], cvc = cv[c], cwc = cw[c];
+        const double cum = (i > 0) ? cu[c - plane] : 0.0, cup = (i < nx - 1) ? cu[c + plane] : 0.0;
+        const double cvm = (j > 0) ? cv[c - nz] : 0.0, cvp = (j < ny - 1) ? cv[c + nz] : 0.0;
+        const double cwm = (k > 0) ? cw[c - 1] : 0.0, cwp = (k < nz - 1) ? cw[c + 1] : 0.0;
+        const double uo = u[uf], vo = v[vf], wo = w[wf];
+        const double uho = (i == nx - 1) ? u[uf + plane] : 0.0;
+        const double vho = (j == ny - 1) ? v[vf + nz] : 0.0;
+        const double who = (k == nz - 1) ? w[wf + 1] : 0.0;
+        const bool fluid = L.ct[c] == CT_FLUID;
+        const double ulo = (i == 0) ? cuc : 0.5 * (cum + cuc);
+        const double uhi = (i == nx - 1) ? cuc : 0.5 * (cuc + cup);
+        const double vlo = (j == 0) ? cvc : 0.5 * (cvm + cvc);
+        const double vhi = (j == ny - 1) ? cvc : 0.5 * (cvc + cvp);
+        const double wlo = (k == 0) ? cwc : 0.5 * (cwm + cwc);
+        const double whi = (k == nz - 1) ? cwc : 0.5 * (cwc + cwp);
+        dmax = fmax(dmax, fabs(ulo - uo));
+        dmax = fmax(dmax, fabs(vlo - vo));
+        dmax = fmax(dmax, fabs(wlo - wo));
+        if (i == nx - 1) dmax = fmax(dmax, fabs(uhi - uho));
+        if (j == ny - 1) dmax = fmax(dmax, fabs(vhi - vho));
+        if (k == nz - 1) dmax = fmax(dmax, fabs(whi - who));
+        if (fluid)
             divmax = fmax(divmax, fabs((uhi - ulo) / L.dxv[i] + (vhi - vlo) / L.dyv[j] + (whi - wlo) / L.dzv[k]));
+        u[uf] = ulo;
+        v[vf] = vlo;
+        w[wf] = wlo;
+        if (i == nx - 1) u[uf + plane] = uhi;
+        if (j == ny - 1) v[vf + nz] = vhi;
+        if (k == nz - 1) w[wf + 1] = whi;
     }
     dmax = block_max(dmax, sh);
     divmax = block_max(divmax, sh);
@@ -500,6 +531,30 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
         for (int c = 0; c < 3; c++) fan_lat[3 * f + c] = s->room.fans[f].vel[c] * p2l;
     std::vector<int> rd, rs;
     resolve_remap(s->room, rd, rs);
+    // step-kernel flags: open interior cells skip every neighbour test
+    std::vector<uint8_t> flags(g.n);
+    {
+        static const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+        static const int ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+        static const int ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+        std::vector<uint8_t> remapped(g.n, 0);
+        for (int d : rd) remapped[d] = 1;
+        for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++)
+                for (int k = 0; k < nz; k++) {
+                    const int c = (i * ny + j) * nz + k;
+                    uint8_t f = s->room.ct[c];
+                    if (remapped[c]) f |= LF_REMAP;
+                    bool open = f != CT_SOLID && !remapped[c];
+                    for (int q = 1; q < 19 && open; q++) {
+                        const int a = i + ex[q], b = j + ey[q], e = k + ez[q];
+                        open = a >= 0 && a < nx && b >= 0 && b < ny && e >= 0 && e < nz &&
+                               s->room.ct[(a * ny + b) * nz + e] != CT_SOLID;
+                    }
+                    if (open) f |= LF_OPEN;
+                    flags[c] = f;
+                }
+    }
     const size_t es = storage == FFR_LBM_FP64 ? 8 : (storage == FFR_LBM_FP32 ? 4 : 2);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = 2 * al(es * 19 * g.n) + 4 * al(8 * g.n) + al(8 * g.nu) + al(8 * g.nv) +
@@ -514,7 +569,7 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     s->cu = a.take<double>(g.n); s->cv = a.take<double>(g.n); s->cw = a.take<double>(g.n);
     s->p = a.take<double>(g.n);
     s->u = a.take<double>(g.nu); s->v = a.take<double>(g.nv); s->w = a.take<double>(g.nw);
-    uint8_t *ct = a.take<uint8_t>(g.n), *fo = a.take<uint8_t>(g.n);
+    uint8_t *ct = a.take<uint8_t>(g.n), *fo = a.take<uint8_t>(g.n), *fld = a.take<uint8_t>(g.n);
     double *fl = a.take<double>(fan_lat.size());
     int *rdd = a.take<int>(rd.size() + 1), *rsd = a.take<int>(rd.size() + 1);
     double *dxv = a.take<double>(g.nx), *dyv = a.take<double>(g.ny), *dzv = a.take<double>(g.nz);
@@ -529,6 +584,7 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     cudaStream_t st = s->stream;
     FFR_CUDA(cudaMemcpyAsync(ct, s->room.ct.data(), g.n, cudaMemcpyHostToDevice, st));
     FFR_CUDA(cudaMemcpyAsync(fo, fan_of.data(), g.n, cudaMemcpyHostToDevice, st));
+    FFR_CUDA(cudaMemcpyAsync(fld, flags.data(), g.n, cudaMemcpyHostToDevice, st));
     FFR_CUDA(cudaMemcpyAsync(fl, fan_lat.data(), 8 * fan_lat.size(), cudaMemcpyHostToDevice, st));
     if (!rd.empty()) {
         FFR_CUDA(cudaMemcpyAsync(rdd, rd.data(), 4 * rd.size(), cudaMemcpyHostToDevice, st));
@@ -548,7 +604,7 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
         return rc;
     }
     FFR_CUDA(cudaMemsetAsync(s->st, 0, sizeof(LbmState), st));
-    s->L = LbmDev{nx, ny, nz, (int)g.n, (int)g.nu, (int)g.nv, (int)g.nw, ct, fo, fl, rdd, rsd,
+    s->L = LbmDev{nx, ny, nz, (int)g.n, (int)g.nu, (int)g.nv, (int)g.nw, ct, fld, fo, fl, rdd, rsd,
                   (int)rd.size(), dxv, dyv, dzv, tau, (g.lx / g.nx) / dt};
     s->blocks = blocks_for(g.n);
     switch (storage) {

@@ -347,7 +347,7 @@ __device__ __forceinline__ double face_rhs(const PCGArgs &A, int c, int i, int j
     return A.rhs_factor * div;
 }
 
-__global__ void __launch_bounds__(256) k_pcg(PCGArgs A)
+__global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
 {
     __shared__ double sh[32];
     if (A.st && A.st->halt) return;
@@ -548,7 +548,7 @@ size_t mg_bytes(const HostRoom &r, const MGHost &h)
 {
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const RoomGeom &g = r.g;
-    size_t b = 2 * al(4 * g.n) + 6 * al(4 * (g.nx + g.ny + g.nz));
+    size_t b = 2 * al(4 * g.n) + 9 * al(4 * std::max(g.nx, std::max(g.ny, g.nz)));
     for (size_t l = 1; l < h.nx.size(); l++) {
         const size_t m = (size_t)h.nx[l] * h.ny[l] * h.nz[l];
         b += al(16 * m) + 2 * al(4 * m);

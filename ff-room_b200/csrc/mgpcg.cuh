@@ -8,7 +8,7 @@ namespace ffr {
 
 constexpr int kMaxLevels = 12;
 // Levels with at most this many cells run inside one CTA (no grid barrier).
-constexpr int kBlockLevelCells = 4096;
+constexpr int kBlockLevelCells = 640;
 
 // One coarse level: per cell (T to the x+, y+, z+ neighbour, diagonal), FP32.
 // Inactive cells (no FLUID/INFLOW child) have diagonal 0.
