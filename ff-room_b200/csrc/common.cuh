@@ -75,13 +75,20 @@ void build_stencil(const HostRoom &r, std::vector<uint16_t> &sc,
 // ------------------------------------------------------ device memory
 
 // One cudaMalloc per handle, carved into 256-byte aligned slices.
+// Exhaustion is sticky: once a take() fails every later take() fails too,
+// so checking the last slice of a carve (before any copy or launch) covers
+// every slice taken before it.
 struct Arena {
     char *base = nullptr;
     size_t size = 0, used = 0;
+    bool failed = false;
     int alloc(size_t bytes);
     template <class T> T *take(size_t count) {
         size_t b = (count * sizeof(T) + 255) & ~size_t(255);
-        if (used + b > size) return nullptr;
+        if (failed || used + b > size) {
+            failed = true;
+            return nullptr;
+        }
         T *p = reinterpret_cast<T *>(base + used);
         used += b;
         return p;

@@ -558,9 +558,9 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     const size_t es = storage == FFR_LBM_FP64 ? 8 : (storage == FFR_LBM_FP32 ? 4 : 2);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = 2 * al(es * 19 * g.n) + 4 * al(8 * g.n) + al(8 * g.nu) + al(8 * g.nv) +
-                         al(8 * g.nw) + 2 * al(g.n) + al(8 * fan_lat.size()) + 2 * al(4 * (rd.size() + 1)) +
-                         al(8 * (g.nx + g.ny + g.nz)) + al(sizeof(LbmState)) +
-                         al(sizeof(ffr_step_result) * kRingL) + 3 * 256;
+                         al(8 * g.nw) + 3 * al(g.n) + al(8 * fan_lat.size()) + 2 * al(4 * (rd.size() + 1)) +
+                         al(8 * g.nx) + al(8 * g.ny) + al(8 * g.nz) + al(sizeof(LbmState)) +
+                         al(sizeof(ffr_step_result) * kRingL) + al(8);
     rc = s->arena.alloc(bytes);
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
     Arena &a = s->arena;
@@ -576,7 +576,7 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     s->st = a.take<LbmState>(1);
     s->ring = a.take<ffr_step_result>(kRingL);
     s->div_slot = a.take<unsigned long long>(1);
-    if (!s->div_slot || cudaMallocHost(&s->st_host, sizeof(LbmState)) != cudaSuccess ||
+    if (!s->div_slot || a.failed || cudaMallocHost(&s->st_host, sizeof(LbmState)) != cudaSuccess ||
         cudaMallocHost(&s->ring_host, sizeof(ffr_step_result) * kRingL) != cudaSuccess) {
         ffr_lbm_destroy(s);
         return fail(FFR_ENOMEM, "LBM allocation");

@@ -146,15 +146,58 @@ __device__ bool grid_barrier(GridSync *gs)
     return s_ok;
 }
 
+__device__ __forceinline__ void decode(int c, int ny, int nz, int &i, int &j, int &k)
+{
+    const int plane = ny * nz;
+    i = c / plane;
+    const int rem = c - i * plane;
+    j = rem / nz;
+    k = rem - j * nz;
+}
+
+// Visits the flat indices start, start + stride, ... < n of a (., ny, nz)
+// grid and keeps (i, j, k) up to date with carries instead of dividing for
+// every cell.
+struct Walk {
+    int c, i, j, k, si, sj, sk, stride, ny, nz, n;
+    __device__ __forceinline__ Walk(int start, int stride_, int ny_, int nz_, int n_)
+        : c(start), stride(stride_), ny(ny_), nz(nz_), n(n_)
+    {
+        decode(start, ny, nz, i, j, k);
+        decode(stride, ny, nz, si, sj, sk);
+    }
+    __device__ __forceinline__ bool ok() const { return c < n; }
+    __device__ __forceinline__ void next()
+    {
+        c += stride;
+        k += sk;
+        j += sj;
+        i += si;
+        if (k >= nz) { k -= nz; j++; }
+        if (j >= ny) { j -= ny; i++; }
+    }
+};
+
 // Level-0 (fine) FP32 coefficients of cell (i,j,k) from its stencil code:
 // t[6] in the order x-, x+, y-, y+, z-, z+ (0 unless the neighbour is an
 // unknown) and the diagonal (Dirichlet ghosts count twice).
 __device__ __forceinline__ void fine_coefs(const MGDev &M, unsigned code, int i, int j, int k, float (&t)[6],
                                            float &D)
 {
-    const float dx = M.dx[i], dy = M.dy[j], dz = M.dz[k];
-    const float tt[6] = {dy * dz * M.ixl[i], dy * dz * M.ixr[i], dx * dz * M.iyl[j],
-                         dx * dz * M.iyr[j], dx * dy * M.izl[k], dx * dy * M.izr[k]};
+    float tt[6];
+    float vol;
+    if (M.uniform) {
+        tt[0] = tt[1] = M.tx;
+        tt[2] = tt[3] = M.ty;
+        tt[4] = tt[5] = M.tz;
+        vol = M.vol;
+    } else {
+        const float dx = M.dx[i], dy = M.dy[j], dz = M.dz[k];
+        tt[0] = dy * dz * M.ixl[i]; tt[1] = dy * dz * M.ixr[i];
+        tt[2] = dx * dz * M.iyl[j]; tt[3] = dx * dz * M.iyr[j];
+        tt[4] = dx * dy * M.izl[k]; tt[5] = dx * dy * M.izr[k];
+        vol = dx * dy * dz;
+    }
     D = 0.0f;
 #pragma unroll
     for (int a = 0; a < 6; a++) {
@@ -162,7 +205,7 @@ __device__ __forceinline__ void fine_coefs(const MGDev &M, unsigned code, int i,
         t[a] = cls == SC_IN ? tt[a] : 0.0f;
         D += cls == SC_IN ? tt[a] : (cls == SC_DIR ? 2.0f * tt[a] : 0.0f);
     }
-    if (!(D > 0.0f)) D = dx * dy * dz;
+    if (!(D > 0.0f)) D = vol;
 }
 
 // sum_nb T_nb * (x_nb [+ e_parent(nb)]) and the diagonal of cell c on
@@ -209,15 +252,6 @@ __device__ __forceinline__ float fine_nbsum(const RoomDev &R, const MGDev &M, co
     return s;
 }
 
-__device__ __forceinline__ void decode(int c, int ny, int nz, int &i, int &j, int &k)
-{
-    const int plane = ny * nz;
-    i = c / plane;
-    const int rem = c - i * plane;
-    j = rem / nz;
-    k = rem - j * nz;
-}
-
 // One Gauss-Seidel half sweep on `color` of level l.  CORR adds the coarse
 // correction of level l+1 to the neighbour values (the post-smoothing pass
 // right after prolongation).
@@ -227,10 +261,12 @@ __device__ void smooth_color(const PCGArgs &A, int l, int color, int start, int 
     const MGDev &M = A.M;
     const MGLevel &L = M.lv[l];
     const MGLevel &Lc = M.lv[l + 1 < M.nlev ? l + 1 : l];
-    for (int c = start; c < L.n; c += stride) {
-        int i, j, k;
-        decode(c, L.ny, L.nz, i, j, k);
-        if (((i + j + k) & 1) != color) continue;
+    // one thread per pair (k, k+1) of a row: exactly one of the two has the colour
+    const int pk = (L.nz + 1) >> 1;
+    for (Walk w(start, stride, L.ny, pk, L.nx * L.ny * pk); w.ok(); w.next()) {
+        const int i = w.i, j = w.j, k = 2 * w.k + ((w.i + w.j + color) & 1);
+        if (k >= L.nz) continue;
+        const int c = (i * L.ny + j) * L.nz + k;
         float D, s;
         if (l == 0) {
             if (!active_ct(A.R.ct[c])) continue;
@@ -251,9 +287,8 @@ __device__ void restrict_level(const PCGArgs &A, int l, int start, int stride)
     const MGDev &M = A.M;
     const MGLevel &L = M.lv[l];
     const MGLevel &C = M.lv[l + 1];
-    for (int P = start; P < C.n; P += stride) {
-        int I, J, K;
-        decode(P, C.ny, C.nz, I, J, K);
+    for (Walk w(start, stride, C.ny, C.nz, C.n); w.ok(); w.next()) {
+        const int P = w.c, I = w.i, J = w.j, K = w.k;
         float sum = 0.0f;
         for (int a = 0; a < 2; a++) {
             const int i = 2 * I + a;
@@ -363,9 +398,8 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
     // phase 0: rhs, r = V*rhs on the unknowns, x = 0, z = red sweep from 0
     {
         double acc[2] = {0.0, 0.0};
-        for (int c = t0; c < n; c += nth) {
-            int i, j, k;
-            decode(c, ny, nz, i, j, k);
+        for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
+            const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
             const uint8_t t = R.ct[c];
             x[c] = 0.0;
             A.da[c] = 0.0;
@@ -395,7 +429,7 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
 
         double *dold = A.da, *dnew = A.db;
         double rz_old = 0.0, alpha = 0.0, alpha_prev = 0.0;
-        bool pending = false, converged = false;
+        bool pending = false;
         for (int it = 0;; it++) {
             // ---- preconditioner: V-cycle from the red sweep already in z
             for (int l = 0; l < M.nlev_grid && l < M.nlev - 1; l++) {
@@ -422,10 +456,9 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
             double acc1[1] = {0.0};
             if (M.nlev_grid >= 1) {
                 const MGLevel &L0 = M.lv[0];
-                for (int c = t0; c < n; c += nth) {
+                for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
+                    const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
                     if (!active_ct(R.ct[c])) continue;
-                    int i, j, k;
-                    decode(c, ny, nz, i, j, k);
                     float zc;
                     if (((i + j + k) & 1) == 0) {
                         float D;
@@ -448,11 +481,10 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
 
             // ---- phase A: d = z + beta d_old, deferred x update, q = M d
             double acc2[1] = {0.0};
-            for (int c = t0; c < n; c += nth) {
+            for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
+                const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
                 const uint8_t t = R.ct[c];
                 if (!active_ct(t)) { dnew[c] = 0.0; q[c] = 0.0; continue; }
-                int i, j, k;
-                decode(c, ny, nz, i, j, k);
                 const double dp = dold[c];
                 const double dc = fma(beta, dp, (double)z[c]);
                 if (it > 0) x[c] = fma(alpha_prev, dp, x[c]);
@@ -477,11 +509,10 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
 
             // ---- phase B: r -= alpha q, ||b - A x||^2, red sweep of the next z
             double acc3[1] = {0.0};
-            for (int c = t0; c < n; c += nth) {
+            for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
+                const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
                 const uint8_t t = R.ct[c];
                 if (!active_ct(t)) continue;
-                int i, j, k;
-                decode(c, ny, nz, i, j, k);
                 const double rv = r[c] - alpha * q[c];
                 r[c] = rv;
                 const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
@@ -501,20 +532,18 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
             pending = true;
             res = sqrt(acc3[0]) / bnorm;
             iters = it + 1;
-            if (res < A.tol) { converged = true; break; }
+            if (res < A.tol) break;
             if (iters >= A.max_iter) { flags |= FFR_FLAG_CG_MAXITER; break; }
             alpha_prev = alpha;
         }
-        (void)converged;
         if (pending)
             for (int c = t0; c < n; c += nth)
                 if (active_ct(R.ct[c])) x[c] = fma(alpha, dold[c], x[c]);
         if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
         // OUTFLOW rows by back-substitution in the reference's own row form
-        for (int c = t0; c < n; c += nth) {
+        for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
+            const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
             if (R.ct[c] != CT_OUTFLOW) continue;
-            int i, j, k;
-            decode(c, ny, nz, i, j, k);
             const double b = face_rhs(A, c, i, j, k);
             const double nx_ = R.nx;
             (void)nx_;
@@ -602,6 +631,15 @@ int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGD
     FFR_CUDA(cudaMemsetAsync(M.lv[0].x, 0, 4 * g.n, s));
     FFR_CUDA(cudaMemsetAsync(M.r32, 0, 4 * g.n, s));
     M.dx = fx; M.dy = fy; M.dz = fz;
+    auto flat = [](const std::vector<double> &hh) {
+        for (double v : hh) if (v != hh[0]) return false;
+        return true;
+    };
+    M.uniform = flat(r.dxv) && flat(r.dyv) && flat(r.dzv);
+    M.tx = (float)(r.dyv[0] * r.dzv[0] / r.dxv[0]);
+    M.ty = (float)(r.dxv[0] * r.dzv[0] / r.dyv[0]);
+    M.tz = (float)(r.dxv[0] * r.dyv[0] / r.dzv[0]);
+    M.vol = (float)(r.dxv[0] * r.dyv[0] * r.dzv[0]);
     M.ixl = fxl; M.ixr = fxr; M.iyl = fyl; M.iyr = fyr; M.izl = fzl; M.izr = fzr;
     for (int l = 1; l < M.nlev; l++) {
         const size_t m = (size_t)h.nx[l] * h.ny[l] * h.nz[l];

@@ -26,6 +26,8 @@ struct MGDev {
     // dy[j]*dz[k]*ix_l[i] and so on; vol = dx*dy*dz
     const float *dx, *dy, *dz, *ixl, *ixr, *iyl, *iyr, *izl, *izr;
     const double *vol_x, *vol_y, *vol_z;   // FP64 spacings for the cell volume
+    int uniform;          // all spacings equal per axis: tx, ty, tz, vol hold the constants
+    float tx, ty, tz, vol;
     float *r32;           // FP32 copy of the scaled CG residual (level-0 rhs)
 };
 

@@ -199,25 +199,6 @@ __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const do
 
 // ------------------------------------------------------------ pressure
 
-struct CGArgs {
-    RoomDev R;
-    const double *us, *vs, *ws;    // rhs from predicted faces when from_faces
-    double rhs_factor;             // -(rho / dt), FluidSolver.cpp:315
-    int from_faces;
-    const double *rhs;             // explicit right-hand side otherwise
-    double *x;
-    double *r, *da, *db, *ad;
-    double *partials;
-    GridSync *gs;
-    CGScalars *sc;
-    int max_iter;
-    double tol;
-    StepState *st;                 // may be null
-    double *out_res;
-    int *out_iters;
-    int *out_flags;
-};
-
 __device__ __forceinline__ void stencil_term(unsigned cls, double s, double xn, double &diag,
                                              double &off)
 {
@@ -772,6 +753,12 @@ unsigned cg_max_blocks()
     return cap;
 }
 
+}  // namespace
+
+unsigned ffr::cg_block_cap() { return cg_max_blocks(); }
+
+namespace {
+
 int launch_cg(const CGArgs &a, unsigned blocks, cudaStream_t s)
 {
     FFR_CUDA(cudaMemsetAsync(a.gs, 0, sizeof(GridSync), s));
@@ -994,7 +981,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     s->cg_iters = a.take<int>(1);
     s->cg_flags = a.take<int>(1);
     s->div_slot = a.take<unsigned long long>(1);
-    if (rc || !s->div_slot) {
+    if (rc || !s->div_slot || s->arena.failed) {
         if (!rc) rc = fail(FFR_ENOMEM, "arena exhausted");
         ffr_fluid_destroy(s);
         return rc;
@@ -1246,7 +1233,7 @@ int ffr_poisson_create(const ffr_room_desc *room, int max_iter, double tol, ffr_
     s->res = a.take<double>(1);
     s->iters = a.take<int>(1);
     s->flags = a.take<int>(1);
-    if (rc || !s->flags) {
+    if (rc || !s->flags || s->arena.failed) {
         if (!rc) rc = fail(FFR_ENOMEM, "arena exhausted");
         ffr_poisson_destroy(s);
         return rc;

@@ -36,4 +36,28 @@ struct RoomDev {
     const double *fanvel;  // 3 per fan
 };
 
+struct CGArgs {
+    RoomDev R;
+    const double *us, *vs, *ws;    // rhs from predicted faces when from_faces
+    double rhs_factor;             // -(rho / dt), FluidSolver.cpp:315
+    int from_faces;
+    const double *rhs;             // explicit right-hand side otherwise
+    double *x;
+    double *r, *da, *db, *ad;
+    double *partials;
+    GridSync *gs;
+    CGScalars *sc;
+    int max_iter;
+    double tol;
+    StepState *st;                 // may be null
+    double *out_res;
+    int *out_iters;
+    int *out_flags;
+};
+
+// The reference's unpreconditioned CG as one cooperative launch
+// (projection.cu).
+__global__ void __launch_bounds__(256) k_cg(CGArgs A);
+unsigned cg_block_cap();
+
 }  // namespace ffr

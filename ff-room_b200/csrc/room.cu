@@ -33,6 +33,7 @@ int Arena::alloc(size_t bytes)
 {
     size = (bytes + 255) & ~size_t(255);
     used = 0;
+    failed = false;
     cudaError_t e = cudaMalloc(&base, size);
     if (e != cudaSuccess) {
         base = nullptr;
