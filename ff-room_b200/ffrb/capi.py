@@ -129,6 +129,8 @@ def lib():
             "ffr_lbm_stream": ([vp, C.POINTER(vp)], C.c_int),
             "ffr_lbm_profile": ([vp, C.c_int], C.c_int),
             "ffr_lbm_profile_read": ([vp, _dp, C.POINTER(C.c_longlong)], C.c_int),
+            "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
+                                           C.c_double, vp, _dp, C.POINTER(C.c_int)], C.c_int),
         }
         for name, (args, res) in sigs.items():
             fn = getattr(L, name)
@@ -384,3 +386,18 @@ class LbmHandle:
 
     def synchronize(self) -> None:
         check(lib().ffr_lbm_synchronize(self.h))
+
+
+def poisson_solve_noalloc(room: RoomSpec, cell_type_ptr: int, rhs_ptr: int, p_ptr: int, max_iter: int,
+                          tol: float, stream: int = 0):
+    """ffr_poisson_solve_noalloc on device buffers (cell types, rhs, p)."""
+    dxv = np.ascontiguousarray(room.dxv, dtype=np.float64)
+    dyv = np.ascontiguousarray(room.dyv, dtype=np.float64)
+    dzv = np.ascontiguousarray(room.dzv, dtype=np.float64)
+    res, it = C.c_double(), C.c_int()
+    check(lib().ffr_poisson_solve_noalloc(room.nx, room.ny, room.nz, dxv.ctypes.data_as(_dp),
+                                          dyv.ctypes.data_as(_dp), dzv.ctypes.data_as(_dp),
+                                          C.c_void_p(cell_type_ptr), C.c_void_p(rhs_ptr), C.c_void_p(p_ptr),
+                                          max_iter, tol, C.c_void_p(stream) if stream else None,
+                                          C.byref(res), C.byref(it)))
+    return res.value, it.value

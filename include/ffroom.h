@@ -213,6 +213,25 @@ int ffr_poisson_solve(ffr_poisson *s, const double *rhs, double *p,
 /* PoissonSolver::apply_laplacian (PoissonSolver.cpp:22-91) on host buffers. */
 int ffr_poisson_apply(ffr_poisson *s, const double *x, double *ax);
 
+/* The same pressure solve as ffr_poisson_solve_dev, for callers that cannot
+ * allocate device memory when they solve: a process whose GPU memory was
+ * handed to another allocator up front, or a latency-critical loop that
+ * must not take the implicit device synchronisation of cudaMalloc/cudaFree.
+ * No counterpart in the reference.  It allocates nothing: its scratch is one
+ * fixed __device__ array (about 9 MB, held on every GPU that loads the
+ * library until exit) sized for at most FFR_NOALLOC_MAX_CELLS cells and
+ * FFR_NOALLOC_MAX_DIM cells per axis; larger rooms get FFR_ERANGE.  The
+ * caller passes the spacings on the host and the cell types, rhs and
+ * pressure on the device.  All calls on a device share that array, so calls
+ * that overlap on the GPU race; the first call on a device looks the array
+ * up (once per device) and should come before any stream capture. */
+#define FFR_NOALLOC_MAX_CELLS (64 * 64 * 64)
+#define FFR_NOALLOC_MAX_DIM 4096
+int ffr_poisson_solve_noalloc(int nx, int ny, int nz, const double *dxv, const double *dyv,
+                              const double *dzv, const uint8_t *cell_type_dev,
+                              const double *rhs_dev, double *p_dev, int max_iter, double tol,
+                              void *stream, double *residual, int *iterations);
+
 /* ------------------------------------------------------------------ LBM */
 typedef struct ffr_lbm ffr_lbm;
 
