@@ -171,10 +171,8 @@ def run_ours(args, rank: int, world: int, dist):
     ms = ev0.elapsed_time(ev1)
     prof = h.profile_read()
     h.profile(False)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from ffrb.replicas import max_over_ranks
+    ms = max_over_ranks(ms, dist, device="cuda")
     steps_done = len(recs)
     value = world * cells * steps_done / (ms / 1e3)
     peak, peak_kind = measured_peak()
@@ -319,6 +317,66 @@ def config_of(args, room, kind, params):
     return c
 
 
+# ------------------------------------------------ serving / batched rooms
+
+def serving_requests(kind: str, n: int, max_cells: int, max_steps: int):
+    """A bounded sample of the serving stream (Poisson arrivals at 200/s,
+    log-uniform sizes; seed 11) or of the 256 uneven rooms (seed 7, all at
+    t = 0): the first n requests with at most max_cells cells, each capped at
+    max_steps steps."""
+    from ffrb import workloads
+    from ffrb.params import params_from_scene
+    from ffrb.serve import requests_from_configs
+    from ffrb.scene import build_room
+    if kind == "serving":
+        stream = workloads.serving_stream()
+        pick = [rq for rq in stream if np.prod(rq.cfg.room.grid) <= max_cells][:n]
+        return requests_from_configs([rq.cfg for rq in pick], [rq.params for rq in pick],
+                                     [rq.t_arrival - pick[0].t_arrival for rq in pick], max_steps)
+    rooms = [c for c in workloads.batch_rooms() if np.prod(c.room.grid) <= max_cells][:n]
+    return requests_from_configs(rooms, [params_from_scene(c) for c in rooms], [0.0] * len(rooms), max_steps)
+
+
+def run_serving(kind: str, n: int, max_cells: int, max_steps: int, tune: bool = True):
+    import torch
+    from ffrb.serve import Server, Tuner, report, serial_solve
+    reqs = serving_requests(kind, n, max_cells, max_steps)
+    tuner = Tuner()
+    if tune:
+        tuner.tune([r.room for r in reqs], [r.params for r in reqs], steps=4, concurrent=4)
+    free, total = torch.cuda.mem_get_info()
+    srv = Server(mem_budget=int(free * 0.6), max_active=64, tuner=tuner)
+    l0 = __import__("ffrb.capi", fromlist=["x"]).launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        out = srv.run(reqs, realtime=(kind == "serving"))
+    launches = __import__("ffrb.capi", fromlist=["x"]).launch_count() - l0
+    rep = report(out)
+    base = serial_solve(reqs, {"precision": "fp64", "poisson": "cg"})
+    rb = report(base, makespan=max(o.t_done for o in base))
+    rep["serial_fp64_room_solves_per_s"] = rb["room_solves_per_s"]
+    rep["serial_fp64_cell_steps_per_s"] = rb["cell_steps_per_s"]
+    rep["speedup_vs_serial_fp64"] = rep["room_solves_per_s"] / rb["room_solves_per_s"]
+    rep["sample"] = (f"{len(reqs)} requests with <= {max_cells} cells, cap {max_steps} steps"
+                     + (", Poisson arrivals in real time" if kind == "serving" else ", all at t = 0"))
+    rep["schedules"] = tuner.to_json()
+    rep["gpu_launches"] = launches
+    rep["clocks"] = clk.summary()
+    return rep
+
+
+def serving_arm(args):
+    import torch
+    torch.cuda.set_device(0)
+    rep = run_serving(args.workload, args.requests, args.max_cells, args.max_steps)
+    line = {"metric": METRIC, "value": rep["room_solves_per_s"], "unit": "room-solves/s", "n_gpus": 1,
+            "steps": args.max_steps, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": args.workload, "requests": rep["requests"], "max_cells": args.max_cells,
+                       "max_steps": args.max_steps, "precision": "mixed", "poisson": "mgpcg"},
+            "serving": rep, "gpu_launches": rep["gpu_launches"], "clocks": rep["clocks"]}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -331,9 +389,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=lambda s: tuple(int(x) for x in s.split(",")), default=None,
                     help="override the grid (profiling runs on a smaller case)")
+    ap.add_argument("--requests", type=int, default=48, help="serving/batch sample size")
+    ap.add_argument("--max-cells", type=int, default=600_000, help="serving/batch: largest room in the sample")
+    ap.add_argument("--max-steps", type=int, default=40, help="serving/batch: step cap per room")
+    ap.add_argument("--no-serving", action="store_true", help="default run: skip the serving sample")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.workload in ("serving", "batch"):
+        serving_arm(args)
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -358,12 +423,16 @@ def main():
                 gi = None
             cb = cpu_reference(args, kind, room, params, gi)
         dtype = {"fp64": "f64", "mixed": "f32/f64", "fp32": "f32", "fp16": "f16/f32"}.get(args.precision, args.precision)
+        serving = None
+        if not args.no_serving and args.workload == "large_thermal" and world == 1:
+            serving = run_serving("serving", 16, 300_000, 20)
         line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
                 "steps": res["steps"], "warmup": args.warmup, "ms_per_step": res["ms"] / max(1, res["steps"]),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
                 "data": "synthetic", "config": config_of(args, room, kind, params),
                 "roofline": res["roofline"], "cpu_baseline": cb, "e2e": res["e2e"],
-                "gpu_launches": res["launches"], "clocks": res["clocks"], "detail": res["extra"]}
+                "gpu_launches": res["launches"], "clocks": res["clocks"], "detail": res["extra"],
+                "serving": serving}
         print(json.dumps(line))
     if dist:
         dist.barrier()

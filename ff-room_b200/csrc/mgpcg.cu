@@ -673,10 +673,11 @@ unsigned pcg_max_blocks()
     return cap;
 }
 
-int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used)
+int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned override_blocks)
 {
     const unsigned want = (unsigned)std::max<long long>(1, (a.R.n + 255) / 256);
-    const unsigned blocks = std::max(1u, std::min(pcg_max_blocks(), want));
+    unsigned blocks = std::max(1u, std::min(pcg_max_blocks(), want));
+    if (override_blocks) blocks = std::min(blocks, override_blocks);
     if (blocks_used) *blocks_used = blocks;
     FFR_CUDA(cudaMemsetAsync(a.gs, 0, sizeof(GridSync), s));
     void *args[] = {(void *)&a};

@@ -61,7 +61,7 @@ struct PCGArgs {
     int *out_flags;
 };
 // Cooperative launch of the whole preconditioned solve.
-int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used);
+int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned override_blocks = 0);
 unsigned pcg_max_blocks();
 
 }  // namespace ffr

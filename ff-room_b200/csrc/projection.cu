@@ -643,6 +643,15 @@ __global__ void k_finalize(FinArgs A, const double *tpart, StepState *st, ffr_st
     if (conv && st->stop_on_converge) st->halt = 1;
 }
 
+// Start of a queued chunk of steps: results go to slot 0 on, the halt
+// flag of an earlier converged chunk is cleared.
+__global__ void k_begin_chunk(StepState *st, int stop_on_converge)
+{
+    st->ring_slot = 0;
+    st->halt = 0;
+    st->stop_on_converge = stop_on_converge;
+}
+
 #undef UIX
 #undef VIX
 #undef WIX
@@ -794,6 +803,13 @@ struct ffr_fluid {
     bool mg = false, mixed = false;
     MGDev M;
     MGHost mgh;
+    unsigned block_override = 0;   // pressure-solve grid size chosen by the caller (0: automatic)
+    int pending = 0;               // steps queued by ffr_fluid_enqueue and not yet polled
+    cudaEvent_t done_ev = nullptr;
+    cudaGraph_t graph = nullptr;   // one captured step, replayed per step when use_graph
+    cudaGraphExec_t graph_exec = nullptr;
+    bool use_graph = false;
+    unsigned graph_launches = 0;   // kernels in the captured step
 };
 
 namespace {
@@ -834,9 +850,9 @@ int fluid_enqueue_step(ffr_fluid *s)
         pa2.partials = s->partials; pa2.gs = s->gs; pa2.sc = s->sc;
         pa2.max_iter = P.poisson_max_iter; pa2.tol = P.poisson_tol;
         pa2.st = s->st;
-        rc = launch_pcg(pa2, st, nullptr);
+        rc = launch_pcg(pa2, st, nullptr, s->block_override);
     } else {
-        rc = launch_cg(ca, s->cg_blocks, st);
+        rc = launch_cg(ca, s->block_override ? std::min(s->block_override, s->cg_blocks) : s->cg_blocks, st);
     }
     if (rc) return rc;
     s->prof.end(st, 1);
@@ -914,6 +930,10 @@ long long field_len(const ffr_fluid *s, int field)
 
 int pull_state(ffr_fluid *s)
 {
+    if (s->pending) {
+        // a queued chunk: wait for it; its results stay available to poll
+        FFR_CUDA(cudaEventSynchronize(s->done_ev));
+    }
     FFR_CUDA(cudaMemcpyAsync(s->st_host, s->st, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
     FFR_CUDA(cudaStreamSynchronize(s->stream));
     s->prof.collect();
@@ -993,6 +1013,10 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     }
     memset(s->st_host, 0, sizeof(StepState));
     s->prof.reset(FFR_PROF_N);
+    if (cudaEventCreateWithFlags(&s->done_ev, cudaEventDisableTiming) != cudaSuccess) {
+        ffr_fluid_destroy(s);
+        return fail(FFR_ECUDA, "cudaEventCreate");
+    }
     cudaStream_t st = s->stream;
 #define UP(dst, src, cnt)                                                                      \
     do {                                                                                       \
@@ -1025,6 +1049,9 @@ int ffr_fluid_destroy(ffr_fluid *s)
     if (!s) return FFR_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     s->prof.destroy();
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    if (s->done_ev) cudaEventDestroy(s->done_ev);
     s->arena.release();
     if (s->ring_host) cudaFreeHost(s->ring_host);
     if (s->st_host) cudaFreeHost(s->st_host);
@@ -1033,36 +1060,69 @@ int ffr_fluid_destroy(ffr_fluid *s)
     return FFR_OK;
 }
 
+int ffr_fluid_enqueue(ffr_fluid *s, int nsteps, int stop_on_converge)
+{
+    if (!s || nsteps < 0 || nsteps > kRing) return fail(FFR_EINVAL, "bad handle or nsteps (1..1024)");
+    if (s->pending) return fail(FFR_EINVAL, "a queued chunk has not been polled yet");
+    k_begin_chunk<<<1, 1, 0, s->stream>>>(s->st, stop_on_converge ? 1 : 0);
+    FFR_LAUNCHED(1);
+    for (int k = 0; k < nsteps; k++) {
+        if (s->use_graph) {
+            FFR_CUDA(cudaGraphLaunch(s->graph_exec, s->stream));
+            count_launch(s->graph_launches);
+            continue;
+        }
+        int rc = fluid_enqueue_step(s);
+        if (rc) return rc;
+    }
+    if (nsteps > 0)
+        FFR_CUDA(cudaMemcpyAsync(s->ring_host, s->ring, sizeof(ffr_step_result) * nsteps, cudaMemcpyDeviceToHost,
+                                 s->stream));
+    FFR_CUDA(cudaMemcpyAsync(s->st_host, s->st, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaEventRecord(s->done_ev, s->stream));
+    s->pending = nsteps > 0 ? nsteps : -1;
+    return FFR_OK;
+}
+
+int ffr_fluid_poll(ffr_fluid *s, ffr_step_result *results, int max_results, int *nresults, int *ready)
+{
+    if (!s || !ready) return fail(FFR_EINVAL, "NULL argument");
+    if (nresults) *nresults = 0;
+    if (!s->pending) { *ready = 1; return FFR_OK; }
+    cudaError_t e = cudaEventQuery(s->done_ev);
+    if (e == cudaErrorNotReady) { *ready = 0; return FFR_OK; }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventQuery");
+    *ready = 1;
+    s->pending = 0;
+    s->prof.collect();
+    const int got = s->st_host->ring_slot;
+    const int n = std::min(got, std::max(0, max_results));
+    if (results && n > 0) memcpy(results, s->ring_host, sizeof(ffr_step_result) * n);
+    if (nresults) *nresults = n;
+    for (int k = 0; k < got; k++)
+        if (s->ring_host[k].flags & FFR_FLAG_TIMEOUT)
+            return fail(FFR_ETIMEDOUT, "pressure-solve grid barrier timed out");
+    return FFR_OK;
+}
+
 int ffr_fluid_advance(ffr_fluid *s, int nsteps, int stop_on_converge, ffr_step_result *results,
                       int *steps_done)
 {
     if (!s || nsteps < 0) return fail(FFR_EINVAL, "bad handle or nsteps");
+    if (s->pending) return fail(FFR_EINVAL, "a queued chunk has not been polled yet");
     int done_total = 0;
     while (done_total < nsteps) {
         const int chunk = std::min(kRing, nsteps - done_total);
-        StepState hs;
-        FFR_CUDA(cudaMemcpyAsync(&hs, s->st, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
-        FFR_CUDA(cudaStreamSynchronize(s->stream));
-        hs.ring_slot = 0;
-        hs.halt = 0;
-        hs.stop_on_converge = stop_on_converge ? 1 : 0;
-        FFR_CUDA(cudaMemcpyAsync(s->st, &hs, sizeof(StepState), cudaMemcpyHostToDevice, s->stream));
-        for (int k = 0; k < chunk; k++) {
-            int rc = fluid_enqueue_step(s);
-            if (rc) return rc;
-        }
-        FFR_CUDA(cudaMemcpyAsync(s->ring_host, s->ring, sizeof(ffr_step_result) * chunk,
-                                 cudaMemcpyDeviceToHost, s->stream));
-        int rc = pull_state(s);
+        int rc = ffr_fluid_enqueue(s, chunk, stop_on_converge);
         if (rc) return rc;
-        GridSync gsh;
-        FFR_CUDA(cudaMemcpy(&gsh, s->gs, sizeof(GridSync), cudaMemcpyDeviceToHost));
-        const int got = s->st_host->ring_slot;
-        if (results) memcpy(results + done_total, s->ring_host, sizeof(ffr_step_result) * got);
+        FFR_CUDA(cudaEventSynchronize(s->done_ev));
+        int got = 0, ready = 0;
+        rc = ffr_fluid_poll(s, results ? results + done_total : nullptr, chunk, &got, &ready);
+        if (!results) got = s->st_host->ring_slot;
         done_total += got;
-        if (gsh.err) {
+        if (rc) {
             if (steps_done) *steps_done = done_total;
-            return fail(FFR_ETIMEDOUT, "pressure-solve grid barrier timed out");
+            return rc;
         }
         if (got < chunk) break;   // halted on convergence
     }
@@ -1070,20 +1130,61 @@ int ffr_fluid_advance(ffr_fluid *s, int nsteps, int stop_on_converge, ffr_step_r
     return FFR_OK;
 }
 
+int ffr_fluid_set_blocks(ffr_fluid *s, int blocks)
+{
+    if (!s || blocks < 0) return fail(FFR_EINVAL, "bad handle or blocks");
+    if (s->use_graph) return fail(FFR_EINVAL, "set the grid size before capturing the step graph");
+    s->block_override = (unsigned)std::min<long long>(blocks, s->cg_blocks);
+    return FFR_OK;
+}
+
+int ffr_fluid_use_graph(ffr_fluid *s, int enable)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    if (s->pending) return fail(FFR_EINVAL, "a queued chunk has not been polled yet");
+    if (!enable) {
+        s->use_graph = false;
+        return FFR_OK;
+    }
+    if (s->graph_exec) {
+        s->use_graph = true;
+        return FFR_OK;
+    }
+    if (s->prof.on) return fail(FFR_EINVAL, "disable kernel-group timing before capturing the step graph");
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
+    const unsigned long long l0 = ffr_launch_count();
+    FFR_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = fluid_enqueue_step(s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture(step)");
+    e = cudaGraphInstantiate(&s->graph_exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(e, "cudaGraphInstantiate(step)");
+    }
+    s->graph = g;
+    s->graph_launches = (unsigned)(ffr_launch_count() - l0);
+    s->use_graph = true;
+    return FFR_OK;
+}
+
+int ffr_fluid_device_bytes(ffr_fluid *s, size_t *bytes)
+{
+    if (!s || !bytes) return fail(FFR_EINVAL, "NULL argument");
+    *bytes = s->arena.size;
+    return FFR_OK;
+}
+
 int ffr_fluid_step(ffr_fluid *s, ffr_step_result *out)
 {
     if (!s) return fail(FFR_EINVAL, "NULL handle");
-    if (!out) {
-        // no result wanted: queue one step without a host round trip
-        StepState hs;
-        FFR_CUDA(cudaMemcpyAsync(&hs, s->st, sizeof(StepState), cudaMemcpyDeviceToHost, s->stream));
-        FFR_CUDA(cudaStreamSynchronize(s->stream));
-        if (hs.ring_slot >= kRing) {
-            hs.ring_slot = 0;
-            FFR_CUDA(cudaMemcpyAsync(s->st, &hs, sizeof(StepState), cudaMemcpyHostToDevice, s->stream));
-        }
-        return fluid_enqueue_step(s);
-    }
+    ffr_step_result tmp;
+    if (!out) out = &tmp;
     int done = 0;
     int rc = ffr_fluid_advance(s, 1, 0, out, &done);
     if (rc) return rc;

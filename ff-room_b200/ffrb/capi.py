@@ -129,6 +129,11 @@ def lib():
             "ffr_lbm_stream": ([vp, C.POINTER(vp)], C.c_int),
             "ffr_lbm_profile": ([vp, C.c_int], C.c_int),
             "ffr_lbm_profile_read": ([vp, _dp, C.POINTER(C.c_longlong)], C.c_int),
+            "ffr_fluid_enqueue": ([vp, C.c_int, C.c_int], C.c_int),
+            "ffr_fluid_poll": ([vp, C.POINTER(StepResultC), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+            "ffr_fluid_set_blocks": ([vp, C.c_int], C.c_int),
+            "ffr_fluid_device_bytes": ([vp, C.POINTER(C.c_size_t)], C.c_int),
+            "ffr_fluid_use_graph": ([vp, C.c_int], C.c_int),
             "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
                                            C.c_double, vp, _dp, C.POINTER(C.c_int)], C.c_int),
         }
@@ -247,6 +252,32 @@ class FluidHandle:
         done = C.c_int(0)
         check(lib().ffr_fluid_advance(self.h, nsteps, int(stop_on_converge), res, C.byref(done)))
         return [res[i].as_dict() for i in range(done.value)] if want_results else [None] * done.value
+
+    def enqueue(self, nsteps: int, stop_on_converge: bool = True) -> None:
+        check(lib().ffr_fluid_enqueue(self.h, nsteps, int(stop_on_converge)))
+        self._pending = nsteps
+
+    def poll(self):
+        """None while the queued chunk runs, else the list of step results."""
+        n = max(1, getattr(self, "_pending", 0))
+        res = (StepResultC * n)()
+        got, ready = C.c_int(0), C.c_int(0)
+        check(lib().ffr_fluid_poll(self.h, res, n, C.byref(got), C.byref(ready)))
+        if not ready.value:
+            return None
+        self._pending = 0
+        return [res[i].as_dict() for i in range(got.value)]
+
+    def set_blocks(self, blocks: int) -> None:
+        check(lib().ffr_fluid_set_blocks(self.h, int(blocks)))
+
+    def use_graph(self, enable: bool = True) -> None:
+        check(lib().ffr_fluid_use_graph(self.h, int(enable)))
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t(0)
+        check(lib().ffr_fluid_device_bytes(self.h, C.byref(b)))
+        return b.value
 
     def get(self, field: str) -> np.ndarray:
         shape = self.room.shapes()[field]

@@ -1,0 +1,269 @@
+"""Continuous-batching room server.
+
+Room solves arrive over time; each admitted room gets its own device-resident
+solver (an ``ffr_fluid`` handle on its own CUDA stream) and advances in
+chunks of steps queued with ``ffr_fluid_enqueue``.  Between chunks the host
+loop only polls (``ffr_fluid_poll``), so every active room's kernels are in
+flight together and their work overlaps on the GPU.  A room leaves at the
+chunk boundary where it converged (max|du|/dt < tol) or reached its step
+cap; a waiting room is admitted as soon as a slot and enough device memory
+are free (admission by footprint).  Per request the server records arrival,
+admission and completion times; the report gives p50/p99 time-to-converged,
+room-solves/s and cell-steps/s.
+
+Every room's arithmetic depends only on its own inputs and on the pressure-
+solve grid size, which the tuner fixes per size class, so a room gives the
+same result alone and in any mix.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import capi
+from .params import FluidParams
+from .scene import RoomSpec, SceneConfig, build_room
+
+# device bytes per cell of a projection solver (8-byte fields u, v, w and
+# their predicted copies, p, two T buffers, four Krylov vectors, codes) and
+# the multigrid extra (FP32 z and residual, coarse levels, about 1/7 of the
+# fine level at 24 bytes per cell)
+BYTES_PER_CELL = 6 * 8 + 3 * 8 + 4 * 8 + 2 + 3 + 1
+MG_BYTES_PER_CELL = 8 + 4
+
+
+def estimate_bytes(room: RoomSpec, params: FluidParams) -> int:
+    per = BYTES_PER_CELL + (MG_BYTES_PER_CELL if params.poisson == "mgpcg" else 0)
+    return int(room.n_cells * per * 1.05) + (4 << 20)
+
+
+def size_class(cells: int) -> int:
+    return int(math.log2(max(1, cells)))
+
+
+@dataclass
+class Schedule:
+    """How one room runs: pressure-solve grid size (0 = automatic), steps
+    per queued chunk, and whether each step replays a captured CUDA graph."""
+    blocks: int = 0
+    chunk: int = 20
+    graph: bool = False
+
+
+class Tuner:
+    """Picks a Schedule per size class (log2 of the cell count).
+
+    ``tune`` times a few candidate schedules on rooms of the class running
+    side by side and keeps the fastest by aggregate cell-steps/s; untuned
+    classes get the default schedule.  The table can be saved and loaded.
+    """
+
+    CANDIDATES = [Schedule(0, 20, False), Schedule(0, 20, True), Schedule(-2, 20, True),
+                  Schedule(-4, 20, True), Schedule(-8, 20, True)]
+
+    def __init__(self, table: Optional[Dict[int, Schedule]] = None):
+        self.table: Dict[int, Schedule] = dict(table or {})
+
+    def schedule(self, room: RoomSpec) -> Schedule:
+        return self.table.get(size_class(room.n_cells), Schedule())
+
+    @staticmethod
+    def _blocks(sched: Schedule, cap: int) -> int:
+        return sched.blocks if sched.blocks >= 0 else max(1, cap // (-sched.blocks))
+
+    def tune(self, rooms: List[RoomSpec], params: List[FluidParams], steps: int = 6, concurrent: int = 4) -> None:
+        by_class: Dict[int, List[int]] = {}
+        for i, r in enumerate(rooms):
+            by_class.setdefault(size_class(r.n_cells), []).append(i)
+        for cls, idx in by_class.items():
+            if cls in self.table:
+                continue
+            pick = idx[:concurrent]
+            best, best_rate = Schedule(), -1.0
+            for cand in self.CANDIDATES:
+                hs = [capi.FluidHandle(rooms[i], params[i]) for i in pick]
+                try:
+                    cap = max(1, (rooms[pick[0]].n_cells + 255) // 256)
+                    for h in hs:
+                        if cand.blocks:
+                            h.set_blocks(self._blocks(cand, min(cap, 1184)))
+                        if cand.graph:
+                            h.use_graph(True)
+                        h.advance(1)
+                    t0 = time.perf_counter()
+                    for h in hs:
+                        h.enqueue(steps, False)
+                    pend = list(hs)
+                    while pend:
+                        pend = [h for h in pend if h.poll() is None]
+                    dt = time.perf_counter() - t0
+                    rate = sum(rooms[i].n_cells for i in pick) * steps / dt
+                finally:
+                    for h in hs:
+                        h.close()
+                if rate > best_rate:
+                    best, best_rate = cand, rate
+            self.table[cls] = best
+
+    def to_json(self) -> dict:
+        return {str(k): [v.blocks, v.chunk, v.graph] for k, v in self.table.items()}
+
+    @classmethod
+    def from_json(cls, d: dict) -> "Tuner":
+        return cls({int(k): Schedule(int(v[0]), int(v[1]), bool(v[2])) for k, v in d.items()})
+
+
+@dataclass
+class Request:
+    rid: int
+    t_arrival: float            # seconds after the start of the run
+    room: RoomSpec
+    params: FluidParams
+    max_steps: int
+
+
+@dataclass
+class Outcome:
+    rid: int
+    cells: int
+    t_arrival: float
+    t_admit: float
+    t_done: float
+    steps: int
+    converged: bool
+    velocity_change: float
+    fields: Optional[dict] = None
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_arrival
+
+
+class _Active:
+    def __init__(self, req: Request, sched: Schedule, t_admit: float, keep_fields: bool):
+        self.req = req
+        self.sched = sched
+        self.t_admit = t_admit
+        self.keep_fields = keep_fields
+        self.h = capi.FluidHandle(req.room, req.params)
+        cap = max(1, (req.room.n_cells + 255) // 256)
+        if sched.blocks:
+            self.h.set_blocks(Tuner._blocks(sched, min(cap, 1184)))
+        if sched.graph:
+            self.h.use_graph(True)
+        self.bytes = self.h.device_bytes()
+        self.steps = 0
+        self.last = None
+        self.queued = 0
+
+    def launch(self) -> None:
+        self.queued = min(self.sched.chunk, self.req.max_steps - self.steps)
+        self.h.enqueue(self.queued, True)
+
+    def poll(self) -> Optional[bool]:
+        """None while running; True when the room is finished."""
+        res = self.h.poll()
+        if res is None:
+            return None
+        self.steps += len(res)
+        if res:
+            self.last = res[-1]
+        halted = len(res) < self.queued
+        done = halted or self.steps >= self.req.max_steps or (self.last is not None and self.last["converged"])
+        return done
+
+
+class Server:
+    """Continuous-batching server over one GPU."""
+
+    def __init__(self, mem_budget: int, max_active: int = 64, tuner: Optional[Tuner] = None,
+                 keep_fields: bool = False):
+        self.mem_budget = mem_budget
+        self.max_active = max_active
+        self.tuner = tuner or Tuner()
+        self.keep_fields = keep_fields
+
+    def run(self, requests: List[Request], realtime: bool = True) -> List[Outcome]:
+        queue = sorted(requests, key=lambda r: r.t_arrival)
+        active: List[_Active] = []
+        used = 0
+        out: List[Outcome] = []
+        t0 = time.perf_counter()
+        qi = 0
+        while qi < len(queue) or active:
+            now = time.perf_counter() - t0
+            # admission: arrived, a free slot, and room in the memory budget
+            while qi < len(queue) and len(active) < self.max_active:
+                req = queue[qi]
+                if realtime and req.t_arrival > now:
+                    break
+                need = estimate_bytes(req.room, req.params)
+                if active and used + need > self.mem_budget:
+                    break
+                a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields)
+                used += a.bytes
+                a.launch()
+                active.append(a)
+                qi += 1
+            progressed = False
+            still = []
+            for a in active:
+                st = a.poll()
+                if st is None:
+                    still.append(a)
+                    continue
+                progressed = True
+                if st:
+                    fields = {k: a.h.get(k) for k in "uvwpT"} if self.keep_fields else None
+                    t = time.perf_counter() - t0
+                    out.append(Outcome(a.req.rid, a.req.room.n_cells, a.req.t_arrival, a.t_admit, t, a.steps,
+                                       bool(a.last and a.last["converged"]),
+                                       float(a.last["velocity_change"]) if a.last else float("nan"), fields))
+                    used -= a.bytes
+                    a.h.close()
+                else:
+                    a.launch()
+                    still.append(a)
+            active = still
+            if not progressed:
+                time.sleep(0.0002)
+        return out
+
+
+def report(outcomes: List[Outcome], makespan: Optional[float] = None) -> dict:
+    if not outcomes:
+        return {}
+    lat = np.array([o.latency for o in outcomes])
+    span = makespan if makespan is not None else max(o.t_done for o in outcomes) - min(o.t_arrival for o in outcomes)
+    cs = sum(o.cells * o.steps for o in outcomes)
+    return {"requests": len(outcomes), "room_solves_per_s": len(outcomes) / span,
+            "cell_steps_per_s": cs / span, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "converged_fraction": float(np.mean([o.converged for o in outcomes])),
+            "makespan_s": span, "mean_steps": float(np.mean([o.steps for o in outcomes]))}
+
+
+def serial_solve(requests: List[Request], params_override: Optional[dict] = None) -> List[Outcome]:
+    """The same rooms solved one after another, each to convergence or its
+    cap (the serial baseline; with params_override precision="fp64",
+    poisson="cg" it is the plain FP64 GPU solver)."""
+    out = []
+    t0 = time.perf_counter()
+    for req in sorted(requests, key=lambda r: r.t_arrival):
+        p = req.params.with_(**(params_override or {}))
+        ta = time.perf_counter() - t0
+        h = capi.FluidHandle(req.room, p)
+        res = h.advance(req.max_steps, stop_on_converge=True)
+        h.close()
+        out.append(Outcome(req.rid, req.room.n_cells, ta, ta, time.perf_counter() - t0, len(res),
+                           bool(res and res[-1]["converged"]), float(res[-1]["velocity_change"]) if res else float("nan")))
+    return out
+
+
+def requests_from_configs(cfgs: List[SceneConfig], params: List[FluidParams], arrivals: List[float],
+                          max_steps: int) -> List[Request]:
+    return [Request(i, t, build_room(c), p.with_(max_steps=max_steps), max_steps)
+            for i, (c, p, t) in enumerate(zip(cfgs, params, arrivals))]

@@ -162,6 +162,27 @@ int ffr_fluid_step(ffr_fluid *s, ffr_step_result *out);
 int ffr_fluid_advance(ffr_fluid *s, int nsteps, int stop_on_converge,
                       ffr_step_result *results, int *steps_done);
 
+/* Asynchronous form of ffr_fluid_advance for serving many rooms at once
+ * (no counterpart in the reference): queues up to 1024 steps on the handle's
+ * stream and returns at once.  One chunk may be pending per handle. */
+int ffr_fluid_enqueue(ffr_fluid *s, int nsteps, int stop_on_converge);
+/* Non-blocking completion check of the pending chunk: *ready = 0 while it
+ * runs; once done, copies up to max_results step results (the executed
+ * steps only) and sets *ready = 1.  With nothing pending, *ready = 1 and no
+ * results. */
+int ffr_fluid_poll(ffr_fluid *s, ffr_step_result *results, int max_results, int *nresults,
+                   int *ready);
+/* Grid size of the cooperative pressure solve (0 = as large as the room can
+ * use).  Smaller grids let several rooms run side by side. */
+int ffr_fluid_set_blocks(ffr_fluid *s, int blocks);
+/* Device memory the handle holds (one allocation, made at create). */
+int ffr_fluid_device_bytes(ffr_fluid *s, size_t *bytes);
+/* Captures one step (all its kernels) as a CUDA graph and replays it for
+ * every later step of ffr_fluid_enqueue/advance/step (enable = 1), or goes
+ * back to direct launches (0).  The kernels read their per-step state from
+ * device memory, so one captured step is valid for every step. */
+int ffr_fluid_use_graph(ffr_fluid *s, int enable);
+
 /* FluidSolver::compute_divergence_max (FluidSolver.cpp:470-484). */
 int ffr_fluid_divergence_max(ffr_fluid *s, double *out);
 /* FluidSolver::current_step (FluidSolver.hpp:63). */

@@ -1,0 +1,83 @@
+"""Continuous-batching server: results alone vs in the mix, admission by
+memory footprint, asynchronous chunks and CUDA-graph replay.
+
+A room's arithmetic depends only on its own inputs and its pressure-solve
+grid size, so its fields must be bit-identical whether it ran alone or
+side by side with other rooms (max |difference| == 0)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_requests(n=5, steps=12):
+    from ffrb import workloads
+    from ffrb.params import params_from_scene
+    from ffrb.serve import requests_from_configs
+    cfgs = workloads.batch_rooms(n_rooms=n, seed=3, dims=(12, 28), steps=steps)
+    params = [params_from_scene(c) for c in cfgs]
+    return requests_from_configs(cfgs, params, [0.0] * n, steps)
+
+
+def test_results_identical_alone_and_in_mix():
+    from ffrb import capi
+    from ffrb.serve import Server, Tuner, Schedule
+    reqs = _small_requests()
+    alone = {}
+    for rq in reqs:
+        h = capi.FluidHandle(rq.room, rq.params)
+        h.advance(rq.max_steps, stop_on_converge=True)
+        alone[rq.rid] = {k: h.get(k) for k in "uvwpT"}
+        h.close()
+    tuner = Tuner({c: Schedule(0, 5, g) for c, g in zip(range(0, 40), [False, True] * 20)})
+    srv = Server(mem_budget=8 << 30, max_active=8, tuner=tuner, keep_fields=True)
+    out = srv.run(reqs, realtime=False)
+    assert len(out) == len(reqs)
+    for o in out:
+        for k in "uvwpT":
+            assert np.max(np.abs(o.fields[k] - alone[o.rid][k])) == 0.0, (o.rid, k)
+
+
+def test_admission_by_memory_footprint():
+    from ffrb.serve import Server, estimate_bytes
+    reqs = _small_requests(6, steps=6)
+    budget = int(2.5 * max(estimate_bytes(r.room, r.params) for r in reqs))
+    srv = Server(mem_budget=budget, max_active=64)
+    out = srv.run(reqs, realtime=False)
+    assert len(out) == len(reqs)
+    # with room for about two rooms, admissions must wait for completions
+    admits = sorted(o.t_admit for o in out)
+    dones = sorted(o.t_done for o in out)
+    assert admits[-1] >= dones[0]
+
+
+def test_graph_replay_matches_direct_launches():
+    from ffrb import capi
+    from conftest import Golden
+    g = Golden("c1_quick_10")
+    a = capi.FluidHandle(g.room, g.params)
+    ra = a.advance(g.nsteps)
+    b = capi.FluidHandle(g.room, g.params)
+    b.use_graph(True)
+    rb = b.advance(g.nsteps)
+    assert [r["cg_iterations"] for r in ra] == [r["cg_iterations"] for r in rb]
+    for k in "uvwpT":
+        assert np.array_equal(a.get(k), b.get(k))
+
+
+def test_enqueue_poll_stops_on_convergence():
+    from ffrb import capi, workloads
+    from ffrb.params import params_from_scene
+    from ffrb.scene import build_room
+    cfg = workloads.basic_room(steps=1000, tol=1.0)
+    h = capi.FluidHandle(build_room(cfg), params_from_scene(cfg))
+    total = 0
+    while True:
+        h.enqueue(100, True)
+        res = None
+        while res is None:
+            res = h.poll()
+        total += len(res)
+        if len(res) < 100:
+            break
+    assert total == 529
