@@ -7,7 +7,8 @@ loop only polls (``ffr_fluid_poll``), so every active room's kernels are in
 flight together and their work overlaps on the GPU.  A room leaves at the
 chunk boundary where it converged (max|du|/dt < tol) or reached its step
 cap; a waiting room is admitted as soon as a slot and enough device memory
-are free (admission by footprint).  Per request the server records arrival,
+are free (admission by footprint: each room is charged its estimated
+device bytes against the budget until it leaves).  Per request the server records arrival,
 admission and completion times; the report gives p50/p99 time-to-converged,
 room-solves/s and cell-steps/s.
 
@@ -156,6 +157,7 @@ class _Active:
         if sched.graph:
             self.h.use_graph(True)
         self.bytes = self.h.device_bytes()
+        self.charge = self.bytes
         self.steps = 0
         self.last = None
         self.queued = 0
@@ -205,7 +207,8 @@ class Server:
                 if active and used + need > self.mem_budget:
                     break
                 a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields)
-                used += a.bytes
+                a.charge = need
+                used += need
                 a.launch()
                 active.append(a)
                 qi += 1
@@ -223,7 +226,7 @@ class Server:
                     out.append(Outcome(a.req.rid, a.req.room.n_cells, a.req.t_arrival, a.t_admit, t, a.steps,
                                        bool(a.last and a.last["converged"]),
                                        float(a.last["velocity_change"]) if a.last else float("nan"), fields))
-                    used -= a.bytes
+                    used -= a.charge
                     a.h.close()
                 else:
                     a.launch()
