@@ -21,6 +21,8 @@
 // remaining small levels by block 0 alone.
 #include "mgpcg.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 
@@ -382,6 +384,78 @@ __device__ __forceinline__ double face_rhs(const PCGArgs &A, int c, int i, int j
     return A.rhs_factor * div;
 }
 
+// Synchronisation groups of the preconditioned solve.
+//  GridGroup    - every block of a cooperative launch (one room on the whole GPU)
+//  ClusterGroup - the blocks of one thread-block cluster (one room on 1-16 SMs;
+//                 hardware cluster barrier, reductions through distributed
+//                 shared memory), so that many small rooms run side by side.
+struct GridGroup {
+    __device__ static int rank() { return blockIdx.x; }
+    __device__ static int size() { return gridDim.x; }
+    __device__ static void init() {}
+    __device__ static bool sync(const PCGArgs &A) { return grid_barrier(A.gs); }
+    template <int NV>
+    __device__ static bool allreduce(const PCGArgs &A, double (&v)[NV], double *sh)
+    {
+        return grid_allreduce<NV>(A.gs, A.partials, A.sc->red, v, sh);
+    }
+    __device__ static void finish() {}
+};
+
+struct ClusterGroup {
+    __device__ static int rank() { return (int)cooperative_groups::this_cluster().block_rank(); }
+    __device__ static int size() { return (int)cooperative_groups::this_cluster().num_blocks(); }
+    __device__ static double (&slots())[2][4]
+    {
+        __shared__ double s_slot[2][4];
+        return s_slot;
+    }
+    __device__ static int &parity()
+    {
+        __shared__ int s_par;
+        return s_par;
+    }
+    __device__ static void init()
+    {
+        if (threadIdx.x == 0) parity() = 0;
+        __syncthreads();
+    }
+    __device__ static bool sync(const PCGArgs &)
+    {
+        __threadfence();
+        cooperative_groups::this_cluster().sync();
+        return true;
+    }
+    // Deterministic: every block adds the blocks' partials in rank order.
+    // Two slot buffers alternate, so a block never overwrites a slot another
+    // block may still be reading (a cluster barrier separates the reuse).
+    template <int NV>
+    __device__ static bool allreduce(const PCGArgs &, double (&v)[NV], double *sh)
+    {
+        auto cl = cooperative_groups::this_cluster();
+        const int p = parity();
+        for (int a = 0; a < NV; a++) {
+            const double t = block_sum(v[a], sh);
+            if (threadIdx.x == 0) slots()[p][a] = t;
+        }
+        __threadfence();
+        cl.sync();
+        const int nb = (int)cl.num_blocks();
+        for (int a = 0; a < NV; a++) {
+            double tot = 0.0;
+            for (int r = 0; r < nb; r++) tot += *cl.map_shared_rank(&slots()[p][a], r);
+            v[a] = tot;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) parity() = p ^ 1;
+        __syncthreads();
+        return true;
+    }
+    // no block may leave while another can still read its shared memory
+    __device__ static void finish() { cooperative_groups::this_cluster().sync(); }
+};
+
+template <class G>
 __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
 {
     __shared__ double sh[32];
@@ -389,7 +463,8 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
     const RoomDev &R = A.R;
     const MGDev &M = A.M;
     const int n = R.n, ny = R.ny, nz = R.nz;
-    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    G::init();
+    const int t0 = G::rank() * blockDim.x + threadIdx.x, nth = G::size() * blockDim.x;
     float *z = M.lv[0].x;
     double *x = A.x, *r = A.r, *q = A.q;
     int flags = 0, iters = 0;
@@ -422,7 +497,7 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
             M.r32[c] = (float)rv;
             z[c] = zv;
         }
-        const bool ok = grid_allreduce<2>(A.gs, A.partials, A.sc->red, acc, sh);
+        const bool ok = G::template allreduce<2>(A, acc, sh);
         if (!ok) { flags = FFR_FLAG_TIMEOUT; goto finish; }
         const double bnorm = sqrt(acc[0]);
         if (bnorm < 1e-15) goto finish;
@@ -434,23 +509,23 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
             // ---- preconditioner: V-cycle from the red sweep already in z
             for (int l = 0; l < M.nlev_grid && l < M.nlev - 1; l++) {
                 smooth_color<false>(A, l, 1, t0, nth);
-                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
                 restrict_level(A, l, t0, nth);
-                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
             if (M.nlev_grid < M.nlev) {
-                if (blockIdx.x == 0) block_vcycle(A, M.nlev_grid);
-                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                if (G::rank() == 0) block_vcycle(A, M.nlev_grid);
+                if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
             for (int l = min(M.nlev_grid, M.nlev - 1) - 1; l >= 1; l--) {
                 smooth_color<true>(A, l, 1, t0, nth);
-                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
                 smooth_color<false>(A, l, 0, t0, nth);
-                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
             if (M.nlev_grid >= 1 && M.nlev > 1) {
                 smooth_color<true>(A, 0, 1, t0, nth);
-                if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
             // final red sweep of level 0 fused with r.z
             double acc1[1] = {0.0};
@@ -474,7 +549,7 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
                 for (int c = t0; c < n; c += nth)
                     if (active_ct(R.ct[c])) acc1[0] += r[c] * (double)z[c];
             }
-            if (!grid_allreduce<1>(A.gs, A.partials, A.sc->red, acc1, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            if (!G::template allreduce<1>(A, acc1, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             const double rz = acc1[0];
             const double beta = it == 0 ? 0.0 : rz / rz_old;
             rz_old = rz;
@@ -496,7 +571,7 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
                 q[c] = qc;
                 acc2[0] += dc * qc;
             }
-            if (!grid_allreduce<1>(A.gs, A.partials, A.sc->red, acc2, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            if (!G::template allreduce<1>(A, acc2, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             { double *tmp = dold; dold = dnew; dnew = tmp; }   // dold = current direction
             pending = false;
             const double dq = acc2[0];
@@ -528,7 +603,7 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
                 }
                 z[c] = zv;
             }
-            if (!grid_allreduce<1>(A.gs, A.partials, A.sc->red, acc3, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+            if (!G::template allreduce<1>(A, acc3, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             pending = true;
             res = sqrt(acc3[0]) / bnorm;
             iters = it + 1;
@@ -539,7 +614,7 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
         if (pending)
             for (int c = t0; c < n; c += nth)
                 if (active_ct(R.ct[c])) x[c] = fma(alpha, dold[c], x[c]);
-        if (!grid_barrier(A.gs)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+        if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
         // OUTFLOW rows by back-substitution in the reference's own row form
         for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
             const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
@@ -555,7 +630,8 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
         }
     }
 finish:
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    G::finish();
+    if (G::rank() == 0 && threadIdx.x == 0) {
         if (A.out_res) *A.out_res = res;
         if (A.out_iters) *A.out_iters = iters;
         if (A.out_flags) *A.out_flags = flags;
@@ -663,7 +739,7 @@ unsigned pcg_max_blocks()
     static unsigned cap = 0;
     if (!cap) {
         int per_sm = 0, dev = 0, sms = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<GridGroup>, 256, 0);
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (per_sm <= 0) per_sm = 1;
@@ -671,6 +747,30 @@ unsigned pcg_max_blocks()
         cap = (unsigned)(per_sm * sms);
     }
     return cap;
+}
+
+int launch_pcg_cluster(const PCGArgs &a, cudaStream_t s, int ctas)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        FFR_CUDA(cudaFuncSetAttribute(k_pcg<ClusterGroup>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr_set = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    FFR_CUDA(cudaLaunchKernelEx(&cfg, k_pcg<ClusterGroup>, a));
+    count_launch(1);
+    return FFR_OK;
 }
 
 int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned override_blocks)
@@ -681,7 +781,7 @@ int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned
     if (blocks_used) *blocks_used = blocks;
     FFR_CUDA(cudaMemsetAsync(a.gs, 0, sizeof(GridSync), s));
     void *args[] = {(void *)&a};
-    FFR_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg, dim3(blocks), dim3(256), args, 0, s));
+    FFR_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg<GridGroup>, dim3(blocks), dim3(256), args, 0, s));
     count_launch(1);
     return FFR_OK;
 }

@@ -63,5 +63,7 @@ struct PCGArgs {
 // Cooperative launch of the whole preconditioned solve.
 int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned override_blocks = 0);
 unsigned pcg_max_blocks();
+// One thread-block cluster of `ctas` blocks (1..16) solves the room.
+int launch_pcg_cluster(const PCGArgs &a, cudaStream_t s, int ctas);
 
 }  // namespace ffr

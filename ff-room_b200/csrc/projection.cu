@@ -804,6 +804,7 @@ struct ffr_fluid {
     MGDev M;
     MGHost mgh;
     unsigned block_override = 0;   // pressure-solve grid size chosen by the caller (0: automatic)
+    int cluster_ctas = 0;          // >0: the multigrid solve runs in one cluster of that many blocks
     int pending = 0;               // steps queued by ffr_fluid_enqueue and not yet polled
     cudaEvent_t done_ev = nullptr;
     cudaGraph_t graph = nullptr;   // one captured step, replayed per step when use_graph
@@ -850,7 +851,8 @@ int fluid_enqueue_step(ffr_fluid *s)
         pa2.partials = s->partials; pa2.gs = s->gs; pa2.sc = s->sc;
         pa2.max_iter = P.poisson_max_iter; pa2.tol = P.poisson_tol;
         pa2.st = s->st;
-        rc = launch_pcg(pa2, st, nullptr, s->block_override);
+        rc = s->cluster_ctas > 0 ? launch_pcg_cluster(pa2, st, s->cluster_ctas)
+                                 : launch_pcg(pa2, st, nullptr, s->block_override);
     } else {
         rc = launch_cg(ca, s->block_override ? std::min(s->block_override, s->cg_blocks) : s->cg_blocks, st);
     }
@@ -1135,6 +1137,15 @@ int ffr_fluid_set_blocks(ffr_fluid *s, int blocks)
     if (!s || blocks < 0) return fail(FFR_EINVAL, "bad handle or blocks");
     if (s->use_graph) return fail(FFR_EINVAL, "set the grid size before capturing the step graph");
     s->block_override = (unsigned)std::min<long long>(blocks, s->cg_blocks);
+    return FFR_OK;
+}
+
+int ffr_fluid_set_cluster(ffr_fluid *s, int ctas)
+{
+    if (!s || ctas < 0 || ctas > 16) return fail(FFR_EINVAL, "bad handle or cluster size (0..16)");
+    if (ctas > 0 && !s->mg) return fail(FFR_ENOTSUP, "cluster schedule is built for the multigrid solve only");
+    if (s->use_graph) return fail(FFR_EINVAL, "set the schedule before capturing the step graph");
+    s->cluster_ctas = ctas;
     return FFR_OK;
 }
 

@@ -134,6 +134,7 @@ def lib():
             "ffr_fluid_set_blocks": ([vp, C.c_int], C.c_int),
             "ffr_fluid_device_bytes": ([vp, C.POINTER(C.c_size_t)], C.c_int),
             "ffr_fluid_use_graph": ([vp, C.c_int], C.c_int),
+            "ffr_fluid_set_cluster": ([vp, C.c_int], C.c_int),
             "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
                                            C.c_double, vp, _dp, C.POINTER(C.c_int)], C.c_int),
         }
@@ -270,6 +271,9 @@ class FluidHandle:
 
     def set_blocks(self, blocks: int) -> None:
         check(lib().ffr_fluid_set_blocks(self.h, int(blocks)))
+
+    def set_cluster(self, ctas: int) -> None:
+        check(lib().ffr_fluid_set_cluster(self.h, int(ctas)))
 
     def use_graph(self, enable: bool = True) -> None:
         check(lib().ffr_fluid_use_graph(self.h, int(enable)))

@@ -48,11 +48,14 @@ def size_class(cells: int) -> int:
 
 @dataclass
 class Schedule:
-    """How one room runs: pressure-solve grid size (0 = automatic), steps
-    per queued chunk, and whether each step replays a captured CUDA graph."""
+    """How one room runs: the pressure-solve grid (0 = the whole GPU, -k = a
+    k-th of its co-resident blocks), or one thread-block cluster of
+    `cluster` blocks (1..16, then `blocks` is unused); steps per queued
+    chunk; whether each step replays a captured CUDA graph."""
     blocks: int = 0
     chunk: int = 20
     graph: bool = False
+    cluster: int = 0
 
 
 class Tuner:
@@ -63,8 +66,9 @@ class Tuner:
     classes get the default schedule.  The table can be saved and loaded.
     """
 
-    CANDIDATES = [Schedule(0, 20, False), Schedule(0, 20, True), Schedule(-2, 20, True),
-                  Schedule(-4, 20, True), Schedule(-8, 20, True)]
+    CANDIDATES = [Schedule(0, 20, False), Schedule(0, 20, True), Schedule(-4, 20, True),
+                  Schedule(-8, 20, True), Schedule(0, 20, True, 16), Schedule(0, 20, True, 8),
+                  Schedule(0, 20, True, 4)]
 
     def __init__(self, table: Optional[Dict[int, Schedule]] = None):
         self.table: Dict[int, Schedule] = dict(table or {})
@@ -88,12 +92,8 @@ class Tuner:
             for cand in self.CANDIDATES:
                 hs = [capi.FluidHandle(rooms[i], params[i]) for i in pick]
                 try:
-                    cap = max(1, (rooms[pick[0]].n_cells + 255) // 256)
-                    for h in hs:
-                        if cand.blocks:
-                            h.set_blocks(self._blocks(cand, min(cap, 1184)))
-                        if cand.graph:
-                            h.use_graph(True)
+                    for h, i in zip(hs, pick):
+                        apply_schedule(h, cand, rooms[i], params[i])
                         h.advance(1)
                     t0 = time.perf_counter()
                     for h in hs:
@@ -111,11 +111,24 @@ class Tuner:
             self.table[cls] = best
 
     def to_json(self) -> dict:
-        return {str(k): [v.blocks, v.chunk, v.graph] for k, v in self.table.items()}
+        return {str(k): [v.blocks, v.chunk, v.graph, v.cluster] for k, v in self.table.items()}
 
     @classmethod
     def from_json(cls, d: dict) -> "Tuner":
-        return cls({int(k): Schedule(int(v[0]), int(v[1]), bool(v[2])) for k, v in d.items()})
+        return cls({int(k): Schedule(int(v[0]), int(v[1]), bool(v[2]), int(v[3]) if len(v) > 3 else 0)
+                    for k, v in d.items()})
+
+
+def apply_schedule(h, sched: Schedule, room: RoomSpec, params: FluidParams) -> None:
+    """Configures a fresh handle for `sched` (cluster schedules need the
+    multigrid solve; other rooms keep the grid schedule)."""
+    cap = max(1, (room.n_cells + 255) // 256)
+    if sched.cluster and params.poisson == "mgpcg":
+        h.set_cluster(sched.cluster)
+    elif sched.blocks:
+        h.set_blocks(Tuner._blocks(sched, min(cap, 1184)))
+    if sched.graph:
+        h.use_graph(True)
 
 
 @dataclass
@@ -151,11 +164,7 @@ class _Active:
         self.t_admit = t_admit
         self.keep_fields = keep_fields
         self.h = capi.FluidHandle(req.room, req.params)
-        cap = max(1, (req.room.n_cells + 255) // 256)
-        if sched.blocks:
-            self.h.set_blocks(Tuner._blocks(sched, min(cap, 1184)))
-        if sched.graph:
-            self.h.use_graph(True)
+        apply_schedule(self.h, sched, req.room, req.params)
         self.bytes = self.h.device_bytes()
         self.charge = self.bytes
         self.steps = 0

@@ -175,6 +175,11 @@ int ffr_fluid_poll(ffr_fluid *s, ffr_step_result *results, int max_results, int 
 /* Grid size of the cooperative pressure solve (0 = as large as the room can
  * use).  Smaller grids let several rooms run side by side. */
 int ffr_fluid_set_blocks(ffr_fluid *s, int blocks);
+/* Runs the multigrid-preconditioned pressure solve of this room in one
+ * thread-block cluster of `ctas` blocks (1..16; 0 = the whole GPU through a
+ * cooperative launch).  Many small rooms then advance side by side, each on
+ * its own SMs, synchronising through the hardware cluster barrier. */
+int ffr_fluid_set_cluster(ffr_fluid *s, int ctas);
 /* Device memory the handle holds (one allocation, made at create). */
 int ffr_fluid_device_bytes(ffr_fluid *s, size_t *bytes);
 /* Captures one step (all its kernels) as a CUDA graph and replays it for

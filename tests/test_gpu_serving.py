@@ -19,18 +19,29 @@ def _small_requests(n=5, steps=12):
     return requests_from_configs(cfgs, params, [0.0] * n, steps)
 
 
+def _tuner():
+    from ffrb.serve import Schedule, Tuner
+    return Tuner({c: Schedule(0, 5, c % 2 == 1, 8 if c % 3 == 0 else 0) for c in range(0, 40)})
+
+
+_TUNER = None
+
+
 def test_results_identical_alone_and_in_mix():
+    global _TUNER
+    _TUNER = _tuner()
     from ffrb import capi
     from ffrb.serve import Server, Tuner, Schedule
     reqs = _small_requests()
+    from ffrb.serve import apply_schedule
     alone = {}
     for rq in reqs:
         h = capi.FluidHandle(rq.room, rq.params)
+        apply_schedule(h, _TUNER.schedule(rq.room), rq.room, rq.params)
         h.advance(rq.max_steps, stop_on_converge=True)
         alone[rq.rid] = {k: h.get(k) for k in "uvwpT"}
         h.close()
-    tuner = Tuner({c: Schedule(0, 5, g) for c, g in zip(range(0, 40), [False, True] * 20)})
-    srv = Server(mem_budget=8 << 30, max_active=8, tuner=tuner, keep_fields=True)
+    srv = Server(mem_budget=8 << 30, max_active=8, tuner=_TUNER, keep_fields=True)
     out = srv.run(reqs, realtime=False)
     assert len(out) == len(reqs)
     for o in out:
@@ -81,3 +92,21 @@ def test_enqueue_poll_stops_on_convergence():
         if len(res) < 100:
             break
     assert total == 529
+
+
+@pytest.mark.parametrize("ctas", [4, 16])
+def test_cluster_schedule_tracks_reference(ctas):
+    """The multigrid solve inside one thread-block cluster gives the same
+    answer as the reference within the mixed-precision bound (1e-4)."""
+    from ffrb import capi
+    from conftest import Golden, rel_err
+    for name in ("c1_quick_10", "vent_quick_10", "oblique_stretch_10"):
+        g = Golden(name)
+        h = capi.FluidHandle(g.room, g.params.with_(poisson="mgpcg", precision="mixed"))
+        h.set_cluster(ctas)
+        h.use_graph(True)
+        recs = h.advance(g.nsteps)
+        assert len(recs) == g.nsteps
+        for k in "uvwpT":
+            assert rel_err(h.get(k), g.fields[k]) <= 1e-4, (name, k)
+        h.close()
