@@ -8,7 +8,11 @@ than L2 (u, v, w, p, T alone are 315 MB), so no flush is needed.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload large_thermal|lbm_room|basic_room]
-                    [--precision fp64|mixed]
+                    [--precision mixed|fp64|fp32|fp16] [--graph 1|0]
+
+The default is the mixed-precision path (FP32 increments and FP32 multigrid
+preconditioner, FP64 state and outer CG), each step replayed from a CUDA
+graph; --precision fp64 runs the reference's method (plain FP64 CG).
 
 Under torchrun every rank runs its own replica of the room on its GPU (rooms
 are independent: weak scaling, no collective on the data path); the time is
@@ -37,7 +41,7 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
 
 # Algorithmic bytes per cell (FP64 fields, 2-byte stencil code, 1-byte
-# masks/codes); see DESIGN.md for the derivation.
+# masks/codes): each array a kernel must read or write, counted once.
 CG_INIT_B = 50.0       # read u*,v*,w* + code, write r, d, x
 CG_ITER_B = 74.0       # phase A (r, d_old, x, code -> d, Ad, x) + phase B (r, Ad -> r)
 CG_FINAL_B = 24.0      # x += alpha d
@@ -151,12 +155,16 @@ def run_ours(args, rank: int, world: int, dist):
     cells = room.n_cells
     if kind == "fluid":
         h = capi.FluidHandle(room, params)
+        h.set_split(args.split)
+        if args.graph:
+            h.use_graph(True)
     else:
         h = capi.LbmHandle(room, params["tau"], args.steps + args.warmup, 0.0, params["dt"], params["storage"])
     h.advance(args.warmup)
     h.synchronize()
     stream = torch.cuda.ExternalStream(h.stream())
-    h.profile(True)
+    if not (kind == "fluid" and args.graph):
+        h.profile(True)
     l0 = capi.launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
@@ -181,20 +189,36 @@ def run_ours(args, rank: int, world: int, dist):
         mg = params.poisson == "mgpcg"
         if mg:
             bytes_cg = sum(cells * (PCG_ONCE_B + PCG_ITER_B * it) for it in iters)
-            kname = "k_pcg (persistent multigrid-preconditioned CG)"
+            split = args.split == 1 or (args.graph and args.split != 0)
+            kname = ("multigrid-preconditioned CG, one kernel per pass (k_sp_*)" +
+                     (" in a CUDA graph" if args.graph else ", host-paced") if split
+                     else "k_pcg (persistent multigrid-preconditioned CG)")
         else:
             bytes_cg = sum(cells * (CG_INIT_B + CG_ITER_B * it + CG_FINAL_B) for it in iters)
             kname = "k_cg (persistent pressure CG)"
-        t_cg = prof["pressure"][0] / 1e3
-        achieved = bytes_cg / t_cg / 1e9
-        launches_cg = max(1, prof["pressure"][1])
+        if args.graph:
+            # events cannot bracket kernels inside a replayed step graph: time
+            # the pressure solve of the last step again from its own graph
+            ms_solve, it_solve = h.time_pressure(3)
+            bytes_one = cells * ((PCG_ONCE_B + PCG_ITER_B * it_solve) if mg else
+                                 (CG_INIT_B + CG_ITER_B * it_solve + CG_FINAL_B))
+            achieved = bytes_one / (ms_solve / 1e3) / 1e9
+            launches_cg = 1
+            bytes_cg = bytes_one
+            prof = {"pressure_estimate": (ms_solve * steps_done, steps_done)}
+        else:
+            t_cg = prof["pressure"][0] / 1e3
+            achieved = bytes_cg / t_cg / 1e9
+            launches_cg = max(1, prof["pressure"][1])
         roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "traffic": load_traffic("k_pcg_per_launch" if mg else "k_cg_per_launch"),
                 "algorithmic_bytes_per_launch": bytes_cg / launches_cg,
-                "share_of_step": round(prof["pressure"][0] / ms, 4),
+                "share_of_step": round(prof.get("pressure", prof.get("pressure_estimate"))[0] / ms, 4),
                 "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}
+        if args.graph:
+            roof["timing"] = "pressure solve of the last step re-run 3x from its own CUDA graph"
         extra = {"cg_iterations_mean": float(np.mean(iters)), "velocity_change_last": recs[-1]["velocity_change"]}
     else:
         b = LBM_STEP_B[params["storage"]] * cells * steps_done
@@ -224,6 +248,9 @@ def run_e2e(args, kind, room, params):
     t0 = time.perf_counter()
     if kind == "fluid":
         h = capi.FluidHandle(room, params, init)
+        h.set_split(args.split)
+        if args.graph:
+            h.use_graph(True)
         recs = h.advance(args.steps)
         out = {k: h.get(k) for k in "uvwpT"}
     else:
@@ -241,9 +268,11 @@ def run_e2e(args, kind, room, params):
 
 # ------------------------------------------------- CPU reference timing
 
-def cpu_reference(args, kind, room, params, gpu_iters=None, max_seconds=30.0):
-    """The reference solver (oracle/_ref driver, OpenMP on all host threads)
-    on a bounded sample of the workload."""
+def cpu_reference(kind, room, params, nsteps=20, budget_s=15.0):
+    """The reference solver (oracle/_ref driver) on a bounded sample of the
+    workload: the first steps of the room from rest, stopping at the first
+    step that starts after `budget_s` seconds of stepping; the value is the
+    cells divided by the median wall time of one step() call."""
     import oracle as orc
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
@@ -252,29 +281,23 @@ def cpu_reference(args, kind, room, params, gpu_iters=None, max_seconds=30.0):
         return None
     drv = orc.RefDriver()
     if kind == "lbm":
-        t0 = time.perf_counter()
-        drv.lbm_run(room, params["tau"], params["dt"], 0.0, 2)
-        t = time.perf_counter() - t0
-        return {"value": cells * 2 / t, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
-                "sample": f"2 LBM steps of the {room.nx}x{room.ny}x{room.nz} lattice (the reference LBM has no OpenMP)"}
-    # projection: time one step at two CG caps, fit the per-iteration cost,
-    # extrapolate to the iteration count the same CG needs per step
-    caps = (20, 60)
-    ts = []
-    for cap in caps:
-        p = params.with_(poisson_max_iter=cap, precision="fp64", poisson="cg")
-        t0 = time.perf_counter()
-        drv.fluid_run(room, p, 1, use_openmp=True)
-        ts.append(time.perf_counter() - t0)
-    per_it = max(1e-9, (ts[1] - ts[0]) / (caps[1] - caps[0]))
-    base = max(0.0, ts[0] - caps[0] * per_it)
-    n_it = gpu_iters if gpu_iters else caps[1]
-    t_step = base + per_it * n_it
-    return {"value": cells / t_step, "unit": "cell-steps/s", "cores": threads, "kind": "reference",
-            "sample": (f"1 step of the {room.nx}x{room.ny}x{room.nz} room through the reference FluidSolver "
-                       f"(OpenMP, {threads} threads) at CG caps {caps[0]} and {caps[1]}; fixed cost "
-                       f"{base:.3f} s + {per_it * 1e3:.2f} ms/CG iteration, extrapolated to {n_it:.0f} "
-                       "iterations per step (the plain FP64 CG count of this room)")}
+        _, recs = drv.lbm_run(room, params["tau"], params["dt"], 0.0, 2)
+        t = statistics.median(r.seconds for r in recs)
+        return {"value": cells / t, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
+                "sample": f"{len(recs)} LBM steps of the {room.nx}x{room.ny}x{room.nz} lattice, median step() "
+                          "time (the reference LBM has no OpenMP)"}
+    # the reference has one pressure method: plain FP64 CG, to the same
+    # tolerance and iteration cap
+    p = params.with_(precision="fp64", poisson="cg")
+    _, _, recs = drv.fluid_run(room, p, nsteps, use_openmp=True, time_budget=budget_s)
+    t = statistics.median(r.seconds for r in recs)
+    its = [r.cg_iterations for r in recs]
+    return {"value": cells / t, "unit": "cell-steps/s", "cores": threads, "kind": "reference",
+            "sample": (f"first {len(recs)} steps of the {room.nx}x{room.ny}x{room.nz} room from rest through the "
+                       f"reference FluidSolver (OpenMP, {threads} threads; plain FP64 CG to tol "
+                       f"{params.poisson_tol:g}, {min(its)}-{max(its)} iterations per step); median step() "
+                       f"wall time {t * 1e3:.1f} ms"),
+            "cg_iterations": its}
 
 
 def reference_arm(args):
@@ -288,13 +311,11 @@ def reference_arm(args):
     if not orc.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}))
         return
-    gpu_iters = args.ref_cg_iters
-    samples = []
-    for _ in range(max(1, args.steps)):
-        cb = cpu_reference(args, kind, room, params, gpu_iters)
-        samples.append(cb["value"])
-    v = statistics.median(samples)
-    cb["value"] = v
+    # one run of up to warmup + steps reference steps, bounded in time so the
+    # whole arm ends within a few minutes
+    cb = cpu_reference(kind, room, params, nsteps=max(1, args.warmup + args.steps),
+                       budget_s=float(args.ref_budget))
+    v = cb["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": room.n_cells / v * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -384,8 +405,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large_thermal")
-    ap.add_argument("--precision", default="fp64")
-    ap.add_argument("--ref-cg-iters", type=float, default=None)
+    ap.add_argument("--precision", default="mixed")
+    ap.add_argument("--ref-budget", type=float, default=90.0,
+                    help="--impl reference: seconds of reference stepping after which the sample stops")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=lambda s: tuple(int(x) for x in s.split(",")), default=None,
                     help="override the grid (profiling runs on a smaller case)")
@@ -393,6 +415,11 @@ def main():
     ap.add_argument("--max-cells", type=int, default=600_000, help="serving/batch: largest room in the sample")
     ap.add_argument("--max-steps", type=int, default=40, help="serving/batch: step cap per room")
     ap.add_argument("--no-serving", action="store_true", help="default run: skip the serving sample")
+    ap.add_argument("--graph", type=int, default=1,
+                    help="replay each step as a CUDA graph (the multigrid solve then runs one kernel per pass)")
+    ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],
+                    help="multigrid schedule: 1 one kernel per pass (host-paced outside graphs), "
+                         "0 one persistent kernel, -1 split in graphs only")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
@@ -418,10 +445,7 @@ def main():
         kind, cfg, room, params = make_workload(args.workload, args.precision, args.grid)
         cb = None
         if not args.no_cpu_baseline:
-            gi = res["extra"].get("cg_iterations_mean")
-            if kind == "fluid" and params.precision != "fp64":
-                gi = None
-            cb = cpu_reference(args, kind, room, params, gi)
+            cb = cpu_reference(kind, room, params)
         dtype = {"fp64": "f64", "mixed": "f32/f64", "fp32": "f32", "fp16": "f16/f32"}.get(args.precision, args.precision)
         serving = None
         if not args.no_serving and args.workload == "large_thermal" and world == 1:

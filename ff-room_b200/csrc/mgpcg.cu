@@ -455,50 +455,154 @@ struct ClusterGroup {
     __device__ static void finish() { cooperative_groups::this_cluster().sync(); }
 };
 
+// ---- the passes of one preconditioned-CG solve, each over the cells
+// start, start + stride, ... (a persistent group or one item per thread)
+
+// rhs, r = V*rhs on the unknowns, x = 0, d = 0, z = red sweep from 0;
+// acc = {||b||^2 over non-SOLID rows, ||b||^2 over unknowns}
+__device__ __forceinline__ void pass_init(const PCGArgs &A, int start, int stride, double (&acc)[2])
+{
+    const RoomDev &R = A.R;
+    const MGDev &M = A.M;
+    float *z = M.lv[0].x;
+    for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        const uint8_t t = R.ct[c];
+        A.x[c] = 0.0;
+        A.da[c] = 0.0;
+        A.db[c] = 0.0;
+        double rv = 0.0;
+        float zv = 0.0f;
+        if (t != CT_SOLID) {
+            const double b = face_rhs(A, c, i, j, k);
+            acc[0] += b * b;
+            if (active_ct(t)) {
+                acc[1] += b * b;
+                rv = b * (M.vol_x[i] * M.vol_y[j] * M.vol_z[k]);
+                if (((i + j + k) & 1) == 0) {
+                    float tt[6], D;
+                    fine_coefs(M, R.sc[c], i, j, k, tt, D);
+                    zv = (float)rv / D;
+                }
+            }
+        }
+        A.r[c] = rv;
+        M.r32[c] = (float)rv;
+        z[c] = zv;
+    }
+}
+
+// the last red sweep of level 0 fused with r.z
+__device__ __forceinline__ void pass_redpost_dot(const PCGArgs &A, int start, int stride, double &acc)
+{
+    const RoomDev &R = A.R;
+    const MGDev &M = A.M;
+    float *z = M.lv[0].x;
+    const MGLevel &L0 = M.lv[0];
+    const bool sweep = M.nlev_grid >= 1;
+    for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        if (!active_ct(R.ct[c])) continue;
+        float zc;
+        if (sweep && ((i + j + k) & 1) == 0) {
+            float D;
+            const float s = fine_nbsum<false>(R, M, L0, L0, c, i, j, k, D);
+            zc = (M.r32[c] + s) / D;
+            z[c] = zc;
+        } else {
+            zc = z[c];
+        }
+        acc += A.r[c] * (double)zc;
+    }
+}
+
+// d = z + beta d_old, the deferred x += alpha_prev d_old, q = M d; acc = d.q
+__device__ __forceinline__ void pass_direction(const PCGArgs &A, int start, int stride, double beta,
+                                               double alpha_prev, bool update_x, const double *__restrict__ dold,
+                                               double *__restrict__ dnew, double &acc)
+{
+    const RoomDev &R = A.R;
+    const MGDev &M = A.M;
+    const float *z = M.lv[0].x;
+    for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        if (!active_ct(R.ct[c])) { dnew[c] = 0.0; A.q[c] = 0.0; continue; }
+        const double dp = dold[c];
+        const double dc = fma(beta, dp, (double)z[c]);
+        if (update_x) A.x[c] = fma(alpha_prev, dp, A.x[c]);
+        dnew[c] = dc;
+        const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
+        const double row = ref_row(R, R.sc[c], i, j, k, dc,
+                                   [&](int o) { return fma(beta, dold[c + o], (double)z[c + o]); });
+        const double qc = vol * row;
+        A.q[c] = qc;
+        acc += dc * qc;
+    }
+}
+
+// r -= alpha q, acc = ||b - A x||^2 (unscaled), the red sweep of the next z
+__device__ __forceinline__ void pass_residual(const PCGArgs &A, int start, int stride, double alpha, double &acc)
+{
+    const RoomDev &R = A.R;
+    const MGDev &M = A.M;
+    float *z = M.lv[0].x;
+    for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        if (!active_ct(R.ct[c])) continue;
+        const double rv = A.r[c] - alpha * A.q[c];
+        A.r[c] = rv;
+        const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
+        const double ru = rv / vol;
+        acc += ru * ru;
+        const float r32 = (float)rv;
+        M.r32[c] = r32;
+        float zv = 0.0f;
+        if (((i + j + k) & 1) == 0) {
+            float tt[6], D;
+            fine_coefs(M, R.sc[c], i, j, k, tt, D);
+            zv = r32 / D;
+        }
+        z[c] = zv;
+    }
+}
+
+__device__ __forceinline__ void pass_final_x(const PCGArgs &A, int start, int stride, double alpha,
+                                             const double *__restrict__ d)
+{
+    for (int c = start; c < A.R.n; c += stride)
+        if (active_ct(A.R.ct[c])) A.x[c] = fma(alpha, d[c], A.x[c]);
+}
+
+// OUTFLOW rows by back-substitution in the reference's own row form:
+// diag*x_o - sum_in s*x_nb = b  ->  x_o = (b + sum) / diag
+__device__ __forceinline__ void pass_backsub(const PCGArgs &A, int start, int stride)
+{
+    const RoomDev &R = A.R;
+    double *x = A.x;
+    for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        if (R.ct[c] != CT_OUTFLOW) continue;
+        const double b = face_rhs(A, c, i, j, k);
+        const double row0 = ref_row(R, R.sc[c], i, j, k, 0.0, [&](int o) { return x[c + o]; });
+        const double diag = ref_row(R, R.sc[c], i, j, k, 1.0, [&](int) { return 0.0; });
+        x[c] = (b - row0) / diag;
+    }
+}
+
 template <class G>
 __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
 {
     __shared__ double sh[32];
     if (A.st && A.st->halt) return;
-    const RoomDev &R = A.R;
     const MGDev &M = A.M;
-    const int n = R.n, ny = R.ny, nz = R.nz;
     G::init();
     const int t0 = G::rank() * blockDim.x + threadIdx.x, nth = G::size() * blockDim.x;
-    float *z = M.lv[0].x;
-    double *x = A.x, *r = A.r, *q = A.q;
     int flags = 0, iters = 0;
     double res = 0.0;
-
-    // phase 0: rhs, r = V*rhs on the unknowns, x = 0, z = red sweep from 0
     {
         double acc[2] = {0.0, 0.0};
-        for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
-            const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-            const uint8_t t = R.ct[c];
-            x[c] = 0.0;
-            A.da[c] = 0.0;
-            double rv = 0.0;
-            float zv = 0.0f;
-            if (t != CT_SOLID) {
-                const double b = face_rhs(A, c, i, j, k);
-                acc[0] += b * b;
-                if (active_ct(t)) {
-                    acc[1] += b * b;
-                    rv = b * (M.vol_x[i] * M.vol_y[j] * M.vol_z[k]);
-                    if (((i + j + k) & 1) == 0) {
-                        float tt[6], D;
-                        fine_coefs(M, R.sc[c], i, j, k, tt, D);
-                        zv = (float)rv / D;
-                    }
-                }
-            }
-            r[c] = rv;
-            M.r32[c] = (float)rv;
-            z[c] = zv;
-        }
-        const bool ok = G::template allreduce<2>(A, acc, sh);
-        if (!ok) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+        pass_init(A, t0, nth, acc);
+        if (!G::template allreduce<2>(A, acc, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
         const double bnorm = sqrt(acc[0]);
         if (bnorm < 1e-15) goto finish;
 
@@ -527,50 +631,15 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
                 smooth_color<true>(A, 0, 1, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
-            // final red sweep of level 0 fused with r.z
             double acc1[1] = {0.0};
-            if (M.nlev_grid >= 1) {
-                const MGLevel &L0 = M.lv[0];
-                for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
-                    const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-                    if (!active_ct(R.ct[c])) continue;
-                    float zc;
-                    if (((i + j + k) & 1) == 0) {
-                        float D;
-                        const float s = fine_nbsum<false>(R, M, L0, L0, c, i, j, k, D);
-                        zc = (M.r32[c] + s) / D;
-                        z[c] = zc;
-                    } else {
-                        zc = z[c];
-                    }
-                    acc1[0] += r[c] * (double)zc;
-                }
-            } else {
-                for (int c = t0; c < n; c += nth)
-                    if (active_ct(R.ct[c])) acc1[0] += r[c] * (double)z[c];
-            }
+            pass_redpost_dot(A, t0, nth, acc1[0]);
             if (!G::template allreduce<1>(A, acc1, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             const double rz = acc1[0];
             const double beta = it == 0 ? 0.0 : rz / rz_old;
             rz_old = rz;
 
-            // ---- phase A: d = z + beta d_old, deferred x update, q = M d
             double acc2[1] = {0.0};
-            for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
-                const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-                const uint8_t t = R.ct[c];
-                if (!active_ct(t)) { dnew[c] = 0.0; q[c] = 0.0; continue; }
-                const double dp = dold[c];
-                const double dc = fma(beta, dp, (double)z[c]);
-                if (it > 0) x[c] = fma(alpha_prev, dp, x[c]);
-                dnew[c] = dc;
-                const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
-                const double row = ref_row(R, R.sc[c], i, j, k, dc,
-                                           [&](int o) { return fma(beta, dold[c + o], (double)z[c + o]); });
-                const double qc = vol * row;
-                q[c] = qc;
-                acc2[0] += dc * qc;
-            }
+            pass_direction(A, t0, nth, beta, alpha_prev, it > 0, dold, dnew, acc2[0]);
             if (!G::template allreduce<1>(A, acc2, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             { double *tmp = dold; dold = dnew; dnew = tmp; }   // dold = current direction
             pending = false;
@@ -582,27 +651,8 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
             }
             alpha = rz / dq;
 
-            // ---- phase B: r -= alpha q, ||b - A x||^2, red sweep of the next z
             double acc3[1] = {0.0};
-            for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
-                const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-                const uint8_t t = R.ct[c];
-                if (!active_ct(t)) continue;
-                const double rv = r[c] - alpha * q[c];
-                r[c] = rv;
-                const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
-                const double ru = rv / vol;
-                acc3[0] += ru * ru;
-                const float r32 = (float)rv;
-                M.r32[c] = r32;
-                float zv = 0.0f;
-                if (((i + j + k) & 1) == 0) {
-                    float tt[6], D;
-                    fine_coefs(M, R.sc[c], i, j, k, tt, D);
-                    zv = r32 / D;
-                }
-                z[c] = zv;
-            }
+            pass_residual(A, t0, nth, alpha, acc3[0]);
             if (!G::template allreduce<1>(A, acc3, sh)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             pending = true;
             res = sqrt(acc3[0]) / bnorm;
@@ -611,23 +661,9 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
             if (iters >= A.max_iter) { flags |= FFR_FLAG_CG_MAXITER; break; }
             alpha_prev = alpha;
         }
-        if (pending)
-            for (int c = t0; c < n; c += nth)
-                if (active_ct(R.ct[c])) x[c] = fma(alpha, dold[c], x[c]);
+        if (pending) pass_final_x(A, t0, nth, alpha, dold);
         if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
-        // OUTFLOW rows by back-substitution in the reference's own row form
-        for (Walk wk(t0, nth, ny, nz, n); wk.ok(); wk.next()) {
-            const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-            if (R.ct[c] != CT_OUTFLOW) continue;
-            const double b = face_rhs(A, c, i, j, k);
-            const double nx_ = R.nx;
-            (void)nx_;
-            // row: diag*x_o - sum_in s*x_nb = b  ->  x_o = (b + sum) / diag
-            const double row0 = ref_row(R, R.sc[c], i, j, k, 0.0, [&](int o) { return x[c + o]; });
-            // ref_row(.., xc = 0) = -sum s*x_nb; the diagonal is ref_row at unit xc with zero neighbours
-            const double diag = ref_row(R, R.sc[c], i, j, k, 1.0, [&](int) { return 0.0; });
-            x[c] = (b - row0) / diag;
-        }
+        pass_backsub(A, t0, nth);
     }
 finish:
     G::finish();
@@ -639,6 +675,181 @@ finish:
             A.st->pres = res;
             A.st->iters = iters;
             atomicOr(&A.st->flags, flags);
+        }
+    }
+}
+
+// ================================================================ split
+//
+// The same solve as k_pcg, one plain kernel per pass (one item per thread,
+// full occupancy), for replay inside a CUDA graph.  Loop control lives on the
+// device: the scalars sit in SplitState, every reducing kernel's last block
+// (ticket counter) adds the block partials in block order and updates them,
+// and the residual kernel sets the conditional handle of the graph's WHILE
+// node to 0 once the solve is over.
+
+constexpr int kSplitMaxBlocks = 2368;   // 16 per SM
+
+struct SplitState {
+    double bnorm, rz_old, beta, alpha, alpha_prev, res;
+    int it, done, pending, flags, dpar, pad;
+    unsigned ticket;
+    unsigned pad2;
+};
+
+// Block partials -> partials[blockIdx.x]; true in the one block that arrives
+// last, which then holds the grid total (summed in block order) in v.
+template <int NV>
+__device__ bool last_block_total(double (&v)[NV], double *partials, unsigned *ticket, double *sh)
+{
+    __shared__ int s_last;
+    for (int a = 0; a < NV; a++) {
+        const double t = block_sum(v[a], sh);
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NV + a] = t;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    for (int a = 0; a < NV; a++) {
+        double t = 0.0;
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += __ldcg(&partials[(size_t)b * NV + a]);
+        v[a] = block_sum(t, sh);
+    }
+    if (threadIdx.x == 0) *ticket = 0;
+    return true;
+}
+
+__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
+
+// use_cond: the kernel runs inside a graph with a WHILE node on `cond`
+// (otherwise the host paces the iterations and reads ss->done).
+__global__ void __launch_bounds__(256) k_sp_init(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
+                                                 int use_cond)
+{
+    __shared__ double sh[32];
+    if (A.st && A.st->halt) {
+        if (gtid() == 0) {
+            ss->done = 1;
+            if (use_cond) cudaGraphSetConditional(cond, 0);
+        }
+        return;
+    }
+    double acc[2] = {0.0, 0.0};
+    pass_init(A, gtid(), gthreads(), acc);
+    if (last_block_total<2>(acc, A.partials, &ss->ticket, sh) && threadIdx.x == 0) {
+        ss->bnorm = sqrt(acc[0]);
+        ss->it = 0;
+        ss->pending = 0;
+        ss->flags = 0;
+        ss->dpar = 0;
+        ss->res = 0.0;
+        ss->alpha = ss->alpha_prev = ss->rz_old = ss->beta = 0.0;
+        ss->done = ss->bnorm < 1e-15;
+        if (use_cond) cudaGraphSetConditional(cond, ss->done ? 0u : 1u);
+    }
+}
+
+template <bool CORR>
+__global__ void __launch_bounds__(256) k_sp_smooth(PCGArgs A, const SplitState *ss, int l, int color)
+{
+    if (ss->done) return;
+    smooth_color<CORR>(A, l, color, gtid(), gthreads());
+}
+
+__global__ void __launch_bounds__(256) k_sp_restrict(PCGArgs A, const SplitState *ss, int l)
+{
+    if (ss->done) return;
+    restrict_level(A, l, gtid(), gthreads());
+}
+
+__global__ void __launch_bounds__(1024) k_sp_coarse(PCGArgs A, const SplitState *ss, int lo)
+{
+    if (ss->done) return;
+    block_vcycle(A, lo);
+}
+
+__global__ void __launch_bounds__(256) k_sp_redpost(PCGArgs A, SplitState *ss)
+{
+    __shared__ double sh[32];
+    if (ss->done) return;
+    double acc[1] = {0.0};
+    pass_redpost_dot(A, gtid(), gthreads(), acc[0]);
+    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh) && threadIdx.x == 0) {
+        ss->beta = ss->it == 0 ? 0.0 : acc[0] / ss->rz_old;
+        ss->rz_old = acc[0];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sp_direction(PCGArgs A, SplitState *ss)
+{
+    __shared__ double sh[32];
+    if (ss->done) return;
+    const double *dold = ss->dpar ? A.db : A.da;
+    double *dnew = ss->dpar ? A.da : A.db;
+    double acc[1] = {0.0};
+    pass_direction(A, gtid(), gthreads(), ss->beta, ss->alpha_prev, ss->it > 0, dold, dnew, acc[0]);
+    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh) && threadIdx.x == 0) {
+        ss->dpar ^= 1;            // the new direction is current from here on
+        ss->pending = 0;
+        if (fabs(acc[0]) < 1e-30) {
+            ss->flags |= FFR_FLAG_CG_BREAKDOWN;
+            ss->done = 1;
+        } else {
+            ss->alpha = ss->rz_old / acc[0];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sp_residual(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
+                                                     int use_cond)
+{
+    __shared__ double sh[32];
+    if (ss->done) {
+        if (use_cond && gtid() == 0) cudaGraphSetConditional(cond, 0);
+        return;
+    }
+    double acc[1] = {0.0};
+    pass_residual(A, gtid(), gthreads(), ss->alpha, acc[0]);
+    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh) && threadIdx.x == 0) {
+        ss->pending = 1;
+        ss->res = sqrt(acc[0]) / ss->bnorm;
+        ss->it += 1;
+        if (ss->res < A.tol) {
+            ss->done = 1;
+        } else if (ss->it >= A.max_iter) {
+            ss->flags |= FFR_FLAG_CG_MAXITER;
+            ss->done = 1;
+        } else {
+            ss->alpha_prev = ss->alpha;
+        }
+        if (use_cond) cudaGraphSetConditional(cond, ss->done ? 0u : 1u);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sp_final(PCGArgs A, const SplitState *ss)
+{
+    if (A.st && A.st->halt) return;
+    if (ss->pending) pass_final_x(A, gtid(), gthreads(), ss->alpha, ss->dpar ? A.db : A.da);
+}
+
+__global__ void __launch_bounds__(256) k_sp_backsub(PCGArgs A, const SplitState *ss)
+{
+    if (A.st && A.st->halt) return;
+    pass_backsub(A, gtid(), gthreads());
+    if (gtid() == 0) {
+        const int iters = ss->bnorm < 1e-15 ? 0 : ss->it;
+        if (A.out_res) *A.out_res = ss->res;
+        if (A.out_iters) *A.out_iters = iters;
+        if (A.out_flags) *A.out_flags = ss->flags;
+        if (A.st) {
+            A.st->pres = ss->res;
+            A.st->iters = iters;
+            atomicOr(&A.st->flags, ss->flags);
         }
     }
 }
@@ -783,6 +994,190 @@ int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned
     void *args[] = {(void *)&a};
     FFR_CUDA(cudaLaunchCooperativeKernel((void *)k_pcg<GridGroup>, dim3(blocks), dim3(256), args, 0, s));
     count_launch(1);
+    return FFR_OK;
+}
+
+}  // namespace ffr
+
+namespace ffr {
+
+namespace {
+
+unsigned split_blocks_pairs(const MGDev &M, int l)
+{
+    const MGLevel &L = M.lv[l];
+    const long long w = (long long)L.nx * L.ny * ((L.nz + 1) / 2);
+    return (unsigned)std::max<long long>(1, (w + 255) / 256);
+}
+
+unsigned split_blocks_cells(const MGDev &M, int l)
+{
+    return (unsigned)std::max<long long>(1, ((long long)M.lv[l].n + 255) / 256);
+}
+
+// Kernels one PCG iteration of the split solve runs (the body below).
+unsigned split_body_kernels(const MGDev &M)
+{
+    const int down = std::min(M.nlev_grid, M.nlev - 1);
+    unsigned k = 2u * (unsigned)std::max(0, down);            // smooth + restrict per level
+    if (M.nlev_grid < M.nlev) k += 1;                         // one-block coarse V-cycle
+    k += 2u * (unsigned)std::max(0, down - 1);                // levels down-1 .. 1 post-smooth
+    if (M.nlev_grid >= 1 && M.nlev > 1) k += 1;               // level-0 black post-smooth
+    return k + 3;                                             // red post + r.z, direction, residual
+}
+
+// Launches one PCG iteration of the split solve on stream bs.
+int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraphConditionalHandle cond,
+                    int use_cond)
+{
+    const MGDev &M = a.M;
+    const unsigned cb = (unsigned)std::min<long long>((a.R.n + 255) / 256, kSplitMaxBlocks);
+    int rc = FFR_OK;
+    auto chk = [&]() {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess && rc == FFR_OK) rc = cuda_fail(e, "split kernel launch");
+        count_launch(1);
+    };
+    for (int l = 0; l < M.nlev_grid && l < M.nlev - 1; l++) {
+        k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
+        chk();
+        k_sp_restrict<<<split_blocks_cells(M, l + 1), 256, 0, bs>>>(a, ss, l);
+        chk();
+    }
+    if (M.nlev_grid < M.nlev) {
+        k_sp_coarse<<<1, 1024, 0, bs>>>(a, ss, M.nlev_grid);
+        chk();
+    }
+    for (int l = std::min(M.nlev_grid, M.nlev - 1) - 1; l >= 1; l--) {
+        k_sp_smooth<true><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
+        chk();
+        k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 0);
+        chk();
+    }
+    if (M.nlev_grid >= 1 && M.nlev > 1) {
+        k_sp_smooth<true><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 1);
+        chk();
+    }
+    k_sp_redpost<<<cb, 256, 0, bs>>>(a, ss);
+    chk();
+    k_sp_direction<<<cb, 256, 0, bs>>>(a, ss);
+    chk();
+    k_sp_residual<<<cb, 256, 0, bs>>>(a, ss, cond, use_cond);
+    chk();
+    return rc;
+}
+
+}  // namespace
+
+size_t split_state_bytes() { return sizeof(SplitState); }
+
+int capture_split_pcg(const PCGArgs &a, void *ss_dev, cudaStream_t s, cudaStream_t bs, unsigned *body_kernels)
+{
+    SplitState *ss = static_cast<SplitState *>(ss_dev);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    FFR_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return fail(FFR_EINVAL, "split solve must be captured");
+    cudaGraphConditionalHandle cond;
+    FFR_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+    const unsigned cb = (unsigned)std::min<long long>((a.R.n + 255) / 256, kSplitMaxBlocks);
+    k_sp_init<<<cb, 256, 0, s>>>(a, ss, cond, 1);
+    FFR_LAUNCHED(1);
+    FFR_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    FFR_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    FFR_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+
+    // one PCG iteration, replayed while the residual kernel keeps the condition set
+    FFR_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    int rc = split_iteration(a, ss, bs, cond, 1);
+    if (body_kernels) *body_kernels = split_body_kernels(a.M);
+    cudaGraph_t body_out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(bs, &body_out);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture(PCG iteration)");
+
+    k_sp_final<<<cb, 256, 0, s>>>(a, ss);
+    FFR_LAUNCHED(1);
+    k_sp_backsub<<<cb, 256, 0, s>>>(a, ss);
+    FFR_LAUNCHED(1);
+    return FFR_OK;
+}
+
+
+int SplitHost::init()
+{
+    if (flags) return FFR_OK;
+    FFR_CUDA(cudaHostAlloc(&flags, 4 * sizeof(int), cudaHostAllocDefault));
+    for (int k = 0; k < 2; k++) FFR_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+    return FFR_OK;
+}
+
+void SplitHost::release()
+{
+    if (flags) cudaFreeHost(flags);
+    for (int k = 0; k < 2; k++)
+        if (ev[k]) cudaEventDestroy(ev[k]);
+    flags = nullptr;
+    ev[0] = ev[1] = nullptr;
+}
+
+int launch_split_pcg(const PCGArgs &a, void *ss_dev, cudaStream_t s, SplitHost &h)
+{
+    int rc = h.init();
+    if (rc) return rc;
+    SplitState *ss = static_cast<SplitState *>(ss_dev);
+    const unsigned cb = (unsigned)std::min<long long>((a.R.n + 255) / 256, kSplitMaxBlocks);
+    k_sp_init<<<cb, 256, 0, s>>>(a, ss, cudaGraphConditionalHandle{}, 0);
+    FFR_LAUNCHED(1);
+    const int max_iter = std::max(0, a.max_iter);
+    int launched = 0;
+    // queue `nb` iterations, then a copy of (it, done) into slot `slot`
+    auto batch = [&](int nb, int slot) -> int {
+        for (int k = 0; k < nb; k++) {
+            int r = split_iteration(a, ss, s, cudaGraphConditionalHandle{}, 0);
+            if (r) return r;
+        }
+        launched += nb;
+        FFR_CUDA(cudaMemcpyAsync(h.flags + 2 * slot, &ss->it, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        FFR_CUDA(cudaEventRecord(h.ev[slot], s));
+        return FFR_OK;
+    };
+    // the first batch is the previous solve's count less two; then batches of
+    // two, each queued before the host waits on the one before it, so the
+    // stream never drains while the host decides
+    int slot = 0;
+    if (max_iter > 0) {
+        rc = batch(std::min(max_iter, std::max(1, h.last_iters - 2)), slot);
+        if (rc) return rc;
+        while (true) {
+            const int prev = slot;
+            const bool more = launched < max_iter;
+            if (more) {
+                slot ^= 1;
+                rc = batch(std::min(2, max_iter - launched), slot);
+                if (rc) return rc;
+            }
+            FFR_CUDA(cudaEventSynchronize(h.ev[prev]));
+            if (h.flags[2 * prev + 1]) {
+                h.last_iters = h.flags[2 * prev];
+                break;
+            }
+            if (!more) break;
+        }
+    }
+    k_sp_final<<<cb, 256, 0, s>>>(a, ss);
+    FFR_LAUNCHED(1);
+    k_sp_backsub<<<cb, 256, 0, s>>>(a, ss);
+    FFR_LAUNCHED(1);
     return FFR_OK;
 }
 

@@ -65,5 +65,30 @@ int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned
 unsigned pcg_max_blocks();
 // One thread-block cluster of `ctas` blocks (1..16) solves the room.
 int launch_pcg_cluster(const PCGArgs &a, cudaStream_t s, int ctas);
+// The same solve as one plain kernel per pass, recorded into the graph being
+// captured on `s` with a conditional WHILE node around one iteration (the
+// iteration body is captured on `bs`).  ss_dev holds split_state_bytes()
+// of zeroed device memory; the partials array needs 2 * 2368 doubles.
+size_t split_state_bytes();
+// Records the split solve into the stream capture in progress on `s`; the
+// loop body (one PCG iteration) is captured on `bs`.  *body_kernels receives
+// the number of kernels one iteration runs.
+int capture_split_pcg(const PCGArgs &a, void *ss_dev, cudaStream_t s, cudaStream_t bs,
+                      unsigned *body_kernels = nullptr);
+// Host-side state of the eagerly launched split solve: a pinned copy of the
+// device iteration count and done flag per batch, and the iteration count of
+// the previous solve (the size of the first batch).
+struct SplitHost {
+    int *flags = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int last_iters = 8;
+    int init();
+    void release();
+};
+// The split solve launched kernel by kernel outside any graph.  The host
+// queues iterations in batches and stops at the first batch whose copy of
+// the done flag reads set; kernels queued past convergence return at once.
+// Blocks the calling thread until the solve's last batch has been queued.
+int launch_split_pcg(const PCGArgs &a, void *ss_dev, cudaStream_t s, SplitHost &h);
 
 }  // namespace ffr

@@ -811,9 +811,51 @@ struct ffr_fluid {
     cudaGraphExec_t graph_exec = nullptr;
     bool use_graph = false;
     unsigned graph_launches = 0;   // kernels in the captured step
+    unsigned split_body = 0;       // kernels per PCG iteration of a captured split solve
+    bool capturing_split = false;  // the multigrid solve is being recorded in its split form
+    void *split_state = nullptr;   // device SplitState of the split solve
+    cudaStream_t body_stream = nullptr;
+    int split_mode = -1;           // multigrid schedule: -1 split in graphs only, 0 never, 1 always
+    SplitHost split_host;          // host pacing of the eager split solve
 };
 
 namespace {
+
+// Pressure solve of the current step on stream st.  capture: 2 = the stream
+// is being captured and the multigrid solve is recorded in its split form
+// (WHILE node); 1 = the stream is being captured (no host-paced launches);
+// 0 = eager launch.
+int enqueue_pressure(ffr_fluid *s, cudaStream_t st, int capture, unsigned *body_kernels)
+{
+    const ffr_fluid_params &P = s->prm;
+    if (s->mg) {
+        PCGArgs pa2{};
+        pa2.R = s->R; pa2.M = s->M;
+        pa2.us = s->us; pa2.vs = s->vs; pa2.ws = s->ws;
+        pa2.rhs_factor = -(P.rho / P.dt);
+        pa2.from_faces = 1;
+        pa2.x = s->p; pa2.r = s->r; pa2.da = s->da; pa2.db = s->db; pa2.q = s->ad;
+        pa2.partials = s->partials; pa2.gs = s->gs; pa2.sc = s->sc;
+        pa2.max_iter = P.poisson_max_iter; pa2.tol = P.poisson_tol;
+        pa2.st = s->st;
+        const bool plain_grid = s->cluster_ctas == 0 && s->block_override == 0;
+        if (capture == 2) return capture_split_pcg(pa2, s->split_state, st, s->body_stream, body_kernels);
+        if (capture == 0 && plain_grid && s->split_mode == 1)
+            return launch_split_pcg(pa2, s->split_state, st, s->split_host);
+        return s->cluster_ctas > 0 ? launch_pcg_cluster(pa2, st, s->cluster_ctas)
+                                   : launch_pcg(pa2, st, nullptr, s->block_override);
+    }
+    CGArgs ca{};
+    ca.R = s->R;
+    ca.us = s->us; ca.vs = s->vs; ca.ws = s->ws;
+    ca.rhs_factor = -(P.rho / P.dt);
+    ca.from_faces = 1;
+    ca.x = s->p; ca.r = s->r; ca.da = s->da; ca.db = s->db; ca.ad = s->ad;
+    ca.partials = s->partials; ca.gs = s->gs; ca.sc = s->sc;
+    ca.max_iter = P.poisson_max_iter; ca.tol = P.poisson_tol;
+    ca.st = s->st;
+    return launch_cg(ca, s->block_override ? std::min(s->block_override, s->cg_blocks) : s->cg_blocks, st);
+}
 
 int fluid_enqueue_step(ffr_fluid *s)
 {
@@ -830,32 +872,8 @@ int fluid_enqueue_step(ffr_fluid *s)
                                                                  s->vs, s->ws, s->st);
     FFR_LAUNCHED(1);
     s->prof.end(st, 1);
-    CGArgs ca{};
-    ca.R = s->R;
-    ca.us = s->us; ca.vs = s->vs; ca.ws = s->ws;
-    ca.rhs_factor = -(P.rho / P.dt);
-    ca.from_faces = 1;
-    ca.x = s->p; ca.r = s->r; ca.da = s->da; ca.db = s->db; ca.ad = s->ad;
-    ca.partials = s->partials; ca.gs = s->gs; ca.sc = s->sc;
-    ca.max_iter = P.poisson_max_iter; ca.tol = P.poisson_tol;
-    ca.st = s->st;
     s->prof.begin(FFR_PROF_PRESSURE, st);
-    int rc;
-    if (s->mg) {
-        PCGArgs pa2{};
-        pa2.R = s->R; pa2.M = s->M;
-        pa2.us = s->us; pa2.vs = s->vs; pa2.ws = s->ws;
-        pa2.rhs_factor = -(P.rho / P.dt);
-        pa2.from_faces = 1;
-        pa2.x = s->p; pa2.r = s->r; pa2.da = s->da; pa2.db = s->db; pa2.q = s->ad;
-        pa2.partials = s->partials; pa2.gs = s->gs; pa2.sc = s->sc;
-        pa2.max_iter = P.poisson_max_iter; pa2.tol = P.poisson_tol;
-        pa2.st = s->st;
-        rc = s->cluster_ctas > 0 ? launch_pcg_cluster(pa2, st, s->cluster_ctas)
-                                 : launch_pcg(pa2, st, nullptr, s->block_override);
-    } else {
-        rc = launch_cg(ca, s->block_override ? std::min(s->block_override, s->cg_blocks) : s->cg_blocks, st);
-    }
+    int rc = enqueue_pressure(s, st, s->capturing_split ? 2 : 0, &s->split_body);
     if (rc) return rc;
     s->prof.end(st, 1);
     CorrArgs co{P.dt / P.rho};
@@ -977,7 +995,8 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     s->blocks_cells = stream_blocks(g.n);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = tables_bytes(s->room) + 2 * (al(8 * g.nu) + al(8 * g.nv) + al(8 * g.nw)) +
-                         7 * al(8 * g.n) + al(8 * s->cg_blocks * 4) + al(8 * s->blocks_cells) +
+                         7 * al(8 * g.n) + al(8 * std::max<size_t>(s->cg_blocks * 4, 2 * 2368)) + al(8 * s->blocks_cells) +
+                         al(256) +
                          al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
                          al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (s->mg ? mg_bytes(s->room, s->mgh) : 0);
     rc = s->arena.alloc(bytes);
@@ -993,8 +1012,9 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     s->p = a.take<double>(g.n); s->T0 = a.take<double>(g.n); s->T1 = a.take<double>(g.n);
     s->r = a.take<double>(g.n); s->da = a.take<double>(g.n); s->db = a.take<double>(g.n);
     s->ad = a.take<double>(g.n);
-    s->partials = a.take<double>(s->cg_blocks * 4);
+    s->partials = a.take<double>(std::max<size_t>(s->cg_blocks * 4, 2 * 2368));
     s->tpart = a.take<double>(s->blocks_cells);
+    s->split_state = a.take<char>(256);
     s->gs = a.take<GridSync>(1);
     s->sc = a.take<CGScalars>(1);
     s->st = a.take<StepState>(1);
@@ -1031,6 +1051,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     UP(s->p, init ? init->p : nullptr, g.n);
 #undef UP
     FFR_CUDA(cudaMemsetAsync(s->st, 0, sizeof(StepState), st));
+    FFR_CUDA(cudaMemsetAsync(s->split_state, 0, 256, st));
     k_fill<<<stream_blocks(g.n), kThreads, 0, st>>>(s->T0, (int)g.n, params->T_initial);
     FFR_LAUNCHED(1);
     if (params->thermal) {
@@ -1053,6 +1074,8 @@ int ffr_fluid_destroy(ffr_fluid *s)
     s->prof.destroy();
     if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
     if (s->graph) cudaGraphDestroy(s->graph);
+    if (s->body_stream) cudaStreamDestroy(s->body_stream);
+    s->split_host.release();
     if (s->done_ev) cudaEventDestroy(s->done_ev);
     s->arena.release();
     if (s->ring_host) cudaFreeHost(s->ring_host);
@@ -1098,6 +1121,10 @@ int ffr_fluid_poll(ffr_fluid *s, ffr_step_result *results, int max_results, int 
     s->pending = 0;
     s->prof.collect();
     const int got = s->st_host->ring_slot;
+    // the graph launch counted the loop body once; it ran once per iteration
+    if (s->use_graph && s->split_body)
+        for (int k = 0; k < got; k++)
+            count_launch(s->split_body * (unsigned)std::max(0, s->ring_host[k].cg_iterations - 1));
     const int n = std::min(got, std::max(0, max_results));
     if (results && n > 0) memcpy(results, s->ring_host, sizeof(ffr_step_result) * n);
     if (nresults) *nresults = n;
@@ -1149,6 +1176,77 @@ int ffr_fluid_set_cluster(ffr_fluid *s, int ctas)
     return FFR_OK;
 }
 
+int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *iterations)
+{
+    if (!s || nrep <= 0 || !ms_per_solve) return fail(FFR_EINVAL, "bad arguments");
+    if (s->pending) return fail(FFR_EINVAL, "a queued chunk has not been polled yet");
+    cudaStream_t st = s->stream;
+    FFR_CUDA(cudaStreamSynchronize(st));
+    // the solve reads the predicted faces and halt flag of the last step
+    StepState hs;
+    FFR_CUDA(cudaMemcpy(&hs, s->st, sizeof(StepState), cudaMemcpyDeviceToHost));
+    const int halt = hs.halt;
+    hs.halt = 0;
+    FFR_CUDA(cudaMemcpy(s->st, &hs, sizeof(StepState), cudaMemcpyHostToDevice));
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    unsigned body = 0;
+    const unsigned long long l0 = ffr_launch_count();
+    unsigned captured = 0;
+    int rc = FFR_OK;
+    if (s->use_graph) {
+        // the same form the step graph holds
+        const bool split = s->mg && s->cluster_ctas == 0 && s->block_override == 0 && s->split_mode != 0;
+        if (split && !s->body_stream) FFR_CUDA(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
+        FFR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+        rc = enqueue_pressure(s, st, split ? 2 : 1, &body);
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture(pressure)");
+        e = cudaGraphInstantiate(&ge, g, 0);
+        if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(e, "cudaGraphInstantiate(pressure)"); }
+        captured = (unsigned)(ffr_launch_count() - l0);
+    }
+    cudaEvent_t a, b;
+    FFR_CUDA(cudaEventCreate(&a));
+    FFR_CUDA(cudaEventCreate(&b));
+    for (int r = 0; r <= nrep && rc == FFR_OK; r++) {   // r = 0 is the warm-up
+        if (r == 1) FFR_CUDA(cudaEventRecord(a, st));
+        if (ge) {
+            FFR_CUDA(cudaGraphLaunch(ge, st));
+        } else {
+            rc = enqueue_pressure(s, st, 0, nullptr);
+        }
+    }
+    FFR_CUDA(cudaEventRecord(b, st));
+    FFR_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    FFR_CUDA(cudaEventElapsedTime(&ms, a, b));
+    *ms_per_solve = ms / nrep;
+    FFR_CUDA(cudaMemcpy(&hs, s->st, sizeof(StepState), cudaMemcpyDeviceToHost));
+    if (iterations) *iterations = hs.iters;
+    hs.halt = halt;
+    FFR_CUDA(cudaMemcpy(s->st, &hs, sizeof(StepState), cudaMemcpyHostToDevice));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ge) {
+        cudaGraphExecDestroy(ge);
+        cudaGraphDestroy(g);
+        // replays ran the loop body once per iteration; the capture counted it once
+        const unsigned per_solve = captured + body * (unsigned)std::max(0, hs.iters - 1);
+        count_launch(per_solve * (unsigned)(nrep + 1) - captured);
+    }
+    return rc;
+}
+
+int ffr_fluid_set_split(ffr_fluid *s, int mode)
+{
+    if (!s || mode < -1 || mode > 1) return fail(FFR_EINVAL, "bad handle or mode (-1, 0, 1)");
+    if (s->use_graph || s->graph_exec) return fail(FFR_EINVAL, "choose the schedule before capturing the step graph");
+    s->split_mode = mode;
+    return FFR_OK;
+}
+
 int ffr_fluid_use_graph(ffr_fluid *s, int enable)
 {
     if (!s) return fail(FFR_EINVAL, "NULL handle");
@@ -1164,10 +1262,14 @@ int ffr_fluid_use_graph(ffr_fluid *s, int enable)
     if (s->prof.on) return fail(FFR_EINVAL, "disable kernel-group timing before capturing the step graph");
     FFR_CUDA(cudaStreamSynchronize(s->stream));
     const unsigned long long l0 = ffr_launch_count();
-    FFR_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    s->capturing_split = s->mg && s->cluster_ctas == 0 && s->block_override == 0 && s->split_mode != 0;
+    if (s->capturing_split && !s->body_stream)
+        FFR_CUDA(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
+    FFR_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeRelaxed));
     int rc = fluid_enqueue_step(s);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    s->capturing_split = false;
     if (rc) {
         if (g) cudaGraphDestroy(g);
         return rc;

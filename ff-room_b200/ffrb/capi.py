@@ -135,6 +135,8 @@ def lib():
             "ffr_fluid_device_bytes": ([vp, C.POINTER(C.c_size_t)], C.c_int),
             "ffr_fluid_use_graph": ([vp, C.c_int], C.c_int),
             "ffr_fluid_set_cluster": ([vp, C.c_int], C.c_int),
+            "ffr_fluid_time_pressure": ([vp, C.c_int, _dp, C.POINTER(C.c_int)], C.c_int),
+            "ffr_fluid_set_split": ([vp, C.c_int], C.c_int),
             "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
                                            C.c_double, vp, _dp, C.POINTER(C.c_int)], C.c_int),
         }
@@ -271,6 +273,16 @@ class FluidHandle:
 
     def set_blocks(self, blocks: int) -> None:
         check(lib().ffr_fluid_set_blocks(self.h, int(blocks)))
+
+    def set_split(self, mode: int) -> None:
+        """Multigrid schedule: 1 kernel per pass, 0 persistent, -1 split in graphs."""
+        check(lib().ffr_fluid_set_split(self.h, mode))
+
+    def time_pressure(self, nrep: int = 3):
+        """(mean ms per pressure solve, iterations) re-solving the last step."""
+        ms, it = C.c_double(), C.c_int()
+        check(lib().ffr_fluid_time_pressure(self.h, nrep, C.byref(ms), C.byref(it)))
+        return ms.value, it.value
 
     def set_cluster(self, ctas: int) -> None:
         check(lib().ffr_fluid_set_cluster(self.h, int(ctas)))

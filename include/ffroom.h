@@ -187,6 +187,18 @@ int ffr_fluid_device_bytes(ffr_fluid *s, size_t *bytes);
  * back to direct launches (0).  The kernels read their per-step state from
  * device memory, so one captured step is valid for every step. */
 int ffr_fluid_use_graph(ffr_fluid *s, int enable);
+/* Benchmark aid (no counterpart in the reference): solves the pressure
+ * system of the last step again `nrep` times from a pressure-only CUDA graph
+ * (the same kernels the step runs, the same result each time) and returns
+ * the mean milliseconds per solve and its iteration count. */
+int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *iterations);
+/* Multigrid-PCG schedule (no counterpart in the reference): 1 = one kernel
+ * per multigrid pass, also outside graphs (the host paces the iterations and
+ * ffr_fluid_enqueue returns only after the last step's solve is queued);
+ * 0 = one persistent cooperative kernel per solve, also in graphs; -1
+ * (default) = split inside captured step graphs, persistent otherwise.
+ * Set before ffr_fluid_use_graph. */
+int ffr_fluid_set_split(ffr_fluid *s, int mode);
 
 /* FluidSolver::compute_divergence_max (FluidSolver.cpp:470-484). */
 int ffr_fluid_divergence_max(ffr_fluid *s, double *out);

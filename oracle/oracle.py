@@ -84,11 +84,13 @@ class StepRecord:
     converged: bool
     T_mean: float
     cg_iterations: int
+    seconds: float = 0.0
 
 
 def _records(arr, n) -> List[StepRecord]:
     return [StepRecord(r.step, r.velocity_change, r.pressure_residual, r.divergence_max,
-                       bool(r.converged), r.T_mean, r.cg_iterations) for r in arr[:n]]
+                       bool(r.converged), r.T_mean, r.cg_iterations, getattr(r, "seconds", 0.0))
+            for r in arr[:n]]
 
 
 def new_fields(room) -> dict:
@@ -238,7 +240,11 @@ class _RefParams(C.Structure):
                 ("advection", C.c_int), ("use_openmp", C.c_int), ("thermal", C.c_int),
                 ("T_initial", C.c_double), ("T_target", C.c_double), ("buoyancy", C.c_int),
                 ("g_accel", C.c_double), ("beta", C.c_double), ("k_thermal", C.c_double),
-                ("cp", C.c_double)]
+                ("cp", C.c_double), ("time_budget", C.c_double)]
+
+
+class _RefResult(C.Structure):
+    _fields_ = _Result._fields_ + [("seconds", C.c_double)]
 
 
 def ref_available() -> bool:
@@ -253,10 +259,10 @@ class RefDriver:
         self.lib = C.CDLL(path)
         self.lib.ffref_fluid_run.argtypes = [C.POINTER(_RefRoom), C.POINTER(_RefParams), C.c_int,
                                              C.c_int, _dp, _dp, _dp, _u8p, _dp, _dp, _dp, _dp, _dp,
-                                             C.POINTER(_Result)]
+                                             C.POINTER(_RefResult)]
         self.lib.ffref_fluid_run.restype = C.c_int
         self.lib.ffref_lbm_run.argtypes = [C.POINTER(_RefRoom), C.c_double, C.c_double, C.c_double,
-                                           C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.POINTER(_Result)]
+                                           C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.POINTER(_RefResult)]
         self.lib.ffref_lbm_run.restype = C.c_int
 
     @staticmethod
@@ -293,16 +299,20 @@ class RefDriver:
                      len(room.heats), _ptr(keep["heat_box"], _ip), _ptr(keep["heat_T"]))
         return r, keep
 
-    def fluid_run(self, room, params, nsteps, stop_on_converge=False, init=None, use_openmp=None):
+    def fluid_run(self, room, params, nsteps, stop_on_converge=False, init=None, use_openmp=None,
+                  time_budget=0.0):
+        """Runs the reference FluidSolver; with time_budget > 0 the run stops
+        before the first step that starts after that many seconds of stepping
+        (each record's ``seconds`` is the wall time of its step())."""
         r, keep = self.room(room)
         omp = params.use_openmp if use_openmp is None else use_openmp
         pr = _RefParams(params.rho, params.nu, params.dt, params.max_steps, params.convergence_tol,
                         params.poisson_max_iter, params.poisson_tol, params.advection, int(omp),
                         int(params.thermal), params.T_initial, params.T_target, int(params.buoyancy),
-                        params.g_accel, params.beta, params.k_thermal, params.cp)
+                        params.g_accel, params.beta, params.k_thermal, params.cp, float(time_budget))
         fl = new_fields(room)
         ct = np.zeros(room.n_cells, dtype=np.uint8)
-        res = (_Result * max(1, nsteps))()
+        res = (_RefResult * max(1, nsteps))()
         init = init or {}
         n = self.lib.ffref_fluid_run(C.byref(r), C.byref(pr), nsteps, int(stop_on_converge),
                                      _ptr(init.get("u")), _ptr(init.get("v")), _ptr(init.get("w")),
@@ -313,7 +323,7 @@ class RefDriver:
     def lbm_run(self, room, tau, dt, tol, nsteps, stop_on_converge=False):
         r, keep = self.room(room)
         fl = new_fields(room)
-        res = (_Result * max(1, nsteps))()
+        res = (_RefResult * max(1, nsteps))()
         n = self.lib.ffref_lbm_run(C.byref(r), tau, dt, tol, nsteps, int(stop_on_converge),
                                    _ptr(fl["u"]), _ptr(fl["v"]), _ptr(fl["w"]), _ptr(fl["p"]), res)
         return fl, _records(res, n)

@@ -16,6 +16,7 @@
 #include <cstdint>
 #include <cstring>
 #include <algorithm>
+#include <chrono>
 
 // Read access to FluidSolver::poisson_ (a private member) for the iteration
 // count; the reference sources themselves are compiled unchanged.
@@ -54,6 +55,7 @@ struct ffref_params {
     double T_initial, T_target;
     int buoyancy;
     double g_accel, beta, k_thermal, cp;
+    double time_budget;   // seconds of stepping after which a run stops (0 = none)
 };
 
 struct ffref_result {
@@ -62,6 +64,7 @@ struct ffref_result {
     int converged;
     double T_mean;
     int cg_iterations;
+    double seconds;       // wall time of the solver's step() call
 };
 
 static void build(const ffref_room *d, Grid &g, BoundaryManager &bm)
@@ -139,9 +142,15 @@ int ffref_fluid_run(const ffref_room *d, const ffref_params *p, int nsteps,
     fp.k_thermal = p->k_thermal; fp.cp = p->cp;
     FluidSolver s(g, bm, fp);
     int done = 0;
+    double spent = 0.0;
     for (; done < nsteps; done++) {
+        if (p->time_budget > 0 && spent >= p->time_budget) break;
+        const auto t0 = std::chrono::steady_clock::now();
         StepResult r = s.step();
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        spent += sec;
         if (res) {
+            res[done].seconds = sec;
             res[done].step = r.step;
             res[done].velocity_change = r.velocity_change;
             res[done].pressure_residual = r.pressure_residual;
@@ -170,8 +179,11 @@ int ffref_lbm_run(const ffref_room *d, double tau, double dt, double tol, int ns
     LBMSolver s(g, bm, tau, nsteps, tol, dt);
     int done = 0;
     for (; done < nsteps; done++) {
+        const auto t0 = std::chrono::steady_clock::now();
         StepResult r = s.step();
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (res) {
+            res[done].seconds = sec;
             res[done].step = r.step;
             res[done].velocity_change = r.velocity_change;
             res[done].pressure_residual = r.pressure_residual;
