@@ -42,7 +42,9 @@ constexpr int kMaxFans = 120;
 // Pressure-stencil code, one uint16 per cell: 2 bits per neighbour in the
 // order x-, x+, y-, y+, z-, z+ (0 no term, 1 interior, 2 Dirichlet ghost of
 // an OUTFLOW neighbour) and bit 12 for a SOLID (identity) row.
-enum : uint16_t { SC_NONE = 0, SC_IN = 1, SC_DIR = 2, SC_SOLID = 1u << 12 };
+// SC_OUTF marks an OUTFLOW cell (a Dirichlet row of the pressure system);
+// SC_ALLIN is the code of a cell whose six neighbours are all unknowns.
+enum : uint16_t { SC_NONE = 0, SC_IN = 1, SC_DIR = 2, SC_SOLID = 1u << 12, SC_OUTF = 1u << 13, SC_ALLIN = 0x555 };
 
 // --------------------------------------------------------- room setup
 

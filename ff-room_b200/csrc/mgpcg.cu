@@ -115,7 +115,8 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
 
 // -------------------------------------------------------------- device
 
-__device__ __forceinline__ bool active_ct(uint8_t t) { return t == CT_FLUID || t == CT_INFLOW; }
+// FLUID or INFLOW from the stencil code alone (no cell-type load)
+__device__ __forceinline__ bool active_code(unsigned code) { return !(code & (SC_SOLID | SC_OUTF)); }
 
 // Grid barrier without a reduction (same protocol as grid_allreduce).
 __device__ bool grid_barrier(GridSync *gs)
@@ -200,69 +201,120 @@ __device__ __forceinline__ void fine_coefs(const MGDev &M, unsigned code, int i,
         tt[4] = dx * dy * M.izl[k]; tt[5] = dx * dy * M.izr[k];
         vol = dx * dy * dz;
     }
-    D = 0.0f;
+    if ((code & 0xFFFu) == SC_ALLIN) {
+        // the general sum below with every class SC_IN, same order
+        D = 0.0f;
 #pragma unroll
-    for (int a = 0; a < 6; a++) {
-        const unsigned cls = (code >> (2 * a)) & 3u;
-        t[a] = cls == SC_IN ? tt[a] : 0.0f;
-        D += cls == SC_IN ? tt[a] : (cls == SC_DIR ? 2.0f * tt[a] : 0.0f);
+        for (int a = 0; a < 6; a++) {
+            t[a] = tt[a];
+            D += tt[a];
+        }
+    } else {
+        D = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 6; a++) {
+            const unsigned cls = (code >> (2 * a)) & 3u;
+            t[a] = cls == SC_IN ? tt[a] : 0.0f;
+            D += cls == SC_IN ? tt[a] : (cls == SC_DIR ? 2.0f * tt[a] : 0.0f);
+        }
     }
     if (!(D > 0.0f)) D = vol;
 }
 
+// The six neighbour indices of cell c (x-, x+, y-, y+, z-, z+), clamped into
+// [0, n): loads through them are always in bounds, so a pass can issue them
+// before it has read the cell's stencil code; a neighbour that is not an
+// unknown gets weight 0 and its value is never used.
+__device__ __forceinline__ void nb_index(int c, int plane, int nz, int n, int (&idx)[6])
+{
+    idx[0] = max(c - plane, 0);
+    idx[1] = min(c + plane, n - 1);
+    idx[2] = max(c - nz, 0);
+    idx[3] = min(c + nz, n - 1);
+    idx[4] = max(c - 1, 0);
+    idx[5] = min(c + 1, n - 1);
+}
+
+// Flat index of the level-(l+1) parent of cell (i, j, k) of level l, clamped
+// into the parent array (a clamped index is only read for a weight-0
+// neighbour outside the room).
+__device__ __forceinline__ int parent_index(const MGLevel &Lc, int i, int j, int k)
+{
+    const int p = ((i >> 1) * Lc.ny + (j >> 1)) * Lc.nz + (k >> 1);
+    return min(max(p, 0), Lc.n - 1);
+}
+
 // sum_nb T_nb * (x_nb [+ e_parent(nb)]) and the diagonal of cell c on
-// level L (L >= 1: explicit coefficients).
+// level L (L >= 1: explicit coefficients).  Every load is issued before any
+// coefficient is tested; the sums are taken in the order x-, x+, y-, y+,
+// z-, z+ over the non-zero couplings.
 template <bool CORR>
 __device__ __forceinline__ float coarse_nbsum(const MGLevel &L, const MGLevel &Lc, int c, int i, int j, int k,
                                               float &D)
 {
-    const int plane = L.ny * L.nz;
+    const int plane = L.ny * L.nz, nz = L.nz;
+    int idx[6];
+    nb_index(c, plane, nz, L.n, idx);
     const float4 cf = L.coef[c];
+    const float txm = L.coef[idx[0]].x, tym = L.coef[idx[2]].y, tzm = L.coef[idx[4]].z;
+    float v[6];
+#pragma unroll
+    for (int a = 0; a < 6; a++) v[a] = L.x[idx[a]];
+    if (CORR) {
+        v[0] += Lc.x[parent_index(Lc, i - 1, j, k)];
+        v[1] += Lc.x[parent_index(Lc, i + 1, j, k)];
+        v[2] += Lc.x[parent_index(Lc, i, j - 1, k)];
+        v[3] += Lc.x[parent_index(Lc, i, j + 1, k)];
+        v[4] += Lc.x[parent_index(Lc, i, j, k - 1)];
+        v[5] += Lc.x[parent_index(Lc, i, j, k + 1)];
+    }
     D = cf.w;
+    const float t[6] = {i > 0 ? txm : 0.0f, i < L.nx - 1 ? cf.x : 0.0f, j > 0 ? tym : 0.0f,
+                        j < L.ny - 1 ? cf.y : 0.0f, k > 0 ? tzm : 0.0f, k < L.nz - 1 ? cf.z : 0.0f};
     float s = 0.0f;
-    auto val = [&](int cn, int ii, int jj, int kk) -> float {
-        float v = L.x[cn];
-        if (CORR) v += Lc.x[((ii >> 1) * Lc.ny + (jj >> 1)) * Lc.nz + (kk >> 1)];
-        return v;
-    };
-    if (i > 0) { const float t = L.coef[c - plane].x; if (t != 0.0f) s += t * val(c - plane, i - 1, j, k); }
-    if (i < L.nx - 1 && cf.x != 0.0f) s += cf.x * val(c + plane, i + 1, j, k);
-    if (j > 0) { const float t = L.coef[c - L.nz].y; if (t != 0.0f) s += t * val(c - L.nz, i, j - 1, k); }
-    if (j < L.ny - 1 && cf.y != 0.0f) s += cf.y * val(c + L.nz, i, j + 1, k);
-    if (k > 0) { const float t = L.coef[c - 1].z; if (t != 0.0f) s += t * val(c - 1, i, j, k - 1); }
-    if (k < L.nz - 1 && cf.z != 0.0f) s += cf.z * val(c + 1, i, j, k + 1);
+#pragma unroll
+    for (int a = 0; a < 6; a++)
+        if (t[a] != 0.0f) s += t[a] * v[a];
     return s;
 }
 
 template <bool CORR>
 __device__ __forceinline__ float fine_nbsum(const RoomDev &R, const MGDev &M, const MGLevel &L0, const MGLevel &L1,
-                                            int c, int i, int j, int k, float &D)
+                                            unsigned code, int c, int i, int j, int k, float &D)
 {
-    float t[6];
-    fine_coefs(M, R.sc[c], i, j, k, t, D);
     const int plane = R.ny * R.nz, nz = R.nz;
-    const int off[6] = {-plane, plane, -nz, nz, -1, 1};
-    const int di[6] = {-1, 1, 0, 0, 0, 0}, dj[6] = {0, 0, -1, 1, 0, 0}, dk[6] = {0, 0, 0, 0, -1, 1};
+    int idx[6];
+    nb_index(c, plane, nz, R.n, idx);
+    float v[6];
+#pragma unroll
+    for (int a = 0; a < 6; a++) v[a] = L0.x[idx[a]];
+    if (CORR) {
+        v[0] += L1.x[parent_index(L1, i - 1, j, k)];
+        v[1] += L1.x[parent_index(L1, i + 1, j, k)];
+        v[2] += L1.x[parent_index(L1, i, j - 1, k)];
+        v[3] += L1.x[parent_index(L1, i, j + 1, k)];
+        v[4] += L1.x[parent_index(L1, i, j, k - 1)];
+        v[5] += L1.x[parent_index(L1, i, j, k + 1)];
+    }
+    float t[6];
+    fine_coefs(M, code, i, j, k, t, D);
     float s = 0.0f;
 #pragma unroll
-    for (int a = 0; a < 6; a++) {
-        if (t[a] == 0.0f) continue;
-        float v = L0.x[c + off[a]];
-        if (CORR) v += L1.x[(((i + di[a]) >> 1) * L1.ny + ((j + dj[a]) >> 1)) * L1.nz + ((k + dk[a]) >> 1)];
-        s += t[a] * v;
-    }
+    for (int a = 0; a < 6; a++)
+        if (t[a] != 0.0f) s += t[a] * v[a];
     return s;
 }
 
-// One Gauss-Seidel half sweep on `color` of level l.  CORR adds the coarse
-// correction of level l+1 to the neighbour values (the post-smoothing pass
-// right after prolongation).
+// One Gauss-Seidel half sweep on `color` of level l of the hierarchy lv.
+// CORR adds the coarse correction of level l+1 to the neighbour values (the
+// post-smoothing pass right after prolongation).
 template <bool CORR>
-__device__ void smooth_color(const PCGArgs &A, int l, int color, int start, int stride)
+__device__ void smooth_color(const PCGArgs &A, const MGLevel *lv, int nlev, int l, int color, int start,
+                             int stride)
 {
     const MGDev &M = A.M;
-    const MGLevel &L = M.lv[l];
-    const MGLevel &Lc = M.lv[l + 1 < M.nlev ? l + 1 : l];
+    const MGLevel &L = lv[l];
+    const MGLevel &Lc = lv[l + 1 < nlev ? l + 1 : l];
     // one thread per pair (k, k+1) of a row: exactly one of the two has the colour
     const int pk = (L.nz + 1) >> 1;
     for (Walk w(start, stride, L.ny, pk, L.nx * L.ny * pk); w.ok(); w.next()) {
@@ -270,106 +322,200 @@ __device__ void smooth_color(const PCGArgs &A, int l, int color, int start, int 
         if (k >= L.nz) continue;
         const int c = (i * L.ny + j) * L.nz + k;
         float D, s;
+        const float bc = L.b[c];
         if (l == 0) {
-            if (!active_ct(A.R.ct[c])) continue;
-            s = fine_nbsum<CORR>(A.R, M, L, Lc, c, i, j, k, D);
+            const unsigned code = A.R.sc[c];
+            s = fine_nbsum<CORR>(A.R, M, L, Lc, code, c, i, j, k, D);
+            if (!active_code(code)) continue;
         } else {
-            if (L.coef[c].w == 0.0f) continue;
             s = coarse_nbsum<CORR>(L, Lc, c, i, j, k, D);
+            if (D == 0.0f) continue;
         }
-        L.x[c] = (L.b[c] + s) / D;
+        L.x[c] = (bc + s) / D;
     }
 }
 
 // Residual of the red cells of level l (the black ones are exact after a
 // black sweep), summed into the parent rhs on level l+1, and the red-only
 // first sweep of level l+1 from a zero guess.
-__device__ void restrict_level(const PCGArgs &A, int l, int start, int stride)
+__device__ void restrict_level(const PCGArgs &A, const MGLevel *lv, int l, int start, int stride)
 {
     const MGDev &M = A.M;
-    const MGLevel &L = M.lv[l];
-    const MGLevel &C = M.lv[l + 1];
+    const MGLevel &L = lv[l];
+    const MGLevel &C = lv[l + 1];
     for (Walk w(start, stride, C.ny, C.nz, C.n); w.ok(); w.next()) {
         const int P = w.c, I = w.i, J = w.j, K = w.k;
+        const float DP = C.coef[P].w;
         float sum = 0.0f;
+#pragma unroll
         for (int a = 0; a < 2; a++) {
-            const int i = 2 * I + a;
-            if (i >= L.nx) break;
+#pragma unroll
             for (int b = 0; b < 2; b++) {
-                const int j = 2 * J + b;
-                if (j >= L.ny) break;
+#pragma unroll
                 for (int e = 0; e < 2; e++) {
-                    const int k = 2 * K + e;
-                    if (k >= L.nz) break;
-                    if (((i + j + k) & 1) != 0) continue;
+                    const int i = 2 * I + a, j = 2 * J + b, k = 2 * K + e;
+                    // red children inside the level (the same order as a
+                    // nested a, b, e loop that skips the rest)
+                    if (i >= L.nx || j >= L.ny || k >= L.nz || ((i + j + k) & 1) != 0) continue;
                     const int c = (i * L.ny + j) * L.nz + k;
+                    const float bc = L.b[c], xc = L.x[c];
                     float D, s;
+                    bool act;
                     if (l == 0) {
-                        if (!active_ct(A.R.ct[c])) continue;
-                        s = fine_nbsum<false>(A.R, M, L, L, c, i, j, k, D);
+                        const unsigned code = A.R.sc[c];
+                        s = fine_nbsum<false>(A.R, M, L, L, code, c, i, j, k, D);
+                        act = active_code(code);
                     } else {
-                        if (L.coef[c].w == 0.0f) continue;
                         s = coarse_nbsum<false>(L, L, c, i, j, k, D);
+                        act = D != 0.0f;
                     }
-                    sum += L.b[c] - (D * L.x[c] - s);
+                    if (act) sum += bc - (D * xc - s);
                 }
             }
         }
         C.b[P] = sum;
-        const float D = C.coef[P].w;
-        C.x[P] = (((I + J + K) & 1) == 0 && D != 0.0f) ? sum / D : 0.0f;
+        C.x[P] = (((I + J + K) & 1) == 0 && DP != 0.0f) ? sum / DP : 0.0f;
     }
 }
 
-// Levels lo .. nlev-1 inside block 0 (__syncthreads only).
+// Levels lo .. nlev-1 inside one block (__syncthreads only).  When they fit,
+// they run in shared memory: level lo's coefficients, rhs and first guess
+// are copied in, the V-cycle below lo runs there, and level lo's solution
+// is copied back.
+constexpr int kBlockSmemCells = 1536;
+
 __device__ void block_vcycle(const PCGArgs &A, int lo)
 {
+    __shared__ float4 s_coef[kBlockSmemCells];
+    __shared__ float s_x[kBlockSmemCells], s_b[kBlockSmemCells];
     const MGDev &M = A.M;
     const int t = threadIdx.x, nt = blockDim.x;
-    for (int l = lo; l < M.nlev - 1; l++) {
-        smooth_color<false>(A, l, 1, t, nt);
-        __syncthreads();
-        restrict_level(A, l, t, nt);
+    const int nlev = M.nlev;
+    MGLevel lv[kMaxLevels];
+    int total = 0;
+    for (int l = 0; l < nlev; l++) {
+        lv[l] = M.lv[l];
+        if (l >= lo) total += M.lv[l].n;
+    }
+    const bool smem = total <= kBlockSmemCells;
+    if (smem) {
+        int off = 0;
+        for (int l = lo; l < nlev; l++) {
+            const MGLevel &G = M.lv[l];
+            for (int c = t; c < G.n; c += nt) {
+                s_coef[off + c] = G.coef[c];
+                if (l == lo) {
+                    s_x[off + c] = G.x[c];
+                    s_b[off + c] = G.b[c];
+                }
+            }
+            lv[l].coef = s_coef + off;
+            lv[l].x = s_x + off;
+            lv[l].b = s_b + off;
+            off += G.n;
+        }
         __syncthreads();
     }
-    const int last = M.nlev - 1;
+    for (int l = lo; l < nlev - 1; l++) {
+        smooth_color<false>(A, lv, nlev, l, 1, t, nt);
+        __syncthreads();
+        restrict_level(A, lv, l, t, nt);
+        __syncthreads();
+    }
+    const int last = nlev - 1;
     for (int sweep = 0; sweep < 8; sweep++) {
-        smooth_color<false>(A, last, 1, t, nt);
+        smooth_color<false>(A, lv, nlev, last, 1, t, nt);
         __syncthreads();
-        smooth_color<false>(A, last, 0, t, nt);
+        smooth_color<false>(A, lv, nlev, last, 0, t, nt);
         __syncthreads();
     }
-    for (int l = M.nlev - 2; l >= lo; l--) {
-        smooth_color<true>(A, l, 1, t, nt);
+    for (int l = nlev - 2; l >= lo; l--) {
+        smooth_color<true>(A, lv, nlev, l, 1, t, nt);
         __syncthreads();
-        smooth_color<false>(A, l, 0, t, nt);
+        smooth_color<false>(A, lv, nlev, l, 0, t, nt);
+        __syncthreads();
+    }
+    if (smem) {
+        const MGLevel &G = M.lv[lo];
+        for (int c = t; c < G.n; c += nt) G.x[c] = lv[lo].x[c];
         __syncthreads();
     }
 }
 
 // The reference's FP64 operator row (PoissonSolver.cpp:22-91) of cell c
-// applied to a direction given by dir(offset).
+// applied to a direction given by dir(offset).  On a uniform grid every
+// scale 1/(h_face h) equals 1/h^2 (M.s64); a cell with six unknown
+// neighbours takes the same sums in the same order without the class tests.
 template <class F>
-__device__ __forceinline__ double ref_row(const RoomDev &R, unsigned code, int i, int j, int k, double xc, F dir)
+__device__ __forceinline__ double ref_row(const RoomDev &R, const MGDev &M, unsigned code, int i, int j, int k,
+                                          double xc, F dir)
 {
     const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
-    const double *sxl = R.scale, *sxr = sxl + nx, *syl = sxr + nx, *syr = syl + ny, *szl = syr + ny,
-                 *szr = szl + nz;
-    const double s[6] = {sxl[i], sxr[i], syl[j], syr[j], szl[k], szr[k]};
+    double s[6];
+    if (M.uniform) {
+        s[0] = s[1] = M.s64x;
+        s[2] = s[3] = M.s64y;
+        s[4] = s[5] = M.s64z;
+    } else {
+        const double *sxl = R.scale, *sxr = sxl + nx, *syl = sxr + nx, *syr = syl + ny, *szl = syr + ny,
+                     *szr = szl + nz;
+        s[0] = sxl[i]; s[1] = sxr[i]; s[2] = syl[j]; s[3] = syr[j]; s[4] = szl[k]; s[5] = szr[k];
+    }
     const int off[6] = {-plane, plane, -nz, nz, -1, 1};
     double diag = 0.0, o = 0.0;
+    if ((code & 0xFFFu) == SC_ALLIN) {
 #pragma unroll
-    for (int a = 0; a < 6; a++) {
-        const unsigned cls = (code >> (2 * a)) & 3u;
-        if (cls == SC_IN) {
+        for (int a = 0; a < 6; a++) {
             diag += s[a];
             o += s[a] * dir(off[a]);
-        } else if (cls == SC_DIR) {
-            diag += 2.0 * s[a];
+        }
+    } else {
+#pragma unroll
+        for (int a = 0; a < 6; a++) {
+            const unsigned cls = (code >> (2 * a)) & 3u;
+            if (cls == SC_IN) {
+                diag += s[a];
+                o += s[a] * dir(off[a]);
+            } else if (cls == SC_DIR) {
+                diag += 2.0 * s[a];
+            }
         }
     }
     if (diag < 1e-30) diag = 1.0;
     return diag * xc - o;
+}
+
+// Cell volume dx*dy*dz in FP64 (the product order of the general case).
+__device__ __forceinline__ double cell_vol(const MGDev &M, int i, int j, int k)
+{
+    return M.uniform ? M.vol64 : M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
+}
+
+// FP64 weights of the reference row: w[a] = scale if neighbour a is an
+// unknown, else 0; diag = sum of scale (unknown) and 2*scale (Dirichlet
+// ghost) in the order a = 0..5, as ref_row accumulates it.
+__device__ __forceinline__ void ref_weights(const RoomDev &R, const MGDev &M, unsigned code, int i, int j, int k,
+                                            double (&w)[6], double &diag)
+{
+    double s[6];
+    if (M.uniform) {
+        s[0] = s[1] = M.s64x;
+        s[2] = s[3] = M.s64y;
+        s[4] = s[5] = M.s64z;
+    } else {
+        const int nx = R.nx, ny = R.ny, nz = R.nz;
+        const double *sxl = R.scale, *sxr = sxl + nx, *syl = sxr + nx, *syr = syl + ny, *szl = syr + ny,
+                     *szr = szl + nz;
+        s[0] = sxl[i]; s[1] = sxr[i]; s[2] = syl[j]; s[3] = syr[j]; s[4] = szl[k]; s[5] = szr[k];
+    }
+    diag = 0.0;
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+        const unsigned cls = (code >> (2 * a)) & 3u;
+        w[a] = cls == SC_IN ? s[a] : 0.0;
+        diag += cls == SC_IN ? s[a] : (cls == SC_DIR ? 2.0 * s[a] : 0.0);
+    }
+    if (diag < 1e-30) diag = 1.0;
 }
 
 __device__ __forceinline__ double face_rhs(const PCGArgs &A, int c, int i, int j, int k)
@@ -467,21 +613,21 @@ __device__ __forceinline__ void pass_init(const PCGArgs &A, int start, int strid
     float *z = M.lv[0].x;
     for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        const uint8_t t = R.ct[c];
+        const unsigned code = R.sc[c];
         A.x[c] = 0.0;
         A.da[c] = 0.0;
         A.db[c] = 0.0;
         double rv = 0.0;
         float zv = 0.0f;
-        if (t != CT_SOLID) {
+        if (!(code & SC_SOLID)) {
             const double b = face_rhs(A, c, i, j, k);
             acc[0] += b * b;
-            if (active_ct(t)) {
+            if (active_code(code)) {
                 acc[1] += b * b;
-                rv = b * (M.vol_x[i] * M.vol_y[j] * M.vol_z[k]);
+                rv = b * cell_vol(M, i, j, k);
                 if (((i + j + k) & 1) == 0) {
                     float tt[6], D;
-                    fine_coefs(M, R.sc[c], i, j, k, tt, D);
+                    fine_coefs(M, code, i, j, k, tt, D);
                     zv = (float)rv / D;
                 }
             }
@@ -498,21 +644,31 @@ __device__ __forceinline__ void pass_redpost_dot(const PCGArgs &A, int start, in
     const RoomDev &R = A.R;
     const MGDev &M = A.M;
     float *z = M.lv[0].x;
-    const MGLevel &L0 = M.lv[0];
     const bool sweep = M.nlev_grid >= 1;
+    const int n = R.n, plane = R.ny * R.nz, nz = R.nz;
     for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        if (!active_ct(R.ct[c])) continue;
-        float zc;
+        const unsigned code = R.sc[c];
+        const double rc = A.r[c];
+        const float zold = z[c], bc = M.r32[c];
+        int idx[6];
+        nb_index(c, plane, nz, n, idx);
+        float zn[6];
+#pragma unroll
+        for (int a = 0; a < 6; a++) zn[a] = z[idx[a]];
+        if (!active_code(code)) continue;
+        float zc = zold;
         if (sweep && ((i + j + k) & 1) == 0) {
-            float D;
-            const float s = fine_nbsum<false>(R, M, L0, L0, c, i, j, k, D);
-            zc = (M.r32[c] + s) / D;
+            float t[6], D;
+            fine_coefs(M, code, i, j, k, t, D);
+            float sum = 0.0f;
+#pragma unroll
+            for (int a = 0; a < 6; a++)
+                if (t[a] != 0.0f) sum += t[a] * zn[a];
+            zc = (bc + sum) / D;
             z[c] = zc;
-        } else {
-            zc = z[c];
         }
-        acc += A.r[c] * (double)zc;
+        acc += rc * (double)zc;
     }
 }
 
@@ -524,17 +680,28 @@ __device__ __forceinline__ void pass_direction(const PCGArgs &A, int start, int 
     const RoomDev &R = A.R;
     const MGDev &M = A.M;
     const float *z = M.lv[0].x;
+    const int n = R.n, plane = R.ny * R.nz, nz = R.nz;
     for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        if (!active_ct(R.ct[c])) { dnew[c] = 0.0; A.q[c] = 0.0; continue; }
+        const unsigned code = R.sc[c];
         const double dp = dold[c];
-        const double dc = fma(beta, dp, (double)z[c]);
-        if (update_x) A.x[c] = fma(alpha_prev, dp, A.x[c]);
+        const float zc = z[c];
+        const double xo = update_x ? A.x[c] : 0.0;
+        int idx[6];
+        nb_index(c, plane, nz, n, idx);
+        double dn[6];
+#pragma unroll
+        for (int a = 0; a < 6; a++) dn[a] = fma(beta, dold[idx[a]], (double)z[idx[a]]);
+        if (!active_code(code)) { dnew[c] = 0.0; A.q[c] = 0.0; continue; }
+        const double dc = fma(beta, dp, (double)zc);
+        if (update_x) A.x[c] = fma(alpha_prev, dp, xo);
         dnew[c] = dc;
-        const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
-        const double row = ref_row(R, R.sc[c], i, j, k, dc,
-                                   [&](int o) { return fma(beta, dold[c + o], (double)z[c + o]); });
-        const double qc = vol * row;
+        double w[6], diag;
+        ref_weights(R, M, code, i, j, k, w, diag);
+        double o = 0.0;
+#pragma unroll
+        for (int a = 0; a < 6; a++) o += w[a] * dn[a];
+        const double qc = cell_vol(M, i, j, k) * (diag * dc - o);
         A.q[c] = qc;
         acc += dc * qc;
     }
@@ -548,10 +715,12 @@ __device__ __forceinline__ void pass_residual(const PCGArgs &A, int start, int s
     float *z = M.lv[0].x;
     for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        if (!active_ct(R.ct[c])) continue;
-        const double rv = A.r[c] - alpha * A.q[c];
+        const unsigned code = R.sc[c];
+        const double r0 = A.r[c], q0 = A.q[c];
+        if (!active_code(code)) continue;
+        const double rv = r0 - alpha * q0;
         A.r[c] = rv;
-        const double vol = M.vol_x[i] * M.vol_y[j] * M.vol_z[k];
+        const double vol = cell_vol(M, i, j, k);
         const double ru = rv / vol;
         acc += ru * ru;
         const float r32 = (float)rv;
@@ -559,7 +728,7 @@ __device__ __forceinline__ void pass_residual(const PCGArgs &A, int start, int s
         float zv = 0.0f;
         if (((i + j + k) & 1) == 0) {
             float tt[6], D;
-            fine_coefs(M, R.sc[c], i, j, k, tt, D);
+            fine_coefs(M, code, i, j, k, tt, D);
             zv = r32 / D;
         }
         z[c] = zv;
@@ -570,7 +739,7 @@ __device__ __forceinline__ void pass_final_x(const PCGArgs &A, int start, int st
                                              const double *__restrict__ d)
 {
     for (int c = start; c < A.R.n; c += stride)
-        if (active_ct(A.R.ct[c])) A.x[c] = fma(alpha, d[c], A.x[c]);
+        if (active_code(A.R.sc[c])) A.x[c] = fma(alpha, d[c], A.x[c]);
 }
 
 // OUTFLOW rows by back-substitution in the reference's own row form:
@@ -581,10 +750,11 @@ __device__ __forceinline__ void pass_backsub(const PCGArgs &A, int start, int st
     double *x = A.x;
     for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        if (R.ct[c] != CT_OUTFLOW) continue;
+        const unsigned code = R.sc[c];
+        if (!(code & SC_OUTF)) continue;
         const double b = face_rhs(A, c, i, j, k);
-        const double row0 = ref_row(R, R.sc[c], i, j, k, 0.0, [&](int o) { return x[c + o]; });
-        const double diag = ref_row(R, R.sc[c], i, j, k, 1.0, [&](int) { return 0.0; });
+        const double row0 = ref_row(R, A.M, code, i, j, k, 0.0, [&](int o) { return x[c + o]; });
+        const double diag = ref_row(R, A.M, code, i, j, k, 1.0, [&](int) { return 0.0; });
         x[c] = (b - row0) / diag;
     }
 }
@@ -612,9 +782,9 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
         for (int it = 0;; it++) {
             // ---- preconditioner: V-cycle from the red sweep already in z
             for (int l = 0; l < M.nlev_grid && l < M.nlev - 1; l++) {
-                smooth_color<false>(A, l, 1, t0, nth);
+                smooth_color<false>(A, M.lv, M.nlev, l, 1, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
-                restrict_level(A, l, t0, nth);
+                restrict_level(A, M.lv, l, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
             if (M.nlev_grid < M.nlev) {
@@ -622,13 +792,13 @@ __global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
             for (int l = min(M.nlev_grid, M.nlev - 1) - 1; l >= 1; l--) {
-                smooth_color<true>(A, l, 1, t0, nth);
+                smooth_color<true>(A, M.lv, M.nlev, l, 1, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
-                smooth_color<false>(A, l, 0, t0, nth);
+                smooth_color<false>(A, M.lv, M.nlev, l, 0, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
             if (M.nlev_grid >= 1 && M.nlev > 1) {
-                smooth_color<true>(A, 0, 1, t0, nth);
+                smooth_color<true>(A, M.lv, M.nlev, 0, 1, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
             double acc1[1] = {0.0};
@@ -758,19 +928,54 @@ template <bool CORR>
 __global__ void __launch_bounds__(256) k_sp_smooth(PCGArgs A, const SplitState *ss, int l, int color)
 {
     if (ss->done) return;
-    smooth_color<CORR>(A, l, color, gtid(), gthreads());
+    smooth_color<CORR>(A, A.M.lv, A.M.nlev, l, color, gtid(), gthreads());
 }
 
 __global__ void __launch_bounds__(256) k_sp_restrict(PCGArgs A, const SplitState *ss, int l)
 {
     if (ss->done) return;
-    restrict_level(A, l, gtid(), gthreads());
+    restrict_level(A, A.M.lv, l, gtid(), gthreads());
 }
 
 __global__ void __launch_bounds__(1024) k_sp_coarse(PCGArgs A, const SplitState *ss, int lo)
 {
     if (ss->done) return;
     block_vcycle(A, lo);
+}
+
+// Levels mid .. nlev-1 of the V-cycle in one thread-block cluster: the
+// grid-sized levels from mid on (pre-smooth + restriction going down,
+// post-smooth coming up) with the hardware cluster barrier between passes,
+// and the levels of at most kBlockLevelCells cells in block 0.  Every cell
+// update is the one the one-kernel-per-pass form makes (the colours are
+// Jacobi sweeps), so the result does not depend on this grouping.
+__global__ void __launch_bounds__(kMidThreads, 1) k_sp_mid(PCGArgs A, const SplitState *ss, int mid)
+{
+    if (ss->done) return;   // the same value in every block of the cluster
+    auto cl = cooperative_groups::this_cluster();
+    const MGDev &M = A.M;
+    const int t0 = (int)cl.block_rank() * blockDim.x + threadIdx.x, nth = (int)cl.num_blocks() * blockDim.x;
+    auto csync = [&]() {
+        __threadfence();
+        cl.sync();
+    };
+    const int top = min(M.nlev_grid, M.nlev - 1);
+    for (int l = mid; l < top; l++) {
+        smooth_color<false>(A, M.lv, M.nlev, l, 1, t0, nth);
+        csync();
+        restrict_level(A, M.lv, l, t0, nth);
+        csync();
+    }
+    if (M.nlev_grid < M.nlev) {
+        if (cl.block_rank() == 0) block_vcycle(A, M.nlev_grid);
+        csync();
+    }
+    for (int l = top - 1; l >= mid; l--) {
+        smooth_color<true>(A, M.lv, M.nlev, l, 1, t0, nth);
+        csync();
+        smooth_color<false>(A, M.lv, M.nlev, l, 0, t0, nth);
+        if (l > mid) csync();
+    }
 }
 
 __global__ void __launch_bounds__(256) k_sp_redpost(PCGArgs A, SplitState *ss)
@@ -785,7 +990,7 @@ __global__ void __launch_bounds__(256) k_sp_redpost(PCGArgs A, SplitState *ss)
     }
 }
 
-__global__ void __launch_bounds__(256) k_sp_direction(PCGArgs A, SplitState *ss)
+__global__ void __launch_bounds__(256, 4) k_sp_direction(PCGArgs A, SplitState *ss)
 {
     __shared__ double sh[32];
     if (ss->done) return;
@@ -879,6 +1084,11 @@ int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGD
     M.nlev_grid = 0;
     for (int l = 0; l < M.nlev; l++)
         if ((long long)h.nx[l] * h.ny[l] * h.nz[l] > kBlockLevelCells) M.nlev_grid = l + 1;
+    // first level (>= 1) small enough for the one-cluster part of the split solve
+    M.nlev_mid = 1;
+    for (int l = 1; l < M.nlev; l++)
+        if ((long long)h.nx[l] * h.ny[l] * h.nz[l] > kMidLevelCells) M.nlev_mid = l + 1;
+    M.nlev_mid = std::min(M.nlev_mid, std::max(1, M.nlev_grid));
     // fine-level factors in FP32 (PoissonSolver.cpp:33-49 centre distances)
     auto axis = [](const std::vector<double> &hh, std::vector<float> &d, std::vector<float> &il,
                    std::vector<float> &ir) {
@@ -927,6 +1137,11 @@ int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGD
     M.ty = (float)(r.dxv[0] * r.dzv[0] / r.dyv[0]);
     M.tz = (float)(r.dxv[0] * r.dyv[0] / r.dzv[0]);
     M.vol = (float)(r.dxv[0] * r.dyv[0] * r.dzv[0]);
+    // the reference's scales 1/(h_face h) with h_face = h (uniform axis)
+    M.s64x = 1.0 / (r.dxv[0] * r.dxv[0]);
+    M.s64y = 1.0 / (r.dyv[0] * r.dyv[0]);
+    M.s64z = 1.0 / (r.dzv[0] * r.dzv[0]);
+    M.vol64 = r.dxv[0] * r.dyv[0] * r.dzv[0];
     M.ixl = fxl; M.ixr = fxr; M.iyl = fyl; M.iyr = fyr; M.izl = fzl; M.izr = fzr;
     for (int l = 1; l < M.nlev; l++) {
         const size_t m = (size_t)h.nx[l] * h.ny[l] * h.nz[l];
@@ -1015,14 +1230,45 @@ unsigned split_blocks_cells(const MGDev &M, int l)
     return (unsigned)std::max<long long>(1, ((long long)M.lv[l].n + 255) / 256);
 }
 
+// Cluster size of k_sp_mid: the largest of 16 and 8 blocks that the device
+// can co-schedule (16 needs the non-portable cluster-size attribute).
+int mid_cluster_ctas()
+{
+    static int ctas = 0;
+    if (ctas) return ctas;
+    cudaFuncSetAttribute(k_sp_mid, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int want : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)want);
+        cfg.blockDim = dim3(kMidThreads);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)want;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, k_sp_mid, &cfg) == cudaSuccess && nclusters > 0) {
+            ctas = want;
+            return ctas;
+        }
+        cudaGetLastError();
+    }
+    ctas = 1;
+    return ctas;
+}
+
 // Kernels one PCG iteration of the split solve runs (the body below).
 unsigned split_body_kernels(const MGDev &M)
 {
-    const int down = std::min(M.nlev_grid, M.nlev - 1);
-    unsigned k = 2u * (unsigned)std::max(0, down);            // smooth + restrict per level
-    if (M.nlev_grid < M.nlev) k += 1;                         // one-block coarse V-cycle
-    k += 2u * (unsigned)std::max(0, down - 1);                // levels down-1 .. 1 post-smooth
-    if (M.nlev_grid >= 1 && M.nlev > 1) k += 1;               // level-0 black post-smooth
+    if (M.nlev <= 1) return 3;
+    const int top = std::min(M.nlev_grid, M.nlev - 1);
+    const int gdown = std::min(M.nlev_mid, top);
+    unsigned k = 2u * (unsigned)gdown;                        // grid levels: smooth + restrict
+    if (M.nlev_mid < top || M.nlev_grid < M.nlev) k += 1;     // k_sp_mid
+    k += 2u * (unsigned)std::max(0, gdown - 1);               // grid levels gdown-1 .. 1 post-smooth
+    if (M.nlev_grid >= 1) k += 1;                             // level-0 black post-smooth
     return k + 3;                                             // red post + r.z, direction, residual
 }
 
@@ -1038,25 +1284,42 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
         if (e != cudaSuccess && rc == FFR_OK) rc = cuda_fail(e, "split kernel launch");
         count_launch(1);
     };
-    for (int l = 0; l < M.nlev_grid && l < M.nlev - 1; l++) {
-        k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
-        chk();
-        k_sp_restrict<<<split_blocks_cells(M, l + 1), 256, 0, bs>>>(a, ss, l);
-        chk();
-    }
-    if (M.nlev_grid < M.nlev) {
-        k_sp_coarse<<<1, 1024, 0, bs>>>(a, ss, M.nlev_grid);
-        chk();
-    }
-    for (int l = std::min(M.nlev_grid, M.nlev - 1) - 1; l >= 1; l--) {
-        k_sp_smooth<true><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
-        chk();
-        k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 0);
-        chk();
-    }
-    if (M.nlev_grid >= 1 && M.nlev > 1) {
-        k_sp_smooth<true><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 1);
-        chk();
+    if (M.nlev > 1) {
+        const int top = std::min(M.nlev_grid, M.nlev - 1);
+        const int gdown = std::min(M.nlev_mid, top);
+        for (int l = 0; l < gdown; l++) {
+            k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
+            chk();
+            k_sp_restrict<<<split_blocks_cells(M, l + 1), 256, 0, bs>>>(a, ss, l);
+            chk();
+        }
+        if (M.nlev_mid < top || M.nlev_grid < M.nlev) {
+            const int ctas = mid_cluster_ctas();
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)ctas);
+            cfg.blockDim = dim3(kMidThreads);
+            cfg.stream = bs;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = (unsigned)ctas;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            cudaError_t e = cudaLaunchKernelEx(&cfg, k_sp_mid, a, (const SplitState *)ss, M.nlev_mid);
+            if (e != cudaSuccess && rc == FFR_OK) rc = cuda_fail(e, "cudaLaunchKernelEx(k_sp_mid)");
+            chk();
+        }
+        for (int l = gdown - 1; l >= 1; l--) {
+            k_sp_smooth<true><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
+            chk();
+            k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 0);
+            chk();
+        }
+        if (M.nlev_grid >= 1) {
+            k_sp_smooth<true><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 1);
+            chk();
+        }
     }
     k_sp_redpost<<<cb, 256, 0, bs>>>(a, ss);
     chk();

@@ -9,6 +9,10 @@ namespace ffr {
 constexpr int kMaxLevels = 12;
 // Levels with at most this many cells run inside one CTA (no grid barrier).
 constexpr int kBlockLevelCells = 640;
+// Levels (>= 1) with at most this many cells run, in the split solve, inside
+// one thread-block cluster of kMidThreads-thread blocks.
+constexpr int kMidLevelCells = 160 * 1024;
+constexpr int kMidThreads = 512;
 
 // One coarse level: per cell (T to the x+, y+, z+ neighbour, diagonal), FP32.
 // Inactive cells (no FLUID/INFLOW child) have diagonal 0.
@@ -21,6 +25,7 @@ struct MGLevel {
 struct MGDev {
     int nlev;             // levels including the fine one
     int nlev_grid;        // levels 0 .. nlev_grid-1 use grid-wide passes
+    int nlev_mid;         // split solve: levels nlev_mid .. nlev_grid-1 run in one cluster
     MGLevel lv[kMaxLevels];
     // fine-level face transmissibility factors (FP32): T_x-(i,j,k) =
     // dy[j]*dz[k]*ix_l[i] and so on; vol = dx*dy*dz
@@ -28,6 +33,7 @@ struct MGDev {
     const double *vol_x, *vol_y, *vol_z;   // FP64 spacings for the cell volume
     int uniform;          // all spacings equal per axis: tx, ty, tz, vol hold the constants
     float tx, ty, tz, vol;
+    double s64x, s64y, s64z, vol64;   // uniform: FP64 stencil scales 1/h^2 and cell volume
     float *r32;           // FP32 copy of the scaled CG residual (level-0 rhs)
 };
 

@@ -58,7 +58,8 @@ __global__ void k_noalloc_codes(const uint8_t *__restrict__ ct, int nx, int ny, 
             return t == CT_OUTFLOW ? SC_DIR : (t == CT_SOLID ? SC_NONE : SC_IN);
         };
         sc[c] = (uint16_t)(cls(i - 1, j, k) | cls(i + 1, j, k) << 2 | cls(i, j - 1, k) << 4 |
-                           cls(i, j + 1, k) << 6 | cls(i, j, k - 1) << 8 | cls(i, j, k + 1) << 10);
+                           cls(i, j + 1, k) << 6 | cls(i, j, k - 1) << 8 | cls(i, j, k + 1) << 10 |
+                           (ct[c] == CT_OUTFLOW ? SC_OUTF : 0));
     }
 }
 

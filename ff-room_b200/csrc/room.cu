@@ -185,6 +185,7 @@ void build_stencil(const HostRoom &r, std::vector<uint16_t> &sc, std::vector<dou
                     c |= cls(i, j + 1, k) << 6;
                     c |= cls(i, j, k - 1) << 8;
                     c |= cls(i, j, k + 1) << 10;
+                    if (r.ct[CI(i, j, k)] == CT_OUTFLOW) c |= SC_OUTF;
                 }
                 sc[CI(i, j, k)] = c;
             }
