@@ -638,6 +638,27 @@ __device__ __forceinline__ void pass_init(const PCGArgs &A, int start, int strid
     }
 }
 
+// The level-0 passes below visit the cells in pairs (k, k+1) of a row: one
+// thread per pair, so exactly one cell of each thread is red and the red-only
+// work does not diverge, and both cells' loads are in flight together.  A row
+// of odd length ends in a single cell (c1 == c0, nothing stored for it).
+struct CellPair {
+    int i, j, k0, c0, c1;
+    bool two, red0;   // a second cell; cell 0 is red ((i + j + k) even)
+    __device__ __forceinline__ CellPair(const Walk &w, int ny, int nz)
+    {
+        i = w.i;
+        j = w.j;
+        k0 = 2 * w.k;
+        two = k0 + 1 < nz;
+        c0 = (i * ny + j) * nz + k0;
+        c1 = two ? c0 + 1 : c0;
+        red0 = ((i + j + k0) & 1) == 0;
+    }
+    __device__ __forceinline__ int kred(int nz) const { return red0 ? k0 : min(k0 + 1, nz - 1); }
+    __device__ __forceinline__ int cred() const { return red0 ? c0 : c1; }
+};
+
 // the last red sweep of level 0 fused with r.z
 __device__ __forceinline__ void pass_redpost_dot(const PCGArgs &A, int start, int stride, double &acc)
 {
@@ -645,30 +666,33 @@ __device__ __forceinline__ void pass_redpost_dot(const PCGArgs &A, int start, in
     const MGDev &M = A.M;
     float *z = M.lv[0].x;
     const bool sweep = M.nlev_grid >= 1;
-    const int n = R.n, plane = R.ny * R.nz, nz = R.nz;
-    for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
-        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        const unsigned code = R.sc[c];
-        const double rc = A.r[c];
-        const float zold = z[c], bc = M.r32[c];
+    const int n = R.n, ny = R.ny, nz = R.nz, plane = ny * nz, pk = (nz + 1) >> 1;
+    for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
+        const CellPair P(w, ny, nz);
+        const unsigned code0 = R.sc[P.c0], code1 = R.sc[P.c1];
+        const double r0 = A.r[P.c0], r1 = A.r[P.c1];
+        float z0 = z[P.c0], z1 = z[P.c1];
+        const int cr = P.cred();
+        const float br = M.r32[cr];
         int idx[6];
-        nb_index(c, plane, nz, n, idx);
+        nb_index(cr, plane, nz, n, idx);
         float zn[6];
 #pragma unroll
         for (int a = 0; a < 6; a++) zn[a] = z[idx[a]];
-        if (!active_code(code)) continue;
-        float zc = zold;
-        if (sweep && ((i + j + k) & 1) == 0) {
+        const unsigned coder = P.red0 ? code0 : code1;
+        if (sweep && active_code(coder) && (P.red0 || P.two)) {
             float t[6], D;
-            fine_coefs(M, code, i, j, k, t, D);
+            fine_coefs(M, coder, P.i, P.j, P.kred(nz), t, D);
             float sum = 0.0f;
 #pragma unroll
             for (int a = 0; a < 6; a++)
                 if (t[a] != 0.0f) sum += t[a] * zn[a];
-            zc = (bc + sum) / D;
-            z[c] = zc;
+            const float zr = (br + sum) / D;
+            z[cr] = zr;
+            if (P.red0) z0 = zr; else z1 = zr;
         }
-        acc += rc * (double)zc;
+        if (active_code(code0)) acc += r0 * (double)z0;
+        if (P.two && active_code(code1)) acc += r1 * (double)z1;
     }
 }
 
@@ -680,30 +704,51 @@ __device__ __forceinline__ void pass_direction(const PCGArgs &A, int start, int 
     const RoomDev &R = A.R;
     const MGDev &M = A.M;
     const float *z = M.lv[0].x;
-    const int n = R.n, plane = R.ny * R.nz, nz = R.nz;
-    for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
-        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        const unsigned code = R.sc[c];
-        const double dp = dold[c];
-        const float zc = z[c];
-        const double xo = update_x ? A.x[c] : 0.0;
-        int idx[6];
-        nb_index(c, plane, nz, n, idx);
-        double dn[6];
+    const int n = R.n, ny = R.ny, nz = R.nz, plane = ny * nz, pk = (nz + 1) >> 1;
+    for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
+        const CellPair P(w, ny, nz);
+        const int c0 = P.c0, c1 = P.c1;
+        const unsigned code0 = R.sc[c0], code1 = R.sc[c1];
+        const double dp0 = dold[c0], dp1 = dold[c1];
+        const float z0 = z[c0], z1 = z[c1];
+        const double x0 = update_x ? A.x[c0] : 0.0, x1 = update_x ? A.x[c1] : 0.0;
+        // new direction values of the neighbours: x-, x+, y-, y+ of each cell,
+        // the row neighbours outside the pair; inside the pair each cell is
+        // the other's z neighbour
+        const int o0[5] = {max(c0 - plane, 0), min(c0 + plane, n - 1), max(c0 - nz, 0), min(c0 + nz, n - 1),
+                           max(c0 - 1, 0)};
+        const int o1[5] = {max(c1 - plane, 0), min(c1 + plane, n - 1), max(c1 - nz, 0), min(c1 + nz, n - 1),
+                           min(c1 + 1, n - 1)};
+        double n0[6], n1[6];
 #pragma unroll
-        for (int a = 0; a < 6; a++) dn[a] = fma(beta, dold[idx[a]], (double)z[idx[a]]);
-        if (!active_code(code)) { dnew[c] = 0.0; A.q[c] = 0.0; continue; }
-        const double dc = fma(beta, dp, (double)zc);
-        if (update_x) A.x[c] = fma(alpha_prev, dp, xo);
-        dnew[c] = dc;
-        double w[6], diag;
-        ref_weights(R, M, code, i, j, k, w, diag);
-        double o = 0.0;
+        for (int a = 0; a < 4; a++) {
+            n0[a] = fma(beta, dold[o0[a]], (double)z[o0[a]]);
+            n1[a] = fma(beta, dold[o1[a]], (double)z[o1[a]]);
+        }
+        n0[4] = fma(beta, dold[o0[4]], (double)z[o0[4]]);
+        n1[5] = fma(beta, dold[o1[4]], (double)z[o1[4]]);
+        const double d0 = fma(beta, dp0, (double)z0), d1 = fma(beta, dp1, (double)z1);
+        n0[5] = P.two ? d1 : n1[5];
+        n1[4] = d0;
+        auto cell = [&](int c, unsigned code, int k, double dp, double dc, double xo, const double (&dn)[6]) {
+            if (!active_code(code)) {
+                dnew[c] = 0.0;
+                A.q[c] = 0.0;
+                return;
+            }
+            if (update_x) A.x[c] = fma(alpha_prev, dp, xo);
+            dnew[c] = dc;
+            double wt[6], diag;
+            ref_weights(R, M, code, P.i, P.j, k, wt, diag);
+            double o = 0.0;
 #pragma unroll
-        for (int a = 0; a < 6; a++) o += w[a] * dn[a];
-        const double qc = cell_vol(M, i, j, k) * (diag * dc - o);
-        A.q[c] = qc;
-        acc += dc * qc;
+            for (int a = 0; a < 6; a++) o += wt[a] * dn[a];
+            const double qc = cell_vol(M, P.i, P.j, k) * (diag * dc - o);
+            A.q[c] = qc;
+            acc += dc * qc;
+        };
+        cell(c0, code0, P.k0, dp0, d0, x0, n0);
+        if (P.two) cell(c1, code1, P.k0 + 1, dp1, d1, x1, n1);
     }
 }
 
@@ -713,25 +758,25 @@ __device__ __forceinline__ void pass_residual(const PCGArgs &A, int start, int s
     const RoomDev &R = A.R;
     const MGDev &M = A.M;
     float *z = M.lv[0].x;
-    for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
-        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        const unsigned code = R.sc[c];
-        const double r0 = A.r[c], q0 = A.q[c];
-        if (!active_code(code)) continue;
-        const double rv = r0 - alpha * q0;
-        A.r[c] = rv;
-        const double vol = cell_vol(M, i, j, k);
-        const double ru = rv / vol;
-        acc += ru * ru;
-        const float r32 = (float)rv;
-        M.r32[c] = r32;
-        float zv = 0.0f;
-        if (((i + j + k) & 1) == 0) {
-            float tt[6], D;
-            fine_coefs(M, code, i, j, k, tt, D);
-            zv = r32 / D;
-        }
-        z[c] = zv;
+    const int ny = R.ny, nz = R.nz, pk = (nz + 1) >> 1;
+    for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
+        const CellPair P(w, ny, nz);
+        const unsigned code0 = R.sc[P.c0], code1 = R.sc[P.c1];
+        const double ra = A.r[P.c0], qa = A.q[P.c0], rb = A.r[P.c1], qb = A.q[P.c1];
+        float tt[6], D;
+        fine_coefs(M, P.red0 ? code0 : code1, P.i, P.j, P.kred(nz), tt, D);
+        auto cell = [&](int c, unsigned code, int k, double r0, double q0, bool red) {
+            if (!active_code(code)) return;
+            const double rv = r0 - alpha * q0;
+            A.r[c] = rv;
+            const double ru = rv / cell_vol(M, P.i, P.j, k);
+            acc += ru * ru;
+            const float r32 = (float)rv;
+            M.r32[c] = r32;
+            z[c] = red ? r32 / D : 0.0f;
+        };
+        cell(P.c0, code0, P.k0, ra, qa, P.red0);
+        if (P.two) cell(P.c1, code1, P.k0 + 1, rb, qb, !P.red0);
     }
 }
 
@@ -990,7 +1035,7 @@ __global__ void __launch_bounds__(256) k_sp_redpost(PCGArgs A, SplitState *ss)
     }
 }
 
-__global__ void __launch_bounds__(256, 4) k_sp_direction(PCGArgs A, SplitState *ss)
+__global__ void __launch_bounds__(256, 3) k_sp_direction(PCGArgs A, SplitState *ss)
 {
     __shared__ double sh[32];
     if (ss->done) return;
