@@ -114,14 +114,20 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def load_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary."""
+def load_traffic(key: str, sub: str = None):
+    """A measured DRAM-traffic figure (bytes per cell, per cell-iteration)
+    from the committed ncu summary profiles/traffic.json, or None."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as fh:
-            return json.load(fh).get(kernel)
+            v = json.load(fh).get(key)
+        return v.get(sub) if (sub is not None and isinstance(v, dict)) else v
     except Exception:
         return None
+
+
+def scaled_traffic(per_unit, units):
+    return None if per_unit is None else per_unit * units
 
 
 # ------------------------------------------------------------- workloads
@@ -213,7 +219,11 @@ def run_ours(args, rank: int, world: int, dist):
         roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "traffic": load_traffic("k_pcg_per_launch" if mg else "k_cg_per_launch"),
+                # measured DRAM bytes per cell and iteration (ncu, full-size
+                # room) times the cells and iterations of one launch
+                "traffic": scaled_traffic(load_traffic("pcg_split_bytes_per_cell_iter" if mg else
+                                                       "cg_bytes_per_cell_iter"),
+                                          cells * (it_solve if args.graph else float(np.mean(iters)))),
                 "algorithmic_bytes_per_launch": bytes_cg / launches_cg,
                 "share_of_step": round(prof.get("pressure", prof.get("pressure_estimate"))[0] / ms, 4),
                 "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}
@@ -226,7 +236,7 @@ def run_ours(args, rank: int, world: int, dist):
         achieved = b / t_k / 1e9
         roof = {"bound": "hbm", "kernel": "k_lbm_step (fused pull-stream/collide)", "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "traffic": load_traffic("k_lbm_step_per_cell"),
+                "traffic": scaled_traffic(load_traffic("lbm_step_bytes_per_cell", params["storage"]), cells),
                 "algorithmic_bytes_per_launch": b / max(1, steps_done),
                 "share_of_step": round(prof["stream_collide"][0] / ms, 4),
                 "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}

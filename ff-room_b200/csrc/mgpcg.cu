@@ -235,13 +235,19 @@ __device__ __forceinline__ void nb_index(int c, int plane, int nz, int n, int (&
     idx[5] = min(c + 1, n - 1);
 }
 
-// Flat index of the level-(l+1) parent of cell (i, j, k) of level l, clamped
-// into the parent array (a clamped index is only read for a weight-0
-// neighbour outside the room).
-__device__ __forceinline__ int parent_index(const MGLevel &Lc, int i, int j, int k)
+// v[a] += the level-(l+1) correction at the parent of neighbour a of cell
+// (i, j, k): the parent of a neighbour is the cell's own parent or the one
+// next to it along the neighbour's axis, by the parity of the coordinate.
+// Indices are clamped into the parent array (a clamped index is only read
+// for a weight-0 neighbour outside the room).
+__device__ __forceinline__ void add_parents(const MGLevel &Lc, int i, int j, int k, float (&v)[6])
 {
-    const int p = ((i >> 1) * Lc.ny + (j >> 1)) * Lc.nz + (k >> 1);
-    return min(max(p, 0), Lc.n - 1);
+    const int pl = Lc.ny * Lc.nz, pz = Lc.nz, last = Lc.n - 1;
+    const int P0 = ((i >> 1) * Lc.ny + (j >> 1)) * pz + (k >> 1);
+    const int p[6] = {(i & 1) ? P0 : P0 - pl, (i & 1) ? P0 + pl : P0, (j & 1) ? P0 : P0 - pz,
+                      (j & 1) ? P0 + pz : P0, (k & 1) ? P0 : P0 - 1, (k & 1) ? P0 + 1 : P0};
+#pragma unroll
+    for (int a = 0; a < 6; a++) v[a] += Lc.x[min(max(p[a], 0), last)];
 }
 
 // sum_nb T_nb * (x_nb [+ e_parent(nb)]) and the diagonal of cell c on
@@ -260,14 +266,7 @@ __device__ __forceinline__ float coarse_nbsum(const MGLevel &L, const MGLevel &L
     float v[6];
 #pragma unroll
     for (int a = 0; a < 6; a++) v[a] = L.x[idx[a]];
-    if (CORR) {
-        v[0] += Lc.x[parent_index(Lc, i - 1, j, k)];
-        v[1] += Lc.x[parent_index(Lc, i + 1, j, k)];
-        v[2] += Lc.x[parent_index(Lc, i, j - 1, k)];
-        v[3] += Lc.x[parent_index(Lc, i, j + 1, k)];
-        v[4] += Lc.x[parent_index(Lc, i, j, k - 1)];
-        v[5] += Lc.x[parent_index(Lc, i, j, k + 1)];
-    }
+    if (CORR) add_parents(Lc, i, j, k, v);
     D = cf.w;
     const float t[6] = {i > 0 ? txm : 0.0f, i < L.nx - 1 ? cf.x : 0.0f, j > 0 ? tym : 0.0f,
                         j < L.ny - 1 ? cf.y : 0.0f, k > 0 ? tzm : 0.0f, k < L.nz - 1 ? cf.z : 0.0f};
@@ -288,14 +287,7 @@ __device__ __forceinline__ float fine_nbsum(const RoomDev &R, const MGDev &M, co
     float v[6];
 #pragma unroll
     for (int a = 0; a < 6; a++) v[a] = L0.x[idx[a]];
-    if (CORR) {
-        v[0] += L1.x[parent_index(L1, i - 1, j, k)];
-        v[1] += L1.x[parent_index(L1, i + 1, j, k)];
-        v[2] += L1.x[parent_index(L1, i, j - 1, k)];
-        v[3] += L1.x[parent_index(L1, i, j + 1, k)];
-        v[4] += L1.x[parent_index(L1, i, j, k - 1)];
-        v[5] += L1.x[parent_index(L1, i, j, k + 1)];
-    }
+    if (CORR) add_parents(L1, i, j, k, v);
     float t[6];
     fine_coefs(M, code, i, j, k, t, D);
     float s = 0.0f;
@@ -497,6 +489,17 @@ __device__ __forceinline__ double cell_vol(const MGDev &M, int i, int j, int k)
 __device__ __forceinline__ void ref_weights(const RoomDev &R, const MGDev &M, unsigned code, int i, int j, int k,
                                             double (&w)[6], double &diag)
 {
+    const bool allin = (code & 0xFFFu) == SC_ALLIN;
+    if (M.uniform) {
+        if (allin) {
+            // six unknown neighbours: the sums below, precomputed in the same order
+            w[0] = w[1] = M.s64x;
+            w[2] = w[3] = M.s64y;
+            w[4] = w[5] = M.s64z;
+            diag = M.diag64;
+            return;
+        }
+    }
     double s[6];
     if (M.uniform) {
         s[0] = s[1] = M.s64x;
@@ -509,11 +512,19 @@ __device__ __forceinline__ void ref_weights(const RoomDev &R, const MGDev &M, un
         s[0] = sxl[i]; s[1] = sxr[i]; s[2] = syl[j]; s[3] = syr[j]; s[4] = szl[k]; s[5] = szr[k];
     }
     diag = 0.0;
+    if (allin) {
 #pragma unroll
-    for (int a = 0; a < 6; a++) {
-        const unsigned cls = (code >> (2 * a)) & 3u;
-        w[a] = cls == SC_IN ? s[a] : 0.0;
-        diag += cls == SC_IN ? s[a] : (cls == SC_DIR ? 2.0 * s[a] : 0.0);
+        for (int a = 0; a < 6; a++) {
+            w[a] = s[a];
+            diag += s[a];
+        }
+    } else {
+#pragma unroll
+        for (int a = 0; a < 6; a++) {
+            const unsigned cls = (code >> (2 * a)) & 3u;
+            w[a] = cls == SC_IN ? s[a] : 0.0;
+            diag += cls == SC_IN ? s[a] : (cls == SC_DIR ? 2.0 * s[a] : 0.0);
+        }
     }
     if (diag < 1e-30) diag = 1.0;
 }
@@ -1187,6 +1198,13 @@ int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGD
     M.s64y = 1.0 / (r.dyv[0] * r.dyv[0]);
     M.s64z = 1.0 / (r.dzv[0] * r.dzv[0]);
     M.vol64 = r.dxv[0] * r.dyv[0] * r.dzv[0];
+    {
+        // diagonal of a row with six unknown neighbours, summed in the row's order
+        double d = 0.0;
+        const double sx[6] = {M.s64x, M.s64x, M.s64y, M.s64y, M.s64z, M.s64z};
+        for (double v : sx) d += v;
+        M.diag64 = d;
+    }
     M.ixl = fxl; M.ixr = fxr; M.iyl = fyl; M.iyr = fyr; M.izl = fzl; M.izr = fzr;
     for (int l = 1; l < M.nlev; l++) {
         const size_t m = (size_t)h.nx[l] * h.ny[l] * h.nz[l];

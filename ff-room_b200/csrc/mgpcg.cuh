@@ -34,6 +34,7 @@ struct MGDev {
     int uniform;          // all spacings equal per axis: tx, ty, tz, vol hold the constants
     float tx, ty, tz, vol;
     double s64x, s64y, s64z, vol64;   // uniform: FP64 stencil scales 1/h^2 and cell volume
+    double diag64;                    // uniform: FP64 diagonal of an all-interior row
     float *r32;           // FP32 copy of the scaled CG residual (level-0 rhs)
 };
 
