@@ -52,7 +52,11 @@ CG_FINAL_B = 24.0      # x += alpha d
 # level); once per solve: set-up 60 and the final x update 24.
 PCG_ITER_B = 163.0
 PCG_ONCE_B = 84.0
-LBM_STEP_B = {"fp64": 2 * 19 * 8 + 1 + 4 * 8, "fp32": 2 * 19 * 4 + 1 + 4 * 8, "fp16": 2 * 19 * 2 + 1 + 4 * 8}
+# LBM step kernel per lattice cell: read and write 19 populations, the
+# flag byte, the cell velocity (FP64 with FP64 populations, else FP32) and
+# p (FP64); boundary cells also read a 4-byte blocked-direction mask.
+LBM_STEP_B = {"fp64": 2 * 19 * 8 + 1 + 3 * 8 + 8, "fp32": 2 * 19 * 4 + 1 + 3 * 4 + 8,
+              "fp16": 2 * 19 * 2 + 1 + 3 * 4 + 8}
 
 
 def measured_peak():

@@ -32,10 +32,55 @@
 
 namespace ffr {
 
-__constant__ int c_ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
-__constant__ int c_ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
-__constant__ int c_ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
-__constant__ int c_opp[19] = {0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17};
+// D3Q19 velocities and opposites (LBMSolver.cpp:11-27) as compile-time
+// functions: in the unrolled q loops every e_q folds into the arithmetic
+// (an add, a subtract or nothing) instead of a load and a conversion.
+//   e_x = +1 for q in {1,7,9,11,13}, -1 for {2,8,10,12,14}
+//   e_y = +1 for q in {3,7,8,15,17}, -1 for {4,9,10,16,18}
+//   e_z = +1 for q in {5,11,12,15,16}, -1 for {6,13,14,17,18}
+__host__ __device__ constexpr int lbm_sign(unsigned plus, unsigned minus, int q)
+{
+    return (int)((plus >> q) & 1u) - (int)((minus >> q) & 1u);
+}
+__host__ __device__ constexpr int c_ex(int q) { return lbm_sign(0x2A82u, 0x5504u, q); }
+__host__ __device__ constexpr int c_ey(int q) { return lbm_sign(0x28188u, 0x50610u, q); }
+__host__ __device__ constexpr int c_ez(int q) { return lbm_sign(0x19820u, 0x66040u, q); }
+// OPP pairs q with q+1 for odd q (1<->2, 3<->4, ..., 17<->18)
+__host__ __device__ constexpr int c_opp(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
+// the direction -e_q (not OPP[q] for the diagonals)
+__host__ __device__ constexpr int c_rev(int q)
+{
+    int r = 0;
+    for (int p = 0; p < 19; p++)
+        if (c_ex(p) == -c_ex(q) && c_ey(p) == -c_ey(q) && c_ez(p) == -c_ez(q)) r = p;
+    return r;
+}
+static_assert(c_rev(7) == 10 && c_rev(8) == 9 && c_rev(11) == 14 && c_rev(12) == 13 && c_rev(15) == 18 &&
+                  c_rev(16) == 17 && c_rev(1) == 2 && c_rev(0) == 0,
+              "D3Q19 reverse directions");
+
+// e_q . (ux, uy, uz) over the non-zero components, in the order x, y, z
+// (the zero terms of the reference's sum add a signed zero only).
+template <class F>
+__device__ __forceinline__ F edot(int q, F ux, F uy, F uz)
+{
+    F s = F(0);
+    bool any = false;
+    if (c_ex(q)) { s = c_ex(q) > 0 ? ux : -ux; any = true; }
+    if (c_ey(q)) { s = any ? (c_ey(q) > 0 ? s + uy : s - uy) : (c_ey(q) > 0 ? uy : -uy); any = true; }
+    if (c_ez(q)) { s = any ? (c_ez(q) > 0 ? s + uz : s - uz) : (c_ez(q) > 0 ? uz : -uz); }
+    return s;
+}
+
+// rho, j += f_q (1, e_q) without the zero products
+template <class F>
+__device__ __forceinline__ void add_moments(int q, F f, F &rho, F &jx, F &jy, F &jz)
+{
+    rho += f;
+    if (c_ex(q) > 0) jx += f; else if (c_ex(q) < 0) jx -= f;
+    if (c_ey(q) > 0) jy += f; else if (c_ey(q) < 0) jy -= f;
+    if (c_ez(q) > 0) jz += f; else if (c_ez(q) < 0) jz -= f;
+}
 
 // D3Q19 weights (LBMSolver.cpp:19-25).
 __host__ __device__ __forceinline__ double lbm_w(int q)
@@ -48,7 +93,7 @@ __host__ __device__ __forceinline__ double lbm_w(int q)
 __device__ __forceinline__ double feq64(int q, double rho, double ux, double uy, double uz)
 {
     const double cs2 = 1.0 / 3.0;
-    const double eu = c_ex[q] * ux + c_ey[q] * uy + c_ez[q] * uz;
+    const double eu = edot<double>(q, ux, uy, uz);
     const double usq = ux * ux + uy * uy + uz * uz;
     return lbm_w(q) * rho * (1.0 + eu / cs2 + eu * eu / (2.0 * cs2 * cs2) - usq / (2.0 * cs2));
 }
@@ -56,7 +101,7 @@ __device__ __forceinline__ double feq64(int q, double rho, double ux, double uy,
 // Shifted equilibrium feq_q - w_q in FP32 for rho = 1 + drho.
 __device__ __forceinline__ float geq32(int q, float drho, float ux, float uy, float uz)
 {
-    const float eu = c_ex[q] * ux + c_ey[q] * uy + c_ez[q] * uz;
+    const float eu = edot<float>(q, ux, uy, uz);
     const float usq = ux * ux + uy * uy + uz * uz;
     const float rho = 1.0f + drho;
     return (float)lbm_w(q) * (drho + rho * (3.0f * eu + 4.5f * eu * eu - 1.5f * usq));
@@ -87,12 +132,14 @@ struct LbmDev {
     int nx, ny, nz, n, nu, nv, nw;
     const uint8_t *ct;          // cell types
     const uint8_t *fl;          // cell type | LF_* flags
+    const uint32_t *blk;        // bit q: x + e_q outside the room or SOLID (non-open cells)
     const uint8_t *fan_of;      // fan index of each INFLOW cell (255: none)
     const double *fan_lat;      // lattice fan velocity, 3 per fan
     const int *remap_dst;       // sorted OUTFLOW destinations
     const int *remap_src;       // their resolved source cells
     int nremap;
     const double *dxv, *dyv, *dzv;
+    const double *idxv, *idyv, *idzv;   // 1 / spacing (the per-step divergence)
     double tau, l2p;
 };
 
@@ -114,79 +161,90 @@ __device__ __forceinline__ int find_src(const LbmDev &L, int c)
     return c;
 }
 
+// Cell-centred velocity between the step and face kernels: FP64 with FP64
+// populations, FP32 with the narrow storage modes (their collision is FP32).
+template <int MODE> using CellVel = typename std::conditional<MODE == 0, double, float>::type;
+
 // One fused step; see the file comment.  fa = f* of this step, fb = f* of
 // the next, cu/cv/cw = cell-centred velocity (m/s), p = rho*cs^2.
 template <int MODE>
-__global__ void __launch_bounds__(256, MODE == 0 ? 2 : 3)
-    k_lbm_step(LbmDev L, const typename Store<MODE>::T *f0, typename Store<MODE>::T *f1, double *__restrict__ cu,
-               double *__restrict__ cv, double *__restrict__ cw, double *__restrict__ p, const LbmState *st)
+__global__ void __launch_bounds__(256, MODE == 0 ? 3 : 4)
+    k_lbm_step(LbmDev L, const typename Store<MODE>::T *f0, typename Store<MODE>::T *f1,
+               CellVel<MODE> *__restrict__ cu, CellVel<MODE> *__restrict__ cv, CellVel<MODE> *__restrict__ cw,
+               double *__restrict__ p, const LbmState *st)
 {
     using S = Store<MODE>;
     using T = typename S::T;
     if (st->halt) return;
     const T *__restrict__ fa = st->par ? f1 : f0;
     T *__restrict__ fb = st->par ? (T *)f0 : f1;
-    const int nx = L.nx, ny = L.ny, nz = L.nz, n = L.n, plane = ny * nz;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        const uint8_t fl = L.fl[c];
+    const int ny = L.ny, nz = L.nz, n = L.n, plane = ny * nz;
+    // The flags and blocked-direction mask of the next cell are loaded while
+    // this cell's populations are in flight, so each cell waits for one
+    // round trip to memory only.
+    const int c0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    uint8_t fl = 0, fln = 0;
+    unsigned Bc = 0, Bn = 0;
+    // (interior cells have no blocked direction and skip the mask load)
+    if (c0 < n) { fl = L.fl[c0]; Bc = (fl & LF_OPEN) ? 0u : L.blk[c0]; }
+    for (int c = c0; c < n; c += stride, fl = fln, Bc = Bn) {
+        if (c + stride < n) {
+            fln = L.fl[c + stride];
+            Bn = (fln & LF_OPEN) ? 0u : L.blk[c + stride];
+        }
         const uint8_t t = fl & 3;
         if (t == CT_SOLID) {
-            cu[c] = 0.0; cv[c] = 0.0; cw[c] = 0.0;
+            cu[c] = 0; cv[c] = 0; cw[c] = 0;
             continue;
         }
         using C = typename std::conditional<MODE == 0, double, float>::type;
         C fq[19];
-        if (fl & LF_OPEN) {
-            // interior cell: every slot is streamed from its upwind neighbour
-#pragma unroll
-            for (int q = 0; q < 19; q++)
-                fq[q] = C(S::ld(fa + (q * n + c - (c_ex[q] * plane + c_ey[q] * nz + c_ez[q]))));
-        } else {
+        // x: the cell whose post-stream populations this cell ends with
         const int o = (fl & LF_REMAP) ? find_src(L, c) : c;
-        if (L.ct[o] == CT_SOLID) {
+        if ((fl & LF_REMAP) && L.ct[o] == CT_SOLID) {
 #pragma unroll
             for (int q = 0; q < 19; q++) fq[q] = MODE == 0 ? C(0) : C(-lbm_w(q));
         } else {
-            const int oi = o / plane, orem = o - oi * plane, oj = orem / nz, ok = orem - oj * nz;
+            // blocked directions of x (bit q: x + e_q outside the room or
+            // SOLID; 0 for an interior cell).  Slot q receives
+            //  (a) f*_q(x - e_q) when x - e_q = x + e_{-q} is not blocked;
+            //  (b) f*_OPP[q](x) when x's own direction OPP[q] is blocked.
+            // OPP of LBMSolver.cpp:27 pairs the diagonals as mirror images
+            // (7 <-> 8 is (1,1,0) <-> (-1,1,0)), so (a) and (b) are
+            // independent and a slot gets 0, 1 or 2 values.
+            const unsigned B = (fl & LF_REMAP) ? L.blk[o] : Bc;
+            // (a) for every slot, unconditionally: a blocked source reads the
+            // cell's own slot instead (a valid address) and is replaced below
 #pragma unroll
             for (int q = 0; q < 19; q++) {
-                // (a) the neighbour x - e_q streams into slot q
-                const int si = oi - c_ex[q], sj = oj - c_ey[q], sk = ok - c_ez[q];
-                const int s = o - c_ex[q] * plane - c_ey[q] * nz - c_ez[q];
-                const bool ina = si >= 0 && si < nx && sj >= 0 && sj < ny && sk >= 0 && sk < nz && L.ct[s] != CT_SOLID;
-                // (b) x's own direction OPP[q] is blocked and reflects into slot q.
-                // OPP of LBMSolver.cpp:27 pairs the diagonals as mirror images
-                // (7 <-> 8 is (1,1,0) <-> (-1,1,0)), so (a) and (b) are
-                // independent and a slot gets 0, 1 or 2 values.
-                const int qq = c_opp[q];
-                const int ti = oi + c_ex[qq], tj = oj + c_ey[qq], tk = ok + c_ez[qq];
-                const int tcell = o + c_ex[qq] * plane + c_ey[qq] * nz + c_ez[qq];
-                const bool inb = !(ti >= 0 && ti < nx && tj >= 0 && tj < ny && tk >= 0 && tk < nz) || L.ct[tcell] == CT_SOLID;
-                if (MODE == 0) {
-                    C v = C(0);
-                    if (ina) v = v + S::ld(fa + (q * n + s));
-                    if (inb) v = v + S::ld(fa + (qq * n + o));
-                    fq[q] = v;
-                } else {
-                    // shifted storage g = f - w (w_q == w_OPP[q]): g_post = sum g + (k-1) w_q
-                    C v = C(-lbm_w(q));
-                    if (ina) v += S::ld(fa + (q * n + s)) + C(lbm_w(q));
-                    if (inb) v += S::ld(fa + (qq * n + o)) + C(lbm_w(q));
-                    fq[q] = v;
+                const int s = o - (c_ex(q) * plane + c_ey(q) * nz + c_ez(q));
+                fq[q] = C(S::ld(fa + (q * n + (((B >> c_rev(q)) & 1u) ? o : s))));
+            }
+            if (B) {
+                // cells next to a wall or SOLID: drop blocked sources, add (b)
+#pragma unroll
+                for (int q = 0; q < 19; q++) {
+                    const int qq = c_opp(q);
+                    const bool ina = !((B >> c_rev(q)) & 1u);
+                    const bool inb = (B >> qq) & 1u;
+                    const C va = fq[q];
+                    const C vb = inb ? C(S::ld(fa + (qq * n + o))) : C(0);
+                    if (MODE == 0) {
+                        // the reference's zeroed slot plus what arrives
+                        fq[q] = ina ? (inb ? va + vb : va) : vb;
+                    } else {
+                        // shifted storage g = f - w (w_q == w_OPP[q]): two
+                        // arrivals give g_a + g_b + w, none gives -w
+                        fq[q] = ina ? (inb ? va + vb + C(lbm_w(q)) : va) : (inb ? vb : C(-lbm_w(q)));
+                    }
                 }
             }
-        }
         }
         // moments (LBMSolver.cpp:306-318) and next-step collision
         if (MODE == 0) {
             double rho = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
 #pragma unroll
-            for (int q = 0; q < 19; q++) {
-                rho += fq[q];
-                ux += fq[q] * c_ex[q];
-                uy += fq[q] * c_ey[q];
-                uz += fq[q] * c_ez[q];
-            }
+            for (int q = 0; q < 19; q++) add_moments<double>(q, fq[q], rho, ux, uy, uz);
             if (rho > 1e-14) { ux /= rho; uy /= rho; uz /= rho; }
             cu[c] = ux * L.l2p; cv[c] = uy * L.l2p; cw[c] = uz * L.l2p;
             p[c] = rho * (1.0 / 3.0);
@@ -208,16 +266,13 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 2 : 3)
         } else {
             float drho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
 #pragma unroll
-            for (int q = 0; q < 19; q++) {
-                drho += fq[q];
-                jx += fq[q] * c_ex[q];
-                jy += fq[q] * c_ey[q];
-                jz += fq[q] * c_ez[q];
-            }
+            for (int q = 0; q < 19; q++) add_moments<float>(q, fq[q], drho, jx, jy, jz);
             const float rho = 1.0f + drho;
             float ux = jx, uy = jy, uz = jz;
             if (rho > 1e-14f) { ux /= rho; uy /= rho; uz /= rho; }
-            cu[c] = (double)ux * L.l2p; cv[c] = (double)uy * L.l2p; cw[c] = (double)uz * L.l2p;
+            cu[c] = (float)((double)ux * L.l2p);
+            cv[c] = (float)((double)uy * L.l2p);
+            cw[c] = (float)((double)uz * L.l2p);
             p[c] = (double)rho * (1.0 / 3.0);
             if (t == CT_INFLOW && L.fan_of[c] != 255) {
                 const double *fv = L.fan_lat + 3 * L.fan_of[c];
@@ -257,7 +312,7 @@ __global__ void k_lbm_init(LbmDev L, typename Store<MODE>::T *f)
             if (t == CT_FLUID || t == CT_OUTFLOW) {
                 double rho = 0.0, ux = 0.0, uy = 0.0, uz = 0.0;
                 for (int q = 0; q < 19; q++) {
-                    rho += fq[q]; ux += fq[q] * c_ex[q]; uy += fq[q] * c_ey[q]; uz += fq[q] * c_ez[q];
+                    rho += fq[q]; ux += fq[q] * c_ex(q); uy += fq[q] * c_ey(q); uz += fq[q] * c_ez(q);
                 }
                 if (rho > 1e-14) { ux /= rho; uy /= rho; uz /= rho; }
                 const double itau = 1.0 / L.tau;
@@ -275,7 +330,7 @@ __global__ void k_lbm_init(LbmDev L, typename Store<MODE>::T *f)
             if (t == CT_FLUID || t == CT_OUTFLOW) {
                 float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
                 for (int q = 0; q < 19; q++) {
-                    drho += g[q]; jx += g[q] * c_ex[q]; jy += g[q] * c_ey[q]; jz += g[q] * c_ez[q];
+                    drho += g[q]; jx += g[q] * c_ex(q); jy += g[q] * c_ey(q); jz += g[q] * c_ez(q);
                 }
                 const float rho = 1.0f + drho;
                 const float itau = (float)(1.0 / L.tau);
@@ -290,9 +345,10 @@ __global__ void k_lbm_init(LbmDev L, typename Store<MODE>::T *f)
 // Face velocities of extract_macroscopic (LBMSolver.cpp:333-375), max
 // |du| against the previous faces (LBMSolver.cpp:423-433) and max |div|
 // over FLUID cells (LBMSolver.cpp:382-396), cell-centric like k_correct.
-__global__ void __launch_bounds__(256) k_lbm_faces(LbmDev L, const double *__restrict__ cu,
-                                                   const double *__restrict__ cv,
-                                                   const double *__restrict__ cw, double *__restrict__ u,
+template <class V>
+__global__ void __launch_bounds__(256) k_lbm_faces(LbmDev L, const V *__restrict__ cu,
+                                                   const V *__restrict__ cv,
+                                                   const V *__restrict__ cw, double *__restrict__ u,
                                                    double *__restrict__ v, double *__restrict__ w,
                                                    LbmState *st)
 {
@@ -300,14 +356,17 @@ __global__ void __launch_bounds__(256) k_lbm_faces(LbmDev L, const double *__res
     if (st->halt) return;
     const int nx = L.nx, ny = L.ny, nz = L.nz, plane = ny * nz;
     double dmax = 0.0, divmax = 0.0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.n; c += gridDim.x * blockDim.x) {
-        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+    for (Walk wk(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, ny, nz, L.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
         const int uf = c, vf = (i * (ny + 1) + j) * nz + k, wf = (i * ny + j) * (nz + 1) + k;
         // every load first, then the arithmetic, then the stores
         const double cuc = cu[c], cvc = cv[c], cwc = cw[c];
-        const double cum = (i > 0) ? cu[c - plane] : 0.0, cup = (i < nx - 1) ? cu[c + plane] : 0.0;
-        const double cvm = (j > 0) ? cv[c - nz] : 0.0, cvp = (j < ny - 1) ? cv[c + nz] : 0.0;
-        const double cwm = (k > 0) ? cw[c - 1] : 0.0, cwp = (k < nz - 1) ? cw[c + 1] : 0.0;
+        // neighbours through indices clamped into the arrays (the value is
+        // only used when the neighbour exists)
+        const int last = L.n - 1;
+        const double cum = cu[max(c - plane, 0)], cup = cu[min(c + plane, last)];
+        const double cvm = cv[max(c - nz, 0)], cvp = cv[min(c + nz, last)];
+        const double cwm = cw[max(c - 1, 0)], cwp = cw[min(c + 1, last)];
         const double uo = u[uf], vo = v[vf], wo = w[wf];
         const double uho = (i == nx - 1) ? u[uf + plane] : 0.0;
         const double vho = (j == ny - 1) ? v[vf + nz] : 0.0;
@@ -326,7 +385,7 @@ __global__ void __launch_bounds__(256) k_lbm_faces(LbmDev L, const double *__res
         if (j == ny - 1) dmax = fmax(dmax, fabs(vhi - vho));
         if (k == nz - 1) dmax = fmax(dmax, fabs(whi - who));
         if (fluid)
-            divmax = fmax(divmax, fabs((uhi - ulo) / L.dxv[i] + (vhi - vlo) / L.dyv[j] + (whi - wlo) / L.dzv[k]));
+            divmax = fmax(divmax, fabs((uhi - ulo) * L.idxv[i] + (vhi - vlo) * L.idyv[j] + (whi - wlo) * L.idzv[k]));
         u[uf] = ulo;
         v[vf] = vlo;
         w[wf] = wlo;
@@ -428,21 +487,28 @@ int lbm_enqueue(ffr_lbm *s)
     s->prof.begin(FFR_LPROF_STREAM_COLLIDE, st);
     switch (s->storage) {
     case FFR_LBM_FP64:
-        k_lbm_step<0><<<s->blocks, kThr, 0, st>>>(s->L, (const double *)s->f0, (double *)s->f1, s->cu, s->cv,
-                                                    s->cw, s->p, s->st);
+        k_lbm_step<0><<<s->blocks, kThr, 0, st>>>(s->L, (const double *)s->f0, (double *)s->f1,
+                                                    (CellVel<0> *)s->cu, (CellVel<0> *)s->cv,
+                                                    (CellVel<0> *)s->cw, s->p, s->st);
         break;
     case FFR_LBM_FP32:
-        k_lbm_step<1><<<s->blocks, kThr, 0, st>>>(s->L, (const float *)s->f0, (float *)s->f1, s->cu, s->cv,
-                                                    s->cw, s->p, s->st);
+        k_lbm_step<1><<<s->blocks, kThr, 0, st>>>(s->L, (const float *)s->f0, (float *)s->f1,
+                                                    (CellVel<1> *)s->cu, (CellVel<1> *)s->cv,
+                                                    (CellVel<1> *)s->cw, s->p, s->st);
         break;
     default:
-        k_lbm_step<2><<<s->blocks, kThr, 0, st>>>(s->L, (const __half *)s->f0, (__half *)s->f1, s->cu, s->cv,
-                                                    s->cw, s->p, s->st);
+        k_lbm_step<2><<<s->blocks, kThr, 0, st>>>(s->L, (const __half *)s->f0, (__half *)s->f1,
+                                                    (CellVel<2> *)s->cu, (CellVel<2> *)s->cv,
+                                                    (CellVel<2> *)s->cw, s->p, s->st);
     }
     FFR_LAUNCHED(1);
     s->prof.end(st, 1);
     s->prof.begin(FFR_LPROF_FACES, st);
-    k_lbm_faces<<<s->blocks, kThr, 0, st>>>(s->L, s->cu, s->cv, s->cw, s->u, s->v, s->w, s->st);
+    if (s->storage == FFR_LBM_FP64)
+        k_lbm_faces<double><<<s->blocks, kThr, 0, st>>>(s->L, s->cu, s->cv, s->cw, s->u, s->v, s->w, s->st);
+    else
+        k_lbm_faces<float><<<s->blocks, kThr, 0, st>>>(s->L, (const float *)s->cu, (const float *)s->cv,
+                                                       (const float *)s->cw, s->u, s->v, s->w, s->st);
     FFR_LAUNCHED(1);
     k_lbm_finalize<<<1, 32, 0, st>>>(s->dt, s->tol, s->st, s->ring);
     FFR_LAUNCHED(1);
@@ -533,6 +599,7 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     resolve_remap(s->room, rd, rs);
     // step-kernel flags: open interior cells skip every neighbour test
     std::vector<uint8_t> flags(g.n);
+    std::vector<uint32_t> blocked(g.n, 0);
     {
         static const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
         static const int ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
@@ -545,21 +612,23 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
                     const int c = (i * ny + j) * nz + k;
                     uint8_t f = s->room.ct[c];
                     if (remapped[c]) f |= LF_REMAP;
-                    bool open = f != CT_SOLID && !remapped[c];
-                    for (int q = 1; q < 19 && open; q++) {
+                    uint32_t bl = 0;
+                    for (int q = 1; q < 19; q++) {
                         const int a = i + ex[q], b = j + ey[q], e = k + ez[q];
-                        open = a >= 0 && a < nx && b >= 0 && b < ny && e >= 0 && e < nz &&
-                               s->room.ct[(a * ny + b) * nz + e] != CT_SOLID;
+                        const bool ok = a >= 0 && a < nx && b >= 0 && b < ny && e >= 0 && e < nz &&
+                                        s->room.ct[(a * ny + b) * nz + e] != CT_SOLID;
+                        if (!ok) bl |= 1u << q;
                     }
-                    if (open) f |= LF_OPEN;
+                    blocked[c] = bl;
+                    if (f != CT_SOLID && !remapped[c] && bl == 0) f |= LF_OPEN;
                     flags[c] = f;
                 }
     }
     const size_t es = storage == FFR_LBM_FP64 ? 8 : (storage == FFR_LBM_FP32 ? 4 : 2);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = 2 * al(es * 19 * g.n) + 4 * al(8 * g.n) + al(8 * g.nu) + al(8 * g.nv) +
-                         al(8 * g.nw) + 3 * al(g.n) + al(8 * fan_lat.size()) + 2 * al(4 * (rd.size() + 1)) +
-                         al(8 * g.nx) + al(8 * g.ny) + al(8 * g.nz) + al(sizeof(LbmState)) +
+                         al(8 * g.nw) + 3 * al(g.n) + al(4 * g.n) + al(8 * fan_lat.size()) + 2 * al(4 * (rd.size() + 1)) +
+                         2 * (al(8 * g.nx) + al(8 * g.ny) + al(8 * g.nz)) + al(sizeof(LbmState)) +
                          al(sizeof(ffr_step_result) * kRingL) + al(8);
     rc = s->arena.alloc(bytes);
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
@@ -570,9 +639,11 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     s->p = a.take<double>(g.n);
     s->u = a.take<double>(g.nu); s->v = a.take<double>(g.nv); s->w = a.take<double>(g.nw);
     uint8_t *ct = a.take<uint8_t>(g.n), *fo = a.take<uint8_t>(g.n), *fld = a.take<uint8_t>(g.n);
+    uint32_t *blk = a.take<uint32_t>(g.n);
     double *fl = a.take<double>(fan_lat.size());
     int *rdd = a.take<int>(rd.size() + 1), *rsd = a.take<int>(rd.size() + 1);
     double *dxv = a.take<double>(g.nx), *dyv = a.take<double>(g.ny), *dzv = a.take<double>(g.nz);
+    double *idxv = a.take<double>(g.nx), *idyv = a.take<double>(g.ny), *idzv = a.take<double>(g.nz);
     s->st = a.take<LbmState>(1);
     s->ring = a.take<ffr_step_result>(kRingL);
     s->div_slot = a.take<unsigned long long>(1);
@@ -585,12 +656,20 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     FFR_CUDA(cudaMemcpyAsync(ct, s->room.ct.data(), g.n, cudaMemcpyHostToDevice, st));
     FFR_CUDA(cudaMemcpyAsync(fo, fan_of.data(), g.n, cudaMemcpyHostToDevice, st));
     FFR_CUDA(cudaMemcpyAsync(fld, flags.data(), g.n, cudaMemcpyHostToDevice, st));
+    FFR_CUDA(cudaMemcpyAsync(blk, blocked.data(), 4 * g.n, cudaMemcpyHostToDevice, st));
     FFR_CUDA(cudaMemcpyAsync(fl, fan_lat.data(), 8 * fan_lat.size(), cudaMemcpyHostToDevice, st));
     if (!rd.empty()) {
         FFR_CUDA(cudaMemcpyAsync(rdd, rd.data(), 4 * rd.size(), cudaMemcpyHostToDevice, st));
         FFR_CUDA(cudaMemcpyAsync(rsd, rs.data(), 4 * rs.size(), cudaMemcpyHostToDevice, st));
     }
     FFR_CUDA(cudaMemcpyAsync(dxv, s->room.dxv.data(), 8 * g.nx, cudaMemcpyHostToDevice, st));
+    std::vector<double> inv(g.nx + g.ny + g.nz);
+    for (int i = 0; i < g.nx; i++) inv[i] = 1.0 / s->room.dxv[i];
+    for (int j = 0; j < g.ny; j++) inv[g.nx + j] = 1.0 / s->room.dyv[j];
+    for (int k = 0; k < g.nz; k++) inv[g.nx + g.ny + k] = 1.0 / s->room.dzv[k];
+    FFR_CUDA(cudaMemcpyAsync(idxv, inv.data(), 8 * g.nx, cudaMemcpyHostToDevice, st));
+    FFR_CUDA(cudaMemcpyAsync(idyv, inv.data() + g.nx, 8 * g.ny, cudaMemcpyHostToDevice, st));
+    FFR_CUDA(cudaMemcpyAsync(idzv, inv.data() + g.nx + g.ny, 8 * g.nz, cudaMemcpyHostToDevice, st));
     FFR_CUDA(cudaMemcpyAsync(dyv, s->room.dyv.data(), 8 * g.ny, cudaMemcpyHostToDevice, st));
     FFR_CUDA(cudaMemcpyAsync(dzv, s->room.dzv.data(), 8 * g.nz, cudaMemcpyHostToDevice, st));
     auto up = [&](double *d, const double *h, long long cnt) -> int {
@@ -604,8 +683,8 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
         return rc;
     }
     FFR_CUDA(cudaMemsetAsync(s->st, 0, sizeof(LbmState), st));
-    s->L = LbmDev{nx, ny, nz, (int)g.n, (int)g.nu, (int)g.nv, (int)g.nw, ct, fld, fo, fl, rdd, rsd,
-                  (int)rd.size(), dxv, dyv, dzv, tau, (g.lx / g.nx) / dt};
+    s->L = LbmDev{nx, ny, nz, (int)g.n, (int)g.nu, (int)g.nv, (int)g.nw, ct, fld, blk, fo, fl, rdd, rsd,
+                  (int)rd.size(), dxv, dyv, dzv, idxv, idyv, idzv, tau, (g.lx / g.nx) / dt};
     s->blocks = blocks_for(g.n);
     switch (storage) {
     case FFR_LBM_FP64: k_lbm_init<0><<<s->blocks, kThr, 0, st>>>(s->L, (double *)s->f0); break;

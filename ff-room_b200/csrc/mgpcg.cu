@@ -149,38 +149,6 @@ __device__ bool grid_barrier(GridSync *gs)
     return s_ok;
 }
 
-__device__ __forceinline__ void decode(int c, int ny, int nz, int &i, int &j, int &k)
-{
-    const int plane = ny * nz;
-    i = c / plane;
-    const int rem = c - i * plane;
-    j = rem / nz;
-    k = rem - j * nz;
-}
-
-// Visits the flat indices start, start + stride, ... < n of a (., ny, nz)
-// grid and keeps (i, j, k) up to date with carries instead of dividing for
-// every cell.
-struct Walk {
-    int c, i, j, k, si, sj, sk, stride, ny, nz, n;
-    __device__ __forceinline__ Walk(int start, int stride_, int ny_, int nz_, int n_)
-        : c(start), stride(stride_), ny(ny_), nz(nz_), n(n_)
-    {
-        decode(start, ny, nz, i, j, k);
-        decode(stride, ny, nz, si, sj, sk);
-    }
-    __device__ __forceinline__ bool ok() const { return c < n; }
-    __device__ __forceinline__ void next()
-    {
-        c += stride;
-        k += sk;
-        j += sj;
-        i += si;
-        if (k >= nz) { k -= nz; j++; }
-        if (j >= ny) { j -= ny; i++; }
-    }
-};
-
 // Level-0 (fine) FP32 coefficients of cell (i,j,k) from its stencil code:
 // t[6] in the order x-, x+, y-, y+, z-, z+ (0 unless the neighbour is an
 // unknown) and the diagonal (Dirichlet ghosts count twice).
