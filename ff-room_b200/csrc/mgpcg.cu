@@ -783,8 +783,12 @@ __device__ __forceinline__ void pass_backsub(const PCGArgs &A, int start, int st
     }
 }
 
-template <class G>
-__global__ void __launch_bounds__(256, 3) k_pcg(PCGArgs A)
+// Threads per block of the one-cluster schedule: a cluster of at most 16
+// blocks must still hold enough warps per SM to hide memory latency.
+constexpr int kClusterThreads = 512;
+
+template <class G, int NT = 256>
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_pcg(PCGArgs A)
 {
     __shared__ double sh[32];
     if (A.st && A.st->halt) return;
@@ -1210,12 +1214,13 @@ int launch_pcg_cluster(const PCGArgs &a, cudaStream_t s, int ctas)
 {
     static bool attr_set = false;
     if (!attr_set) {
-        FFR_CUDA(cudaFuncSetAttribute(k_pcg<ClusterGroup>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        FFR_CUDA(cudaFuncSetAttribute(k_pcg<ClusterGroup, kClusterThreads>,
+                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         attr_set = true;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)ctas);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(kClusterThreads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -1225,7 +1230,7 @@ int launch_pcg_cluster(const PCGArgs &a, cudaStream_t s, int ctas)
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    FFR_CUDA(cudaLaunchKernelEx(&cfg, k_pcg<ClusterGroup>, a));
+    FFR_CUDA(cudaLaunchKernelEx(&cfg, k_pcg<ClusterGroup, kClusterThreads>, a));
     count_launch(1);
     return FFR_OK;
 }
