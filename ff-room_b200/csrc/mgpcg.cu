@@ -895,51 +895,51 @@ struct SplitState {
     unsigned pad2;
 };
 
-// Block partials -> partials[blockIdx.x]; true in the one block that arrives
-// last, which then holds the grid total (summed in block order) in v.
+
+// Block partials -> partials[lb]; true in the one block of the room that
+// arrives last, which then holds the room total (summed in block order) in v.
 template <int NV>
-__device__ bool last_block_total(double (&v)[NV], double *partials, unsigned *ticket, double *sh)
+__device__ bool last_block_total(double (&v)[NV], double *partials, unsigned *ticket, double *sh, BPos P)
 {
     __shared__ int s_last;
     for (int a = 0; a < NV; a++) {
         const double t = block_sum(v[a], sh);
-        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NV + a] = t;
+        if (threadIdx.x == 0) partials[(size_t)P.lb * NV + a] = t;
     }
     if (threadIdx.x == 0) {
         __threadfence();
-        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+        s_last = atomicAdd(ticket, 1u) == (unsigned)P.nb - 1;
     }
     __syncthreads();
     if (!s_last) return false;
     __threadfence();
     for (int a = 0; a < NV; a++) {
         double t = 0.0;
-        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += __ldcg(&partials[(size_t)b * NV + a]);
+        for (int b = threadIdx.x; b < P.nb; b += blockDim.x) t += __ldcg(&partials[(size_t)b * NV + a]);
         v[a] = block_sum(t, sh);
     }
     if (threadIdx.x == 0) *ticket = 0;
     return true;
 }
 
-__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
-__device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
+// ---- bodies of the split solve's kernels, for one room, given the block's
+// position among that room's blocks.  `active` (batched solves only) counts
+// the rooms still iterating: +1 when a room starts, -1 when it finishes.
 
-// use_cond: the kernel runs inside a graph with a WHILE node on `cond`
-// (otherwise the host paces the iterations and reads ss->done).
-__global__ void __launch_bounds__(256) k_sp_init(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
-                                                 int use_cond)
+__device__ __forceinline__ void sp_init_body(const PCGArgs &A, SplitState *ss, BPos P, int *active,
+                                             cudaGraphConditionalHandle cond, int use_cond)
 {
     __shared__ double sh[32];
     if (A.st && A.st->halt) {
-        if (gtid() == 0) {
+        if (P.lb == 0 && threadIdx.x == 0) {
             ss->done = 1;
             if (use_cond) cudaGraphSetConditional(cond, 0);
         }
         return;
     }
     double acc[2] = {0.0, 0.0};
-    pass_init(A, gtid(), gthreads(), acc);
-    if (last_block_total<2>(acc, A.partials, &ss->ticket, sh) && threadIdx.x == 0) {
+    pass_init(A, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x, acc);
+    if (last_block_total<2>(acc, A.partials, &ss->ticket, sh, P) && threadIdx.x == 0) {
         ss->bnorm = sqrt(acc[0]);
         ss->it = 0;
         ss->pending = 0;
@@ -948,27 +948,86 @@ __global__ void __launch_bounds__(256) k_sp_init(PCGArgs A, SplitState *ss, cuda
         ss->res = 0.0;
         ss->alpha = ss->alpha_prev = ss->rz_old = ss->beta = 0.0;
         ss->done = ss->bnorm < 1e-15;
+        if (!ss->done && active) atomicAdd(active, 1);
         if (use_cond) cudaGraphSetConditional(cond, ss->done ? 0u : 1u);
     }
 }
 
-template <bool CORR>
-__global__ void __launch_bounds__(256) k_sp_smooth(PCGArgs A, const SplitState *ss, int l, int color)
+__device__ __forceinline__ void sp_redpost_body(const PCGArgs &A, SplitState *ss, BPos P)
 {
-    if (ss->done) return;
-    smooth_color<CORR>(A, A.M.lv, A.M.nlev, l, color, gtid(), gthreads());
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    pass_redpost_dot(A, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x, acc[0]);
+    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh, P) && threadIdx.x == 0) {
+        ss->beta = ss->it == 0 ? 0.0 : acc[0] / ss->rz_old;
+        ss->rz_old = acc[0];
+    }
 }
 
-__global__ void __launch_bounds__(256) k_sp_restrict(PCGArgs A, const SplitState *ss, int l)
+__device__ __forceinline__ void sp_direction_body(const PCGArgs &A, SplitState *ss, BPos P, int *active)
 {
-    if (ss->done) return;
-    restrict_level(A, A.M.lv, l, gtid(), gthreads());
+    __shared__ double sh[32];
+    const double *dold = ss->dpar ? A.db : A.da;
+    double *dnew = ss->dpar ? A.da : A.db;
+    double acc[1] = {0.0};
+    pass_direction(A, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x, ss->beta, ss->alpha_prev, ss->it > 0,
+                   dold, dnew, acc[0]);
+    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh, P) && threadIdx.x == 0) {
+        ss->dpar ^= 1;            // the new direction is current from here on
+        ss->pending = 0;
+        if (fabs(acc[0]) < 1e-30) {
+            ss->flags |= FFR_FLAG_CG_BREAKDOWN;
+            ss->done = 1;
+            if (active) atomicSub(active, 1);
+        } else {
+            ss->alpha = ss->rz_old / acc[0];
+        }
+    }
 }
 
-__global__ void __launch_bounds__(1024) k_sp_coarse(PCGArgs A, const SplitState *ss, int lo)
+__device__ __forceinline__ void sp_residual_body(const PCGArgs &A, SplitState *ss, BPos P, int *active,
+                                                 cudaGraphConditionalHandle cond, int use_cond)
 {
-    if (ss->done) return;
-    block_vcycle(A, lo);
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    pass_residual(A, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x, ss->alpha, acc[0]);
+    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh, P) && threadIdx.x == 0) {
+        ss->pending = 1;
+        ss->res = sqrt(acc[0]) / ss->bnorm;
+        ss->it += 1;
+        if (ss->res < A.tol) {
+            ss->done = 1;
+        } else if (ss->it >= A.max_iter) {
+            ss->flags |= FFR_FLAG_CG_MAXITER;
+            ss->done = 1;
+        } else {
+            ss->alpha_prev = ss->alpha;
+        }
+        if (ss->done && active) atomicSub(active, 1);
+        if (use_cond) cudaGraphSetConditional(cond, ss->done ? 0u : 1u);
+    }
+}
+
+__device__ __forceinline__ void sp_final_body(const PCGArgs &A, const SplitState *ss, BPos P)
+{
+    if (ss->pending)
+        pass_final_x(A, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x, ss->alpha, ss->dpar ? A.db : A.da);
+}
+
+__device__ __forceinline__ void sp_backsub_body(const PCGArgs &A, const SplitState *ss, BPos P)
+{
+    pass_backsub(A, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x);
+    if (P.lb == 0 && threadIdx.x == 0) {
+        const int iters = ss->bnorm < 1e-15 ? 0 : ss->it;
+        if (A.out_res) *A.out_res = ss->res;
+        if (A.out_iters) *A.out_iters = iters;
+        if (A.out_flags) *A.out_flags = ss->flags;
+        if (A.st) {
+            A.st->pres = ss->res;
+            A.st->iters = iters;
+            atomicOr(&A.st->flags, ss->flags);
+        }
+    }
 }
 
 // Levels mid .. nlev-1 of the V-cycle in one thread-block cluster: the
@@ -977,9 +1036,8 @@ __global__ void __launch_bounds__(1024) k_sp_coarse(PCGArgs A, const SplitState 
 // and the levels of at most kBlockLevelCells cells in block 0.  Every cell
 // update is the one the one-kernel-per-pass form makes (the colours are
 // Jacobi sweeps), so the result does not depend on this grouping.
-__global__ void __launch_bounds__(kMidThreads, 1) k_sp_mid(PCGArgs A, const SplitState *ss, int mid)
+__device__ __forceinline__ void sp_mid_body(const PCGArgs &A, int mid)
 {
-    if (ss->done) return;   // the same value in every block of the cluster
     auto cl = cooperative_groups::this_cluster();
     const MGDev &M = A.M;
     const int t0 = (int)cl.block_rank() * blockDim.x + threadIdx.x, nth = (int)cl.num_blocks() * blockDim.x;
@@ -1006,85 +1064,181 @@ __global__ void __launch_bounds__(kMidThreads, 1) k_sp_mid(PCGArgs A, const Spli
     }
 }
 
+// ---- one-room kernels (the grid is the room's)
+
+__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
+
+// use_cond: the kernel runs inside a graph with a WHILE node on `cond`
+// (otherwise the host paces the iterations and reads ss->done).
+__global__ void __launch_bounds__(256) k_sp_init(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
+                                                 int use_cond)
+{
+    sp_init_body(A, ss, grid_pos(), nullptr, cond, use_cond);
+}
+
+template <bool CORR>
+__global__ void __launch_bounds__(256) k_sp_smooth(PCGArgs A, const SplitState *ss, int l, int color)
+{
+    if (ss->done) return;
+    smooth_color<CORR>(A, A.M.lv, A.M.nlev, l, color, gtid(), gthreads());
+}
+
+__global__ void __launch_bounds__(256) k_sp_restrict(PCGArgs A, const SplitState *ss, int l)
+{
+    if (ss->done) return;
+    restrict_level(A, A.M.lv, l, gtid(), gthreads());
+}
+
+__global__ void __launch_bounds__(1024) k_sp_coarse(PCGArgs A, const SplitState *ss, int lo)
+{
+    if (ss->done) return;
+    block_vcycle(A, lo);
+}
+
+__global__ void __launch_bounds__(kMidThreads, 1) k_sp_mid(PCGArgs A, const SplitState *ss, int mid)
+{
+    if (ss->done) return;   // the same value in every block of the cluster
+    sp_mid_body(A, mid);
+}
+
 __global__ void __launch_bounds__(256) k_sp_redpost(PCGArgs A, SplitState *ss)
 {
-    __shared__ double sh[32];
     if (ss->done) return;
-    double acc[1] = {0.0};
-    pass_redpost_dot(A, gtid(), gthreads(), acc[0]);
-    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh) && threadIdx.x == 0) {
-        ss->beta = ss->it == 0 ? 0.0 : acc[0] / ss->rz_old;
-        ss->rz_old = acc[0];
-    }
+    sp_redpost_body(A, ss, grid_pos());
 }
 
 __global__ void __launch_bounds__(256, 3) k_sp_direction(PCGArgs A, SplitState *ss)
 {
-    __shared__ double sh[32];
     if (ss->done) return;
-    const double *dold = ss->dpar ? A.db : A.da;
-    double *dnew = ss->dpar ? A.da : A.db;
-    double acc[1] = {0.0};
-    pass_direction(A, gtid(), gthreads(), ss->beta, ss->alpha_prev, ss->it > 0, dold, dnew, acc[0]);
-    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh) && threadIdx.x == 0) {
-        ss->dpar ^= 1;            // the new direction is current from here on
-        ss->pending = 0;
-        if (fabs(acc[0]) < 1e-30) {
-            ss->flags |= FFR_FLAG_CG_BREAKDOWN;
-            ss->done = 1;
-        } else {
-            ss->alpha = ss->rz_old / acc[0];
-        }
-    }
+    sp_direction_body(A, ss, grid_pos(), nullptr);
 }
 
 __global__ void __launch_bounds__(256) k_sp_residual(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
                                                      int use_cond)
 {
-    __shared__ double sh[32];
     if (ss->done) {
         if (use_cond && gtid() == 0) cudaGraphSetConditional(cond, 0);
         return;
     }
-    double acc[1] = {0.0};
-    pass_residual(A, gtid(), gthreads(), ss->alpha, acc[0]);
-    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh) && threadIdx.x == 0) {
-        ss->pending = 1;
-        ss->res = sqrt(acc[0]) / ss->bnorm;
-        ss->it += 1;
-        if (ss->res < A.tol) {
-            ss->done = 1;
-        } else if (ss->it >= A.max_iter) {
-            ss->flags |= FFR_FLAG_CG_MAXITER;
-            ss->done = 1;
-        } else {
-            ss->alpha_prev = ss->alpha;
-        }
-        if (use_cond) cudaGraphSetConditional(cond, ss->done ? 0u : 1u);
-    }
+    sp_residual_body(A, ss, grid_pos(), nullptr, cond, use_cond);
 }
 
 __global__ void __launch_bounds__(256) k_sp_final(PCGArgs A, const SplitState *ss)
 {
     if (A.st && A.st->halt) return;
-    if (ss->pending) pass_final_x(A, gtid(), gthreads(), ss->alpha, ss->dpar ? A.db : A.da);
+    sp_final_body(A, ss, grid_pos());
 }
 
 __global__ void __launch_bounds__(256) k_sp_backsub(PCGArgs A, const SplitState *ss)
 {
     if (A.st && A.st->halt) return;
-    pass_backsub(A, gtid(), gthreads());
-    if (gtid() == 0) {
-        const int iters = ss->bnorm < 1e-15 ? 0 : ss->it;
-        if (A.out_res) *A.out_res = ss->res;
-        if (A.out_iters) *A.out_iters = iters;
-        if (A.out_flags) *A.out_flags = ss->flags;
-        if (A.st) {
-            A.st->pres = ss->res;
-            A.st->iters = iters;
-            atomicOr(&A.st->flags, ss->flags);
-        }
-    }
+    sp_backsub_body(A, ss, grid_pos());
+}
+
+// ---- batched kernels: one launch works on every room of a batch.  Block b
+// belongs to room m.room[b]; the room's blocks are m.first[r] ..
+// m.first[r + 1] - 1, as many as its one-room launch has, so every room
+// computes exactly what its own launch would.  Each block copies its room's
+// arguments to shared memory first.
+
+__device__ __forceinline__ void load_args(PCGArgs &dst, const PCGArgs *src)
+{
+    static_assert(sizeof(PCGArgs) % 8 == 0, "PCGArgs copy in 8-byte words");
+    const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(PCGArgs) / 8); i += blockDim.x) d[i] = s[i];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_bsp_init(BatchDev D, BMap m)
+{
+    __shared__ __align__(16) PCGArgs A;
+    BPos P;
+    const int r = bmap(m, P);
+    load_args(A, D.args + r);
+    sp_init_body(A, D.ss[r], P, D.active, cudaGraphConditionalHandle{}, 0);
+}
+
+template <bool CORR>
+__global__ void __launch_bounds__(256) k_bsp_smooth(BatchDev D, BMap m, int l, int color)
+{
+    __shared__ __align__(16) PCGArgs A;
+    BPos P;
+    const int r = bmap(m, P);
+    if (D.ss[r]->done) return;
+    load_args(A, D.args + r);
+    smooth_color<CORR>(A, A.M.lv, A.M.nlev, l, color, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x);
+}
+
+__global__ void __launch_bounds__(256) k_bsp_restrict(BatchDev D, BMap m, int l)
+{
+    __shared__ __align__(16) PCGArgs A;
+    BPos P;
+    const int r = bmap(m, P);
+    if (D.ss[r]->done) return;
+    load_args(A, D.args + r);
+    restrict_level(A, A.M.lv, l, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x);
+}
+
+// one cluster per room of the list
+__global__ void __launch_bounds__(kMidThreads, 1) k_bsp_mid(BatchDev D, const int *rooms)
+{
+    __shared__ __align__(16) PCGArgs A;
+    const int r = rooms[blockIdx.x / cooperative_groups::this_cluster().num_blocks()];
+    if (D.ss[r]->done) return;   // the same value in every block of the cluster
+    load_args(A, D.args + r);
+    sp_mid_body(A, A.M.nlev_mid);
+}
+
+__global__ void __launch_bounds__(256) k_bsp_redpost(BatchDev D, BMap m)
+{
+    __shared__ __align__(16) PCGArgs A;
+    BPos P;
+    const int r = bmap(m, P);
+    if (D.ss[r]->done) return;
+    load_args(A, D.args + r);
+    sp_redpost_body(A, D.ss[r], P);
+}
+
+__global__ void __launch_bounds__(256, 3) k_bsp_direction(BatchDev D, BMap m)
+{
+    __shared__ __align__(16) PCGArgs A;
+    BPos P;
+    const int r = bmap(m, P);
+    if (D.ss[r]->done) return;
+    load_args(A, D.args + r);
+    sp_direction_body(A, D.ss[r], P, D.active);
+}
+
+__global__ void __launch_bounds__(256) k_bsp_residual(BatchDev D, BMap m)
+{
+    __shared__ __align__(16) PCGArgs A;
+    BPos P;
+    const int r = bmap(m, P);
+    if (D.ss[r]->done) return;
+    load_args(A, D.args + r);
+    sp_residual_body(A, D.ss[r], P, D.active, cudaGraphConditionalHandle{}, 0);
+}
+
+__global__ void __launch_bounds__(256) k_bsp_final(BatchDev D, BMap m)
+{
+    __shared__ __align__(16) PCGArgs A;
+    BPos P;
+    const int r = bmap(m, P);
+    load_args(A, D.args + r);
+    if (A.st && A.st->halt) return;
+    sp_final_body(A, D.ss[r], P);
+}
+
+__global__ void __launch_bounds__(256) k_bsp_backsub(BatchDev D, BMap m)
+{
+    __shared__ __align__(16) PCGArgs A;
+    BPos P;
+    const int r = bmap(m, P);
+    load_args(A, D.args + r);
+    if (A.st && A.st->halt) return;
+    sp_backsub_body(A, D.ss[r], P);
 }
 
 }  // namespace ffr
@@ -1476,6 +1630,244 @@ int launch_split_pcg(const PCGArgs &a, void *ss_dev, cudaStream_t s, SplitHost &
     k_sp_final<<<cb, 256, 0, s>>>(a, ss);
     FFR_LAUNCHED(1);
     k_sp_backsub<<<cb, 256, 0, s>>>(a, ss);
+    FFR_LAUNCHED(1);
+    return FFR_OK;
+}
+
+
+// ---------------------------------------------------------- batched solve
+
+namespace {
+
+// Room -> (grid size) of each launch shape, from the one-room launch sizes.
+struct RoomShape {
+    unsigned cb;                  // level-0 passes
+    int gdown;                    // grid levels smoothed and restricted on the way down
+    unsigned pairs[kMaxLevels], coarse[kMaxLevels];
+    bool mid;                     // has a one-cluster part
+};
+
+RoomShape room_shape(const PCGArgs &a)
+{
+    RoomShape r{};
+    const MGDev &M = a.M;
+    r.cb = (unsigned)std::min<long long>((a.R.n + 255) / 256, kSplitMaxBlocks);
+    if (M.nlev > 1) {
+        const int top = std::min(M.nlev_grid, M.nlev - 1);
+        r.gdown = std::min(M.nlev_mid, top);
+        for (int l = 0; l < r.gdown; l++) {
+            r.pairs[l] = split_blocks_pairs(M, l);
+            r.coarse[l] = split_blocks_cells(M, l + 1);
+        }
+        r.mid = M.nlev_mid < top || M.nlev_grid < M.nlev;
+    }
+    return r;
+}
+
+// Appends the table of one launch shape: room[] over all blocks, first[]
+// per room (nrooms + 1 entries; rooms without blocks get an empty range).
+unsigned build_map(std::vector<int> &room, std::vector<int> &first, const std::vector<unsigned> &nb)
+{
+    first.push_back(0);
+    unsigned total = 0;
+    for (size_t r = 0; r < nb.size(); r++) {
+        for (unsigned b = 0; b < nb[r]; b++) room.push_back((int)r);
+        total += nb[r];
+        first.push_back((int)total);
+    }
+    return total;
+}
+
+}  // namespace
+
+int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std::vector<void *> &ss)
+{
+    batch_split_release(B);
+    const int n = (int)args.size();
+    B.nrooms = n;
+    if (n == 0) return FFR_OK;
+    std::vector<RoomShape> sh(n);
+    int nlev = 0;
+    for (int r = 0; r < n; r++) {
+        sh[r] = room_shape(args[r]);
+        nlev = std::max(nlev, sh[r].gdown);
+    }
+    B.nlev = nlev;
+    // host images of every table, then one device allocation
+    struct Tab {
+        std::vector<int> room, first;
+        unsigned total = 0;
+    };
+    Tab t_cells0, t_pairs[kMaxLevels], t_coarse[kMaxLevels];
+    std::vector<unsigned> nb(n);
+    for (int r = 0; r < n; r++) nb[r] = sh[r].cb;
+    t_cells0.total = build_map(t_cells0.room, t_cells0.first, nb);
+    for (int l = 0; l < nlev; l++) {
+        for (int r = 0; r < n; r++) nb[r] = l < sh[r].gdown ? sh[r].pairs[l] : 0;
+        t_pairs[l].total = build_map(t_pairs[l].room, t_pairs[l].first, nb);
+        for (int r = 0; r < n; r++) nb[r] = l < sh[r].gdown ? sh[r].coarse[l] : 0;
+        t_coarse[l].total = build_map(t_coarse[l].room, t_coarse[l].first, nb);
+    }
+    std::vector<int> mids;
+    for (int r = 0; r < n; r++)
+        if (sh[r].mid) mids.push_back(r);
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    size_t bytes = al(sizeof(PCGArgs) * n) + al(sizeof(void *) * n) + al(sizeof(int)) +
+                   al(4 * (t_cells0.room.size() + t_cells0.first.size())) + al(4 * (mids.size() + 1));
+    for (int l = 0; l < nlev; l++)
+        bytes += al(4 * (t_pairs[l].room.size() + t_pairs[l].first.size())) +
+                 al(4 * (t_coarse[l].room.size() + t_coarse[l].first.size()));
+    std::vector<unsigned char> host(bytes, 0);
+    FFR_CUDA(cudaMalloc(&B.dev, bytes));
+    if (!B.active_host) FFR_CUDA(cudaHostAlloc(&B.active_host, 2 * sizeof(int), cudaHostAllocDefault));
+    for (int k = 0; k < 2; k++)
+        if (!B.ev[k]) FFR_CUDA(cudaEventCreateWithFlags(&B.ev[k], cudaEventDisableTiming));
+    unsigned char *dbase = static_cast<unsigned char *>(B.dev);
+    size_t off = 0;
+    auto put = [&](const void *src, size_t len) -> unsigned char * {
+        if (len) std::memcpy(host.data() + off, src, len);
+        unsigned char *d = dbase + off;
+        off += al(len);
+        return d;
+    };
+    B.D.args = reinterpret_cast<const PCGArgs *>(put(args.data(), sizeof(PCGArgs) * n));
+    B.D.ss = reinterpret_cast<SplitState *const *>(put(ss.data(), sizeof(void *) * n));
+    int zero = 0;
+    B.D.active = reinterpret_cast<int *>(put(&zero, sizeof(int)));
+    auto put_map = [&](const Tab &t, BMap &m) {
+        std::vector<int> both(t.room);
+        both.insert(both.end(), t.first.begin(), t.first.end());
+        const int *d = reinterpret_cast<const int *>(put(both.data(), 4 * both.size()));
+        m.room = d;
+        m.first = d + t.room.size();
+    };
+    put_map(t_cells0, B.cells0);
+    B.nb_cells0 = t_cells0.total;
+    for (int l = 0; l < nlev; l++) {
+        put_map(t_pairs[l], B.pairs[l]);
+        B.nb_pairs[l] = t_pairs[l].total;
+        put_map(t_coarse[l], B.coarse[l]);
+        B.nb_coarse[l] = t_coarse[l].total;
+    }
+    mids.push_back(0);
+    B.mid_rooms = reinterpret_cast<const int *>(put(mids.data(), 4 * mids.size()));
+    B.nmid = (int)mids.size() - 1;
+    FFR_CUDA(cudaMemcpy(B.dev, host.data(), bytes, cudaMemcpyHostToDevice));
+    return FFR_OK;
+}
+
+void batch_split_release(BatchSplit &B)
+{
+    if (B.dev) cudaFree(B.dev);
+    B.dev = nullptr;
+    B.nrooms = 0;
+    B.nlev = 0;
+    B.nmid = 0;
+}
+
+namespace {
+
+int batch_iteration(BatchSplit &B, cudaStream_t s)
+{
+    int rc = FFR_OK;
+    auto chk = [&](const char *what) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess && rc == FFR_OK) rc = cuda_fail(e, what);
+        count_launch(1);
+    };
+    for (int l = 0; l < B.nlev; l++) {
+        if (!B.nb_pairs[l]) continue;
+        k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 1);
+        chk("k_bsp_smooth");
+        k_bsp_restrict<<<B.nb_coarse[l], 256, 0, s>>>(B.D, B.coarse[l], l);
+        chk("k_bsp_restrict");
+    }
+    if (B.nmid) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_bsp_mid, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            attr = true;
+        }
+        const int ctas = mid_cluster_ctas();
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(ctas * B.nmid));
+        cfg.blockDim = dim3(kMidThreads);
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)ctas;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, k_bsp_mid, B.D, B.mid_rooms);
+        if (e != cudaSuccess && rc == FFR_OK) rc = cuda_fail(e, "cudaLaunchKernelEx(k_bsp_mid)");
+        chk("k_bsp_mid");
+    }
+    for (int l = B.nlev - 1; l >= 1; l--) {
+        if (!B.nb_pairs[l]) continue;
+        k_bsp_smooth<true><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 1);
+        chk("k_bsp_smooth");
+        k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 0);
+        chk("k_bsp_smooth");
+    }
+    if (B.nlev >= 1 && B.nb_pairs[0]) {
+        k_bsp_smooth<true><<<B.nb_pairs[0], 256, 0, s>>>(B.D, B.pairs[0], 0, 1);
+        chk("k_bsp_smooth");
+    }
+    k_bsp_redpost<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    chk("k_bsp_redpost");
+    k_bsp_direction<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    chk("k_bsp_direction");
+    k_bsp_residual<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    chk("k_bsp_residual");
+    return rc;
+}
+
+}  // namespace
+
+int batch_split_solve(BatchSplit &B, cudaStream_t s, int max_iter)
+{
+    if (B.nrooms == 0) return FFR_OK;
+    FFR_CUDA(cudaMemsetAsync(B.D.active, 0, sizeof(int), s));
+    k_bsp_init<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    FFR_LAUNCHED(1);
+    int launched = 0, rc = FFR_OK;
+    auto batch = [&](int nb, int slot) -> int {
+        for (int k = 0; k < nb; k++) {
+            int r = batch_iteration(B, s);
+            if (r) return r;
+        }
+        launched += nb;
+        FFR_CUDA(cudaMemcpyAsync(B.active_host + slot, B.D.active, sizeof(int), cudaMemcpyDeviceToHost, s));
+        FFR_CUDA(cudaEventRecord(B.ev[slot], s));
+        return FFR_OK;
+    };
+    // paced as launch_split_pcg: a first batch of the previous solve's
+    // count less two, then batches of two queued ahead of the host's wait
+    int slot = 0;
+    if (max_iter > 0) {
+        rc = batch(std::min(max_iter, std::max(1, B.last_iters - 2)), slot);
+        if (rc) return rc;
+        while (true) {
+            const int prev = slot;
+            const bool more = launched < max_iter;
+            if (more) {
+                slot ^= 1;
+                rc = batch(std::min(2, max_iter - launched), slot);
+                if (rc) return rc;
+            }
+            FFR_CUDA(cudaEventSynchronize(B.ev[prev]));
+            if (B.active_host[prev] <= 0) {
+                B.last_iters = launched - (more ? 2 : 0);
+                break;
+            }
+            if (!more) break;
+        }
+    }
+    k_bsp_final<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    FFR_LAUNCHED(1);
+    k_bsp_backsub<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
     FFR_LAUNCHED(1);
     return FFR_OK;
 }

@@ -92,6 +92,72 @@ struct SplitHost {
     int init();
     void release();
 };
+// ---- batched split solve: one launch per pass over every room of a batch.
+struct SplitState;
+// Block -> room table of one launch shape: room[b] for every block b of the
+// launch; the blocks of room r are first[r] .. first[r + 1] - 1.
+struct BMap {
+    const int *room;
+    const int *first;
+};
+// Position of a block among the blocks that work on one room: its index
+// lb and their number nb (the whole grid for a one-room launch).
+struct BPos {
+    int lb, nb;
+};
+__device__ __forceinline__ BPos grid_pos() { return BPos{(int)blockIdx.x, (int)gridDim.x}; }
+// The room of this block in a batched launch, and its position there.
+__device__ __forceinline__ int bmap(const BMap &m, BPos &P)
+{
+    const int r = m.room[blockIdx.x];
+    const int f = m.first[r];
+    P.lb = (int)blockIdx.x - f;
+    P.nb = m.first[r + 1] - f;
+    return r;
+}
+// Device view of a batch: per-room arguments and split states, and the
+// count of rooms still iterating.
+struct BatchDev {
+    const PCGArgs *args;
+    SplitState *const *ss;
+    int *active;
+};
+// Host side: the launch shapes of a batch (device tables built by
+// batch_split_build) and the pacing state.
+struct BatchSplit {
+    BatchDev D{};
+    int nrooms = 0;
+    // level-0 passes (init, red post-smooth, direction, residual, final,
+    // back-substitution): the one-room grid of each room
+    BMap cells0{};
+    unsigned nb_cells0 = 0;
+    // per grid level l: smoothing (pairs of level l) and restriction (cells
+    // of level l + 1), for the rooms that smooth level l on the grid
+    int nlev = 0;
+    BMap pairs[kMaxLevels]{}, coarse[kMaxLevels]{};
+    unsigned nb_pairs[kMaxLevels]{}, nb_coarse[kMaxLevels]{};
+    BMap post[kMaxLevels]{};          // up-sweep smoothing of level l >= 1
+    unsigned nb_post[kMaxLevels]{};
+    BMap post0{};                     // level-0 black post-smoothing
+    unsigned nb_post0 = 0;
+    const int *mid_rooms = nullptr;   // rooms with a one-cluster part
+    int nmid = 0;
+    void *dev = nullptr;              // device allocation holding all tables
+    int *active_host = nullptr;       // pinned copy of the active count
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int last_iters = 8;
+};
+// Builds the tables for rooms with the given per-room arguments (host
+// copies; device pointers inside) and device split states.
+int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std::vector<void *> &ss);
+void batch_split_release(BatchSplit &B);
+// The split solve of every room of the batch, host-paced like
+// launch_split_pcg: iterations are queued in batches until no room is
+// still iterating.
+// max_iter bounds the batches queued (the largest poisson_max_iter of the
+// rooms; every room also stops itself at its own).
+int batch_split_solve(BatchSplit &B, cudaStream_t s, int max_iter);
+
 // The split solve launched kernel by kernel outside any graph.  The host
 // queues iterations in batches and stops at the first batch whose copy of
 // the done flag reads set; kernels queued past convergence return at once.

@@ -102,22 +102,20 @@ struct PredArgs {
 // then the no-slip / inflow codes (BoundaryManager.cpp:60-130).  F is the
 // arithmetic of the increment: double reproduces the reference; float is
 // the mixed-precision mode (FP32 increment added to the FP64 state).
+// The body over faces start, start + stride, ... (all blocks of one room).
 template <class F>
-__global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const double *__restrict__ u,
-                                                 const double *__restrict__ v,
-                                                 const double *__restrict__ w,
-                                                 const double *__restrict__ T0,
-                                                 const double *__restrict__ T1,
-                                                 double *__restrict__ us, double *__restrict__ vs,
-                                                 double *__restrict__ ws, const StepState *st)
+__device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A, const double *__restrict__ u,
+                                             const double *__restrict__ v, const double *__restrict__ w,
+                                             const double *__restrict__ T0, const double *__restrict__ T1,
+                                             double *__restrict__ us, double *__restrict__ vs,
+                                             double *__restrict__ ws, const StepState *st, int start, int stride)
 {
-    if (st->halt) return;
     const int nx = R.nx, ny = R.ny, nz = R.nz;
     const int total = R.nu + R.nv + R.nw;
     const int quick = A.scheme == 1, lw = A.scheme == 2;
     const F dt = F(A.dt), nu = F(A.nu);
     const double *T = st->tpar ? T1 : T0;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    for (int t = start; t < total; t += stride) {
         if (t < R.nu) {
             const int i = t / (ny * nz), rem = t - i * ny * nz, j = rem / nz, k = rem - j * nz;
             double val = u[t];
@@ -195,6 +193,20 @@ __global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const do
             ws[f] = face_code(R.fcw[f], val, R.fanvel, 2);
         }
     }
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) k_predict(RoomDev R, PredArgs A, const double *__restrict__ u,
+                                                 const double *__restrict__ v,
+                                                 const double *__restrict__ w,
+                                                 const double *__restrict__ T0,
+                                                 const double *__restrict__ T1,
+                                                 double *__restrict__ us, double *__restrict__ vs,
+                                                 double *__restrict__ ws, const StepState *st)
+{
+    if (st->halt) return;
+    predict_body<F>(R, A, u, v, w, T0, T1, us, vs, ws, st, blockIdx.x * blockDim.x + threadIdx.x,
+                    gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------------------ pressure
@@ -367,20 +379,18 @@ struct CorrArgs {
 // recomputes the three high faces, so it can also fold max |u_new - u_old|
 // (FluidSolver.cpp:527-534) and, for FLUID cells, |div u|
 // (compute_divergence_max, FluidSolver.cpp:470-484) in the same pass.
-__global__ void __launch_bounds__(256) k_correct(RoomDev R, CorrArgs A, double *__restrict__ u,
-                                                 double *__restrict__ v, double *__restrict__ w,
-                                                 const double *__restrict__ us,
-                                                 const double *__restrict__ vs,
-                                                 const double *__restrict__ ws,
-                                                 const double *__restrict__ p, StepState *st)
+__device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A, double *__restrict__ u,
+                                             double *__restrict__ v, double *__restrict__ w,
+                                             const double *__restrict__ us, const double *__restrict__ vs,
+                                             const double *__restrict__ ws, const double *__restrict__ p,
+                                             StepState *st, int start, int stride)
 {
     __shared__ double sh[32];
-    if (st->halt) return;
     const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
     const double c0 = A.c0;
     double dmax = 0.0, divmax = 0.0;
     int nan = 0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.n; c += gridDim.x * blockDim.x) {
+    for (int c = start; c < R.n; c += stride) {
         const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
         const double pc = p[c];
         // x faces
@@ -450,6 +460,17 @@ __global__ void __launch_bounds__(256) k_correct(RoomDev R, CorrArgs A, double *
     }
 }
 
+__global__ void __launch_bounds__(256) k_correct(RoomDev R, CorrArgs A, double *__restrict__ u,
+                                                 double *__restrict__ v, double *__restrict__ w,
+                                                 const double *__restrict__ us,
+                                                 const double *__restrict__ vs,
+                                                 const double *__restrict__ ws,
+                                                 const double *__restrict__ p, StepState *st)
+{
+    if (st->halt) return;
+    correct_body(R, A, u, v, w, us, vs, ws, p, st, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 // compute_divergence_max (FluidSolver.cpp:470-484) on demand.
 __global__ void k_divergence(RoomDev R, const double *u, const double *v, const double *w,
                              unsigned long long *out)
@@ -474,15 +495,15 @@ __global__ void k_divergence(RoomDev R, const double *u, const double *v, const 
 
 // BoundaryManager::apply_opening_temperature (BoundaryManager.cpp:137-178)
 // for one opening patch; `next` picks the T buffer the step is writing.
-__global__ void k_opening_T(RoomDev R, ffr_patch P, const double *u, const double *v,
-                            const double *w, double *T0, double *T1, const StepState *st, int next)
+__device__ __forceinline__ void opening_body(const RoomDev &R, const ffr_patch &P, const double *u,
+                                             const double *v, const double *w, double *T0, double *T1,
+                                             const StepState *st, int next, int start, int stride)
 {
-    if (st && st->halt) return;
     const int nx = R.nx, ny = R.ny, nz = R.nz;
     double *T = ((st ? st->tpar : 0) ^ next) ? T1 : T0;
     const int na = P.a_max - P.a_min + 1, nb = P.b_max - P.b_min + 1;
     const int sd = P.side;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na * nb; t += gridDim.x * blockDim.x) {
+    for (int t = start; t < na * nb; t += stride) {
         const int a = P.a_min + t / nb, b = P.b_min + t % nb;
         double vf;
         int cw, cin;
@@ -504,6 +525,13 @@ __global__ void k_opening_T(RoomDev R, ffr_patch P, const double *u, const doubl
     }
 }
 
+__global__ void k_opening_T(RoomDev R, ffr_patch P, const double *u, const double *v,
+                            const double *w, double *T0, double *T1, const StepState *st, int next)
+{
+    if (st && st->halt) return;
+    opening_body(R, P, u, v, w, T0, T1, st, next, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 struct ThermArgs {
     double dt, alpha;
     int scheme;
@@ -512,20 +540,20 @@ struct ThermArgs {
 // FluidSolver::advect_temperature (FluidSolver.cpp:388-456) with the block
 // partial sums of the new T over FLUID cells for compute_T_mean
 // (FluidSolver.cpp:458-468).  F as for k_predict.
+// tpart[lblock] receives this block's partial sum.
 template <class F>
-__global__ void __launch_bounds__(256) k_advect_T(RoomDev R, ThermArgs A, const double *__restrict__ u,
-                                                  const double *__restrict__ v,
-                                                  const double *__restrict__ w, double *T0,
-                                                  double *T1, double *tpart, const StepState *st)
+__device__ __forceinline__ void advect_T_body(const RoomDev &R, const ThermArgs &A, const double *__restrict__ u,
+                                              const double *__restrict__ v, const double *__restrict__ w,
+                                              double *T0, double *T1, double *tpart, const StepState *st,
+                                              int start, int stride, int lblock)
 {
     __shared__ double sh[32];
-    if (st->halt) return;
     const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
     const double *T = st->tpar ? T1 : T0;
     double *Tn = st->tpar ? T0 : T1;
     const int quick = A.scheme == 1, lw = A.scheme == 2;
     double sum = 0.0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.n; c += gridDim.x * blockDim.x) {
+    for (int c = start; c < R.n; c += stride) {
         if (R.ct[c] != CT_FLUID) {
             Tn[c] = T[c];
             continue;
@@ -567,15 +595,25 @@ __global__ void __launch_bounds__(256) k_advect_T(RoomDev R, ThermArgs A, const 
         sum += tn;
     }
     sum = block_sum(sum, sh);
-    if (threadIdx.x == 0) tpart[blockIdx.x] = sum;
+    if (threadIdx.x == 0) tpart[lblock] = sum;
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) k_advect_T(RoomDev R, ThermArgs A, const double *__restrict__ u,
+                                                  const double *__restrict__ v,
+                                                  const double *__restrict__ w, double *T0,
+                                                  double *T1, double *tpart, const StepState *st)
+{
+    if (st->halt) return;
+    advect_T_body<F>(R, A, u, v, w, T0, T1, tpart, st, blockIdx.x * blockDim.x + threadIdx.x,
+                     gridDim.x * blockDim.x, blockIdx.x);
 }
 
 // Fixed-temperature box (heat-patch extension) on the buffer that is
 // current once the step completes.
-__global__ void k_heat(RoomDev R, ffr_heat_patch H, double *T0, double *T1, const StepState *st,
-                       int next)
+__device__ __forceinline__ void heat_body(const RoomDev &R, const ffr_heat_patch &H, double *T0, double *T1,
+                                          const StepState *st, int next, int start, int stride)
 {
-    if (st->halt) return;
     const int ny = R.ny, nz = R.nz;
     double *T = (st->tpar ^ next) ? T1 : T0;
     const int i0 = max(0, H.i_min), i1 = min(R.nx - 1, H.i_max);
@@ -583,10 +621,17 @@ __global__ void k_heat(RoomDev R, ffr_heat_patch H, double *T0, double *T1, cons
     const int k0 = max(0, H.k_min), k1 = min(nz - 1, H.k_max);
     if (i0 > i1 || j0 > j1 || k0 > k1) return;
     const int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ni * nj * nk; t += gridDim.x * blockDim.x) {
+    for (int t = start; t < ni * nj * nk; t += stride) {
         const int a = t / (nj * nk), rem = t - a * nj * nk, b = rem / nk, e = rem - b * nk;
         T[UIX(i0 + a, j0 + b, k0 + e)] = H.T;
     }
+}
+
+__global__ void k_heat(RoomDev R, ffr_heat_patch H, double *T0, double *T1, const StepState *st,
+                       int next)
+{
+    if (st->halt) return;
+    heat_body(R, H, T0, T1, st, next, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // T := T_initial on every cell (FluidSolver ctor, FluidSolver.cpp:28).
@@ -605,10 +650,10 @@ struct FinArgs {
 // StepResult and convergence test of FluidSolver::step (FluidSolver.cpp:
 // 526-549); the velocity change max and divergence max were folded by
 // k_correct, the pressure residual by k_cg, the T partials by k_advect_T.
-__global__ void k_finalize(FinArgs A, const double *tpart, StepState *st, ffr_step_result *ring)
+__device__ __forceinline__ void finalize_body(const FinArgs &A, const double *tpart, StepState *st,
+                                              ffr_step_result *ring)
 {
     __shared__ double sh[32];
-    if (st->halt) return;
     double tmean = A.T_initial;
     if (A.thermal) {
         double s = 0.0;
@@ -643,6 +688,12 @@ __global__ void k_finalize(FinArgs A, const double *tpart, StepState *st, ffr_st
     if (conv && st->stop_on_converge) st->halt = 1;
 }
 
+__global__ void k_finalize(FinArgs A, const double *tpart, StepState *st, ffr_step_result *ring)
+{
+    if (st->halt) return;
+    finalize_body(A, tpart, st, ring);
+}
+
 // Start of a queued chunk of steps: results go to slot 0 on, the halt
 // flag of an earlier converged chunk is cleared.
 __global__ void k_begin_chunk(StepState *st, int stop_on_converge)
@@ -650,6 +701,128 @@ __global__ void k_begin_chunk(StepState *st, int stop_on_converge)
     st->ring_slot = 0;
     st->halt = 0;
     st->stop_on_converge = stop_on_converge;
+}
+
+// ---------------------------------------------------------- batched rooms
+//
+// One launch per stage advances every room of a batch.  Block b works on
+// room m.room[b] with the position it would have in that room's own launch
+// (the same block count per room), so each room's arithmetic, including
+// the order of every partial sum, is the one its own launches perform.
+
+// Everything the step kernels need about one room (a device array, one
+// entry per room of the batch).
+struct BRoom {
+    RoomDev R;
+    PredArgs pa;
+    CorrArgs co;
+    ThermArgs ta;
+    FinArgs fa;
+    double *u, *v, *w, *us, *vs, *ws, *p, *T0, *T1, *tpart;
+    StepState *st;
+    ffr_step_result *ring;
+    int mixed, thermal;
+};
+
+// An opening or heat patch of one room (one launch item).
+struct OpenItem {
+    int room, pad;
+    ffr_patch P;
+};
+struct HeatItem {
+    int room, pad;
+    ffr_heat_patch H;
+};
+
+template <class T>
+__device__ __forceinline__ void load_shared(T &dst, const T *src)
+{
+    static_assert(sizeof(T) % 8 == 0, "8-byte words");
+    const unsigned long long *a = reinterpret_cast<const unsigned long long *>(src);
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(T) / 8); i += blockDim.x) d[i] = a[i];
+    __syncthreads();
+}
+
+__global__ void k_b_begin(const BRoom *rooms, int n, int stop_on_converge)
+{
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        StepState *st = rooms[r].st;
+        st->ring_slot = 0;
+        st->halt = 0;
+        st->stop_on_converge = stop_on_converge;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_b_predict(const BRoom *rooms, BMap m)
+{
+    __shared__ __align__(16) BRoom B;
+    BPos P;
+    const int r = bmap(m, P);
+    load_shared(B, rooms + r);
+    if (B.st->halt) return;
+    const int start = P.lb * blockDim.x + threadIdx.x, stride = P.nb * blockDim.x;
+    if (B.mixed)
+        predict_body<float>(B.R, B.pa, B.u, B.v, B.w, B.T0, B.T1, B.us, B.vs, B.ws, B.st, start, stride);
+    else
+        predict_body<double>(B.R, B.pa, B.u, B.v, B.w, B.T0, B.T1, B.us, B.vs, B.ws, B.st, start, stride);
+}
+
+__global__ void __launch_bounds__(256) k_b_correct(const BRoom *rooms, BMap m)
+{
+    __shared__ __align__(16) BRoom B;
+    BPos P;
+    const int r = bmap(m, P);
+    load_shared(B, rooms + r);
+    if (B.st->halt) return;
+    correct_body(B.R, B.co, B.u, B.v, B.w, B.us, B.vs, B.ws, B.p, B.st, P.lb * blockDim.x + threadIdx.x,
+                 P.nb * blockDim.x);
+}
+
+__global__ void k_b_opening(const BRoom *rooms, const OpenItem *items, BMap m, int next)
+{
+    __shared__ __align__(16) BRoom B;
+    BPos P;
+    const int it = bmap(m, P);
+    const OpenItem I = items[it];
+    load_shared(B, rooms + I.room);
+    if (B.st->halt) return;
+    opening_body(B.R, I.P, B.u, B.v, B.w, B.T0, B.T1, B.st, next, P.lb * blockDim.x + threadIdx.x,
+                 P.nb * blockDim.x);
+}
+
+__global__ void __launch_bounds__(256) k_b_advect_T(const BRoom *rooms, BMap m)
+{
+    __shared__ __align__(16) BRoom B;
+    BPos P;
+    const int r = bmap(m, P);
+    load_shared(B, rooms + r);
+    if (B.st->halt || !B.thermal) return;
+    const int start = P.lb * blockDim.x + threadIdx.x, stride = P.nb * blockDim.x;
+    if (B.mixed)
+        advect_T_body<float>(B.R, B.ta, B.u, B.v, B.w, B.T0, B.T1, B.tpart, B.st, start, stride, P.lb);
+    else
+        advect_T_body<double>(B.R, B.ta, B.u, B.v, B.w, B.T0, B.T1, B.tpart, B.st, start, stride, P.lb);
+}
+
+__global__ void k_b_heat(const BRoom *rooms, const HeatItem *items, BMap m)
+{
+    __shared__ __align__(16) BRoom B;
+    BPos P;
+    const int it = bmap(m, P);
+    const HeatItem I = items[it];
+    load_shared(B, rooms + I.room);
+    if (B.st->halt) return;
+    heat_body(B.R, I.H, B.T0, B.T1, B.st, B.thermal, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x);
+}
+
+// one block per room
+__global__ void k_b_finalize(const BRoom *rooms)
+{
+    __shared__ __align__(16) BRoom B;
+    load_shared(B, rooms + blockIdx.x);
+    if (B.st->halt) return;
+    finalize_body(B.fa, B.tpart, B.st, B.ring);
 }
 
 #undef UIX
@@ -1390,6 +1563,250 @@ int ffr_fluid_profile_read(ffr_fluid *s, double *ms, long long *launches)
     for (int g = 0; g < FFR_PROF_N; g++) {
         if (ms) ms[g] = s->prof.ms[g];
         if (launches) launches[g] = s->prof.launches[g];
+    }
+    return FFR_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------- batched rooms
+
+struct ffr_batch {
+    std::vector<ffr_fluid *> rooms;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    BatchSplit split;
+    void *dev = nullptr;          // BRoom array, launch tables, patch items
+    const BRoom *broom = nullptr;
+    BMap faces{}, cells{}, openm{}, heatm{};
+    unsigned nb_faces = 0, nb_cells = 0, nb_open = 0, nb_heat = 0;
+    const OpenItem *open = nullptr;
+    const HeatItem *heat = nullptr;
+    bool any_thermal = false;
+    int max_iter = 0;
+};
+
+namespace {
+
+void batch_free(ffr_batch *b)
+{
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_split_release(b->split);
+    if (b->split.active_host) cudaFreeHost(b->split.active_host);
+    for (int k = 0; k < 2; k++)
+        if (b->split.ev[k]) cudaEventDestroy(b->split.ev[k]);
+    if (b->dev) cudaFree(b->dev);
+    if (b->ev) cudaEventDestroy(b->ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+PCGArgs room_pcg_args(ffr_fluid *s)
+{
+    const ffr_fluid_params &P = s->prm;
+    PCGArgs a{};
+    a.R = s->R; a.M = s->M;
+    a.us = s->us; a.vs = s->vs; a.ws = s->ws;
+    a.rhs_factor = -(P.rho / P.dt);
+    a.from_faces = 1;
+    a.x = s->p; a.r = s->r; a.da = s->da; a.db = s->db; a.q = s->ad;
+    a.partials = s->partials; a.gs = s->gs; a.sc = s->sc;
+    a.max_iter = P.poisson_max_iter; a.tol = P.poisson_tol;
+    a.st = s->st;
+    return a;
+}
+
+BRoom room_step_args(ffr_fluid *s)
+{
+    const ffr_fluid_params &P = s->prm;
+    BRoom b{};
+    b.R = s->R;
+    b.pa = PredArgs{P.dt, P.nu, P.advection, P.buoyancy ? 1 : 0, P.g_accel * P.beta * P.dt, P.T_initial};
+    b.co = CorrArgs{P.dt / P.rho};
+    b.ta = ThermArgs{P.dt, P.k_thermal / (P.rho * P.cp), P.advection};
+    b.fa = FinArgs{P.dt, P.convergence_tol, P.T_initial, P.T_target, P.thermal ? 1 : 0, s->room.n_fluid,
+                   (int)s->blocks_cells};
+    b.u = s->u; b.v = s->v; b.w = s->w; b.us = s->us; b.vs = s->vs; b.ws = s->ws;
+    b.p = s->p; b.T0 = s->T0; b.T1 = s->T1; b.tpart = s->tpart;
+    b.st = s->st;
+    b.ring = s->ring;
+    b.mixed = s->mixed ? 1 : 0;
+    b.thermal = P.thermal ? 1 : 0;
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out)
+{
+    if (!out || nrooms <= 0 || !rooms) return fail(FFR_EINVAL, "bad arguments");
+    *out = nullptr;
+    for (int r = 0; r < nrooms; r++) {
+        ffr_fluid *s = rooms[r];
+        if (!s) return fail(FFR_EINVAL, "NULL room handle");
+        if (!s->mg) return fail(FFR_EINVAL, "a batch takes rooms with the multigrid pressure solve");
+        if (s->pending) return fail(FFR_EINVAL, "a room has a queued chunk that was not polled");
+        if (s->cluster_ctas || s->block_override) return fail(FFR_EINVAL, "a batched room keeps the default grid");
+        for (int q = 0; q < r; q++)
+            if (rooms[q] == s) return fail(FFR_EINVAL, "a room appears twice in the batch");
+    }
+    ffr_batch *b = new (std::nothrow) ffr_batch();
+    if (!b) return fail(FFR_ENOMEM, "host allocation");
+    b->rooms.assign(rooms, rooms + nrooms);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
+        batch_free(b);
+        return fail(FFR_ECUDA, "batch stream");
+    }
+    // per-room arguments, block tables of the step kernels, patch items
+    std::vector<BRoom> br(nrooms);
+    std::vector<PCGArgs> pa(nrooms);
+    std::vector<void *> ss(nrooms);
+    std::vector<int> froom, ffirst{0}, croom, cfirst{0}, oroom, ofirst{0}, hroom, hfirst{0};
+    std::vector<OpenItem> oitems;
+    std::vector<HeatItem> hitems;
+    for (int r = 0; r < nrooms; r++) {
+        ffr_fluid *s = rooms[r];
+        br[r] = room_step_args(s);
+        pa[r] = room_pcg_args(s);
+        ss[r] = s->split_state;
+        b->any_thermal |= s->prm.thermal != 0;
+        b->max_iter = std::max(b->max_iter, s->prm.poisson_max_iter);
+        for (unsigned k = 0; k < s->blocks_faces; k++) froom.push_back(r);
+        ffirst.push_back((int)froom.size());
+        for (unsigned k = 0; k < s->blocks_cells; k++) croom.push_back(r);
+        cfirst.push_back((int)croom.size());
+        if (s->prm.thermal) {
+            for (const ffr_patch &op : s->room.patches) {
+                if (!op.is_opening) continue;
+                const int it = (int)oitems.size();
+                oitems.push_back(OpenItem{r, 0, op});
+                const unsigned nb = stream_blocks((long long)(op.a_max - op.a_min + 1) * (op.b_max - op.b_min + 1));
+                for (unsigned k = 0; k < nb; k++) oroom.push_back(it);
+                ofirst.push_back((int)oroom.size());
+            }
+        }
+        for (const ffr_heat_patch &h : s->room.heats) {
+            const int it = (int)hitems.size();
+            hitems.push_back(HeatItem{r, 0, h});
+            const unsigned nb = stream_blocks((long long)(h.i_max - h.i_min + 1) * (h.j_max - h.j_min + 1) *
+                                              (h.k_max - h.k_min + 1));
+            for (unsigned k = 0; k < nb; k++) hroom.push_back(it);
+            hfirst.push_back((int)hroom.size());
+        }
+    }
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t bytes = al(sizeof(BRoom) * nrooms) + al(4 * (froom.size() + ffirst.size())) +
+                         al(4 * (croom.size() + cfirst.size())) + al(4 * (oroom.size() + ofirst.size())) +
+                         al(4 * (hroom.size() + hfirst.size())) + al(sizeof(OpenItem) * (oitems.size() + 1)) +
+                         al(sizeof(HeatItem) * (hitems.size() + 1));
+    std::vector<unsigned char> host(bytes, 0);
+    if (cudaMalloc(&b->dev, bytes) != cudaSuccess) {
+        batch_free(b);
+        return fail(FFR_ENOMEM, "batch tables");
+    }
+    unsigned char *d = static_cast<unsigned char *>(b->dev);
+    size_t off = 0;
+    auto put = [&](const void *src, size_t len) -> unsigned char * {
+        if (len) std::memcpy(host.data() + off, src, len);
+        unsigned char *p = d + off;
+        off += al(len);
+        return p;
+    };
+    auto put_map = [&](const std::vector<int> &room, const std::vector<int> &first, BMap &m) {
+        std::vector<int> both(room);
+        both.insert(both.end(), first.begin(), first.end());
+        const int *p = reinterpret_cast<const int *>(put(both.data(), 4 * both.size()));
+        m.room = p;
+        m.first = p + room.size();
+        return (unsigned)room.size();
+    };
+    b->broom = reinterpret_cast<const BRoom *>(put(br.data(), sizeof(BRoom) * nrooms));
+    b->nb_faces = put_map(froom, ffirst, b->faces);
+    b->nb_cells = put_map(croom, cfirst, b->cells);
+    b->nb_open = put_map(oroom, ofirst, b->openm);
+    b->nb_heat = put_map(hroom, hfirst, b->heatm);
+    oitems.push_back(OpenItem{});
+    hitems.push_back(HeatItem{});
+    b->open = reinterpret_cast<const OpenItem *>(put(oitems.data(), sizeof(OpenItem) * oitems.size()));
+    b->heat = reinterpret_cast<const HeatItem *>(put(hitems.data(), sizeof(HeatItem) * hitems.size()));
+    if (cudaMemcpy(b->dev, host.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+        batch_free(b);
+        return fail(FFR_ECUDA, "batch tables upload");
+    }
+    int rc = batch_split_build(b->split, pa, ss);
+    if (rc) {
+        batch_free(b);
+        return rc;
+    }
+    *out = b;
+    return FFR_OK;
+}
+
+int ffr_batch_destroy(ffr_batch *b)
+{
+    batch_free(b);
+    return FFR_OK;
+}
+
+int ffr_batch_size(const ffr_batch *b, int *nrooms)
+{
+    if (!b || !nrooms) return fail(FFR_EINVAL, "NULL argument");
+    *nrooms = (int)b->rooms.size();
+    return FFR_OK;
+}
+
+int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge)
+{
+    if (!b || nsteps < 0 || nsteps > kRing) return fail(FFR_EINVAL, "bad handle or nsteps (0..1024)");
+    cudaStream_t st = b->stream;
+    for (ffr_fluid *s : b->rooms) {
+        if (s->pending) return fail(FFR_EINVAL, "a room has a queued chunk that was not polled");
+        // the batch stream follows everything queued on the room's own stream
+        FFR_CUDA(cudaEventRecord(b->ev, s->stream));
+        FFR_CUDA(cudaStreamWaitEvent(st, b->ev, 0));
+    }
+    const int n = (int)b->rooms.size();
+    k_b_begin<<<1, 256, 0, st>>>(b->broom, n, stop_on_converge ? 1 : 0);
+    FFR_LAUNCHED(1);
+    for (int k = 0; k < nsteps; k++) {
+        k_b_predict<<<b->nb_faces, kThreads, 0, st>>>(b->broom, b->faces);
+        FFR_LAUNCHED(1);
+        int rc = batch_split_solve(b->split, st, b->max_iter);
+        if (rc) return rc;
+        k_b_correct<<<b->nb_cells, kThreads, 0, st>>>(b->broom, b->cells);
+        FFR_LAUNCHED(1);
+        if (b->any_thermal) {
+            if (b->nb_open) {
+                k_b_opening<<<b->nb_open, kThreads, 0, st>>>(b->broom, b->open, b->openm, 0);
+                FFR_LAUNCHED(1);
+            }
+            k_b_advect_T<<<b->nb_cells, kThreads, 0, st>>>(b->broom, b->cells);
+            FFR_LAUNCHED(1);
+            if (b->nb_open) {
+                k_b_opening<<<b->nb_open, kThreads, 0, st>>>(b->broom, b->open, b->openm, 1);
+                FFR_LAUNCHED(1);
+            }
+        }
+        if (b->nb_heat) {
+            k_b_heat<<<b->nb_heat, kThreads, 0, st>>>(b->broom, b->heat, b->heatm);
+            FFR_LAUNCHED(1);
+        }
+        k_b_finalize<<<n, kThreads, 0, st>>>(b->broom);
+        FFR_LAUNCHED(1);
+    }
+    // each room's results as ffr_fluid_enqueue leaves them, for ffr_fluid_poll
+    for (ffr_fluid *s : b->rooms) {
+        if (nsteps > 0)
+            FFR_CUDA(cudaMemcpyAsync(s->ring_host, s->ring, sizeof(ffr_step_result) * nsteps,
+                                     cudaMemcpyDeviceToHost, st));
+        FFR_CUDA(cudaMemcpyAsync(s->st_host, s->st, sizeof(StepState), cudaMemcpyDeviceToHost, st));
+        FFR_CUDA(cudaEventRecord(s->done_ev, st));
+        FFR_CUDA(cudaStreamWaitEvent(s->stream, s->done_ev, 0));
+        s->pending = nsteps > 0 ? nsteps : -1;
     }
     return FFR_OK;
 }

@@ -137,6 +137,10 @@ def lib():
             "ffr_fluid_set_cluster": ([vp, C.c_int], C.c_int),
             "ffr_fluid_time_pressure": ([vp, C.c_int, _dp, C.POINTER(C.c_int)], C.c_int),
             "ffr_fluid_set_split": ([vp, C.c_int], C.c_int),
+            "ffr_batch_create": ([C.POINTER(vp), C.c_int, C.POINTER(vp)], C.c_int),
+            "ffr_batch_destroy": ([vp], C.c_int),
+            "ffr_batch_size": ([vp, C.POINTER(C.c_int)], C.c_int),
+            "ffr_batch_enqueue": ([vp, C.c_int, C.c_int], C.c_int),
             "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
                                            C.c_double, vp, _dp, C.POINTER(C.c_int)], C.c_int),
         }
@@ -322,6 +326,45 @@ class FluidHandle:
 
     def synchronize(self) -> None:
         check(lib().ffr_fluid_synchronize(self.h))
+
+
+class BatchHandle:
+    """Several rooms advanced together (ffr_batch): one launch per stage for
+    all of them.  Each room's results are polled on its own FluidHandle."""
+
+    def __init__(self, rooms: List["FluidHandle"]):
+        self.rooms = list(rooms)
+        arr = (C.c_void_p * len(self.rooms))(*[r.h for r in self.rooms])
+        h = C.c_void_p()
+        check(lib().ffr_batch_create(arr, len(self.rooms), C.byref(h)))
+        self.h = h
+
+    def enqueue(self, nsteps: int, stop_on_converge: bool = True) -> None:
+        check(lib().ffr_batch_enqueue(self.h, nsteps, int(stop_on_converge)))
+        for r in self.rooms:
+            r._pending = nsteps
+
+    def advance(self, nsteps: int, stop_on_converge: bool = False) -> List[List[dict]]:
+        """Runs nsteps on every room; the step results of each room."""
+        self.enqueue(nsteps, stop_on_converge)
+        out = []
+        for r in self.rooms:
+            res = None
+            while res is None:
+                res = r.poll()
+            out.append(res)
+        return out
+
+    def close(self) -> None:
+        if self.h:
+            lib().ffr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class PoissonHandle:

@@ -200,6 +200,22 @@ int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *i
  * Set before ffr_fluid_use_graph. */
 int ffr_fluid_set_split(ffr_fluid *s, int mode);
 
+/* Batched rooms (no counterpart in the reference, which solves one room at a
+ * time): one kernel launch per stage advances every room of a batch, each
+ * room's blocks doing what its own launch would (results identical to the
+ * room solved alone with the one-kernel-per-pass multigrid schedule).  The
+ * rooms stay ordinary handles: after ffr_batch_enqueue each room's results
+ * are collected with ffr_fluid_poll, and fields are read as usual.  Rooms
+ * must use the multigrid pressure solve and the default grid; a room may
+ * belong to several batches but only one may run at a time. */
+typedef struct ffr_batch ffr_batch;
+int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out);
+int ffr_batch_destroy(ffr_batch *b);
+int ffr_batch_size(const ffr_batch *b, int *nrooms);
+/* Queues nsteps (0..1024) steps of every room; returns once the last
+ * step's pressure solve is queued (the solves are paced by the host). */
+int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge);
+
 /* FluidSolver::compute_divergence_max (FluidSolver.cpp:470-484). */
 int ffr_fluid_divergence_max(ffr_fluid *s, double *out);
 /* FluidSolver::current_step (FluidSolver.hpp:63). */

@@ -1,0 +1,95 @@
+"""Batched rooms (ffr_batch): one launch per stage for every room of a batch.
+
+Each room's blocks do exactly what that room's own launches do with the
+one-kernel-per-pass multigrid schedule (same block counts, same order of
+every partial sum), so a room's fields and step histories must be
+bit-identical whether it ran alone or in a batch, and within the mixed-
+precision bound (1e-4 max-norm relative) of the FP64 oracle fixtures."""
+import numpy as np
+import pytest
+
+from conftest import Golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+# uniform and stretched grids, openings with thermal transport, heated
+# patches, QUICK / upwind / Lax-Wendroff, odd dimensions
+NAMES = ["c1_upwind_10", "summer_cooling_10", "oblique_stretch_10", "thermal_small_10", "edge_odd_quick_10",
+         "vent_quick_10", "updraft_laxw_10", "two_fans_10"]
+HIST = ("step", "velocity_change", "pressure_residual", "divergence_max", "converged", "T_mean", "cg_iterations",
+        "flags")
+
+
+def _handle(g):
+    from ffrb import capi
+    h = capi.FluidHandle(g.room, g.params.with_(poisson="mgpcg", precision="mixed"))
+    h.set_split(1)
+    return h
+
+
+def test_batch_matches_rooms_alone():
+    from ffrb import capi
+    gs = [Golden(n) for n in NAMES]
+    steps = min(g.nsteps for g in gs)
+    alone = []
+    for g in gs:
+        h = _handle(g)
+        recs = h.advance(steps)
+        alone.append((recs, {k: h.get(k) for k in "uvwpT"}))
+        h.close()
+    hs = [_handle(g) for g in gs]
+    b = capi.BatchHandle(hs)
+    out = b.advance(steps)
+    for g, h, recs, (recs_a, fa) in zip(gs, hs, out, alone):
+        assert len(recs) == steps
+        for ra, rb in zip(recs_a, recs):
+            for k in HIST:
+                assert ra[k] == rb[k], (g.name, k, ra[k], rb[k])
+        for k in "uvwpT":
+            assert np.array_equal(h.get(k), fa[k]), (g.name, k)
+    b.close()
+    for h in hs:
+        h.close()
+
+
+def test_batch_tracks_oracle_and_continues():
+    """Two chunks in a row on the same batch; then the fields against the
+    FP64 fixtures (rooms whose fixture has exactly 10 steps)."""
+    from ffrb import capi
+    gs = [Golden(n) for n in NAMES]
+    hs = [_handle(g) for g in gs]
+    b = capi.BatchHandle(hs)
+    first = b.advance(4)
+    second = b.advance(6)
+    for g, h, r1, r2 in zip(gs, hs, first, second):
+        assert [r["step"] for r in r1 + r2] == list(range(1, 11))
+        if g.nsteps != 10:
+            continue
+        for k in "uvwpT":
+            assert rel_err(h.get(k), g.fields[k]) <= 1e-4, (g.name, k)
+    b.close()
+
+
+def test_batch_room_halts_on_convergence_alone():
+    """A room that converges stops (stop_on_converge) while the others run on."""
+    from ffrb import capi
+    g1, g2 = Golden("c1_upwind_10"), Golden("thermal_small_10")
+    h1 = capi.FluidHandle(g1.room, g1.params.with_(poisson="mgpcg", precision="mixed", convergence_tol=1e30))
+    h2 = _handle(g2)
+    h1.set_split(1)
+    b = capi.BatchHandle([h1, h2])
+    r1, r2 = b.advance(5, stop_on_converge=True)
+    assert len(r1) == 1 and r1[0]["converged"]
+    assert len(r2) == 5
+    b.close()
+
+
+def test_batch_rejects_rooms_it_cannot_take():
+    from ffrb import capi
+    g = Golden("c1_upwind_10")
+    h = capi.FluidHandle(g.room, g.params)          # plain CG
+    with pytest.raises(capi.FfrError):
+        capi.BatchHandle([h])
+    h2 = _handle(g)
+    with pytest.raises(capi.FfrError):
+        capi.BatchHandle([h2, h2])
