@@ -372,28 +372,31 @@ def serving_requests(kind: str, n: int, max_cells: int, max_steps: int):
     return requests_from_configs(rooms, [params_from_scene(c) for c in rooms], [0.0] * len(rooms), max_steps)
 
 
-def run_serving(kind: str, n: int, max_cells: int, max_steps: int, tune: bool = True):
+def run_serving(kind: str, n: int, max_cells: int, max_steps: int, batched: bool = True, chunk: int = 10):
+    """The serving sample through the continuous-batching server: batched
+    (every active room in one launch per stage, rooms joining and leaving
+    between chunks) or one stream per room with tuned schedules."""
     import torch
     from ffrb.serve import Server, Tuner, report, serial_solve
     reqs = serving_requests(kind, n, max_cells, max_steps)
     tuner = Tuner()
-    if tune:
+    if not batched:
         tuner.tune([r.room for r in reqs], [r.params for r in reqs], steps=4, concurrent=4)
     free, total = torch.cuda.mem_get_info()
-    srv = Server(mem_budget=int(free * 0.6), max_active=64, tuner=tuner)
+    srv = Server(mem_budget=int(free * 0.6), max_active=64, tuner=tuner, batched=batched, chunk=chunk)
     l0 = __import__("ffrb.capi", fromlist=["x"]).launch_count()
     with ClockSampler(torch.cuda.current_device()) as clk:
         out = srv.run(reqs, realtime=(kind == "serving"))
     launches = __import__("ffrb.capi", fromlist=["x"]).launch_count() - l0
     rep = report(out)
-    base = serial_solve(reqs, {"precision": "fp64", "poisson": "cg"})
+    base = serial_solve(reqs, {"precision": "fp64", "poisson": "cg", "use_multigrid": False})
     rb = report(base, makespan=max(o.t_done for o in base))
     rep["serial_fp64_room_solves_per_s"] = rb["room_solves_per_s"]
     rep["serial_fp64_cell_steps_per_s"] = rb["cell_steps_per_s"]
     rep["speedup_vs_serial_fp64"] = rep["room_solves_per_s"] / rb["room_solves_per_s"]
     rep["sample"] = (f"{len(reqs)} requests with <= {max_cells} cells, cap {max_steps} steps"
                      + (", Poisson arrivals in real time" if kind == "serving" else ", all at t = 0"))
-    rep["schedules"] = tuner.to_json()
+    rep["schedules"] = (f"batched, chunks of {chunk} steps" if batched else tuner.to_json())
     rep["gpu_launches"] = launches
     rep["clocks"] = clk.summary()
     return rep
@@ -402,7 +405,7 @@ def run_serving(kind: str, n: int, max_cells: int, max_steps: int, tune: bool = 
 def serving_arm(args):
     import torch
     torch.cuda.set_device(0)
-    rep = run_serving(args.workload, args.requests, args.max_cells, args.max_steps)
+    rep = run_serving(args.workload, args.requests, args.max_cells, args.max_steps, bool(args.batched), args.chunk)
     line = {"metric": METRIC, "value": rep["room_solves_per_s"], "unit": "room-solves/s", "n_gpus": 1,
             "steps": args.max_steps, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
@@ -429,6 +432,8 @@ def main():
     ap.add_argument("--max-cells", type=int, default=600_000, help="serving/batch: largest room in the sample")
     ap.add_argument("--max-steps", type=int, default=40, help="serving/batch: step cap per room")
     ap.add_argument("--no-serving", action="store_true", help="default run: skip the serving sample")
+    ap.add_argument("--batched", type=int, default=1, help="serving/batch: one launch per stage for all rooms")
+    ap.add_argument("--chunk", type=int, default=10, help="serving/batch: steps between membership changes")
     ap.add_argument("--graph", type=int, default=1,
                     help="replay each step as a CUDA graph (the multigrid solve then runs one kernel per pass)")
     ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],

@@ -1181,14 +1181,14 @@ __global__ void __launch_bounds__(256) k_bsp_restrict(BatchDev D, BMap m, int l)
     restrict_level(A, A.M.lv, l, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x);
 }
 
-// one cluster per room of the list
-__global__ void __launch_bounds__(kMidThreads, 1) k_bsp_mid(BatchDev D, const int *rooms)
+// one block per room of the list: the levels from nlev_grid on
+__global__ void __launch_bounds__(1024) k_bsp_coarse(BatchDev D, const int *rooms)
 {
     __shared__ __align__(16) PCGArgs A;
-    const int r = rooms[blockIdx.x / cooperative_groups::this_cluster().num_blocks()];
-    if (D.ss[r]->done) return;   // the same value in every block of the cluster
+    const int r = rooms[blockIdx.x];
+    if (D.ss[r]->done) return;
     load_args(A, D.args + r);
-    sp_mid_body(A, A.M.nlev_mid);
+    block_vcycle(A, A.M.nlev_grid);
 }
 
 __global__ void __launch_bounds__(256) k_bsp_redpost(BatchDev D, BMap m)
@@ -1408,16 +1408,26 @@ namespace ffr {
 
 namespace {
 
+// Level-0 passes (over cells or cell pairs): four cells per thread, at most
+// kSplitMaxBlocks blocks.
+unsigned split_blocks_level0(long long n)
+{
+    return (unsigned)std::max<long long>(1, std::min<long long>((n + 1023) / 1024, kSplitMaxBlocks));
+}
+
+// Grid sizes of the split solve's launches: two items (pairs or coarse
+// cells) per thread, so each block amortises its start-up over more work
+// (many rooms in one batched launch fill the GPU by their number).
 unsigned split_blocks_pairs(const MGDev &M, int l)
 {
     const MGLevel &L = M.lv[l];
     const long long w = (long long)L.nx * L.ny * ((L.nz + 1) / 2);
-    return (unsigned)std::max<long long>(1, (w + 255) / 256);
+    return (unsigned)std::max<long long>(1, (w + 511) / 512);
 }
 
 unsigned split_blocks_cells(const MGDev &M, int l)
 {
-    return (unsigned)std::max<long long>(1, ((long long)M.lv[l].n + 255) / 256);
+    return (unsigned)std::max<long long>(1, ((long long)M.lv[l].n + 511) / 512);
 }
 
 // Cluster size of k_sp_mid: the largest of 16 and 8 blocks that the device
@@ -1467,7 +1477,7 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
                     int use_cond)
 {
     const MGDev &M = a.M;
-    const unsigned cb = (unsigned)std::min<long long>((a.R.n + 255) / 256, kSplitMaxBlocks);
+    const unsigned cb = split_blocks_level0(a.R.n);
     int rc = FFR_OK;
     auto chk = [&]() {
         cudaError_t e = cudaGetLastError();
@@ -1535,7 +1545,7 @@ int capture_split_pcg(const PCGArgs &a, void *ss_dev, cudaStream_t s, cudaStream
     if (cs != cudaStreamCaptureStatusActive) return fail(FFR_EINVAL, "split solve must be captured");
     cudaGraphConditionalHandle cond;
     FFR_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
-    const unsigned cb = (unsigned)std::min<long long>((a.R.n + 255) / 256, kSplitMaxBlocks);
+    const unsigned cb = split_blocks_level0(a.R.n);
     k_sp_init<<<cb, 256, 0, s>>>(a, ss, cond, 1);
     FFR_LAUNCHED(1);
     FFR_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
@@ -1588,7 +1598,7 @@ int launch_split_pcg(const PCGArgs &a, void *ss_dev, cudaStream_t s, SplitHost &
     int rc = h.init();
     if (rc) return rc;
     SplitState *ss = static_cast<SplitState *>(ss_dev);
-    const unsigned cb = (unsigned)std::min<long long>((a.R.n + 255) / 256, kSplitMaxBlocks);
+    const unsigned cb = split_blocks_level0(a.R.n);
     k_sp_init<<<cb, 256, 0, s>>>(a, ss, cudaGraphConditionalHandle{}, 0);
     FFR_LAUNCHED(1);
     const int max_iter = std::max(0, a.max_iter);
@@ -1644,22 +1654,26 @@ struct RoomShape {
     unsigned cb;                  // level-0 passes
     int gdown;                    // grid levels smoothed and restricted on the way down
     unsigned pairs[kMaxLevels], coarse[kMaxLevels];
-    bool mid;                     // has a one-cluster part
+    bool mid;                     // has levels small enough for one block
 };
 
 RoomShape room_shape(const PCGArgs &a)
 {
     RoomShape r{};
     const MGDev &M = a.M;
-    r.cb = (unsigned)std::min<long long>((a.R.n + 255) / 256, kSplitMaxBlocks);
+    r.cb = split_blocks_level0(a.R.n);
     if (M.nlev > 1) {
+        // every grid-sized level in batched launches (many rooms fill the
+        // GPU there), the levels of at most kBlockLevelCells cells in one
+        // block per room; the cell updates are those of the one-room split
+        // solve, which runs the levels from nlev_mid on in one cluster
         const int top = std::min(M.nlev_grid, M.nlev - 1);
-        r.gdown = std::min(M.nlev_mid, top);
+        r.gdown = top;
         for (int l = 0; l < r.gdown; l++) {
             r.pairs[l] = split_blocks_pairs(M, l);
             r.coarse[l] = split_blocks_cells(M, l + 1);
         }
-        r.mid = M.nlev_mid < top || M.nlev_grid < M.nlev;
+        r.mid = M.nlev_grid < M.nlev;
     }
     return r;
 }
@@ -1682,7 +1696,6 @@ unsigned build_map(std::vector<int> &room, std::vector<int> &first, const std::v
 
 int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std::vector<void *> &ss)
 {
-    batch_split_release(B);
     const int n = (int)args.size();
     B.nrooms = n;
     if (n == 0) return FFR_OK;
@@ -1718,7 +1731,13 @@ int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std
         bytes += al(4 * (t_pairs[l].room.size() + t_pairs[l].first.size())) +
                  al(4 * (t_coarse[l].room.size() + t_coarse[l].first.size()));
     std::vector<unsigned char> host(bytes, 0);
-    FFR_CUDA(cudaMalloc(&B.dev, bytes));
+    if (bytes > B.cap) {
+        if (B.dev) cudaFree(B.dev);
+        B.dev = nullptr;
+        B.cap = 0;
+        FFR_CUDA(cudaMalloc(&B.dev, bytes + bytes / 2));
+        B.cap = bytes + bytes / 2;
+    }
     if (!B.active_host) FFR_CUDA(cudaHostAlloc(&B.active_host, 2 * sizeof(int), cudaHostAllocDefault));
     for (int k = 0; k < 2; k++)
         if (!B.ev[k]) FFR_CUDA(cudaEventCreateWithFlags(&B.ev[k], cudaEventDisableTiming));
@@ -1760,6 +1779,7 @@ void batch_split_release(BatchSplit &B)
 {
     if (B.dev) cudaFree(B.dev);
     B.dev = nullptr;
+    B.cap = 0;
     B.nrooms = 0;
     B.nlev = 0;
     B.nmid = 0;
@@ -1783,26 +1803,8 @@ int batch_iteration(BatchSplit &B, cudaStream_t s)
         chk("k_bsp_restrict");
     }
     if (B.nmid) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_bsp_mid, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-            attr = true;
-        }
-        const int ctas = mid_cluster_ctas();
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(ctas * B.nmid));
-        cfg.blockDim = dim3(kMidThreads);
-        cfg.stream = s;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = (unsigned)ctas;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        cudaError_t e = cudaLaunchKernelEx(&cfg, k_bsp_mid, B.D, B.mid_rooms);
-        if (e != cudaSuccess && rc == FFR_OK) rc = cuda_fail(e, "cudaLaunchKernelEx(k_bsp_mid)");
-        chk("k_bsp_mid");
+        k_bsp_coarse<<<B.nmid, 1024, 0, s>>>(B.D, B.mid_rooms);
+        chk("k_bsp_coarse");
     }
     for (int l = B.nlev - 1; l >= 1; l--) {
         if (!B.nb_pairs[l]) continue;

@@ -140,15 +140,18 @@ struct BatchSplit {
     unsigned nb_post[kMaxLevels]{};
     BMap post0{};                     // level-0 black post-smoothing
     unsigned nb_post0 = 0;
-    const int *mid_rooms = nullptr;   // rooms with a one-cluster part
+    const int *mid_rooms = nullptr;   // rooms with levels small enough for one block
     int nmid = 0;
     void *dev = nullptr;              // device allocation holding all tables
+    size_t cap = 0;                   // its size (reused while large enough)
     int *active_host = nullptr;       // pinned copy of the active count
     cudaEvent_t ev[2] = {nullptr, nullptr};
     int last_iters = 8;
 };
 // Builds the tables for rooms with the given per-room arguments (host
-// copies; device pointers inside) and device split states.
+// copies; device pointers inside) and device split states.  The device
+// buffer of an earlier build is reused when large enough; no launch of an
+// earlier build may still be running.
 int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std::vector<void *> &ss);
 void batch_split_release(BatchSplit &B);
 // The split solve of every room of the batch, host-paced like

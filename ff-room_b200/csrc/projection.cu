@@ -852,10 +852,12 @@ int sm_count()
     return n;
 }
 
+// Grid of a streaming kernel: four items per thread, at most 8 blocks per
+// SM (many rooms in one batched launch fill the GPU by their number).
 unsigned stream_blocks(long long work)
 {
     const long long cap = (long long)sm_count() * 8;
-    return (unsigned)std::max<long long>(1, std::min<long long>(cap, (work + kThreads - 1) / kThreads));
+    return (unsigned)std::max<long long>(1, std::min<long long>(cap, (work + 4 * kThreads - 1) / (4 * kThreads)));
 }
 
 // Device copy of the room-derived tables shared by a solver and its CG.
@@ -1577,6 +1579,7 @@ struct ffr_batch {
     cudaEvent_t ev = nullptr;
     BatchSplit split;
     void *dev = nullptr;          // BRoom array, launch tables, patch items
+    size_t cap = 0;               // its size (reused while large enough)
     const BRoom *broom = nullptr;
     BMap faces{}, cells{}, openm{}, heatm{};
     unsigned nb_faces = 0, nb_cells = 0, nb_open = 0, nb_heat = 0;
@@ -1640,10 +1643,9 @@ BRoom room_step_args(ffr_fluid *s)
 
 extern "C" {
 
-int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out)
+int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms)
 {
-    if (!out || nrooms <= 0 || !rooms) return fail(FFR_EINVAL, "bad arguments");
-    *out = nullptr;
+    if (!b || nrooms <= 0 || !rooms) return fail(FFR_EINVAL, "bad arguments");
     for (int r = 0; r < nrooms; r++) {
         ffr_fluid *s = rooms[r];
         if (!s) return fail(FFR_EINVAL, "NULL room handle");
@@ -1653,14 +1655,11 @@ int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out)
         for (int q = 0; q < r; q++)
             if (rooms[q] == s) return fail(FFR_EINVAL, "a room appears twice in the batch");
     }
-    ffr_batch *b = new (std::nothrow) ffr_batch();
-    if (!b) return fail(FFR_ENOMEM, "host allocation");
+    // the tables of the previous membership may still be read by its launches
+    FFR_CUDA(cudaStreamSynchronize(b->stream));
     b->rooms.assign(rooms, rooms + nrooms);
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
-        batch_free(b);
-        return fail(FFR_ECUDA, "batch stream");
-    }
+    b->any_thermal = false;
+    b->max_iter = 0;
     // per-room arguments, block tables of the step kernels, patch items
     std::vector<BRoom> br(nrooms);
     std::vector<PCGArgs> pa(nrooms);
@@ -1704,9 +1703,12 @@ int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out)
                          al(4 * (hroom.size() + hfirst.size())) + al(sizeof(OpenItem) * (oitems.size() + 1)) +
                          al(sizeof(HeatItem) * (hitems.size() + 1));
     std::vector<unsigned char> host(bytes, 0);
-    if (cudaMalloc(&b->dev, bytes) != cudaSuccess) {
-        batch_free(b);
-        return fail(FFR_ENOMEM, "batch tables");
+    if (bytes > b->cap) {
+        if (b->dev) cudaFree(b->dev);
+        b->dev = nullptr;
+        b->cap = 0;
+        if (cudaMalloc(&b->dev, bytes + bytes / 2) != cudaSuccess) return fail(FFR_ENOMEM, "batch tables");
+        b->cap = bytes + bytes / 2;
     }
     unsigned char *d = static_cast<unsigned char *>(b->dev);
     size_t off = 0;
@@ -1733,11 +1735,22 @@ int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out)
     hitems.push_back(HeatItem{});
     b->open = reinterpret_cast<const OpenItem *>(put(oitems.data(), sizeof(OpenItem) * oitems.size()));
     b->heat = reinterpret_cast<const HeatItem *>(put(hitems.data(), sizeof(HeatItem) * hitems.size()));
-    if (cudaMemcpy(b->dev, host.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    FFR_CUDA(cudaMemcpy(b->dev, host.data(), bytes, cudaMemcpyHostToDevice));
+    return batch_split_build(b->split, pa, ss);
+}
+
+int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out)
+{
+    if (!out || nrooms <= 0 || !rooms) return fail(FFR_EINVAL, "bad arguments");
+    *out = nullptr;
+    ffr_batch *b = new (std::nothrow) ffr_batch();
+    if (!b) return fail(FFR_ENOMEM, "host allocation");
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
         batch_free(b);
-        return fail(FFR_ECUDA, "batch tables upload");
+        return fail(FFR_ECUDA, "batch stream");
     }
-    int rc = batch_split_build(b->split, pa, ss);
+    int rc = ffr_batch_set_rooms(b, rooms, nrooms);
     if (rc) {
         batch_free(b);
         return rc;

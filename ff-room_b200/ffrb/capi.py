@@ -139,6 +139,7 @@ def lib():
             "ffr_fluid_set_split": ([vp, C.c_int], C.c_int),
             "ffr_batch_create": ([C.POINTER(vp), C.c_int, C.POINTER(vp)], C.c_int),
             "ffr_batch_destroy": ([vp], C.c_int),
+            "ffr_batch_set_rooms": ([vp, C.POINTER(vp), C.c_int], C.c_int),
             "ffr_batch_size": ([vp, C.POINTER(C.c_int)], C.c_int),
             "ffr_batch_enqueue": ([vp, C.c_int, C.c_int], C.c_int),
             "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
@@ -338,6 +339,11 @@ class BatchHandle:
         h = C.c_void_p()
         check(lib().ffr_batch_create(arr, len(self.rooms), C.byref(h)))
         self.h = h
+
+    def set_rooms(self, rooms: List["FluidHandle"]) -> None:
+        arr = (C.c_void_p * len(rooms))(*[r.h for r in rooms])
+        check(lib().ffr_batch_set_rooms(self.h, arr, len(rooms)))
+        self.rooms = list(rooms)
 
     def enqueue(self, nsteps: int, stop_on_converge: bool = True) -> None:
         check(lib().ffr_batch_enqueue(self.h, nsteps, int(stop_on_converge)))

@@ -158,13 +158,16 @@ class Outcome:
 
 
 class _Active:
-    def __init__(self, req: Request, sched: Schedule, t_admit: float, keep_fields: bool):
+    def __init__(self, req: Request, sched: Schedule, t_admit: float, keep_fields: bool, split: int = -1):
         self.req = req
         self.sched = sched
         self.t_admit = t_admit
         self.keep_fields = keep_fields
         self.h = capi.FluidHandle(req.room, req.params)
-        apply_schedule(self.h, sched, req.room, req.params)
+        if split != -1:
+            self.h.set_split(split)
+        else:
+            apply_schedule(self.h, sched, req.room, req.params)
         self.bytes = self.h.device_bytes()
         self.charge = self.bytes
         self.steps = 0
@@ -189,16 +192,88 @@ class _Active:
 
 
 class Server:
-    """Continuous-batching server over one GPU."""
+    """Continuous-batching server over one GPU.
+
+    batched=False: every room runs on its own stream with its own launches
+    (the tuner's schedule per size class); batched=True: all active rooms
+    advance together, one launch per stage for the whole set (ffr_batch),
+    in chunks of `chunk` steps; rooms join and leave between chunks."""
 
     def __init__(self, mem_budget: int, max_active: int = 64, tuner: Optional[Tuner] = None,
-                 keep_fields: bool = False):
+                 keep_fields: bool = False, batched: bool = False, chunk: int = 10):
         self.mem_budget = mem_budget
         self.max_active = max_active
         self.tuner = tuner or Tuner()
         self.keep_fields = keep_fields
+        self.batched = batched
+        self.chunk = chunk
 
     def run(self, requests: List[Request], realtime: bool = True) -> List[Outcome]:
+        if self.batched:
+            return self._run_batched(requests, realtime)
+        return self._run_streams(requests, realtime)
+
+    def _finish(self, a: "_Active", t0: float) -> Outcome:
+        fields = {k: a.h.get(k) for k in "uvwpT"} if self.keep_fields else None
+        t = time.perf_counter() - t0
+        o = Outcome(a.req.rid, a.req.room.n_cells, a.req.t_arrival, a.t_admit, t, a.steps,
+                    bool(a.last and a.last["converged"]),
+                    float(a.last["velocity_change"]) if a.last else float("nan"), fields)
+        a.h.close()
+        return o
+
+    def _run_batched(self, requests: List[Request], realtime: bool) -> List[Outcome]:
+        queue = sorted(requests, key=lambda r: r.t_arrival)
+        active: List[_Active] = []
+        used = 0
+        out: List[Outcome] = []
+        t0 = time.perf_counter()
+        qi = 0
+        batch = None
+        members: List[int] = []
+        while qi < len(queue) or active:
+            now = time.perf_counter() - t0
+            while qi < len(queue) and len(active) < self.max_active:
+                req = queue[qi]
+                if realtime and req.t_arrival > now:
+                    break
+                need = estimate_bytes(req.room, req.params)
+                if active and used + need > self.mem_budget:
+                    break
+                a = _Active(req, Schedule(0, self.chunk, False, 0), now, self.keep_fields, split=1)
+                a.charge = need
+                used += need
+                active.append(a)
+                qi += 1
+            if not active:
+                time.sleep(0.0002)
+                continue
+            ids = [id(a) for a in active]
+            if batch is None:
+                batch = capi.BatchHandle([a.h for a in active])
+                members = ids
+            elif ids != members:
+                batch.set_rooms([a.h for a in active])
+                members = ids
+            nsteps = min([self.chunk] + [a.req.max_steps - a.steps for a in active])
+            batch.enqueue(nsteps, True)
+            still = []
+            for a in active:
+                a.queued = nsteps
+                done = None
+                while done is None:
+                    done = a.poll()
+                if done:
+                    out.append(self._finish(a, t0))
+                    used -= a.charge
+                else:
+                    still.append(a)
+            active = still
+        if batch is not None:
+            batch.close()
+        return out
+
+    def _run_streams(self, requests: List[Request], realtime: bool = True) -> List[Outcome]:
         queue = sorted(requests, key=lambda r: r.t_arrival)
         active: List[_Active] = []
         used = 0
@@ -261,7 +336,8 @@ def report(outcomes: List[Outcome], makespan: Optional[float] = None) -> dict:
 def serial_solve(requests: List[Request], params_override: Optional[dict] = None) -> List[Outcome]:
     """The same rooms solved one after another, each to convergence or its
     cap (the serial baseline; with params_override precision="fp64",
-    poisson="cg" it is the plain FP64 GPU solver)."""
+    poisson="cg", use_multigrid=False it is the plain FP64 GPU solver, the
+    reference's method)."""
     out = []
     t0 = time.perf_counter()
     for req in sorted(requests, key=lambda r: r.t_arrival):

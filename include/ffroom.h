@@ -210,6 +210,9 @@ int ffr_fluid_set_split(ffr_fluid *s, int mode);
  * belong to several batches but only one may run at a time. */
 typedef struct ffr_batch ffr_batch;
 int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out);
+/* Replaces the member rooms (the batch's device tables are rebuilt in
+ * place, reusing their memory while it is large enough). */
+int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms);
 int ffr_batch_destroy(ffr_batch *b);
 int ffr_batch_size(const ffr_batch *b, int *nrooms);
 /* Queues nsteps (0..1024) steps of every room; returns once the last

@@ -52,17 +52,26 @@ def test_batch_matches_rooms_alone():
         h.close()
 
 
-def test_batch_tracks_oracle_and_continues():
-    """Two chunks in a row on the same batch; then the fields against the
-    FP64 fixtures (rooms whose fixture has exactly 10 steps)."""
+def test_batch_tracks_oracle_across_membership_changes():
+    """Chunks on one batch object whose members change between chunks (a
+    subset in reverse order, then all again): every room still ends on its
+    own 10-step result, within the mixed bound of the FP64 fixtures."""
     from ffrb import capi
     gs = [Golden(n) for n in NAMES]
     hs = [_handle(g) for g in gs]
     b = capi.BatchHandle(hs)
     first = b.advance(4)
-    second = b.advance(6)
-    for g, h, r1, r2 in zip(gs, hs, first, second):
-        assert [r["step"] for r in r1 + r2] == list(range(1, 11))
+    half = hs[::-2]
+    b.set_rooms(half)
+    mid = dict(zip([id(h) for h in half], b.advance(3)))
+    b.set_rooms(hs)
+    # the rooms left out of the middle chunk catch up alone
+    for h in hs:
+        if id(h) not in mid:
+            mid[id(h)] = h.advance(3)
+    last = b.advance(3)
+    for g, h, r1, r3 in zip(gs, hs, first, last):
+        assert [r["step"] for r in r1 + mid[id(h)] + r3] == list(range(1, 11))
         if g.nsteps != 10:
             continue
         for k in "uvwpT":
