@@ -432,7 +432,8 @@ def main():
     ap.add_argument("--max-cells", type=int, default=600_000, help="serving/batch: largest room in the sample")
     ap.add_argument("--max-steps", type=int, default=40, help="serving/batch: step cap per room")
     ap.add_argument("--no-serving", action="store_true", help="default run: skip the serving sample")
-    ap.add_argument("--batched", type=int, default=1, help="serving/batch: one launch per stage for all rooms")
+    ap.add_argument("--batched", type=int, default=0,
+                    help="serving/batch: 1 = one launch per stage for all active rooms, 0 = one stream per room")
     ap.add_argument("--chunk", type=int, default=10, help="serving/batch: steps between membership changes")
     ap.add_argument("--graph", type=int, default=1,
                     help="replay each step as a CUDA graph (the multigrid solve then runs one kernel per pass)")
@@ -468,7 +469,10 @@ def main():
         dtype = {"fp64": "f64", "mixed": "f32/f64", "fp32": "f32", "fp16": "f16/f32"}.get(args.precision, args.precision)
         serving = None
         if not args.no_serving and args.workload == "large_thermal" and world == 1:
-            serving = run_serving("serving", 16, 300_000, 20)
+            serving = run_serving("serving", 16, 300_000, 20, batched=False)
+            alt = run_serving("serving", 16, 300_000, 20, batched=True)
+            serving["batched_mode"] = {k: alt[k] for k in ("room_solves_per_s", "p50_s", "p99_s",
+                                                          "speedup_vs_serial_fp64", "gpu_launches")}
         line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
                 "steps": res["steps"], "warmup": args.warmup, "ms_per_step": res["ms"] / max(1, res["steps"]),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
