@@ -89,13 +89,16 @@ __host__ __device__ __forceinline__ double lbm_w(int q)
 }
 
 // LBMSolver::feq (LBMSolver.hpp:89-93), cs2 = 1/3, in the reference's
-// operation order.
+// operation order, except that the divisions by cs2, 2 cs2^2 and 2 cs2 are
+// multiplications by their FP64 reciprocals (each term within one rounding
+// of the reference's quotient).
 __device__ __forceinline__ double feq64(int q, double rho, double ux, double uy, double uz)
 {
     const double cs2 = 1.0 / 3.0;
+    const double r1 = 1.0 / cs2, r2 = 1.0 / (2.0 * cs2 * cs2), r3 = 1.0 / (2.0 * cs2);
     const double eu = edot<double>(q, ux, uy, uz);
     const double usq = ux * ux + uy * uy + uz * uz;
-    return lbm_w(q) * rho * (1.0 + eu / cs2 + eu * eu / (2.0 * cs2 * cs2) - usq / (2.0 * cs2));
+    return lbm_w(q) * rho * (1.0 + eu * r1 + eu * eu * r2 - usq * r3);
 }
 
 // Shifted equilibrium feq_q - w_q in FP32 for rho = 1 + drho.

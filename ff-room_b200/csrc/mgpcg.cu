@@ -30,16 +30,25 @@ namespace ffr {
 
 // ---------------------------------------------------------------- host
 
+// Coarsening.  Each level halves the axes whose spacing is within a factor
+// two of the level's smallest spacing (semi-coarsening of anisotropic
+// cells: the strongly coupled directions first), so that the coarse cells
+// approach cubes; isotropic cells halve every axis.  The coarse operator is
+// the fine one re-discretised on the coarse cells: a coarse face couples
+// with the sum of the fine couplings it covers divided by the coarsening
+// factor along its normal (area summed, distance scaled), and likewise
+// for the Dirichlet (outflow) part of the diagonal, kept per axis.
 void build_mg_levels(const HostRoom &r, MGHost &out)
 {
     out.nx.clear(); out.ny.clear(); out.nz.clear(); out.coef.clear();
+    out.sx.clear(); out.sy.clear(); out.sz.clear();
     int nx = r.g.nx, ny = r.g.ny, nz = r.g.nz;
     out.nx.push_back(nx); out.ny.push_back(ny); out.nz.push_back(nz);
     out.coef.emplace_back();
     // fine faces in FP64: T to the + neighbour (0 unless both active) and
-    // the Dirichlet part of the diagonal
+    // the Dirichlet part of the diagonal per axis
     const size_t n0 = (size_t)nx * ny * nz;
-    std::vector<double> tx(n0, 0.0), ty(n0, 0.0), tz(n0, 0.0), dir(n0, 0.0);
+    std::vector<double> tx(n0, 0.0), ty(n0, 0.0), tz(n0, 0.0), dx(n0, 0.0), dy(n0, 0.0), dz(n0, 0.0);
     std::vector<uint8_t> act(n0, 0);
     auto C0 = [&](int i, int j, int k) { return ((size_t)i * ny + j) * nz + k; };
     auto isact = [](uint8_t t) { return t == CT_FLUID || t == CT_INFLOW; };
@@ -55,27 +64,35 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
                 if (i + 1 < nx) {
                     const double t = ax / hc(r.dxv, i, i + 1);
                     const uint8_t nt = r.ct[C0(i + 1, j, k)];
-                    if (isact(nt)) tx[c] = t; else if (nt == CT_OUTFLOW) dir[c] += 2 * t;
+                    if (isact(nt)) tx[c] = t; else if (nt == CT_OUTFLOW) dx[c] += 2 * t;
                 }
                 if (j + 1 < ny) {
                     const double t = ay / hc(r.dyv, j, j + 1);
                     const uint8_t nt = r.ct[C0(i, j + 1, k)];
-                    if (isact(nt)) ty[c] = t; else if (nt == CT_OUTFLOW) dir[c] += 2 * t;
+                    if (isact(nt)) ty[c] = t; else if (nt == CT_OUTFLOW) dy[c] += 2 * t;
                 }
                 if (k + 1 < nz) {
                     const double t = az / hc(r.dzv, k, k + 1);
                     const uint8_t nt = r.ct[C0(i, j, k + 1)];
-                    if (isact(nt)) tz[c] = t; else if (nt == CT_OUTFLOW) dir[c] += 2 * t;
+                    if (isact(nt)) tz[c] = t; else if (nt == CT_OUTFLOW) dz[c] += 2 * t;
                 }
                 // - neighbours that are Dirichlet ghosts
-                if (i > 0 && r.ct[C0(i - 1, j, k)] == CT_OUTFLOW) dir[c] += 2 * ax / hc(r.dxv, i - 1, i);
-                if (j > 0 && r.ct[C0(i, j - 1, k)] == CT_OUTFLOW) dir[c] += 2 * ay / hc(r.dyv, j - 1, j);
-                if (k > 0 && r.ct[C0(i, j, k - 1)] == CT_OUTFLOW) dir[c] += 2 * az / hc(r.dzv, k - 1, k);
+                if (i > 0 && r.ct[C0(i - 1, j, k)] == CT_OUTFLOW) dx[c] += 2 * ax / hc(r.dxv, i - 1, i);
+                if (j > 0 && r.ct[C0(i, j - 1, k)] == CT_OUTFLOW) dy[c] += 2 * ay / hc(r.dyv, j - 1, j);
+                if (k > 0 && r.ct[C0(i, j, k - 1)] == CT_OUTFLOW) dz[c] += 2 * az / hc(r.dzv, k - 1, k);
             }
+    const double lx = r.g.lx, ly = r.g.ly, lz = r.g.lz;
     while ((size_t)nx * ny * nz > 512 && (int)out.nx.size() < kMaxLevels) {
-        const int mx = (nx + 1) / 2, my = (ny + 1) / 2, mz = (nz + 1) / 2;
+        // axes to halve at this level
+        const double hx = lx / nx, hy = ly / ny, hz = lz / nz;
+        const double hmin = std::min(hx, std::min(hy, hz));
+        const int sx = (nx > 1 && hx < 2.0 * hmin) ? 1 : 0;
+        const int sy = (ny > 1 && hy < 2.0 * hmin) ? 1 : 0;
+        const int sz = (nz > 1 && hz < 2.0 * hmin) ? 1 : 0;
+        if (!sx && !sy && !sz) break;
+        const int mx = sx ? (nx + 1) / 2 : nx, my = sy ? (ny + 1) / 2 : ny, mz = sz ? (nz + 1) / 2 : nz;
         const size_t m = (size_t)mx * my * mz;
-        std::vector<double> cx(m, 0.0), cy(m, 0.0), cz(m, 0.0), cd(m, 0.0);
+        std::vector<double> cx(m, 0.0), cy(m, 0.0), cz(m, 0.0), ex(m, 0.0), ey(m, 0.0), ez(m, 0.0);
         std::vector<uint8_t> ca(m, 0);
         auto CC = [&](int i, int j, int k) { return ((size_t)i * my + j) * mz + k; };
         for (int i = 0; i < nx; i++)
@@ -83,14 +100,18 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
                 for (int k = 0; k < nz; k++) {
                     const size_t c = ((size_t)i * ny + j) * nz + k;
                     if (!act[c]) continue;
-                    const size_t P = CC(i / 2, j / 2, k / 2);
+                    const size_t P = CC(i >> sx, j >> sy, k >> sz);
                     ca[P] = 1;
-                    cd[P] += dir[c];
-                    if (tx[c] > 0 && (i + 1) / 2 != i / 2) cx[P] += tx[c];
-                    if (ty[c] > 0 && (j + 1) / 2 != j / 2) cy[P] += ty[c];
-                    if (tz[c] > 0 && (k + 1) / 2 != k / 2) cz[P] += tz[c];
+                    ex[P] += dx[c]; ey[P] += dy[c]; ez[P] += dz[c];
+                    if (tx[c] > 0 && ((i + 1) >> sx) != (i >> sx)) cx[P] += tx[c];
+                    if (ty[c] > 0 && ((j + 1) >> sy) != (j >> sy)) cy[P] += ty[c];
+                    if (tz[c] > 0 && ((k + 1) >> sz) != (k >> sz)) cz[P] += tz[c];
                 }
-        for (size_t P = 0; P < m; P++) { cx[P] *= 0.5; cy[P] *= 0.5; cz[P] *= 0.5; cd[P] *= 0.5; }
+        const double fx = sx ? 0.5 : 1.0, fy = sy ? 0.5 : 1.0, fz = sz ? 0.5 : 1.0;
+        for (size_t P = 0; P < m; P++) {
+            cx[P] *= fx; cy[P] *= fy; cz[P] *= fz;
+            ex[P] *= fx; ey[P] *= fy; ez[P] *= fz;
+        }
         std::vector<float4> coef(m);
         for (int i = 0; i < mx; i++)
             for (int j = 0; j < my; j++)
@@ -98,7 +119,7 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
                     const size_t P = CC(i, j, k);
                     double D = 0.0;
                     if (ca[P]) {
-                        D = cx[P] + cy[P] + cz[P] + cd[P];
+                        D = cx[P] + cy[P] + cz[P] + ex[P] + ey[P] + ez[P];
                         if (i > 0) D += cx[CC(i - 1, j, k)];
                         if (j > 0) D += cy[CC(i, j - 1, k)];
                         if (k > 0) D += cz[CC(i, j, k - 1)];
@@ -106,11 +127,14 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
                     }
                     coef[P] = make_float4((float)cx[P], (float)cy[P], (float)cz[P], (float)D);
                 }
+        out.sx.push_back(sx); out.sy.push_back(sy); out.sz.push_back(sz);
         out.nx.push_back(mx); out.ny.push_back(my); out.nz.push_back(mz);
         out.coef.push_back(std::move(coef));
         nx = mx; ny = my; nz = mz;
-        tx.swap(cx); ty.swap(cy); tz.swap(cz); dir.swap(cd); act.swap(ca);
+        tx.swap(cx); ty.swap(cy); tz.swap(cz); dx.swap(ex); dy.swap(ey); dz.swap(ez); act.swap(ca);
     }
+    // the coarsest level has no next level
+    out.sx.push_back(0); out.sy.push_back(0); out.sz.push_back(0);
 }
 
 // -------------------------------------------------------------- device
@@ -204,16 +228,19 @@ __device__ __forceinline__ void nb_index(int c, int plane, int nz, int n, int (&
 }
 
 // v[a] += the level-(l+1) correction at the parent of neighbour a of cell
-// (i, j, k): the parent of a neighbour is the cell's own parent or the one
-// next to it along the neighbour's axis, by the parity of the coordinate.
-// Indices are clamped into the parent array (a clamped index is only read
-// for a weight-0 neighbour outside the room).
-__device__ __forceinline__ void add_parents(const MGLevel &Lc, int i, int j, int k, float (&v)[6])
+// (i, j, k) of level L: the parent of a neighbour is the cell's own parent
+// or the one next to it along the neighbour's axis (when that axis is
+// halved, by the parity of the coordinate).  Indices are clamped into the
+// parent array (a clamped index is only read for a weight-0 neighbour
+// outside the room).
+__device__ __forceinline__ void add_parents(const MGLevel &L, const MGLevel &Lc, int i, int j, int k, float (&v)[6])
 {
     const int pl = Lc.ny * Lc.nz, pz = Lc.nz, last = Lc.n - 1;
-    const int P0 = ((i >> 1) * Lc.ny + (j >> 1)) * pz + (k >> 1);
-    const int p[6] = {(i & 1) ? P0 : P0 - pl, (i & 1) ? P0 + pl : P0, (j & 1) ? P0 : P0 - pz,
-                      (j & 1) ? P0 + pz : P0, (k & 1) ? P0 : P0 - 1, (k & 1) ? P0 + 1 : P0};
+    const int P0 = ((i >> L.sx) * Lc.ny + (j >> L.sy)) * pz + (k >> L.sz);
+    const bool ox = L.sx && (i & 1), oy = L.sy && (j & 1), oz = L.sz && (k & 1);
+    const bool ex = L.sx && !(i & 1), ey = L.sy && !(j & 1), ez = L.sz && !(k & 1);
+    const int p[6] = {ox ? P0 : P0 - pl, ex ? P0 : P0 + pl, oy ? P0 : P0 - pz,
+                      ey ? P0 : P0 + pz, oz ? P0 : P0 - 1, ez ? P0 : P0 + 1};
 #pragma unroll
     for (int a = 0; a < 6; a++) v[a] += Lc.x[min(max(p[a], 0), last)];
 }
@@ -234,7 +261,7 @@ __device__ __forceinline__ float coarse_nbsum(const MGLevel &L, const MGLevel &L
     float v[6];
 #pragma unroll
     for (int a = 0; a < 6; a++) v[a] = L.x[idx[a]];
-    if (CORR) add_parents(Lc, i, j, k, v);
+    if (CORR) add_parents(L, Lc, i, j, k, v);
     D = cf.w;
     const float t[6] = {i > 0 ? txm : 0.0f, i < L.nx - 1 ? cf.x : 0.0f, j > 0 ? tym : 0.0f,
                         j < L.ny - 1 ? cf.y : 0.0f, k > 0 ? tzm : 0.0f, k < L.nz - 1 ? cf.z : 0.0f};
@@ -255,7 +282,7 @@ __device__ __forceinline__ float fine_nbsum(const RoomDev &R, const MGDev &M, co
     float v[6];
 #pragma unroll
     for (int a = 0; a < 6; a++) v[a] = L0.x[idx[a]];
-    if (CORR) add_parents(L1, i, j, k, v);
+    if (CORR) add_parents(L0, L1, i, j, k, v);
     float t[6];
     fine_coefs(M, code, i, j, k, t, D);
     float s = 0.0f;
@@ -313,7 +340,9 @@ __device__ void restrict_level(const PCGArgs &A, const MGLevel *lv, int l, int s
             for (int b = 0; b < 2; b++) {
 #pragma unroll
                 for (int e = 0; e < 2; e++) {
-                    const int i = 2 * I + a, j = 2 * J + b, k = 2 * K + e;
+                    // children of P along the halved axes
+                    if ((a && !L.sx) || (b && !L.sy) || (e && !L.sz)) continue;
+                    const int i = (I << L.sx) + a, j = (J << L.sy) + b, k = (K << L.sz) + e;
                     // red children inside the level (the same order as a
                     // nested a, b, e loop that skips the rest)
                     if (i >= L.nx || j >= L.ny || k >= L.nz || ((i + j + k) & 1) != 0) continue;
@@ -1293,6 +1322,7 @@ int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGD
     float *fz = ar.take<float>(g.nz), *fzl = ar.take<float>(g.nz), *fzr = ar.take<float>(g.nz);
     // (6 arrays were budgeted per axis set; dx/dy/dz reuse the same slots)
     M.lv[0].nx = g.nx; M.lv[0].ny = g.ny; M.lv[0].nz = g.nz; M.lv[0].n = (int)g.n;
+    M.lv[0].sx = h.sx[0]; M.lv[0].sy = h.sy[0]; M.lv[0].sz = h.sz[0];
     M.lv[0].coef = nullptr;
     M.lv[0].x = ar.take<float>(g.n);
     M.r32 = ar.take<float>(g.n);
@@ -1336,6 +1366,7 @@ int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGD
         const size_t m = (size_t)h.nx[l] * h.ny[l] * h.nz[l];
         MGLevel &L = M.lv[l];
         L.nx = h.nx[l]; L.ny = h.ny[l]; L.nz = h.nz[l]; L.n = (int)m;
+        L.sx = h.sx[l]; L.sy = h.sy[l]; L.sz = h.sz[l];
         float4 *cf = ar.take<float4>(m);
         L.x = ar.take<float>(m);
         L.b = ar.take<float>(m);

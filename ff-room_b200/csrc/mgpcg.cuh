@@ -18,6 +18,7 @@ constexpr int kMidThreads = 512;
 // Inactive cells (no FLUID/INFLOW child) have diagonal 0.
 struct MGLevel {
     int nx, ny, nz, n;
+    int sx, sy, sz, pad;  // 1 where the next coarser level halves the axis
     const float4 *coef;   // level >= 1
     float *x, *b;
 };
@@ -41,6 +42,7 @@ struct MGDev {
 // Host side: builds the coarse levels of a room and uploads them.
 struct MGHost {
     std::vector<int> nx, ny, nz;
+    std::vector<int> sx, sy, sz;             // axes halved towards the next level
     std::vector<std::vector<float4>> coef;   // index 0 unused
 };
 void build_mg_levels(const HostRoom &r, MGHost &out);
