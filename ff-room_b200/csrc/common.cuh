@@ -80,11 +80,17 @@ void build_stencil(const HostRoom &r, std::vector<uint16_t> &sc,
 // Exhaustion is sticky: once a take() fails every later take() fails too,
 // so checking the last slice of a carve (before any copy or launch) covers
 // every slice taken before it.
+// One device allocation per handle, carved into 256-byte aligned slices.
+// With a stream it comes from the device's stream-ordered memory pool
+// (cudaMallocAsync / cudaFreeAsync, memory kept cached in the pool), so
+// creating and destroying handles while other rooms run does not
+// synchronise the device the way cudaMalloc / cudaFree do.
 struct Arena {
     char *base = nullptr;
     size_t size = 0, used = 0;
     bool failed = false;
-    int alloc(size_t bytes);
+    cudaStream_t stream = nullptr;   // set: pool allocation ordered on this stream
+    int alloc(size_t bytes, cudaStream_t s = nullptr);
     template <class T> T *take(size_t count) {
         size_t b = (count * sizeof(T) + 255) & ~size_t(255);
         if (failed || used + b > size) {
@@ -97,6 +103,11 @@ struct Arena {
     }
     void release();
 };
+
+// Page-locked host buffers from a process-wide cache (cudaFreeHost may
+// synchronise the device; returned buffers are kept for the next handle).
+void *pinned_get(size_t bytes);
+void pinned_put(void *p, size_t bytes);
 
 // ------------------------------------------------ grid-wide barrier
 

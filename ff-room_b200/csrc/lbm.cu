@@ -633,7 +633,7 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
                          al(8 * g.nw) + 3 * al(g.n) + al(4 * g.n) + al(8 * fan_lat.size()) + 2 * al(4 * (rd.size() + 1)) +
                          2 * (al(8 * g.nx) + al(8 * g.ny) + al(8 * g.nz)) + al(sizeof(LbmState)) +
                          al(sizeof(ffr_step_result) * kRingL) + al(8);
-    rc = s->arena.alloc(bytes);
+    rc = s->arena.alloc(bytes, s->stream);
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
     Arena &a = s->arena;
     s->f0 = a.take<char>(es * 19 * g.n);
@@ -650,8 +650,9 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     s->st = a.take<LbmState>(1);
     s->ring = a.take<ffr_step_result>(kRingL);
     s->div_slot = a.take<unsigned long long>(1);
-    if (!s->div_slot || a.failed || cudaMallocHost(&s->st_host, sizeof(LbmState)) != cudaSuccess ||
-        cudaMallocHost(&s->ring_host, sizeof(ffr_step_result) * kRingL) != cudaSuccess) {
+    s->st_host = static_cast<LbmState *>(pinned_get(sizeof(LbmState)));
+    s->ring_host = static_cast<ffr_step_result *>(pinned_get(sizeof(ffr_step_result) * kRingL));
+    if (!s->div_slot || a.failed || !s->st_host || !s->ring_host) {
         ffr_lbm_destroy(s);
         return fail(FFR_ENOMEM, "LBM allocation");
     }
@@ -708,8 +709,8 @@ int ffr_lbm_destroy(ffr_lbm *s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     s->prof.destroy();
     s->arena.release();
-    if (s->st_host) cudaFreeHost(s->st_host);
-    if (s->ring_host) cudaFreeHost(s->ring_host);
+    pinned_put(s->st_host, sizeof(LbmState));
+    pinned_put(s->ring_host, sizeof(ffr_step_result) * kRingL);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return FFR_OK;

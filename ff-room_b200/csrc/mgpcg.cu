@@ -1610,14 +1610,15 @@ int capture_split_pcg(const PCGArgs &a, void *ss_dev, cudaStream_t s, cudaStream
 int SplitHost::init()
 {
     if (flags) return FFR_OK;
-    FFR_CUDA(cudaHostAlloc(&flags, 4 * sizeof(int), cudaHostAllocDefault));
+    flags = static_cast<int *>(pinned_get(4 * sizeof(int)));
+    if (!flags) return fail(FFR_ENOMEM, "pinned host memory");
     for (int k = 0; k < 2; k++) FFR_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
     return FFR_OK;
 }
 
 void SplitHost::release()
 {
-    if (flags) cudaFreeHost(flags);
+    pinned_put(flags, 4 * sizeof(int));
     for (int k = 0; k < 2; k++)
         if (ev[k]) cudaEventDestroy(ev[k]);
     flags = nullptr;

@@ -1174,7 +1174,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
                          al(256) +
                          al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
                          al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (s->mg ? mg_bytes(s->room, s->mgh) : 0);
-    rc = s->arena.alloc(bytes);
+    rc = s->arena.alloc(bytes, s->stream);
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
     rc = upload_tables(s->room, s->arena, s->stream, s->tab, s->R);
     if (!rc && s->mg) {
@@ -1203,8 +1203,9 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
         ffr_fluid_destroy(s);
         return rc;
     }
-    if (cudaMallocHost(&s->ring_host, sizeof(ffr_step_result) * kRing) != cudaSuccess ||
-        cudaMallocHost(&s->st_host, sizeof(StepState)) != cudaSuccess) {
+    s->ring_host = static_cast<ffr_step_result *>(pinned_get(sizeof(ffr_step_result) * kRing));
+    s->st_host = static_cast<StepState *>(pinned_get(sizeof(StepState)));
+    if (!s->ring_host || !s->st_host) {
         ffr_fluid_destroy(s);
         return fail(FFR_ENOMEM, "pinned host allocation");
     }
@@ -1253,8 +1254,8 @@ int ffr_fluid_destroy(ffr_fluid *s)
     s->split_host.release();
     if (s->done_ev) cudaEventDestroy(s->done_ev);
     s->arena.release();
-    if (s->ring_host) cudaFreeHost(s->ring_host);
-    if (s->st_host) cudaFreeHost(s->st_host);
+    pinned_put(s->ring_host, sizeof(ffr_step_result) * kRing);
+    pinned_put(s->st_host, sizeof(StepState));
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return FFR_OK;

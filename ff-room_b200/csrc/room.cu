@@ -1,6 +1,10 @@
 // room.cu — room validation, mask-derived codes, arena, error plumbing.
 #include "common.cuh"
 
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
@@ -29,24 +33,82 @@ int cuda_fail(cudaError_t e, const char *what)
 
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
-int Arena::alloc(size_t bytes)
+namespace {
+// Keep freed pool memory cached (the default release threshold returns it
+// to the system at every synchronisation), once per device.
+void keep_pool_cached()
+{
+    static std::mutex mu;
+    static bool done[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        unsigned long long thr = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done[dev] = true;
+}
+}  // namespace
+
+int Arena::alloc(size_t bytes, cudaStream_t s)
 {
     size = (bytes + 255) & ~size_t(255);
     used = 0;
     failed = false;
-    cudaError_t e = cudaMalloc(&base, size);
+    stream = s;
+    cudaError_t e;
+    if (s) {
+        keep_pool_cached();
+        e = cudaMallocAsync(reinterpret_cast<void **>(&base), size, s);
+    } else {
+        e = cudaMalloc(&base, size);
+    }
     if (e != cudaSuccess) {
         base = nullptr;
-        return cuda_fail(e, "cudaMalloc(arena)");
+        return cuda_fail(e, s ? "cudaMallocAsync(arena)" : "cudaMalloc(arena)");
     }
     return FFR_OK;
 }
 
 void Arena::release()
 {
-    if (base) cudaFree(base);
+    if (base) {
+        if (stream) cudaFreeAsync(base, stream);
+        else cudaFree(base);
+    }
     base = nullptr;
     size = used = 0;
+}
+
+namespace {
+std::mutex g_pinned_mu;
+std::unordered_map<size_t, std::vector<void *>> g_pinned;
+}  // namespace
+
+void *pinned_get(size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        auto it = g_pinned.find(bytes);
+        if (it != g_pinned.end() && !it->second.empty()) {
+            void *p = it->second.back();
+            it->second.pop_back();
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void pinned_put(void *p, size_t bytes)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned[bytes].push_back(p);
 }
 
 // Validates a room descriptor and copies it.  The reference accepts some of

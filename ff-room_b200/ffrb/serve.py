@@ -63,7 +63,8 @@ class Tuner:
 
     ``tune`` times a few candidate schedules on rooms of the class running
     side by side and keeps the fastest by aggregate cell-steps/s; untuned
-    classes get the default schedule.  The table can be saved and loaded.
+    classes get the default schedule (default_schedule).  The table can be
+    saved and loaded.
     """
 
     CANDIDATES = [Schedule(0, 20, False), Schedule(0, 20, True), Schedule(-4, 20, True),
@@ -73,8 +74,19 @@ class Tuner:
     def __init__(self, table: Optional[Dict[int, Schedule]] = None):
         self.table: Dict[int, Schedule] = dict(table or {})
 
+    # rooms up to this size default to one 16-block cluster per room (many
+    # such rooms run side by side); larger ones to the split solve on the
+    # whole GPU; both replay each step from a CUDA graph
+    CLUSTER_MAX_CELLS = 1 << 20
+
+    @classmethod
+    def default_schedule(cls, room: RoomSpec) -> Schedule:
+        if room.n_cells <= cls.CLUSTER_MAX_CELLS:
+            return Schedule(0, 20, True, 16)
+        return Schedule(0, 20, True, 0)
+
     def schedule(self, room: RoomSpec) -> Schedule:
-        return self.table.get(size_class(room.n_cells), Schedule())
+        return self.table.get(size_class(room.n_cells), self.default_schedule(room))
 
     @staticmethod
     def _blocks(sched: Schedule, cap: int) -> int:
