@@ -703,6 +703,26 @@ __global__ void k_begin_chunk(StepState *st, int stop_on_converge)
     st->stop_on_converge = stop_on_converge;
 }
 
+// Cell-centred velocity (face averages) and speed, the snapshot of
+// SolverBridge.run_animated (solver_bridge.py:222-238), on the device.
+__global__ void __launch_bounds__(256) k_snapshot(RoomDev R, const double *__restrict__ u,
+                                                  const double *__restrict__ v, const double *__restrict__ w,
+                                                  double *__restrict__ uc, double *__restrict__ vc,
+                                                  double *__restrict__ wc, double *__restrict__ speed)
+{
+    const int ny = R.ny, nz = R.nz, plane = ny * nz;
+    for (Walk wk(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, ny, nz, R.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        const double a = 0.5 * (u[c] + u[c + plane]);
+        const double b = 0.5 * (v[VIX(i, j, k)] + v[VIX(i, j + 1, k)]);
+        const double e = 0.5 * (w[WIX(i, j, k)] + w[WIX(i, j, k + 1)]);
+        uc[c] = a;
+        vc[c] = b;
+        wc[c] = e;
+        speed[c] = sqrt(a * a + b * b + e * e);
+    }
+}
+
 // ---------------------------------------------------------- batched rooms
 //
 // One launch per stage advances every room of a batch.  Block b works on
@@ -1490,6 +1510,23 @@ int ffr_fluid_divergence_max(ffr_fluid *s, double *out)
     FFR_CUDA(cudaMemcpyAsync(&bits, s->div_slot, 8, cudaMemcpyDeviceToHost, s->stream));
     FFR_CUDA(cudaStreamSynchronize(s->stream));
     memcpy(out, &bits, 8);
+    return FFR_OK;
+}
+
+int ffr_fluid_snapshot(ffr_fluid *s, double *uc, double *vc, double *wc, double *speed)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    int rc = pull_state(s);
+    if (rc) return rc;
+    // the CG work vectors are free between steps: they hold the snapshot
+    k_snapshot<<<s->blocks_cells, kThreads, 0, s->stream>>>(s->R, s->u, s->v, s->w, s->r, s->da, s->db, s->ad);
+    FFR_LAUNCHED(1);
+    const size_t bytes = 8 * (size_t)s->room.g.n;
+    if (uc) FFR_CUDA(cudaMemcpyAsync(uc, s->r, bytes, cudaMemcpyDeviceToHost, s->stream));
+    if (vc) FFR_CUDA(cudaMemcpyAsync(vc, s->da, bytes, cudaMemcpyDeviceToHost, s->stream));
+    if (wc) FFR_CUDA(cudaMemcpyAsync(wc, s->db, bytes, cudaMemcpyDeviceToHost, s->stream));
+    if (speed) FFR_CUDA(cudaMemcpyAsync(speed, s->ad, bytes, cudaMemcpyDeviceToHost, s->stream));
+    FFR_CUDA(cudaStreamSynchronize(s->stream));
     return FFR_OK;
 }
 

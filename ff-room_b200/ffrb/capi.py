@@ -137,6 +137,7 @@ def lib():
             "ffr_fluid_set_cluster": ([vp, C.c_int], C.c_int),
             "ffr_fluid_time_pressure": ([vp, C.c_int, _dp, C.POINTER(C.c_int)], C.c_int),
             "ffr_fluid_set_split": ([vp, C.c_int], C.c_int),
+            "ffr_fluid_snapshot": ([vp, _dp, _dp, _dp, _dp], C.c_int),
             "ffr_batch_create": ([C.POINTER(vp), C.c_int, C.POINTER(vp)], C.c_int),
             "ffr_batch_destroy": ([vp], C.c_int),
             "ffr_batch_set_rooms": ([vp, C.POINTER(vp), C.c_int], C.c_int),
@@ -278,6 +279,20 @@ class FluidHandle:
 
     def set_blocks(self, blocks: int) -> None:
         check(lib().ffr_fluid_set_blocks(self.h, int(blocks)))
+
+    def snapshot(self, with_velocity: bool = True) -> dict:
+        """run_animated's snapshot from the device: {"speed": (nx, ny, nz),
+        "vel": (nx, ny, nz, 3)} (vel only with with_velocity)."""
+        shape = (self.room.nx, self.room.ny, self.room.nz)
+        n = int(np.prod(shape))
+        speed = np.empty(n)
+        comps = [np.empty(n) for _ in range(3)] if with_velocity else [None, None, None]
+        ptr = lambda a: a.ctypes.data_as(_dp) if a is not None else None
+        check(lib().ffr_fluid_snapshot(self.h, ptr(comps[0]), ptr(comps[1]), ptr(comps[2]), ptr(speed)))
+        out = {"speed": speed.reshape(shape)}
+        if with_velocity:
+            out["vel"] = np.stack([c.reshape(shape) for c in comps], axis=-1)
+        return out
 
     def set_split(self, mode: int) -> None:
         """Multigrid schedule: 1 kernel per pass, 0 persistent, -1 split in graphs."""

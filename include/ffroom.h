@@ -221,6 +221,11 @@ int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge);
 
 /* FluidSolver::compute_divergence_max (FluidSolver.cpp:470-484). */
 int ffr_fluid_divergence_max(ffr_fluid *s, double *out);
+/* Snapshot of SolverBridge.run_animated (python/ff_room/solver_bridge.py:
+ * 222-238) computed on the device: cell-centred velocity components (face
+ * averages) and speed, each nx*ny*nz doubles in the field layout; any
+ * output may be NULL.  Only the requested arrays cross PCIe. */
+int ffr_fluid_snapshot(ffr_fluid *s, double *uc, double *vc, double *wc, double *speed);
 /* FluidSolver::current_step (FluidSolver.hpp:63). */
 int ffr_fluid_current_step(ffr_fluid *s, int *out);
 
