@@ -8,6 +8,10 @@
 
 #include "ffroom.h"
 
+#include <algorithm>
+#include <thread>
+#include <vector>
+
 namespace ffr {
 
 // ------------------------------------------------------------ errors
@@ -103,6 +107,26 @@ struct Arena {
     }
     void release();
 };
+
+// Host loop over [0, n) split into contiguous slabs, one per host thread:
+// f(begin, end).  For set-up work over cells or planes of a room.
+template <class F>
+void parallel_slabs(int n, F f)
+{
+    const unsigned hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    const int nt = (int)std::min<unsigned>(hw, (unsigned)std::max(1, n / 2));
+    if (nt <= 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const int chunk = (n + nt - 1) / nt;
+    for (int t = 0; t < nt; t++) {
+        const int b = t * chunk, e = std::min(n, b + chunk);
+        if (b < e) th.emplace_back(f, b, e);
+    }
+    for (auto &x : th) x.join();
+}
 
 // Page-locked host buffers from a process-wide cache (cudaFreeHost may
 // synchronise the device; returned buffers are kept for the next handle).

@@ -24,6 +24,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <thread>
 #include <cmath>
 
 namespace ffr {
@@ -38,6 +39,66 @@ namespace ffr {
 // with the sum of the fine couplings it covers divided by the coarsening
 // factor along its normal (area summed, distance scaled), and likewise
 // for the Dirichlet (outflow) part of the diagonal, kept per axis.
+//
+// Each coarse cell gathers from its children, so the build runs on all
+// host threads (slabs of coarse x-planes); the fine level's couplings are
+// formed on the fly from the cell types and spacings.
+namespace {
+
+// Per cell: couplings to the +x, +y, +z neighbour and the Dirichlet
+// diagonal parts along x, y, z.
+struct LevelOps {
+    std::vector<double> t[6];
+    std::vector<uint8_t> act;
+    void resize(size_t m)
+    {
+        for (auto &v : t) v.assign(m, 0.0);
+        act.assign(m, 0);
+    }
+};
+
+// Coarse level (mx, my, mz) of a level whose cell (i, j, k) is described by
+// `cell(i, j, k, t) -> active`.
+template <class Cell>
+void coarsen(const Cell &cell, int nx, int ny, int nz, int sx, int sy, int sz, int mx, int my, int mz, LevelOps &out)
+{
+    out.resize((size_t)mx * my * mz);
+    const double f[3] = {sx ? 0.5 : 1.0, sy ? 0.5 : 1.0, sz ? 0.5 : 1.0};
+    parallel_slabs(mx, [&](int I0, int I1) {
+        for (int I = I0; I < I1; I++)
+            for (int J = 0; J < my; J++)
+                for (int K = 0; K < mz; K++) {
+                    const size_t P = ((size_t)I * my + J) * mz + K;
+                    double acc[6] = {0, 0, 0, 0, 0, 0};
+                    bool any = false;
+                    for (int a = 0; a <= sx; a++) {
+                        const int i = (I << sx) + a;
+                        if (i >= nx) break;
+                        for (int b = 0; b <= sy; b++) {
+                            const int j = (J << sy) + b;
+                            if (j >= ny) break;
+                            for (int e = 0; e <= sz; e++) {
+                                const int k = (K << sz) + e;
+                                if (k >= nz) break;
+                                double t[6];
+                                if (!cell(i, j, k, t)) continue;
+                                any = true;
+                                for (int d = 3; d < 6; d++) acc[d] += t[d];
+                                // couplings across the parent's + faces only
+                                if (t[0] > 0 && ((i + 1) >> sx) != (i >> sx)) acc[0] += t[0];
+                                if (t[1] > 0 && ((j + 1) >> sy) != (j >> sy)) acc[1] += t[1];
+                                if (t[2] > 0 && ((k + 1) >> sz) != (k >> sz)) acc[2] += t[2];
+                            }
+                        }
+                    }
+                    out.act[P] = any;
+                    for (int d = 0; d < 6; d++) out.t[d][P] = acc[d] * f[d % 3];
+                }
+    });
+}
+
+}  // namespace
+
 void build_mg_levels(const HostRoom &r, MGHost &out)
 {
     out.nx.clear(); out.ny.clear(); out.nz.clear(); out.coef.clear();
@@ -45,43 +106,40 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
     int nx = r.g.nx, ny = r.g.ny, nz = r.g.nz;
     out.nx.push_back(nx); out.ny.push_back(ny); out.nz.push_back(nz);
     out.coef.emplace_back();
-    // fine faces in FP64: T to the + neighbour (0 unless both active) and
-    // the Dirichlet part of the diagonal per axis
-    const size_t n0 = (size_t)nx * ny * nz;
-    std::vector<double> tx(n0, 0.0), ty(n0, 0.0), tz(n0, 0.0), dx(n0, 0.0), dy(n0, 0.0), dz(n0, 0.0);
-    std::vector<uint8_t> act(n0, 0);
-    auto C0 = [&](int i, int j, int k) { return ((size_t)i * ny + j) * nz + k; };
+    const int fnx = nx, fny = ny, fnz = nz;
+    auto C0 = [&](int i, int j, int k) { return ((size_t)i * fny + j) * fnz + k; };
     auto isact = [](uint8_t t) { return t == CT_FLUID || t == CT_INFLOW; };
-    for (size_t c = 0; c < n0; c++) act[c] = isact(r.ct[c]);
     auto hc = [](const std::vector<double> &h, int a, int b) { return 0.5 * (h[a] + h[b]); };
-    for (int i = 0; i < nx; i++)
-        for (int j = 0; j < ny; j++)
-            for (int k = 0; k < nz; k++) {
-                const size_t c = C0(i, j, k);
-                if (!act[c]) continue;
-                const double ax = r.dyv[j] * r.dzv[k], ay = r.dxv[i] * r.dzv[k], az = r.dxv[i] * r.dyv[j];
-                // + neighbours
-                if (i + 1 < nx) {
-                    const double t = ax / hc(r.dxv, i, i + 1);
-                    const uint8_t nt = r.ct[C0(i + 1, j, k)];
-                    if (isact(nt)) tx[c] = t; else if (nt == CT_OUTFLOW) dx[c] += 2 * t;
-                }
-                if (j + 1 < ny) {
-                    const double t = ay / hc(r.dyv, j, j + 1);
-                    const uint8_t nt = r.ct[C0(i, j + 1, k)];
-                    if (isact(nt)) ty[c] = t; else if (nt == CT_OUTFLOW) dy[c] += 2 * t;
-                }
-                if (k + 1 < nz) {
-                    const double t = az / hc(r.dzv, k, k + 1);
-                    const uint8_t nt = r.ct[C0(i, j, k + 1)];
-                    if (isact(nt)) tz[c] = t; else if (nt == CT_OUTFLOW) dz[c] += 2 * t;
-                }
-                // - neighbours that are Dirichlet ghosts
-                if (i > 0 && r.ct[C0(i - 1, j, k)] == CT_OUTFLOW) dx[c] += 2 * ax / hc(r.dxv, i - 1, i);
-                if (j > 0 && r.ct[C0(i, j - 1, k)] == CT_OUTFLOW) dy[c] += 2 * ay / hc(r.dyv, j - 1, j);
-                if (k > 0 && r.ct[C0(i, j, k - 1)] == CT_OUTFLOW) dz[c] += 2 * az / hc(r.dzv, k - 1, k);
-            }
+    // fine level (FP64): T to the + neighbour (0 unless both active) and the
+    // Dirichlet part of the diagonal per axis
+    auto fine = [&](int i, int j, int k, double (&t)[6]) -> bool {
+        for (int d = 0; d < 6; d++) t[d] = 0.0;
+        if (!isact(r.ct[C0(i, j, k)])) return false;
+        const double ax = r.dyv[j] * r.dzv[k], ay = r.dxv[i] * r.dzv[k], az = r.dxv[i] * r.dyv[j];
+        if (i + 1 < fnx) {
+            const double v = ax / hc(r.dxv, i, i + 1);
+            const uint8_t nt = r.ct[C0(i + 1, j, k)];
+            if (isact(nt)) t[0] = v; else if (nt == CT_OUTFLOW) t[3] += 2 * v;
+        }
+        if (j + 1 < fny) {
+            const double v = ay / hc(r.dyv, j, j + 1);
+            const uint8_t nt = r.ct[C0(i, j + 1, k)];
+            if (isact(nt)) t[1] = v; else if (nt == CT_OUTFLOW) t[4] += 2 * v;
+        }
+        if (k + 1 < fnz) {
+            const double v = az / hc(r.dzv, k, k + 1);
+            const uint8_t nt = r.ct[C0(i, j, k + 1)];
+            if (isact(nt)) t[2] = v; else if (nt == CT_OUTFLOW) t[5] += 2 * v;
+        }
+        // - neighbours that are Dirichlet ghosts
+        if (i > 0 && r.ct[C0(i - 1, j, k)] == CT_OUTFLOW) t[3] += 2 * ax / hc(r.dxv, i - 1, i);
+        if (j > 0 && r.ct[C0(i, j - 1, k)] == CT_OUTFLOW) t[4] += 2 * ay / hc(r.dyv, j - 1, j);
+        if (k > 0 && r.ct[C0(i, j, k - 1)] == CT_OUTFLOW) t[5] += 2 * az / hc(r.dzv, k - 1, k);
+        return true;
+    };
+    LevelOps cur, next;
     const double lx = r.g.lx, ly = r.g.ly, lz = r.g.lz;
+    bool first = true;
     while ((size_t)nx * ny * nz > 512 && (int)out.nx.size() < kMaxLevels) {
         // axes to halve at this level
         const double hx = lx / nx, hy = ly / ny, hz = lz / nz;
@@ -91,47 +149,44 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
         const int sz = (nz > 1 && hz < 2.0 * hmin) ? 1 : 0;
         if (!sx && !sy && !sz) break;
         const int mx = sx ? (nx + 1) / 2 : nx, my = sy ? (ny + 1) / 2 : ny, mz = sz ? (nz + 1) / 2 : nz;
-        const size_t m = (size_t)mx * my * mz;
-        std::vector<double> cx(m, 0.0), cy(m, 0.0), cz(m, 0.0), ex(m, 0.0), ey(m, 0.0), ez(m, 0.0);
-        std::vector<uint8_t> ca(m, 0);
-        auto CC = [&](int i, int j, int k) { return ((size_t)i * my + j) * mz + k; };
-        for (int i = 0; i < nx; i++)
-            for (int j = 0; j < ny; j++)
-                for (int k = 0; k < nz; k++) {
-                    const size_t c = ((size_t)i * ny + j) * nz + k;
-                    if (!act[c]) continue;
-                    const size_t P = CC(i >> sx, j >> sy, k >> sz);
-                    ca[P] = 1;
-                    ex[P] += dx[c]; ey[P] += dy[c]; ez[P] += dz[c];
-                    if (tx[c] > 0 && ((i + 1) >> sx) != (i >> sx)) cx[P] += tx[c];
-                    if (ty[c] > 0 && ((j + 1) >> sy) != (j >> sy)) cy[P] += ty[c];
-                    if (tz[c] > 0 && ((k + 1) >> sz) != (k >> sz)) cz[P] += tz[c];
-                }
-        const double fx = sx ? 0.5 : 1.0, fy = sy ? 0.5 : 1.0, fz = sz ? 0.5 : 1.0;
-        for (size_t P = 0; P < m; P++) {
-            cx[P] *= fx; cy[P] *= fy; cz[P] *= fz;
-            ex[P] *= fx; ey[P] *= fy; ez[P] *= fz;
+        if (first) {
+            coarsen(fine, nx, ny, nz, sx, sy, sz, mx, my, mz, next);
+        } else {
+            const int cny = ny, cnz = nz;
+            auto lvl = [&](int i, int j, int k, double (&t)[6]) -> bool {
+                const size_t c = ((size_t)i * cny + j) * cnz + k;
+                for (int d = 0; d < 6; d++) t[d] = cur.t[d][c];
+                return cur.act[c] != 0;
+            };
+            coarsen(lvl, nx, ny, nz, sx, sy, sz, mx, my, mz, next);
         }
+        first = false;
+        const size_t m = (size_t)mx * my * mz;
         std::vector<float4> coef(m);
-        for (int i = 0; i < mx; i++)
-            for (int j = 0; j < my; j++)
-                for (int k = 0; k < mz; k++) {
-                    const size_t P = CC(i, j, k);
-                    double D = 0.0;
-                    if (ca[P]) {
-                        D = cx[P] + cy[P] + cz[P] + ex[P] + ey[P] + ez[P];
-                        if (i > 0) D += cx[CC(i - 1, j, k)];
-                        if (j > 0) D += cy[CC(i, j - 1, k)];
-                        if (k > 0) D += cz[CC(i, j, k - 1)];
-                        if (!(D > 0)) D = 1.0;
+        auto CC = [&](int i, int j, int k) { return ((size_t)i * my + j) * mz + k; };
+        parallel_slabs(mx, [&](int i0, int i1) {
+            for (int i = i0; i < i1; i++)
+                for (int j = 0; j < my; j++)
+                    for (int k = 0; k < mz; k++) {
+                        const size_t P = CC(i, j, k);
+                        double D = 0.0;
+                        if (next.act[P]) {
+                            D = next.t[0][P] + next.t[1][P] + next.t[2][P] + next.t[3][P] + next.t[4][P] +
+                                next.t[5][P];
+                            if (i > 0) D += next.t[0][CC(i - 1, j, k)];
+                            if (j > 0) D += next.t[1][CC(i, j - 1, k)];
+                            if (k > 0) D += next.t[2][CC(i, j, k - 1)];
+                            if (!(D > 0)) D = 1.0;
+                        }
+                        coef[P] = make_float4((float)next.t[0][P], (float)next.t[1][P], (float)next.t[2][P],
+                                              (float)D);
                     }
-                    coef[P] = make_float4((float)cx[P], (float)cy[P], (float)cz[P], (float)D);
-                }
+        });
         out.sx.push_back(sx); out.sy.push_back(sy); out.sz.push_back(sz);
         out.nx.push_back(mx); out.ny.push_back(my); out.nz.push_back(mz);
         out.coef.push_back(std::move(coef));
         nx = mx; ny = my; nz = mz;
-        tx.swap(cx); ty.swap(cy); tz.swap(cz); dx.swap(ex); dy.swap(ey); dz.swap(ez); act.swap(ca);
+        std::swap(cur, next);
     }
     // the coarsest level has no next level
     out.sx.push_back(0); out.sy.push_back(0); out.sz.push_back(0);

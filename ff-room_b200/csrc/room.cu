@@ -234,7 +234,8 @@ void build_stencil(const HostRoom &r, std::vector<uint16_t> &sc, std::vector<dou
         const uint8_t t = r.ct[CI(i, j, k)];
         return t == CT_OUTFLOW ? SC_DIR : (t == CT_SOLID ? SC_NONE : SC_IN);
     };
-    for (int i = 0; i < nx; i++)
+    parallel_slabs(nx, [&](int i0, int i1) {
+    for (int i = i0; i < i1; i++)
         for (int j = 0; j < ny; j++)
             for (int k = 0; k < nz; k++) {
                 uint16_t c = 0;
@@ -251,6 +252,7 @@ void build_stencil(const HostRoom &r, std::vector<uint16_t> &sc, std::vector<dou
                 }
                 sc[CI(i, j, k)] = c;
             }
+    });
     // layout: [sxl(nx) sxr(nx) syl(ny) syr(ny) szl(nz) szr(nz)]
     scale.assign(2 * (size_t)(nx + ny + nz), 0.0);
     auto axis = [&](const std::vector<double> &h, int m, double *sl, double *sr) {
