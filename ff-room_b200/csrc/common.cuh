@@ -128,6 +128,11 @@ void parallel_slabs(int n, F f)
     for (auto &x : th) x.join();
 }
 
+// Synchronous copy between pageable host memory and the device through two
+// page-locked bounce buffers: the DMA of one chunk overlaps the host copy
+// (on several threads) of the other.  Small copies go direct.
+int staged_copy(void *dst, const void *src, size_t bytes, bool to_host, cudaStream_t st);
+
 // Page-locked host buffers from a process-wide cache (cudaFreeHost may
 // synchronise the device; returned buffers are kept for the next handle).
 void *pinned_get(size_t bytes);

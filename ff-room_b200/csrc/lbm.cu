@@ -677,7 +677,7 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
     FFR_CUDA(cudaMemcpyAsync(dyv, s->room.dyv.data(), 8 * g.ny, cudaMemcpyHostToDevice, st));
     FFR_CUDA(cudaMemcpyAsync(dzv, s->room.dzv.data(), 8 * g.nz, cudaMemcpyHostToDevice, st));
     auto up = [&](double *d, const double *h, long long cnt) -> int {
-        if (h) FFR_CUDA(cudaMemcpyAsync(d, h, 8 * cnt, cudaMemcpyHostToDevice, st));
+        if (h) return staged_copy(d, h, 8 * cnt, false, st);
         else FFR_CUDA(cudaMemsetAsync(d, 0, 8 * cnt, st));
         return FFR_OK;
     };
@@ -791,9 +791,7 @@ int ffr_lbm_get_field(ffr_lbm *s, int field, double *host)
     long long len = 0;
     double *d = s && host ? lbm_field(s, field, &len) : nullptr;
     if (!d) return fail(FFR_EINVAL, "bad LBM get_field arguments");
-    FFR_CUDA(cudaMemcpyAsync(host, d, 8 * len, cudaMemcpyDeviceToHost, s->stream));
-    FFR_CUDA(cudaStreamSynchronize(s->stream));
-    return FFR_OK;
+    return staged_copy(host, d, 8 * len, true, s->stream);
 }
 
 int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host)
@@ -801,9 +799,7 @@ int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host)
     long long len = 0;
     double *d = s && host ? lbm_field(s, field, &len) : nullptr;
     if (!d) return fail(FFR_EINVAL, "bad LBM set_field arguments");
-    FFR_CUDA(cudaMemcpyAsync(d, host, 8 * len, cudaMemcpyHostToDevice, s->stream));
-    FFR_CUDA(cudaStreamSynchronize(s->stream));
-    return FFR_OK;
+    return staged_copy(d, host, 8 * len, false, s->stream);
 }
 
 int ffr_lbm_synchronize(ffr_lbm *s)

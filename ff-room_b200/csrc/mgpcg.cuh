@@ -11,7 +11,7 @@ constexpr int kMaxLevels = 12;
 constexpr int kBlockLevelCells = 640;
 // Levels (>= 1) with at most this many cells run, in the split solve, inside
 // one thread-block cluster of kMidThreads-thread blocks.
-constexpr int kMidLevelCells = 160 * 1024;
+constexpr int kMidLevelCells = 32 * 1024;
 constexpr int kMidThreads = 512;
 
 // One coarse level: per cell (T to the x+, y+, z+ neighbour, diagonal), FP32.

@@ -922,11 +922,11 @@ int upload_tables(const HostRoom &h, Arena &ar, cudaStream_t s, RoomTables &t, R
     FFR_CUDA(cudaMemcpyAsync(t.dzv, h.dzv.data(), 8 * g.nz, cudaMemcpyHostToDevice, s));
     FFR_CUDA(cudaMemcpyAsync(t.scale, scale.data(), 8 * scale.size(), cudaMemcpyHostToDevice, s));
     FFR_CUDA(cudaMemcpyAsync(t.fanvel, fan.data(), 8 * fan.size(), cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.ct, h.ct.data(), g.n, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.fcu, fu.data(), g.nu, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.fcv, fv.data(), g.nv, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.fcw, fw.data(), g.nw, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.sc, sc.data(), 2 * g.n, cudaMemcpyHostToDevice, s));
+    int rc;
+    if ((rc = staged_copy(t.ct, h.ct.data(), g.n, false, s)) || (rc = staged_copy(t.fcu, fu.data(), g.nu, false, s)) ||
+        (rc = staged_copy(t.fcv, fv.data(), g.nv, false, s)) || (rc = staged_copy(t.fcw, fw.data(), g.nw, false, s)) ||
+        (rc = staged_copy(t.sc, sc.data(), 2 * g.n, false, s)))
+        return rc;
     // The host vectors die at return: wait for the copies.
     FFR_CUDA(cudaStreamSynchronize(s));
     R.nx = g.nx; R.ny = g.ny; R.nz = g.nz;
@@ -1238,8 +1238,12 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     cudaStream_t st = s->stream;
 #define UP(dst, src, cnt)                                                                      \
     do {                                                                                       \
-        if (src) FFR_CUDA(cudaMemcpyAsync(dst, src, 8 * (cnt), cudaMemcpyHostToDevice, st));   \
-        else FFR_CUDA(cudaMemsetAsync(dst, 0, 8 * (cnt), st));                                 \
+        if (src) {                                                                             \
+            rc = staged_copy(dst, src, 8 * (cnt), false, st);                                  \
+            if (rc) { ffr_fluid_destroy(s); return rc; }                                       \
+        } else {                                                                               \
+            FFR_CUDA(cudaMemsetAsync(dst, 0, 8 * (cnt), st));                                  \
+        }                                                                                      \
     } while (0)
     UP(s->u, init ? init->u : nullptr, g.nu);
     UP(s->v, init ? init->v : nullptr, g.nv);
@@ -1544,10 +1548,7 @@ int ffr_fluid_get_field(ffr_fluid *s, int field, double *host)
     if (!s || !host || field < 0 || field > 4) return fail(FFR_EINVAL, "bad get_field arguments");
     int rc = pull_state(s);
     if (rc) return rc;
-    FFR_CUDA(cudaMemcpyAsync(host, field_ptr(s, field), 8 * field_len(s, field), cudaMemcpyDeviceToHost,
-                             s->stream));
-    FFR_CUDA(cudaStreamSynchronize(s->stream));
-    return FFR_OK;
+    return staged_copy(host, field_ptr(s, field), 8 * field_len(s, field), true, s->stream);
 }
 
 int ffr_fluid_set_field(ffr_fluid *s, int field, const double *host)
@@ -1555,10 +1556,7 @@ int ffr_fluid_set_field(ffr_fluid *s, int field, const double *host)
     if (!s || !host || field < 0 || field > 4) return fail(FFR_EINVAL, "bad set_field arguments");
     int rc = pull_state(s);
     if (rc) return rc;
-    FFR_CUDA(cudaMemcpyAsync(field_ptr(s, field), host, 8 * field_len(s, field), cudaMemcpyHostToDevice,
-                             s->stream));
-    FFR_CUDA(cudaStreamSynchronize(s->stream));
-    return FFR_OK;
+    return staged_copy(field_ptr(s, field), host, 8 * field_len(s, field), false, s->stream);
 }
 
 int ffr_fluid_field_dev(ffr_fluid *s, int field, double **dev)

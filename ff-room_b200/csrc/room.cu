@@ -111,6 +111,89 @@ void pinned_put(void *p, size_t bytes)
     g_pinned[bytes].push_back(p);
 }
 
+namespace {
+// memcpy of n bytes on up to four host threads (pieces of at least 1 MB)
+void host_copy(char *d, const char *s, size_t n)
+{
+    const int parts = (int)std::min<size_t>(4, std::max<size_t>(1, n >> 20));
+    const size_t piece = (n + parts - 1) / parts;
+    auto one = [&](int q) {
+        const size_t o = (size_t)q * piece;
+        if (o < n) std::memcpy(d + o, s + o, std::min(piece, n - o));
+    };
+    std::vector<std::thread> th;
+    for (int q = 1; q < parts; q++) th.emplace_back(one, q);
+    one(0);
+    for (auto &t : th) t.join();
+}
+}  // namespace
+
+int staged_copy(void *dst, const void *src, size_t bytes, bool to_host, cudaStream_t st)
+{
+    constexpr size_t kChunk = 8u << 20;
+    const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice;
+    char *buf[2] = {nullptr, nullptr};
+    if (bytes > 2 * kChunk) {
+        buf[0] = static_cast<char *>(pinned_get(kChunk));
+        buf[1] = static_cast<char *>(pinned_get(kChunk));
+    }
+    if (!buf[0] || !buf[1]) {
+        pinned_put(buf[0], kChunk);
+        pinned_put(buf[1], kChunk);
+        FFR_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, st));
+        FFR_CUDA(cudaStreamSynchronize(st));
+        return FFR_OK;
+    }
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int rc = FFR_OK;
+    auto done = [&]() {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        pinned_put(buf[0], kChunk);
+        pinned_put(buf[1], kChunk);
+        return rc;
+    };
+    for (cudaEvent_t &e : ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            rc = fail(FFR_ECUDA, "cudaEventCreate");
+            return done();
+        }
+    char *d = static_cast<char *>(dst);
+    const char *s = static_cast<const char *>(src);
+    const size_t nch = (bytes + kChunk - 1) / kChunk;
+    auto len = [&](size_t c) { return std::min(kChunk, bytes - c * kChunk); };
+    cudaError_t e = cudaSuccess;
+    for (size_t c = 0; c < nch && e == cudaSuccess; c++) {
+        const int b = (int)(c & 1);
+        if (to_host) {
+            // chunk c into buf[b] (its previous contents, chunk c-2, were
+            // copied out in the last iteration), then chunk c-1 to the host
+            e = cudaMemcpyAsync(buf[b], s + c * kChunk, len(c), kind, st);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[b], st);
+            if (e == cudaSuccess && c > 0) {
+                e = cudaEventSynchronize(ev[b ^ 1]);
+                if (e == cudaSuccess) host_copy(d + (c - 1) * kChunk, buf[b ^ 1], len(c - 1));
+            }
+        } else {
+            // buf[b] is free once the DMA of chunk c-2 has finished
+            if (c > 1) e = cudaEventSynchronize(ev[b]);
+            if (e == cudaSuccess) {
+                host_copy(buf[b], s + c * kChunk, len(c));
+                e = cudaMemcpyAsync(d + c * kChunk, buf[b], len(c), kind, st);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(ev[b], st);
+        }
+    }
+    if (e == cudaSuccess && to_host) {
+        const int b = (int)((nch - 1) & 1);
+        e = cudaEventSynchronize(ev[b]);
+        if (e == cudaSuccess) host_copy(d + (nch - 1) * kChunk, buf[b], len(nch - 1));
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "staged copy");
+    return done();
+}
+
 // Validates a room descriptor and copies it.  The reference accepts some of
 // the rejected inputs silently (an outflow patch outside the grid writes out
 // of bounds in BoundaryManager::add_outflow, BoundaryManager.cpp:24-44); a
