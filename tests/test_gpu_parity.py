@@ -188,3 +188,23 @@ def test_snapshot_matches_fields():
     assert [r["cg_iterations"] for r in bb[3:]] == [r["cg_iterations"] for r in a]
     for k in "uvwp":
         assert np.array_equal(h.get(k), b.get(k)), k
+
+
+def test_large_field_transfers_round_trip():
+    """Fields of tens of MB cross PCIe through page-locked bounce buffers in
+    chunks (uploads at creation and set_field, downloads in get): every
+    byte arrives, including a ragged last chunk."""
+    from ffrb import capi, workloads
+    from ffrb.scene import build_room
+    cfg, prm = workloads.large_thermal(grid=(203, 160, 96))     # ~25 MB per cell field
+    room = build_room(cfg)
+    rng = np.random.default_rng(5)
+    shapes = room.shapes()
+    init = {k: rng.standard_normal(int(np.prod(shapes[k]))) for k in ("u", "v", "w", "p")}
+    h = capi.FluidHandle(room, prm, init)
+    for k in ("u", "v", "w", "p"):
+        assert np.array_equal(h.get(k), init[k]), k
+    t = rng.standard_normal(room.n_cells)
+    h.set("T", t)
+    assert np.array_equal(h.get("T"), t)
+    h.close()
