@@ -111,87 +111,113 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
                                              double *__restrict__ ws, const StepState *st, int start, int stride)
 {
     const int nx = R.nx, ny = R.ny, nz = R.nz;
-    const int total = R.nu + R.nv + R.nw;
     const int quick = A.scheme == 1, lw = A.scheme == 2;
     const F dt = F(A.dt), nu = F(A.nu);
     const double *T = st->tpar ? T1 : T0;
-    for (int t = start; t < total; t += stride) {
-        if (t < R.nu) {
-            const int i = t / (ny * nz), rem = t - i * ny * nz, j = rem / nz, k = rem - j * nz;
-            double val = u[t];
-            if (i > 0 && i < nx) {
-                const double uc = val;
-                const double xm = (i > 1) ? u[t - ny * nz] : 0.0;
-                const double xp = (i < nx - 1) ? u[t + ny * nz] : 0.0;
-                const double av = (j > 0 && j < ny) ? 0.5 * (v[VIX(i - 1, j, k)] + v[VIX(i, j, k)]) : 0.0;
-                const double ym = (j > 0) ? u[t - nz] : 0.0;
-                const double yp = (j < ny - 1) ? u[t + nz] : 0.0;
-                const double aw = (k > 0 && k < nz) ? 0.5 * (w[WIX(i - 1, j, k)] + w[WIX(i, j, k)]) : 0.0;
-                const double zm = (k > 0) ? u[t - 1] : 0.0;
-                const double zp = (k < nz - 1) ? u[t + 1] : 0.0;
-                const int q = quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
-                // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1
-                // (k=1) they fall into the previous row of the flat array
-                const double xmm = q ? u[t - 2 * ny * nz] : 0.0, ymm = q ? u[t - 2 * nz] : 0.0,
-                             zmm = q ? u[t - 2] : 0.0;
-                val = uc + (double)face_increment<F>(q, lw, F(uc), F(xmm), F(xm), F(xp), F(ymm), F(ym), F(yp),
-                                                     F(zmm), F(zm), F(zp), F(uc), F(av), F(aw), F(R.dxv[i]),
-                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
+    // The three face arrays in turn, each with carried (i, j, k).  Neighbour
+    // loads go through indices clamped into the array and are all issued
+    // before the boundary tests select them (a neighbour outside reads as 0,
+    // as in the reference); the advecting-velocity pairs are always inside
+    // for an interior face.
+    const int pu = ny * nz, lastu = R.nu - 1;
+    for (Walk wk(start, stride, ny, nz, R.nu); wk.ok(); wk.next()) {
+        const int t = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        const uint8_t code = R.fcu[t];
+        double val = u[t];
+        if (i > 0 && i < nx) {
+            const double uc = val;
+            const double xm0 = u[max(t - pu, 0)], xp0 = u[min(t + pu, lastu)];
+            const double ym0 = u[max(t - nz, 0)], yp0 = u[min(t + nz, lastu)];
+            const double zm0 = u[max(t - 1, 0)], zp0 = u[min(t + 1, lastu)];
+            const double v0 = v[VIX(i - 1, j, k)], v1 = v[VIX(i, j, k)];
+            const double w0 = w[WIX(i - 1, j, k)], w1 = w[WIX(i, j, k)];
+            const int q = quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+            // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1
+            // (k=1) they fall into the previous row of the flat array
+            double xmm = 0.0, ymm = 0.0, zmm = 0.0;
+            if (quick) {
+                const double a = u[max(t - 2 * pu, 0)], b = u[max(t - 2 * nz, 0)], c = u[max(t - 2, 0)];
+                xmm = q ? a : 0.0; ymm = q ? b : 0.0; zmm = q ? c : 0.0;
             }
-            us[t] = face_code(R.fcu[t], val, R.fanvel, 0);
-        } else if (t < R.nu + R.nv) {
-            const int f = t - R.nu;
-            const int i = f / ((ny + 1) * nz), rem = f - i * (ny + 1) * nz, j = rem / nz,
-                      k = rem - j * nz;
-            double val = v[f];
-            if (j > 0 && j < ny) {
-                const double vc = val;
-                const double au = (i > 0) ? 0.5 * (u[UIX(i, j - 1, k)] + u[UIX(i, j, k)]) : 0.0;
-                const double xm = (i > 0) ? v[f - (ny + 1) * nz] : 0.0;
-                const double xp = (i < nx - 1) ? v[f + (ny + 1) * nz] : 0.0;
-                const double ym = (j > 1) ? v[f - nz] : 0.0;
-                const double yp = (j < ny - 1) ? v[f + nz] : 0.0;
-                const double aw = (k > 0 && k < nz) ? 0.5 * (w[WIX(i, j - 1, k)] + w[WIX(i, j, k)]) : 0.0;
-                const double zm = (k > 0) ? v[f - 1] : 0.0;
-                const double zp = (k < nz - 1) ? v[f + 1] : 0.0;
-                const int q = quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2;
-                // v's x and z "far" neighbours are the near ones
-                // (FluidSolver.cpp:208,211)
-                const double ymm = q ? v[f - 2 * nz] : 0.0;
-                val = vc + (double)face_increment<F>(q, lw, F(vc), F(xm), F(xm), F(xp), F(ymm), F(ym), F(yp),
-                                                     F(zm), F(zm), F(zp), F(au), F(vc), F(aw), F(R.dxv[i]),
-                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
-            }
-            vs[f] = face_code(R.fcv[f], val, R.fanvel, 1);
-        } else {
-            const int f = t - R.nu - R.nv;
-            const int i = f / (ny * (nz + 1)), rem = f - i * ny * (nz + 1), j = rem / (nz + 1),
-                      k = rem - j * (nz + 1);
-            double val = w[f];
-            if (k > 0 && k < nz) {
-                const double wc = val;
-                const double au = (i > 0) ? 0.5 * (u[UIX(i, j, k - 1)] + u[UIX(i, j, k)]) : 0.0;
-                const double xm = (i > 0) ? w[f - ny * (nz + 1)] : 0.0;
-                const double xp = (i < nx - 1) ? w[f + ny * (nz + 1)] : 0.0;
-                const double av = (j > 0) ? 0.5 * (v[VIX(i, j, k - 1)] + v[VIX(i, j, k)]) : 0.0;
-                const double ym = (j > 0) ? w[f - (nz + 1)] : 0.0;
-                const double yp = (j < ny - 1) ? w[f + (nz + 1)] : 0.0;
-                const double zm = (k > 1) ? w[f - 1] : 0.0;
-                const double zp = (k < nz - 1) ? w[f + 1] : 0.0;
-                const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2;
-                // w's x and y "far" neighbours are the near ones
-                // (FluidSolver.cpp:275-276)
-                const double zmm = q ? w[f - 2] : 0.0;
-                val = wc + (double)face_increment<F>(q, lw, F(wc), F(xm), F(xm), F(xp), F(ym), F(ym), F(yp),
-                                                     F(zmm), F(zm), F(zp), F(au), F(av), F(wc), F(R.dxv[i]),
-                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
-                if (A.buoyancy) {
-                    const int c = UIX(i, j, k);
-                    val += (double)(F(A.bcoeff) * (F(0.5) * (F(T[c - 1]) + F(T[c])) - F(A.T_ref)));
-                }
-            }
-            ws[f] = face_code(R.fcw[f], val, R.fanvel, 2);
+            const double xm = (i > 1) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+            const double av = (j > 0 && j < ny) ? 0.5 * (v0 + v1) : 0.0;
+            const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+            const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
+            const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+            val = uc + (double)face_increment<F>(q, lw, F(uc), F(xmm), F(xm), F(xp), F(ymm), F(ym), F(yp),
+                                                 F(zmm), F(zm), F(zp), F(uc), F(av), F(aw), F(R.dxv[i]),
+                                                 F(R.dyv[j]), F(R.dzv[k]), nu, dt);
         }
+        us[t] = face_code(code, val, R.fanvel, 0);
+    }
+    const int pv = (ny + 1) * nz, lastv = R.nv - 1;
+    for (Walk wk(start, stride, ny + 1, nz, R.nv); wk.ok(); wk.next()) {
+        const int f = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        const uint8_t code = R.fcv[f];
+        double val = v[f];
+        if (j > 0 && j < ny) {
+            const double vc = val;
+            const double u0 = u[UIX(i, j - 1, k)], u1 = u[UIX(i, j, k)];
+            const double xm0 = v[max(f - pv, 0)], xp0 = v[min(f + pv, lastv)];
+            const double ym0 = v[max(f - nz, 0)], yp0 = v[min(f + nz, lastv)];
+            const double w0 = w[WIX(i, j - 1, k)], w1 = w[WIX(i, j, k)];
+            const double zm0 = v[max(f - 1, 0)], zp0 = v[min(f + 1, lastv)];
+            const int q = quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+            // v's x and z "far" neighbours are the near ones
+            // (FluidSolver.cpp:208,211)
+            double ymm = 0.0;
+            if (quick) {
+                const double a = v[max(f - 2 * nz, 0)];
+                ymm = q ? a : 0.0;
+            }
+            const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
+            const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+            const double ym = (j > 1) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+            const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
+            const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+            val = vc + (double)face_increment<F>(q, lw, F(vc), F(xm), F(xm), F(xp), F(ymm), F(ym), F(yp),
+                                                 F(zm), F(zm), F(zp), F(au), F(vc), F(aw), F(R.dxv[i]),
+                                                 F(R.dyv[j]), F(R.dzv[k]), nu, dt);
+        }
+        vs[f] = face_code(code, val, R.fanvel, 1);
+    }
+    const int pw = ny * (nz + 1), lastw = R.nw - 1;
+    for (Walk wk(start, stride, ny, nz + 1, R.nw); wk.ok(); wk.next()) {
+        const int f = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        const uint8_t code = R.fcw[f];
+        double val = w[f];
+        if (k > 0 && k < nz) {
+            const double wc = val;
+            const double u0 = u[UIX(i, j, k - 1)], u1 = u[UIX(i, j, k)];
+            const double xm0 = w[max(f - pw, 0)], xp0 = w[min(f + pw, lastw)];
+            const double v0 = v[VIX(i, j, k - 1)], v1 = v[VIX(i, j, k)];
+            const double ym0 = w[max(f - (nz + 1), 0)], yp0 = w[min(f + (nz + 1), lastw)];
+            const double zm0 = w[max(f - 1, 0)], zp0 = w[min(f + 1, lastw)];
+            double tb = 0.0, tc = 0.0;
+            if (A.buoyancy) {
+                const int c = UIX(i, j, k);
+                tb = T[c - 1];
+                tc = T[c];
+            }
+            const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2;
+            // w's x and y "far" neighbours are the near ones
+            // (FluidSolver.cpp:275-276)
+            double zmm = 0.0;
+            if (quick) {
+                const double a = w[max(f - 2, 0)];
+                zmm = q ? a : 0.0;
+            }
+            const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
+            const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+            const double av = (j > 0) ? 0.5 * (v0 + v1) : 0.0;
+            const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+            const double zm = (k > 1) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+            val = wc + (double)face_increment<F>(q, lw, F(wc), F(xm), F(xm), F(xp), F(ym), F(ym), F(yp),
+                                                 F(zmm), F(zm), F(zp), F(au), F(av), F(wc), F(R.dxv[i]),
+                                                 F(R.dyv[j]), F(R.dzv[k]), nu, dt);
+            if (A.buoyancy) val += (double)(F(A.bcoeff) * (F(0.5) * (F(tb) + F(tc)) - F(A.T_ref)));
+        }
+        ws[f] = face_code(code, val, R.fanvel, 2);
     }
 }
 
@@ -390,14 +416,19 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
     const double c0 = A.c0;
     double dmax = 0.0, divmax = 0.0;
     int nan = 0;
-    for (int c = start; c < R.n; c += stride) {
-        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+    const int last = R.n - 1;
+    for (Walk wk(start, stride, ny, nz, R.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        // the pressure stencil and the old low faces, loaded before any test
         const double pc = p[c];
+        const double pxm = p[max(c - plane, 0)], pxp = p[min(c + plane, last)];
+        const double pym = p[max(c - nz, 0)], pyp = p[min(c + nz, last)];
+        const double pzm = p[max(c - 1, 0)], pzp = p[min(c + 1, last)];
         // x faces
         const int ul = c, uh = c + plane;
         double lo = us[ul], hi = us[uh];
-        if (i >= 1) lo = lo - c0 * ((pc - p[c - plane]) / (0.5 * (R.dxv[i - 1] + R.dxv[i])));
-        if (i + 1 <= nx - 1) hi = hi - c0 * ((p[c + plane] - pc) / (0.5 * (R.dxv[i] + R.dxv[i + 1])));
+        if (i >= 1) lo = lo - c0 * ((pc - pxm) / (0.5 * (R.dxv[i - 1] + R.dxv[i])));
+        if (i + 1 <= nx - 1) hi = hi - c0 * ((pxp - pc) / (0.5 * (R.dxv[i] + R.dxv[i + 1])));
         uint8_t cl = R.fcu[ul], ch = R.fcu[uh];
         lo = face_code(cl, lo, R.fanvel, 0);
         hi = face_code(ch, hi, R.fanvel, 0);
@@ -413,8 +444,8 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
         // y faces
         const int vl = VIX(i, j, k), vh = vl + nz;
         lo = vs[vl]; hi = vs[vh];
-        if (j >= 1) lo = lo - c0 * ((pc - p[c - nz]) / (0.5 * (R.dyv[j - 1] + R.dyv[j])));
-        if (j + 1 <= ny - 1) hi = hi - c0 * ((p[c + nz] - pc) / (0.5 * (R.dyv[j] + R.dyv[j + 1])));
+        if (j >= 1) lo = lo - c0 * ((pc - pym) / (0.5 * (R.dyv[j - 1] + R.dyv[j])));
+        if (j + 1 <= ny - 1) hi = hi - c0 * ((pyp - pc) / (0.5 * (R.dyv[j] + R.dyv[j + 1])));
         cl = R.fcv[vl]; ch = R.fcv[vh];
         lo = face_code(cl, lo, R.fanvel, 1);
         hi = face_code(ch, hi, R.fanvel, 1);
@@ -430,8 +461,8 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
         // z faces
         const int wl = WIX(i, j, k), wh = wl + 1;
         lo = ws[wl]; hi = ws[wh];
-        if (k >= 1) lo = lo - c0 * ((pc - p[c - 1]) / (0.5 * (R.dzv[k - 1] + R.dzv[k])));
-        if (k + 1 <= nz - 1) hi = hi - c0 * ((p[c + 1] - pc) / (0.5 * (R.dzv[k] + R.dzv[k + 1])));
+        if (k >= 1) lo = lo - c0 * ((pc - pzm) / (0.5 * (R.dzv[k - 1] + R.dzv[k])));
+        if (k + 1 <= nz - 1) hi = hi - c0 * ((pzp - pc) / (0.5 * (R.dzv[k] + R.dzv[k + 1])));
         cl = R.fcw[wl]; ch = R.fcw[wh];
         lo = face_code(cl, lo, R.fanvel, 2);
         hi = face_code(ch, hi, R.fanvel, 2);
@@ -553,25 +584,45 @@ __device__ __forceinline__ void advect_T_body(const RoomDev &R, const ThermArgs 
     double *Tn = st->tpar ? T0 : T1;
     const int quick = A.scheme == 1, lw = A.scheme == 2;
     double sum = 0.0;
-    for (int c = start; c < R.n; c += stride) {
-        if (R.ct[c] != CT_FLUID) {
-            Tn[c] = T[c];
+    const int last = R.n - 1;
+    for (Walk wk(start, stride, ny, nz, R.n); wk.ok(); wk.next()) {
+        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+        const uint8_t tcell = R.ct[c];
+        const double tc = T[c];
+        // the six neighbours' types and temperatures and the face velocities,
+        // loaded before any test (indices clamped into the arrays)
+        const int nb[6] = {max(c - plane, 0), min(c + plane, last), max(c - nz, 0),
+                           min(c + nz, last), max(c - 1, 0), min(c + 1, last)};
+        uint8_t nct[6];
+        double nT[6];
+#pragma unroll
+        for (int a = 0; a < 6; a++) {
+            nct[a] = R.ct[nb[a]];
+            nT[a] = T[nb[a]];
+        }
+        const double u0 = u[c], u1 = u[c + plane];
+        const double v0 = v[VIX(i, j, k)], v1 = v[VIX(i, j + 1, k)];
+        const double w0 = w[WIX(i, j, k)], w1 = w[WIX(i, j, k + 1)];
+        if (tcell != CT_FLUID) {
+            Tn[c] = tc;
             continue;
         }
-        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
-        const double tc = T[c];
-        const double ac = 0.5 * (u[c] + u[c + plane]);
-        const double bc = 0.5 * (v[VIX(i, j, k)] + v[VIX(i, j + 1, k)]);
-        const double cc = 0.5 * (w[WIX(i, j, k)] + w[WIX(i, j, k + 1)]);
+        const double ac = 0.5 * (u0 + u1);
+        const double bc = 0.5 * (v0 + v1);
+        const double cc = 0.5 * (w0 + w1);
         // Neumann at the domain edge and at SOLID cells (FluidSolver.cpp:417-422)
+        const bool inside[6] = {i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
+        double tn6[6];
+#pragma unroll
+        for (int a = 0; a < 6; a++) tn6[a] = (inside[a] && nct[a] != CT_SOLID) ? nT[a] : tc;
         auto tat = [&](int ii, int jj, int kk) -> double {
             if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) return tc;
             const int qq = UIX(ii, jj, kk);
             return R.ct[qq] == CT_SOLID ? tc : T[qq];
         };
-        const double xm = tat(i - 1, j, k), xp = tat(i + 1, j, k);
-        const double ym = tat(i, j - 1, k), yp = tat(i, j + 1, k);
-        const double zm = tat(i, j, k - 1), zp = tat(i, j, k + 1);
+        const double xm = tn6[0], xp = tn6[1];
+        const double ym = tn6[2], yp = tn6[3];
+        const double zm = tn6[4], zp = tn6[5];
         const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
         const double xmm = q ? tat(i - 2, j, k) : 0.0, ymm = q ? tat(i, j - 2, k) : 0.0,
                      zmm = q ? tat(i, j, k - 2) : 0.0;
