@@ -207,7 +207,9 @@ int ffr_fluid_set_split(ffr_fluid *s, int mode);
  * rooms stay ordinary handles: after ffr_batch_enqueue each room's results
  * are collected with ffr_fluid_poll, and fields are read as usual.  Rooms
  * must use the multigrid pressure solve and the default grid; a room may
- * belong to several batches but only one may run at a time. */
+ * belong to several batches but only one may run at a time.  A batch keeps
+ * pointers to its rooms: after destroying a member, replace the members
+ * (ffr_batch_set_rooms) before the next ffr_batch_enqueue. */
 typedef struct ffr_batch ffr_batch;
 int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out);
 /* Replaces the member rooms (the batch's device tables are rebuilt in
