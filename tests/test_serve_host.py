@@ -24,3 +24,85 @@ def test_tuner_table_roundtrip():
     t2 = Tuner.from_json(t.to_json())
     assert t2.table == t.table
     assert t2.schedule(empty_room(16, 32, 32, 1, 1, 1)).blocks == -4
+
+
+def test_default_schedule_by_room_size():
+    small, big = empty_room(64, 64, 64, 1, 1, 1), empty_room(128, 128, 96, 1, 1, 1)
+    t = Tuner()
+    assert t.schedule(small).cluster == 16 and t.schedule(small).graph
+    assert t.schedule(big).cluster == 0 and t.schedule(big).blocks == 0 and t.schedule(big).graph
+
+
+class _FakeRoom:
+    """Stands in for capi.FluidHandle: a chunk of n steps completes at once."""
+
+    def __init__(self, room, params):
+        self.steps = 0
+        self.pending = 0
+        self.split = None
+        self.closed = False
+
+    def set_split(self, mode):
+        self.split = mode
+
+    def poll(self):
+        n, self.pending = self.pending, 0
+        out = [{"step": self.steps + i + 1, "converged": False, "velocity_change": 1.0} for i in range(n)]
+        self.steps += n
+        return out
+
+    def get(self, k):
+        return None
+
+    def device_bytes(self):
+        return 1
+
+    def close(self):
+        self.closed = True
+
+
+class _FakeBatch:
+    log = []
+
+    def __init__(self, rooms):
+        self.rooms = list(rooms)
+        _FakeBatch.log.append(("create", len(self.rooms)))
+
+    def set_rooms(self, rooms):
+        assert all(not r.closed for r in rooms)
+        self.rooms = list(rooms)
+        _FakeBatch.log.append(("set", len(self.rooms)))
+
+    def enqueue(self, n, stop):
+        assert all(not r.closed for r in self.rooms)
+        for r in self.rooms:
+            r.pending = n
+        _FakeBatch.log.append(("enqueue", n))
+
+    def close(self):
+        pass
+
+
+def test_batched_server_chunks_membership_and_admission(monkeypatch):
+    """The batched server's host logic: rooms join between chunks, a chunk
+    never runs a room past its cap, finished rooms leave before the next
+    chunk, and admission respects the memory budget."""
+    import types
+    from ffrb import serve
+    from ffrb.serve import Request, Server
+    fake = types.SimpleNamespace(FluidHandle=_FakeRoom, BatchHandle=_FakeBatch)
+    monkeypatch.setattr(serve, "capi", fake)
+    _FakeBatch.log = []
+    p = FluidParams(poisson="mgpcg")
+    rooms = [empty_room(16, 16, 8 + i, 1, 1, 1) for i in range(6)]
+    caps = [5, 12, 7, 20, 3, 9]
+    reqs = [Request(i, 0.0, rooms[i], p, caps[i]) for i in range(6)]
+    need = max(estimate_bytes(r, p) for r in rooms)
+    srv = Server(mem_budget=3 * need, max_active=8, batched=True, chunk=4)
+    out = srv.run(reqs, realtime=False)
+    assert sorted(o.rid for o in out) == list(range(6))
+    for o in out:
+        assert o.steps == caps[o.rid]
+    sizes = [n for kind, n in _FakeBatch.log if kind in ("create", "set")]
+    assert max(sizes) <= 3                       # memory admission: three rooms at a time
+    assert all(n <= 4 for kind, n in _FakeBatch.log if kind == "enqueue")
