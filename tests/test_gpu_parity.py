@@ -208,3 +208,21 @@ def test_large_field_transfers_round_trip():
     h.set("T", t)
     assert np.array_equal(h.get("T"), t)
     h.close()
+
+
+def test_result_files_from_a_device_room(tmp_path):
+    """ResultStore-layout archive and velocity CSV written from a handle."""
+    from ffrb import capi
+    from ffrb.results import save_npz, save_velocity_csv
+    g = Golden("summer_cooling_10")
+    h = capi.FluidHandle(g.room, g.params)
+    recs = h.advance(2)
+    save_npz(h, g.cfg, str(tmp_path / "r.npz"), last=recs[-1], steps=len(recs))
+    z = np.load(tmp_path / "r.npz", allow_pickle=True)
+    assert np.array_equal(z["p_field"].ravel(), h.get("p"))
+    assert np.array_equal(z["u_field"].ravel(), h.get("u"))
+    assert int(z["_steps"]) == 2 and float(z["_velocity_change"]) == recs[-1]["velocity_change"]
+    save_velocity_csv(h, str(tmp_path / "v.csv"))
+    rows = np.loadtxt(tmp_path / "v.csv", delimiter=",", skiprows=1)
+    assert np.array_equal(rows[:, 6], h.snapshot(with_velocity=False)["speed"].ravel())
+    h.close()
