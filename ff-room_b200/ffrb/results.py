@@ -11,14 +11,21 @@ SimResult and the CSV has the same columns:
 * ``save_velocity_csv`` — one row per cell: cell-centre coordinates,
   cell-centred velocity and speed (io.py:80-104), the velocity and speed
   formed on the device (``FluidHandle.snapshot``), so only those arrays
-  cross PCIe.
+  cross PCIe;
+* ``log_outcome`` — one JSON line per finished room in ExperimentLog's
+  format (io.py:107-140: timestamp, 8-hex config hash, run diagnostics,
+  notes, configuration), plus the room's cell count and throughput in
+  cell-steps per second of its own residence on the server, so
+  ``ExperimentLog.load_all`` reads a serving run's log.
 
 A serving or batched run has no SolverBridge and no Grid on the host;
 these writers take the room's handle directly.
 """
 from __future__ import annotations
 
+import hashlib
 import json
+import time
 from typing import Optional
 
 import numpy as np
@@ -53,7 +60,7 @@ def save_npz(handle, cfg: SceneConfig, path: str, last: Optional[dict] = None, s
         p_field=handle.get("p").reshape(nx, ny, nz),
         T_field=handle.get("T").reshape(nx, ny, nz),
         cell_type=np.asarray(room.cell_type, dtype=np.uint8).reshape(nx, ny, nz),
-        _config_json=np.array(json.dumps(cfg.to_dict())),
+        _config_json=np.array(json.dumps(cfg.to_reference_dict())),
         **_diagnostics(last, steps, wall_time_s),
     )
 
@@ -73,3 +80,34 @@ def save_velocity_csv(handle, path: str) -> None:
     rows = np.column_stack([X.ravel(), Y.ravel(), Z.ravel(), vel[..., 0].ravel(), vel[..., 1].ravel(),
                             vel[..., 2].ravel(), snap["speed"].ravel()])
     np.savetxt(path, rows, delimiter=",", header="x_m,y_m,z_m,u_ms,v_ms,w_ms,speed_ms", comments="")
+
+
+def config_hash(cfg: SceneConfig) -> str:
+    """First 8 hex digits of sha256 over the sorted-key JSON of the
+    configuration (io.py:118-119); equal to the reference's hash for any
+    scene the reference can express."""
+    return hashlib.sha256(json.dumps(cfg.to_reference_dict(), sort_keys=True).encode()).hexdigest()[:8]
+
+
+def log_outcome(path: str, cfg: SceneConfig, outcome, notes: str = "") -> str:
+    """Appends one finished server request (``serve.Outcome``) to a JSON
+    Lines experiment log and returns its config hash.  wall_time_s is the
+    room's time from admission to completion."""
+    wall = float(outcome.t_done - outcome.t_admit)
+    entry = {
+        "timestamp": time.strftime("%Y-%m-%dT%H:%M:%S"),
+        "config_hash": config_hash(cfg),
+        "steps": int(outcome.steps),
+        "converged": bool(outcome.converged),
+        "velocity_change": float(outcome.velocity_change),
+        "divergence_max": float(outcome.divergence_max),
+        "T_mean": float(outcome.T_mean),
+        "wall_time_s": wall,
+        "notes": notes,
+        "config": cfg.to_reference_dict(),
+        "cells": int(outcome.cells),
+        "cell_steps_per_s": outcome.cells * outcome.steps / wall if wall > 0 else float("nan"),
+    }
+    with open(path, "a") as fh:
+        fh.write(json.dumps(entry) + "\n")
+    return entry["config_hash"]

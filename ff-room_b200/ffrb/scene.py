@@ -141,8 +141,27 @@ class SceneConfig:
             return o
         return cvt(self)
 
+    def to_reference_dict(self) -> dict:
+        """The dict ff-room's own SceneConfig.from_dict accepts
+        (config.py:172-186): the reference's keys only, with this build's
+        extensions kept where its from_dict skips them — the storage
+        precision as a top-level ``precision`` (only when not fp64) and
+        ``heat_patches`` (only when there are any).  For a scene the
+        reference can express, this is exactly the reference's to_dict."""
+        d = self.to_dict()
+        prec = d["solver"].pop("precision")
+        hp = d.pop("heat_patches")
+        if hp:
+            d["heat_patches"] = hp
+        if prec != "fp64":
+            d["precision"] = prec
+        return d
+
     @classmethod
     def from_dict(cls, d: dict) -> "SceneConfig":
+        solver = SolverConfig(**(d.get("solver", {}) or {}))
+        if "precision" in d:
+            solver.precision = d["precision"]
         return cls(
             room=RoomConfig(**{k: _tup(v) for k, v in d.get("room", {}).items()}),
             fans=[FanConfig(**{k: _tup(v) for k, v in f.items()}) for f in d.get("fans", []) or []],
@@ -150,7 +169,7 @@ class SceneConfig:
                        for o in d.get("obstacles", []) or []],
             openings=[OpeningConfig(**{k: _tup(v) for k, v in o.items()})
                       for o in d.get("openings", []) or []],
-            solver=SolverConfig(**(d.get("solver", {}) or {})),
+            solver=solver,
             metadata=d.get("metadata", {}) or {},
             heat_patches=[HeatPatchConfig(**{k: _tup(v) for k, v in h.items()})
                           for h in d.get("heat_patches", []) or []],

@@ -163,6 +163,8 @@ class Outcome:
     converged: bool
     velocity_change: float
     fields: Optional[dict] = None
+    T_mean: float = float("nan")
+    divergence_max: float = float("nan")
 
     @property
     def latency(self) -> float:
@@ -230,7 +232,9 @@ class Server:
         t = time.perf_counter() - t0
         o = Outcome(a.req.rid, a.req.room.n_cells, a.req.t_arrival, a.t_admit, t, a.steps,
                     bool(a.last and a.last["converged"]),
-                    float(a.last["velocity_change"]) if a.last else float("nan"), fields)
+                    float(a.last["velocity_change"]) if a.last else float("nan"), fields,
+                    float(a.last["T_mean"]) if a.last else float("nan"),
+                    float(a.last["divergence_max"]) if a.last else float("nan"))
         a.h.close()
         return o
 
@@ -317,13 +321,8 @@ class Server:
                     continue
                 progressed = True
                 if st:
-                    fields = {k: a.h.get(k) for k in "uvwpT"} if self.keep_fields else None
-                    t = time.perf_counter() - t0
-                    out.append(Outcome(a.req.rid, a.req.room.n_cells, a.req.t_arrival, a.t_admit, t, a.steps,
-                                       bool(a.last and a.last["converged"]),
-                                       float(a.last["velocity_change"]) if a.last else float("nan"), fields))
+                    out.append(self._finish(a, t0))
                     used -= a.charge
-                    a.h.close()
                 else:
                     a.launch()
                     still.append(a)
@@ -359,7 +358,9 @@ def serial_solve(requests: List[Request], params_override: Optional[dict] = None
         res = h.advance(req.max_steps, stop_on_converge=True)
         h.close()
         out.append(Outcome(req.rid, req.room.n_cells, ta, ta, time.perf_counter() - t0, len(res),
-                           bool(res and res[-1]["converged"]), float(res[-1]["velocity_change"]) if res else float("nan")))
+                           bool(res and res[-1]["converged"]), float(res[-1]["velocity_change"]) if res else float("nan"),
+                           None, float(res[-1]["T_mean"]) if res else float("nan"),
+                           float(res[-1]["divergence_max"]) if res else float("nan")))
     return out
 
 

@@ -172,6 +172,59 @@ def run_case(name, cfg, nsteps, extra, core, drv, Oracle):
     return path
 
 
+SWEEP_CAP = 80
+
+
+def sweep_placements():
+    """Two fan positions near the window × the two directions the scene's
+    notes compare, plus a slow fan that should not reach the target."""
+    from ffrb.sweep import Placement, placement_grid
+    pls = placement_grid([(3.0, 3.8, 0.9), (1.0, 3.8, 0.9)], [(270.0, 0.0), (90.0, 0.0)])
+    pls.append(Placement("slow", 0, (3.0, 3.8, 0.9), (270.0, 0.0), 0.5))
+    return pls
+
+
+def cooling_sweep(drv):
+    """tests/golden/cooling_sweep.json: time to cool of summer_cooling.yaml
+    per fan placement, from the reference's own SolverBridge.run (which
+    stops on FluidSolver's T_target test).  The target is chosen from the
+    reference's uncapped temperature histories (the C driver) so that no
+    step's T_mean lies within reach of mixed-precision rounding of it, with
+    some placements reaching it inside the cap and at least one not."""
+    from ffrb.sweep import variant
+    base = SceneConfig.load_yaml(os.path.join(REF, "examples", "summer_cooling.yaml"))
+    pls = sweep_placements()
+    hist = []
+    for pl in pls:
+        cfg = variant(base, pl)
+        cfg.solver.T_target = None
+        _, _, recs = drv.fluid_run(build_room(cfg), params_from_scene(cfg), SWEEP_CAP)
+        hist.append(np.array([r.T_mean for r in recs]))
+    best = None
+    for tgt in np.round(np.arange(31.950, 31.995, 0.0005), 4):
+        reached = [bool(np.any(h <= tgt)) for h in hist]
+        if sum(reached) < 3 or all(reached):
+            continue
+        margin = min(float(np.min(np.abs(h - tgt))) for h in hist)
+        if best is None or margin > best[1]:
+            best = (float(tgt), margin)
+    tgt, margin = best
+    out = {"base": base.to_dict(), "T_target": tgt, "cap": SWEEP_CAP, "margin": margin, "placements": []}
+    for pl, h in zip(pls, hist):
+        cfg = variant(base, pl, tgt, SWEEP_CAP)
+        seen = []
+        res = ref_bridge.SolverBridge(ref_config(cfg)).run(
+            progress_callback=lambda s, vc, dm, tm: seen.append(tm), print_interval=0)
+        k = res.steps
+        assert np.array_equal(np.array(seen), h[:k]), f"{pl.label}: bridge and driver histories differ"
+        out["placements"].append({"label": pl.label, "fan": pl.fan, "position": list(pl.position),
+                                  "direction": list(pl.direction), "velocity": pl.velocity,
+                                  "steps": int(k), "reached": bool(res.converged),
+                                  "T_mean": [float(x) for x in seen]})
+    with open(os.path.join(HERE, "cooling_sweep.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+
+
 def mask_hashes():
     """sha256 of the masks of the synthetic workloads, built by the
     reference Scene, so that CPU tests can pin the restated scene builder
@@ -200,6 +253,7 @@ def mask_hashes():
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default="", help="comma-separated case names (also cooling_sweep, mask_hashes)")
     args = ap.parse_args()
     REF = args.ref
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
@@ -211,8 +265,14 @@ if __name__ == "__main__":
     import ff_room.solver_bridge as ref_bridge  # noqa: E402
     from oracle import Oracle, RefDriver  # noqa: E402
     drv = RefDriver()
+    only = set(args.only.split(",")) if args.only else None
     for name, cfg, n, extra in cases():
+        if only is not None and name not in only:
+            continue
         print("case", name, flush=True)
         run_case(name, cfg, n, extra, core, drv, Oracle)
-    mask_hashes()
+    if only is None or "cooling_sweep" in only:
+        cooling_sweep(drv)
+    if only is None or "mask_hashes" in only:
+        mask_hashes()
     print("done")

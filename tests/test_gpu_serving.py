@@ -136,3 +136,30 @@ def test_batched_server_results_identical_alone_and_in_mix():
         assert o.steps == reqs[o.rid].max_steps
         for k in "uvwpT":
             assert np.array_equal(o.fields[k], alone[o.rid][k]), (o.rid, k)
+
+
+@pytest.mark.parametrize("precision,poisson", [("mixed", "mgpcg"), ("fp64", "cg")])
+def test_cooling_sweep_stops_on_the_reference_steps(precision, poisson):
+    """summer_cooling.yaml per fan placement, run to T_target on the server
+    (batched for MG-PCG, one stream per room for plain CG): every placement
+    stops on the reference's step, or runs to the cap where the reference
+    did not reach the target, with T_mean within the mixed bound."""
+    import json
+    import os
+    from conftest import GOLDEN
+    from ffrb.scene import SceneConfig
+    from ffrb.sweep import Placement, cooling_sweep
+    with open(os.path.join(GOLDEN, "cooling_sweep.json")) as fh:
+        fx = json.load(fh)
+    base = SceneConfig.from_dict(fx["base"])
+    pls = [Placement(p["label"], p["fan"], tuple(p["position"]), tuple(p["direction"]), p["velocity"])
+           for p in fx["placements"]]
+    res = {r.label: r for r in cooling_sweep(base, pls, fx["T_target"], fx["cap"], precision=precision,
+                                             poisson=poisson)}
+    tol = 1e-4 if precision == "mixed" else 1e-9
+    for want in fx["placements"]:
+        r = res[want["label"]]
+        assert (r.steps, r.reached) == (want["steps"], want["reached"]), (want["label"], r)
+        assert abs(r.T_mean - want["T_mean"][-1]) <= tol * abs(want["T_mean"][-1]), (want["label"], r.T_mean)
+        if r.reached:
+            assert r.time_to_target_s == pytest.approx(want["steps"] * base.solver.dt)

@@ -47,7 +47,8 @@ class _FakeRoom:
 
     def poll(self):
         n, self.pending = self.pending, 0
-        out = [{"step": self.steps + i + 1, "converged": False, "velocity_change": 1.0} for i in range(n)]
+        out = [{"step": self.steps + i + 1, "converged": False, "velocity_change": 1.0, "T_mean": 20.0,
+                "divergence_max": 0.0} for i in range(n)]
         self.steps += n
         return out
 
