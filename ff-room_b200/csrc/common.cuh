@@ -71,12 +71,14 @@ struct HostRoom {
 
 int load_room(const ffr_room_desc *d, HostRoom &out);
 
-// Face codes (fc_u/v/w) from the reference BC appliers, replayed on codes.
-void build_face_codes(const HostRoom &r, std::vector<uint8_t> &fu,
-                      std::vector<uint8_t> &fv, std::vector<uint8_t> &fw);
-// Pressure stencil codes and per-axis stencil scales (PoissonSolver.cpp:33-49).
-void build_stencil(const HostRoom &r, std::vector<uint16_t> &sc,
-                   std::vector<double> &scale /* 2*(nx+ny+nz): l,r per index */);
+// On the device, from the cell types already there (ct): the pressure
+// stencil codes (sc, one per cell) and the face codes (fu/fv/fw) that
+// replay the reference's BC appliers.  Kernels queued on `s`.
+int build_codes(const HostRoom &r, const uint8_t *ct, uint16_t *sc, uint8_t *fu, uint8_t *fv, uint8_t *fw,
+                cudaStream_t s);
+int launch_stencil_codes(const uint8_t *ct, int nx, int ny, int nz, uint16_t *sc, cudaStream_t s);
+// Per-axis stencil scales (PoissonSolver.cpp:33-49): 2*(nx+ny+nz), l,r per index.
+void stencil_scales(const HostRoom &r, std::vector<double> &scale);
 
 // ------------------------------------------------------ device memory
 
@@ -128,9 +130,11 @@ void parallel_slabs(int n, F f)
     for (auto &x : th) x.join();
 }
 
-// Synchronous copy between pageable host memory and the device through two
-// page-locked bounce buffers: the DMA of one chunk overlaps the host copy
-// (on several threads) of the other.  Small copies go direct.
+// Synchronous copy between pageable host memory and the device, ordered
+// after the work queued on `st`: large copies run on up to 16 host threads,
+// each staging its slice through two page-locked bounce buffers on its own
+// stream (the DMA of one chunk overlaps the host copy of the other).  Small
+// copies go direct.
 int staged_copy(void *dst, const void *src, size_t bytes, bool to_host, cudaStream_t st);
 
 // Page-locked host buffers from a process-wide cache (cudaFreeHost may

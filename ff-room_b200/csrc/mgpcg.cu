@@ -40,106 +40,17 @@ namespace ffr {
 // factor along its normal (area summed, distance scaled), and likewise
 // for the Dirichlet (outflow) part of the diagonal, kept per axis.
 //
-// Each coarse cell gathers from its children, so the build runs on all
-// host threads (slabs of coarse x-planes); the fine level's couplings are
-// formed on the fly from the cell types and spacings.
-namespace {
-
-// Per cell: couplings to the +x, +y, +z neighbour and the Dirichlet
-// diagonal parts along x, y, z.
-struct LevelOps {
-    std::vector<double> t[6];
-    std::vector<uint8_t> act;
-    void resize(size_t m)
-    {
-        for (auto &v : t) v.assign(m, 0.0);
-        act.assign(m, 0);
-    }
-};
-
-// Coarse level (mx, my, mz) of a level whose cell (i, j, k) is described by
-// `cell(i, j, k, t) -> active`.
-template <class Cell>
-void coarsen(const Cell &cell, int nx, int ny, int nz, int sx, int sy, int sz, int mx, int my, int mz, LevelOps &out)
-{
-    out.resize((size_t)mx * my * mz);
-    const double f[3] = {sx ? 0.5 : 1.0, sy ? 0.5 : 1.0, sz ? 0.5 : 1.0};
-    parallel_slabs(mx, [&](int I0, int I1) {
-        for (int I = I0; I < I1; I++)
-            for (int J = 0; J < my; J++)
-                for (int K = 0; K < mz; K++) {
-                    const size_t P = ((size_t)I * my + J) * mz + K;
-                    double acc[6] = {0, 0, 0, 0, 0, 0};
-                    bool any = false;
-                    for (int a = 0; a <= sx; a++) {
-                        const int i = (I << sx) + a;
-                        if (i >= nx) break;
-                        for (int b = 0; b <= sy; b++) {
-                            const int j = (J << sy) + b;
-                            if (j >= ny) break;
-                            for (int e = 0; e <= sz; e++) {
-                                const int k = (K << sz) + e;
-                                if (k >= nz) break;
-                                double t[6];
-                                if (!cell(i, j, k, t)) continue;
-                                any = true;
-                                for (int d = 3; d < 6; d++) acc[d] += t[d];
-                                // couplings across the parent's + faces only
-                                if (t[0] > 0 && ((i + 1) >> sx) != (i >> sx)) acc[0] += t[0];
-                                if (t[1] > 0 && ((j + 1) >> sy) != (j >> sy)) acc[1] += t[1];
-                                if (t[2] > 0 && ((k + 1) >> sz) != (k >> sz)) acc[2] += t[2];
-                            }
-                        }
-                    }
-                    out.act[P] = any;
-                    for (int d = 0; d < 6; d++) out.t[d][P] = acc[d] * f[d % 3];
-                }
-    });
-}
-
-}  // namespace
-
+// The host plans the level sizes (they depend on the dimensions and room
+// size only); the coefficients are gathered on the device, one thread per
+// coarse cell, from the uploaded cell types and spacings (level 1) or the
+// previous level's couplings (mg_upload).
 void build_mg_levels(const HostRoom &r, MGHost &out)
 {
-    out.nx.clear(); out.ny.clear(); out.nz.clear(); out.coef.clear();
+    out.nx.clear(); out.ny.clear(); out.nz.clear();
     out.sx.clear(); out.sy.clear(); out.sz.clear();
     int nx = r.g.nx, ny = r.g.ny, nz = r.g.nz;
     out.nx.push_back(nx); out.ny.push_back(ny); out.nz.push_back(nz);
-    out.coef.emplace_back();
-    const int fnx = nx, fny = ny, fnz = nz;
-    auto C0 = [&](int i, int j, int k) { return ((size_t)i * fny + j) * fnz + k; };
-    auto isact = [](uint8_t t) { return t == CT_FLUID || t == CT_INFLOW; };
-    auto hc = [](const std::vector<double> &h, int a, int b) { return 0.5 * (h[a] + h[b]); };
-    // fine level (FP64): T to the + neighbour (0 unless both active) and the
-    // Dirichlet part of the diagonal per axis
-    auto fine = [&](int i, int j, int k, double (&t)[6]) -> bool {
-        for (int d = 0; d < 6; d++) t[d] = 0.0;
-        if (!isact(r.ct[C0(i, j, k)])) return false;
-        const double ax = r.dyv[j] * r.dzv[k], ay = r.dxv[i] * r.dzv[k], az = r.dxv[i] * r.dyv[j];
-        if (i + 1 < fnx) {
-            const double v = ax / hc(r.dxv, i, i + 1);
-            const uint8_t nt = r.ct[C0(i + 1, j, k)];
-            if (isact(nt)) t[0] = v; else if (nt == CT_OUTFLOW) t[3] += 2 * v;
-        }
-        if (j + 1 < fny) {
-            const double v = ay / hc(r.dyv, j, j + 1);
-            const uint8_t nt = r.ct[C0(i, j + 1, k)];
-            if (isact(nt)) t[1] = v; else if (nt == CT_OUTFLOW) t[4] += 2 * v;
-        }
-        if (k + 1 < fnz) {
-            const double v = az / hc(r.dzv, k, k + 1);
-            const uint8_t nt = r.ct[C0(i, j, k + 1)];
-            if (isact(nt)) t[2] = v; else if (nt == CT_OUTFLOW) t[5] += 2 * v;
-        }
-        // - neighbours that are Dirichlet ghosts
-        if (i > 0 && r.ct[C0(i - 1, j, k)] == CT_OUTFLOW) t[3] += 2 * ax / hc(r.dxv, i - 1, i);
-        if (j > 0 && r.ct[C0(i, j - 1, k)] == CT_OUTFLOW) t[4] += 2 * ay / hc(r.dyv, j - 1, j);
-        if (k > 0 && r.ct[C0(i, j, k - 1)] == CT_OUTFLOW) t[5] += 2 * az / hc(r.dzv, k - 1, k);
-        return true;
-    };
-    LevelOps cur, next;
     const double lx = r.g.lx, ly = r.g.ly, lz = r.g.lz;
-    bool first = true;
     while ((size_t)nx * ny * nz > 512 && (int)out.nx.size() < kMaxLevels) {
         // axes to halve at this level
         const double hx = lx / nx, hy = ly / ny, hz = lz / nz;
@@ -149,48 +60,149 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
         const int sz = (nz > 1 && hz < 2.0 * hmin) ? 1 : 0;
         if (!sx && !sy && !sz) break;
         const int mx = sx ? (nx + 1) / 2 : nx, my = sy ? (ny + 1) / 2 : ny, mz = sz ? (nz + 1) / 2 : nz;
-        if (first) {
-            coarsen(fine, nx, ny, nz, sx, sy, sz, mx, my, mz, next);
-        } else {
-            const int cny = ny, cnz = nz;
-            auto lvl = [&](int i, int j, int k, double (&t)[6]) -> bool {
-                const size_t c = ((size_t)i * cny + j) * cnz + k;
-                for (int d = 0; d < 6; d++) t[d] = cur.t[d][c];
-                return cur.act[c] != 0;
-            };
-            coarsen(lvl, nx, ny, nz, sx, sy, sz, mx, my, mz, next);
-        }
-        first = false;
-        const size_t m = (size_t)mx * my * mz;
-        std::vector<float4> coef(m);
-        auto CC = [&](int i, int j, int k) { return ((size_t)i * my + j) * mz + k; };
-        parallel_slabs(mx, [&](int i0, int i1) {
-            for (int i = i0; i < i1; i++)
-                for (int j = 0; j < my; j++)
-                    for (int k = 0; k < mz; k++) {
-                        const size_t P = CC(i, j, k);
-                        double D = 0.0;
-                        if (next.act[P]) {
-                            D = next.t[0][P] + next.t[1][P] + next.t[2][P] + next.t[3][P] + next.t[4][P] +
-                                next.t[5][P];
-                            if (i > 0) D += next.t[0][CC(i - 1, j, k)];
-                            if (j > 0) D += next.t[1][CC(i, j - 1, k)];
-                            if (k > 0) D += next.t[2][CC(i, j, k - 1)];
-                            if (!(D > 0)) D = 1.0;
-                        }
-                        coef[P] = make_float4((float)next.t[0][P], (float)next.t[1][P], (float)next.t[2][P],
-                                              (float)D);
-                    }
-        });
         out.sx.push_back(sx); out.sy.push_back(sy); out.sz.push_back(sz);
         out.nx.push_back(mx); out.ny.push_back(my); out.nz.push_back(mz);
-        out.coef.push_back(std::move(coef));
         nx = mx; ny = my; nz = mz;
-        std::swap(cur, next);
     }
     // the coarsest level has no next level
     out.sx.push_back(0); out.sy.push_back(0); out.sz.push_back(0);
 }
+
+namespace {
+
+// Per cell of a level: couplings to the +x, +y, +z neighbour (t0..t2) and
+// the Dirichlet diagonal parts along x, y, z (t3..t5); act = the cell has
+// a FLUID/INFLOW child.  Device scratch of the coefficient build.
+struct LevelOps {
+    double *t[6];
+    uint8_t *act;
+};
+
+__device__ __forceinline__ bool ct_active(uint8_t t) { return t == CT_FLUID || t == CT_INFLOW; }
+
+// Fine-level (FP64) couplings of cell (i, j, k): T to the + neighbour (0
+// unless both are unknowns) and the Dirichlet part of the diagonal per
+// axis, from the reference's centre distances (PoissonSolver.cpp:33-49).
+// The additions are explicit round-to-nearest operations, so the values do
+// not depend on how the compiler contracts them.
+__device__ __forceinline__ bool fine_ops(const uint8_t *__restrict__ ct, const double *__restrict__ dxv,
+                                         const double *__restrict__ dyv, const double *__restrict__ dzv, int nx,
+                                         int ny, int nz, int i, int j, int k, double (&t)[6])
+{
+    for (int d = 0; d < 6; d++) t[d] = 0.0;
+    auto C0 = [&](int a, int b, int c) { return ((size_t)a * ny + b) * nz + c; };
+    if (!ct_active(ct[C0(i, j, k)])) return false;
+    auto hc = [](const double *h, int a, int b) { return 0.5 * __dadd_rn(h[a], h[b]); };
+    const double ax = __dmul_rn(dyv[j], dzv[k]), ay = __dmul_rn(dxv[i], dzv[k]), az = __dmul_rn(dxv[i], dyv[j]);
+    if (i + 1 < nx) {
+        const double v = ax / hc(dxv, i, i + 1);
+        const uint8_t nt = ct[C0(i + 1, j, k)];
+        if (ct_active(nt)) t[0] = v; else if (nt == CT_OUTFLOW) t[3] = __dadd_rn(t[3], 2 * v);
+    }
+    if (j + 1 < ny) {
+        const double v = ay / hc(dyv, j, j + 1);
+        const uint8_t nt = ct[C0(i, j + 1, k)];
+        if (ct_active(nt)) t[1] = v; else if (nt == CT_OUTFLOW) t[4] = __dadd_rn(t[4], 2 * v);
+    }
+    if (k + 1 < nz) {
+        const double v = az / hc(dzv, k, k + 1);
+        const uint8_t nt = ct[C0(i, j, k + 1)];
+        if (ct_active(nt)) t[2] = v; else if (nt == CT_OUTFLOW) t[5] = __dadd_rn(t[5], 2 * v);
+    }
+    // - neighbours that are Dirichlet ghosts
+    if (i > 0 && ct[C0(i - 1, j, k)] == CT_OUTFLOW) t[3] = __dadd_rn(t[3], 2 * ax / hc(dxv, i - 1, i));
+    if (j > 0 && ct[C0(i, j - 1, k)] == CT_OUTFLOW) t[4] = __dadd_rn(t[4], 2 * ay / hc(dyv, j - 1, j));
+    if (k > 0 && ct[C0(i, j, k - 1)] == CT_OUTFLOW) t[5] = __dadd_rn(t[5], 2 * az / hc(dzv, k - 1, k));
+    return true;
+}
+
+struct CoarsenArgs {
+    // level 1 from the fine cells (cur.act == nullptr) or level l+1 from
+    // level l's couplings
+    const uint8_t *ct;
+    const double *dxv, *dyv, *dzv;
+    LevelOps cur, next;
+    int nx, ny, nz;       // the finer level
+    int sx, sy, sz;       // axes halved
+    int mx, my, mz;       // the coarser level
+};
+
+// One thread per coarse cell: sums its children's couplings (only those
+// across the parent's + faces for t0..t2, every child's Dirichlet parts),
+// then scales by the coarsening factor along each normal.
+__global__ void k_mg_coarsen(CoarsenArgs a)
+{
+    const long long m = (long long)a.mx * a.my * a.mz;
+    const double f[3] = {a.sx ? 0.5 : 1.0, a.sy ? 0.5 : 1.0, a.sz ? 0.5 : 1.0};
+    const bool from_fine = a.cur.act == nullptr;
+    for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < m;
+         P += (long long)gridDim.x * blockDim.x) {
+        const int I = (int)(P / ((long long)a.my * a.mz)), rem = (int)(P - (long long)I * a.my * a.mz);
+        const int J = rem / a.mz, K = rem - J * a.mz;
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        bool any = false;
+        for (int x = 0; x <= a.sx; x++) {
+            const int i = (I << a.sx) + x;
+            if (i >= a.nx) break;
+            for (int y = 0; y <= a.sy; y++) {
+                const int j = (J << a.sy) + y;
+                if (j >= a.ny) break;
+                for (int z = 0; z <= a.sz; z++) {
+                    const int k = (K << a.sz) + z;
+                    if (k >= a.nz) break;
+                    double t[6];
+                    bool act;
+                    if (from_fine) {
+                        act = fine_ops(a.ct, a.dxv, a.dyv, a.dzv, a.nx, a.ny, a.nz, i, j, k, t);
+                    } else {
+                        const size_t c = ((size_t)i * a.ny + j) * a.nz + k;
+                        for (int d = 0; d < 6; d++) t[d] = a.cur.t[d][c];
+                        act = a.cur.act[c] != 0;
+                    }
+                    if (!act) continue;
+                    any = true;
+                    for (int d = 3; d < 6; d++) acc[d] = __dadd_rn(acc[d], t[d]);
+                    // couplings across the parent's + faces only
+                    if (t[0] > 0 && ((i + 1) >> a.sx) != (i >> a.sx)) acc[0] = __dadd_rn(acc[0], t[0]);
+                    if (t[1] > 0 && ((j + 1) >> a.sy) != (j >> a.sy)) acc[1] = __dadd_rn(acc[1], t[1]);
+                    if (t[2] > 0 && ((k + 1) >> a.sz) != (k >> a.sz)) acc[2] = __dadd_rn(acc[2], t[2]);
+                }
+            }
+        }
+        a.next.act[P] = any;
+        for (int d = 0; d < 6; d++) a.next.t[d][P] = __dmul_rn(acc[d], f[d % 3]);
+    }
+}
+
+// FP32 coefficients of a coarse level: (T x+, T y+, T z+, diagonal), the
+// diagonal summed in the order t0..t5, then the - neighbours' + couplings;
+// inactive cells get diagonal 0, an active cell without couplings 1.
+__global__ void k_mg_coef(LevelOps L, int mx, int my, int mz, float4 *__restrict__ coef)
+{
+    const long long m = (long long)mx * my * mz;
+    for (long long P = blockIdx.x * (long long)blockDim.x + threadIdx.x; P < m;
+         P += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(P / ((long long)my * mz)), rem = (int)(P - (long long)i * my * mz);
+        const int j = rem / mz, k = rem - j * mz;
+        double D = 0.0;
+        if (L.act[P]) {
+            D = L.t[0][P];
+            for (int d = 1; d < 6; d++) D = __dadd_rn(D, L.t[d][P]);
+            if (i > 0) D = __dadd_rn(D, L.t[0][P - (long long)my * mz]);
+            if (j > 0) D = __dadd_rn(D, L.t[1][P - mz]);
+            if (k > 0) D = __dadd_rn(D, L.t[2][P - 1]);
+            if (!(D > 0)) D = 1.0;
+        }
+        coef[P] = make_float4((float)L.t[0][P], (float)L.t[1][P], (float)L.t[2][P], (float)D);
+    }
+}
+
+unsigned coarse_blocks(long long m)
+{
+    return (unsigned)std::max<long long>(1, std::min<long long>(8 * 148, (m + 255) / 256));
+}
+
+}  // namespace
 
 // -------------------------------------------------------------- device
 
@@ -1343,7 +1355,7 @@ size_t mg_bytes(const HostRoom &r, const MGHost &h)
     return b + 256;
 }
 
-int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGDev &M)
+int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, cudaStream_t s, MGDev &M)
 {
     const RoomGeom &g = r.g;
     M.nlev = (int)h.nx.size();
@@ -1422,14 +1434,46 @@ int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGD
         MGLevel &L = M.lv[l];
         L.nx = h.nx[l]; L.ny = h.ny[l]; L.nz = h.nz[l]; L.n = (int)m;
         L.sx = h.sx[l]; L.sy = h.sy[l]; L.sz = h.sz[l];
-        float4 *cf = ar.take<float4>(m);
+        L.coef = ar.take<float4>(m);
         L.x = ar.take<float>(m);
         L.b = ar.take<float>(m);
         if (!L.b) return fail(FFR_ENOMEM, "arena exhausted (multigrid levels)");
-        FFR_CUDA(cudaMemcpyAsync(cf, h.coef[l].data(), 16 * m, cudaMemcpyHostToDevice, s));
         FFR_CUDA(cudaMemsetAsync(L.x, 0, 4 * m, s));
         FFR_CUDA(cudaMemsetAsync(L.b, 0, 4 * m, s));
-        L.coef = cf;
+    }
+    if (M.nlev > 1) {
+        // couplings of two consecutive levels in stream-ordered scratch
+        // (level 1 is the largest coarse level)
+        const size_t m1 = (size_t)h.nx[1] * h.ny[1] * h.nz[1];
+        const size_t per = 6 * 8 * m1 + ((m1 + 255) & ~size_t(255));
+        char *scratch = nullptr;
+        FFR_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&scratch), 2 * per, s));
+        LevelOps ops[2];
+        for (int b = 0; b < 2; b++) {
+            char *p = scratch + b * per;
+            for (int d = 0; d < 6; d++) ops[b].t[d] = reinterpret_cast<double *>(p + (size_t)d * 8 * m1);
+            ops[b].act = reinterpret_cast<uint8_t *>(p + 6 * 8 * m1);
+        }
+        int rc = FFR_OK;
+        for (int l = 1; l < M.nlev && !rc; l++) {
+            CoarsenArgs c{};
+            c.ct = R.ct; c.dxv = R.dxv; c.dyv = R.dyv; c.dzv = R.dzv;
+            c.cur = ops[l & 1];
+            if (l == 1) c.cur.act = nullptr;     // gather from the fine cells
+            c.next = ops[(l + 1) & 1];
+            c.nx = h.nx[l - 1]; c.ny = h.ny[l - 1]; c.nz = h.nz[l - 1];
+            c.sx = h.sx[l - 1]; c.sy = h.sy[l - 1]; c.sz = h.sz[l - 1];
+            c.mx = h.nx[l]; c.my = h.ny[l]; c.mz = h.nz[l];
+            const long long m = (long long)c.mx * c.my * c.mz;
+            k_mg_coarsen<<<coarse_blocks(m), 256, 0, s>>>(c);
+            k_mg_coef<<<coarse_blocks(m), 256, 0, s>>>(c.next, c.mx, c.my, c.mz,
+                                                       const_cast<float4 *>(M.lv[l].coef));
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) rc = cuda_fail(e, "multigrid coefficient kernels");
+            count_launch(2);
+        }
+        cudaFreeAsync(scratch, s);
+        if (rc) return rc;
     }
     FFR_CUDA(cudaStreamSynchronize(s));   // the host vectors die at return
     return FFR_OK;

@@ -39,17 +39,17 @@ struct MGDev {
     float *r32;           // FP32 copy of the scaled CG residual (level-0 rhs)
 };
 
-// Host side: builds the coarse levels of a room and uploads them.
+// Host side: the level sizes of a room's hierarchy.
 struct MGHost {
     std::vector<int> nx, ny, nz;
     std::vector<int> sx, sy, sz;             // axes halved towards the next level
-    std::vector<std::vector<float4>> coef;   // index 0 unused
 };
 void build_mg_levels(const HostRoom &r, MGHost &out);
 // Device bytes the hierarchy needs (FP32 z, r32, coarse levels, factors).
 size_t mg_bytes(const HostRoom &r, const MGHost &h);
-// Carves the hierarchy from `ar`, uploads it and fills `M`.
-int mg_upload(const HostRoom &r, const MGHost &h, Arena &ar, cudaStream_t s, MGDev &M);
+// Carves the hierarchy from `ar`, builds its coarse coefficients on the
+// device from the room's uploaded cell types and spacings (R) and fills `M`.
+int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, cudaStream_t s, MGDev &M);
 
 struct PCGArgs {
     RoomDev R;

@@ -43,26 +43,6 @@ constexpr size_t kScratchBytes = kOffOut + al256(64);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Pressure-stencil codes from a device cell-type array, the same classes as
-// build_stencil (PoissonSolver.cpp:61-77).
-__global__ void k_noalloc_codes(const uint8_t *__restrict__ ct, int nx, int ny, int nz,
-                                uint16_t *__restrict__ sc)
-{
-    const int n = nx * ny * nz, plane = ny * nz;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        if (ct[c] == CT_SOLID) { sc[c] = SC_SOLID; continue; }
-        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
-        auto cls = [&](int ii, int jj, int kk) -> unsigned {
-            if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) return SC_NONE;
-            const uint8_t t = ct[(ii * ny + jj) * nz + kk];
-            return t == CT_OUTFLOW ? SC_DIR : (t == CT_SOLID ? SC_NONE : SC_IN);
-        };
-        sc[c] = (uint16_t)(cls(i - 1, j, k) | cls(i + 1, j, k) << 2 | cls(i, j - 1, k) << 4 |
-                           cls(i, j + 1, k) << 6 | cls(i, j, k - 1) << 8 | cls(i, j, k + 1) << 10 |
-                           (ct[c] == CT_OUTFLOW ? SC_OUTF : 0));
-    }
-}
-
 namespace {
 std::mutex g_setup_mu;
 unsigned char *g_scratch_dev[256] = {nullptr};
@@ -100,7 +80,7 @@ extern "C" int ffr_poisson_solve_noalloc(int nx, int ny, int nz, const double *d
     }
     cudaStream_t st = (cudaStream_t)stream;
     // per-axis stencil scales (PoissonSolver.cpp:33-49), computed on the host
-    // exactly as build_stencil does, copied into the scratch array
+    // exactly as stencil_scales does, copied into the scratch array
     std::vector<double> scale(6 * (size_t)kNoAllocMaxDim);
     auto axis = [](const double *h, int m, double *sl, double *sr) {
         for (int i = 0; i < m; i++) {
@@ -122,9 +102,8 @@ extern "C" int ffr_poisson_solve_noalloc(int nx, int ny, int nz, const double *d
     // the barrier state must start at zero on every call
     FFR_CUDA(cudaMemsetAsync(base + kOffSync, 0, sizeof(GridSync), st));
     uint16_t *codes = reinterpret_cast<uint16_t *>(base + kOffCodes);
-    const unsigned cb = (unsigned)std::min<long long>(1184, (n + 255) / 256);
-    k_noalloc_codes<<<cb, 256, 0, st>>>(cell_type_dev, nx, ny, nz, codes);
-    FFR_LAUNCHED(1);
+    int rc = launch_stencil_codes(cell_type_dev, nx, ny, nz, codes, st);
+    if (rc) return rc;
 
     CGArgs a{};
     a.R.nx = nx; a.R.ny = ny; a.R.nz = nz; a.R.n = (int)n;

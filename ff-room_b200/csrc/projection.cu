@@ -949,11 +949,8 @@ size_t tables_bytes(const HostRoom &h)
 int upload_tables(const HostRoom &h, Arena &ar, cudaStream_t s, RoomTables &t, RoomDev &R)
 {
     const RoomGeom &g = h.g;
-    std::vector<uint8_t> fu, fv, fw;
-    std::vector<uint16_t> sc;
     std::vector<double> scale;
-    build_face_codes(h, fu, fv, fw);
-    build_stencil(h, sc, scale);
+    stencil_scales(h, scale);
     std::vector<double> fan(3 * kMaxFans, 0.0);
     for (size_t f = 0; f < h.fans.size(); f++)
         for (int c = 0; c < 3; c++) fan[3 * f + c] = h.fans[f].vel[c];
@@ -973,11 +970,9 @@ int upload_tables(const HostRoom &h, Arena &ar, cudaStream_t s, RoomTables &t, R
     FFR_CUDA(cudaMemcpyAsync(t.dzv, h.dzv.data(), 8 * g.nz, cudaMemcpyHostToDevice, s));
     FFR_CUDA(cudaMemcpyAsync(t.scale, scale.data(), 8 * scale.size(), cudaMemcpyHostToDevice, s));
     FFR_CUDA(cudaMemcpyAsync(t.fanvel, fan.data(), 8 * fan.size(), cudaMemcpyHostToDevice, s));
-    int rc;
-    if ((rc = staged_copy(t.ct, h.ct.data(), g.n, false, s)) || (rc = staged_copy(t.fcu, fu.data(), g.nu, false, s)) ||
-        (rc = staged_copy(t.fcv, fv.data(), g.nv, false, s)) || (rc = staged_copy(t.fcw, fw.data(), g.nw, false, s)) ||
-        (rc = staged_copy(t.sc, sc.data(), 2 * g.n, false, s)))
-        return rc;
+    int rc = staged_copy(t.ct, h.ct.data(), g.n, false, s);
+    if (!rc) rc = build_codes(h, t.ct, t.sc, t.fcu, t.fcv, t.fcw, s);
+    if (rc) return rc;
     // The host vectors die at return: wait for the copies.
     FFR_CUDA(cudaStreamSynchronize(s));
     R.nx = g.nx; R.ny = g.ny; R.nz = g.nz;
@@ -1249,7 +1244,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
     rc = upload_tables(s->room, s->arena, s->stream, s->tab, s->R);
     if (!rc && s->mg) {
-        rc = mg_upload(s->room, s->mgh, s->arena, s->stream, s->M);
+        rc = mg_upload(s->room, s->mgh, s->R, s->arena, s->stream, s->M);
         s->M.vol_x = s->R.dxv; s->M.vol_y = s->R.dyv; s->M.vol_z = s->R.dzv;
     }
     Arena &a = s->arena;
