@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
+#include <unordered_map>
 #include <type_traits>
 
 namespace ffr {
@@ -444,6 +445,59 @@ __global__ void k_lbm_divergence(LbmDev L, const double *u, const double *v, con
     if (threadIdx.x == 0) atomic_max_nonneg(out, m);
 }
 
+// ------------------------------------------------------- set-up kernels
+
+// Step-kernel flags and blocked-direction masks from the cell types: bit q
+// of blocked[c] is set when x + e_q is outside the grid or SOLID (halfway
+// bounce-back, LBMSolver.cpp:151-190); LF_OPEN marks a non-SOLID cell with
+// no blocked direction.  Re-mapped OUTFLOW cells are flagged afterwards
+// (k_lbm_remap_flags).
+__global__ void k_lbm_flags(const uint8_t *__restrict__ ct, int nx, int ny, int nz, uint8_t *__restrict__ flags,
+                            uint32_t *__restrict__ blocked)
+{
+    const int n = nx * ny * nz, plane = ny * nz;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+        uint32_t bl = 0;
+#pragma unroll
+        for (int q = 1; q < 19; q++) {
+            const int a = i + c_ex(q), b = j + c_ey(q), e = k + c_ez(q);
+            const bool ok = a >= 0 && a < nx && b >= 0 && b < ny && e >= 0 && e < nz &&
+                            ct[(a * ny + b) * nz + e] != CT_SOLID;
+            if (!ok) bl |= 1u << q;
+        }
+        blocked[c] = bl;
+        const uint8_t t = ct[c];
+        flags[c] = (uint8_t)(t | ((t != CT_SOLID && bl == 0) ? LF_OPEN : 0));
+    }
+}
+
+// OUTFLOW cells that take their populations from another cell: the cell
+// type plus LF_REMAP, never LF_OPEN.
+__global__ void k_lbm_remap_flags(const uint8_t *__restrict__ ct, const int *__restrict__ dst, int m,
+                                  uint8_t *__restrict__ flags)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x)
+        flags[dst[t]] = (uint8_t)(ct[dst[t]] | LF_REMAP);
+}
+
+// Fan index of the INFLOW cells of one fan's box; fans are applied in
+// order, so the last fan whose box holds a cell wins.
+__global__ void k_lbm_fan_of(const uint8_t *__restrict__ ct, int nx, int ny, int nz, ffr_fan fn, uint8_t f,
+                             uint8_t *__restrict__ fan_of)
+{
+    const int i0 = max(0, fn.i_min), j0 = max(0, fn.j_min), k0 = max(0, fn.k_min);
+    const int bi = min(nx - 1, fn.i_max) - i0 + 1, bj = min(ny - 1, fn.j_max) - j0 + 1,
+              bk = min(nz - 1, fn.k_max) - k0 + 1;
+    const long long cells = (long long)bi * bj * bk;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = i0 + (int)(t / ((long long)bj * bk)), rem = (int)(t % ((long long)bj * bk));
+        const int c = (i * ny + j0 + rem / bk) * nz + k0 + rem % bk;
+        if (ct[c] == CT_INFLOW) fan_of[c] = f;
+    }
+}
+
 }  // namespace ffr
 
 using namespace ffr;
@@ -533,8 +587,12 @@ int lbm_pull(ffr_lbm *s)
 void resolve_remap(const HostRoom &h, std::vector<int> &dst, std::vector<int> &src)
 {
     const int nx = h.g.nx, ny = h.g.ny, nz = h.g.nz;
-    std::vector<int> map(h.g.n);
-    for (long long c = 0; c < h.g.n; c++) map[c] = (int)c;
+    // source of each cell that differs from itself (patch cells only)
+    std::unordered_map<int, int> map;
+    auto get = [&](int c) {
+        auto it = map.find(c);
+        return it == map.end() ? c : it->second;
+    };
     auto CI = [&](int i, int j, int k) { return (i * ny + j) * nz + k; };
     auto pass = [&](const ffr_patch &p) {
         const int N[3] = {nx, ny, nz};
@@ -549,14 +607,17 @@ void resolve_remap(const HostRoom &h, std::vector<int> &dst, std::vector<int> &s
                 else if (p.axis == 1) { cd = CI(a, wall, b); cs = CI(a, s, b); }
                 else { cd = CI(a, b, wall); cs = CI(a, b, s); }
                 if (h.ct[cd] != CT_OUTFLOW) continue;
-                map[cd] = map[cs];
+                map[cd] = get(cs);
             }
     };
     for (const ffr_patch &p : h.patches) pass(p);
     for (const ffr_patch &p : h.patches) if (p.is_opening) pass(p);
+    std::vector<std::pair<int, int>> moved;
+    for (const auto &kv : map)
+        if (kv.second != kv.first) moved.push_back(kv);
+    std::sort(moved.begin(), moved.end());
     dst.clear(); src.clear();
-    for (long long c = 0; c < h.g.n; c++)
-        if (map[c] != (int)c) { dst.push_back((int)c); src.push_back(map[c]); }
+    for (const auto &kv : moved) { dst.push_back(kv.first); src.push_back(kv.second); }
 }
 
 }  // namespace
@@ -581,52 +642,13 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
         delete s;
         return fail(FFR_ECUDA, "cudaStreamCreate");
     }
-    // per-cell fan index: the last fan whose box holds an INFLOW cell
-    std::vector<uint8_t> fan_of(g.n, 255);
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    for (size_t f = 0; f < s->room.fans.size(); f++) {
-        const ffr_fan &fn = s->room.fans[f];
-        for (int i = fn.i_min; i <= fn.i_max; i++)
-            for (int j = fn.j_min; j <= fn.j_max; j++)
-                for (int k = fn.k_min; k <= fn.k_max; k++) {
-                    if (i < 0 || i >= nx || j < 0 || j >= ny || k < 0 || k >= nz) continue;
-                    const int c = (i * ny + j) * nz + k;
-                    if (s->room.ct[c] == CT_INFLOW) fan_of[c] = (uint8_t)f;
-                }
-    }
     const double p2l = dt / (g.lx / g.nx);   // phys_to_lat = dt / grid.dx (LBMSolver.cpp:42-44)
     std::vector<double> fan_lat(3 * std::max<size_t>(1, s->room.fans.size()), 0.0);
     for (size_t f = 0; f < s->room.fans.size(); f++)
         for (int c = 0; c < 3; c++) fan_lat[3 * f + c] = s->room.fans[f].vel[c] * p2l;
     std::vector<int> rd, rs;
     resolve_remap(s->room, rd, rs);
-    // step-kernel flags: open interior cells skip every neighbour test
-    std::vector<uint8_t> flags(g.n);
-    std::vector<uint32_t> blocked(g.n, 0);
-    {
-        static const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
-        static const int ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
-        static const int ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
-        std::vector<uint8_t> remapped(g.n, 0);
-        for (int d : rd) remapped[d] = 1;
-        for (int i = 0; i < nx; i++)
-            for (int j = 0; j < ny; j++)
-                for (int k = 0; k < nz; k++) {
-                    const int c = (i * ny + j) * nz + k;
-                    uint8_t f = s->room.ct[c];
-                    if (remapped[c]) f |= LF_REMAP;
-                    uint32_t bl = 0;
-                    for (int q = 1; q < 19; q++) {
-                        const int a = i + ex[q], b = j + ey[q], e = k + ez[q];
-                        const bool ok = a >= 0 && a < nx && b >= 0 && b < ny && e >= 0 && e < nz &&
-                                        s->room.ct[(a * ny + b) * nz + e] != CT_SOLID;
-                        if (!ok) bl |= 1u << q;
-                    }
-                    blocked[c] = bl;
-                    if (f != CT_SOLID && !remapped[c] && bl == 0) f |= LF_OPEN;
-                    flags[c] = f;
-                }
-    }
     const size_t es = storage == FFR_LBM_FP64 ? 8 : (storage == FFR_LBM_FP32 ? 4 : 2);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = 2 * al(es * 19 * g.n) + 4 * al(8 * g.n) + al(8 * g.nu) + al(8 * g.nv) +
@@ -657,14 +679,30 @@ int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps, double 
         return fail(FFR_ENOMEM, "LBM allocation");
     }
     cudaStream_t st = s->stream;
-    FFR_CUDA(cudaMemcpyAsync(ct, s->room.ct.data(), g.n, cudaMemcpyHostToDevice, st));
-    FFR_CUDA(cudaMemcpyAsync(fo, fan_of.data(), g.n, cudaMemcpyHostToDevice, st));
-    FFR_CUDA(cudaMemcpyAsync(fld, flags.data(), g.n, cudaMemcpyHostToDevice, st));
-    FFR_CUDA(cudaMemcpyAsync(blk, blocked.data(), 4 * g.n, cudaMemcpyHostToDevice, st));
+    rc = staged_copy(ct, s->room.ct.data(), g.n, false, st);
+    if (rc) { ffr_lbm_destroy(s); return rc; }
     FFR_CUDA(cudaMemcpyAsync(fl, fan_lat.data(), 8 * fan_lat.size(), cudaMemcpyHostToDevice, st));
     if (!rd.empty()) {
         FFR_CUDA(cudaMemcpyAsync(rdd, rd.data(), 4 * rd.size(), cudaMemcpyHostToDevice, st));
         FFR_CUDA(cudaMemcpyAsync(rsd, rs.data(), 4 * rs.size(), cudaMemcpyHostToDevice, st));
+    }
+    // per-cell fan index (255: none), step flags and blocked directions,
+    // formed on the device from the cell types
+    FFR_CUDA(cudaMemsetAsync(fo, 255, g.n, st));
+    for (size_t f = 0; f < s->room.fans.size(); f++) {
+        const ffr_fan &fn = s->room.fans[f];
+        const long long bi = std::min(nx - 1, fn.i_max) - std::max(0, fn.i_min) + 1,
+                        bj = std::min(ny - 1, fn.j_max) - std::max(0, fn.j_min) + 1,
+                        bk = std::min(nz - 1, fn.k_max) - std::max(0, fn.k_min) + 1;
+        if (bi <= 0 || bj <= 0 || bk <= 0) continue;
+        k_lbm_fan_of<<<blocks_for(bi * bj * bk), kThr, 0, st>>>(ct, nx, ny, nz, fn, (uint8_t)f, fo);
+        FFR_LAUNCHED(1);
+    }
+    k_lbm_flags<<<blocks_for(g.n), kThr, 0, st>>>(ct, nx, ny, nz, fld, blk);
+    FFR_LAUNCHED(1);
+    if (!rd.empty()) {
+        k_lbm_remap_flags<<<blocks_for((long long)rd.size()), kThr, 0, st>>>(ct, rdd, (int)rd.size(), fld);
+        FFR_LAUNCHED(1);
     }
     FFR_CUDA(cudaMemcpyAsync(dxv, s->room.dxv.data(), 8 * g.nx, cudaMemcpyHostToDevice, st));
     std::vector<double> inv(g.nx + g.ny + g.nz);

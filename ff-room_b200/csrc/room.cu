@@ -118,7 +118,7 @@ namespace {
 // the work queued on the caller's stream before the copy.
 cudaError_t staged_slice(char *d, const char *s, size_t bytes, bool to_host, cudaEvent_t start, int dev)
 {
-    constexpr size_t kChunk = 4u << 20;
+    constexpr size_t kChunk = 2u << 20;
     cudaError_t e = cudaSetDevice(dev);
     if (e != cudaSuccess) return e;
     cudaStream_t ws = nullptr;
@@ -174,12 +174,12 @@ cudaError_t staged_slice(char *d, const char *s, size_t bytes, bool to_host, cud
 
 // Synchronous copy between pageable host memory and the device.  Large
 // copies are cut into page-aligned slices, one per host thread (up to 16,
-// at least 16 MB each), each staged through its own bounce buffers and
+// at least 4 MB each), each staged through its own bounce buffers and
 // stream, so the host-side copies (and the page faults of a freshly
 // allocated destination) run in parallel while the DMAs share the link.
 int staged_copy(void *dst, const void *src, size_t bytes, bool to_host, cudaStream_t st)
 {
-    constexpr size_t kSlice = 16u << 20;
+    constexpr size_t kSlice = 4u << 20;
     const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice;
     if (bytes < 2 * kSlice) {
         FFR_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, st));
