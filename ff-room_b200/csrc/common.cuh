@@ -130,6 +130,18 @@ void parallel_slabs(int n, F f)
     for (auto &x : th) x.join();
 }
 
+// Page-locked staging of a handle's small set-up arrays (spacings, scales,
+// fan velocities, multigrid factors): each array is copied into the block
+// and sent with an asynchronous copy, so queuing a handle's set-up never
+// waits on its stream.  The block lives as long as the handle.
+struct HostStage {
+    char *base = nullptr;
+    size_t size = 0, used = 0;
+    int reserve(size_t bytes);
+    int put(void *dev, const void *src, size_t bytes, cudaStream_t s);
+    void release();
+};
+
 // Synchronous copy between pageable host memory and the device, ordered
 // after the work queued on `st`: large copies run on up to 16 host threads,
 // each staging its slice through two page-locked bounce buffers on its own

@@ -1355,7 +1355,13 @@ size_t mg_bytes(const HostRoom &r, const MGHost &h)
     return b + 256;
 }
 
-int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, cudaStream_t s, MGDev &M)
+size_t mg_stage_bytes(const HostRoom &r)
+{
+    return 4 * 3 * (size_t)(r.g.nx + r.g.ny + r.g.nz) + 9 * 16;
+}
+
+int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, HostStage &hs, cudaStream_t s,
+              MGDev &M)
 {
     const RoomGeom &g = r.g;
     M.nlev = (int)h.nx.size();
@@ -1395,15 +1401,14 @@ int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, c
     M.r32 = ar.take<float>(g.n);
     M.lv[0].b = M.r32;
     if (!M.r32 || !fzr) return fail(FFR_ENOMEM, "arena exhausted (multigrid)");
-    FFR_CUDA(cudaMemcpyAsync(fx, dx.data(), 4 * g.nx, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(fxl, ixl.data(), 4 * g.nx, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(fxr, ixr.data(), 4 * g.nx, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(fy, dy.data(), 4 * g.ny, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(fyl, iyl.data(), 4 * g.ny, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(fyr, iyr.data(), 4 * g.ny, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(fz, dz.data(), 4 * g.nz, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(fzl, izl.data(), 4 * g.nz, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(fzr, izr.data(), 4 * g.nz, cudaMemcpyHostToDevice, s));
+    {
+        float *dev[9] = {fx, fxl, fxr, fy, fyl, fyr, fz, fzl, fzr};
+        const std::vector<float> *src[9] = {&dx, &ixl, &ixr, &dy, &iyl, &iyr, &dz, &izl, &izr};
+        for (int q = 0; q < 9; q++) {
+            const int rc = hs.put(dev[q], src[q]->data(), 4 * src[q]->size(), s);
+            if (rc) return rc;
+        }
+    }
     FFR_CUDA(cudaMemsetAsync(M.lv[0].x, 0, 4 * g.n, s));
     FFR_CUDA(cudaMemsetAsync(M.r32, 0, 4 * g.n, s));
     M.dx = fx; M.dy = fy; M.dz = fz;
@@ -1475,7 +1480,6 @@ int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, c
         cudaFreeAsync(scratch, s);
         if (rc) return rc;
     }
-    FFR_CUDA(cudaStreamSynchronize(s));   // the host vectors die at return
     return FFR_OK;
 }
 

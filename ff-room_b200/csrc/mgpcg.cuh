@@ -47,9 +47,14 @@ struct MGHost {
 void build_mg_levels(const HostRoom &r, MGHost &out);
 // Device bytes the hierarchy needs (FP32 z, r32, coarse levels, factors).
 size_t mg_bytes(const HostRoom &r, const MGHost &h);
-// Carves the hierarchy from `ar`, builds its coarse coefficients on the
-// device from the room's uploaded cell types and spacings (R) and fills `M`.
-int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, cudaStream_t s, MGDev &M);
+// Carves the hierarchy from `ar`, fills `M` and queues on s, without
+// waiting: the fine-level factors (through the staging block hs) and the
+// coarse coefficients, built by kernels from the room's uploaded cell
+// types and spacings (R).
+int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, HostStage &hs, cudaStream_t s,
+              MGDev &M);
+// Staging bytes mg_upload needs.
+size_t mg_stage_bytes(const HostRoom &r);
 
 struct PCGArgs {
     RoomDev R;

@@ -946,7 +946,47 @@ size_t tables_bytes(const HostRoom &h)
            al(8 * 3 * kMaxFans) + al(g.n) + al(g.nu) + al(g.nv) + al(g.nw) + al(2 * g.n);
 }
 
-int upload_tables(const HostRoom &h, Arena &ar, cudaStream_t s, RoomTables &t, RoomDev &R)
+// Carves the tables from the arena and points R at them (no device work).
+int carve_tables(const HostRoom &h, Arena &ar, RoomTables &t, RoomDev &R)
+{
+    const RoomGeom &g = h.g;
+    t.dxv = ar.take<double>(g.nx);
+    t.dyv = ar.take<double>(g.ny);
+    t.dzv = ar.take<double>(g.nz);
+    t.scale = ar.take<double>(2 * (size_t)(g.nx + g.ny + g.nz));
+    t.fanvel = ar.take<double>(3 * kMaxFans);
+    t.ct = ar.take<uint8_t>(g.n);
+    t.fcu = ar.take<uint8_t>(g.nu);
+    t.fcv = ar.take<uint8_t>(g.nv);
+    t.fcw = ar.take<uint8_t>(g.nw);
+    t.sc = ar.take<uint16_t>(g.n);
+    if (!t.sc) return fail(FFR_ENOMEM, "arena exhausted (tables)");
+    R.nx = g.nx; R.ny = g.ny; R.nz = g.nz;
+    R.n = (int)g.n; R.nu = (int)g.nu; R.nv = (int)g.nv; R.nw = (int)g.nw;
+    R.dxv = t.dxv; R.dyv = t.dyv; R.dzv = t.dzv;
+    R.ct = t.ct; R.fcu = t.fcu; R.fcv = t.fcv; R.fcw = t.fcw;
+    R.sc = t.sc; R.scale = t.scale; R.fanvel = t.fanvel;
+    return FFR_OK;
+}
+
+// Staging bytes queue_tables needs.
+size_t tables_stage_bytes(const HostRoom &h)
+{
+    const RoomGeom &g = h.g;
+    return 8 * 3 * (size_t)(g.nx + g.ny + g.nz) + 8 * 3 * kMaxFans + 5 * 16;
+}
+
+// The cell types, by a synchronous staged copy.  Made before any kernel is
+// queued on s, it waits for nothing but the link.
+int upload_cell_types(const HostRoom &h, const RoomTables &t, cudaStream_t s)
+{
+    return staged_copy(t.ct, h.ct.data(), h.g.n, false, s);
+}
+
+// Queues the rest of the tables on s without waiting: spacings, stencil
+// scales and fan velocities through the staging block, the stencil and
+// face codes by kernels from the uploaded cell types.
+int queue_tables(const HostRoom &h, const RoomTables &t, HostStage &hs, cudaStream_t s)
 {
     const RoomGeom &g = h.g;
     std::vector<double> scale;
@@ -954,33 +994,12 @@ int upload_tables(const HostRoom &h, Arena &ar, cudaStream_t s, RoomTables &t, R
     std::vector<double> fan(3 * kMaxFans, 0.0);
     for (size_t f = 0; f < h.fans.size(); f++)
         for (int c = 0; c < 3; c++) fan[3 * f + c] = h.fans[f].vel[c];
-    t.dxv = ar.take<double>(g.nx);
-    t.dyv = ar.take<double>(g.ny);
-    t.dzv = ar.take<double>(g.nz);
-    t.scale = ar.take<double>(scale.size());
-    t.fanvel = ar.take<double>(fan.size());
-    t.ct = ar.take<uint8_t>(g.n);
-    t.fcu = ar.take<uint8_t>(g.nu);
-    t.fcv = ar.take<uint8_t>(g.nv);
-    t.fcw = ar.take<uint8_t>(g.nw);
-    t.sc = ar.take<uint16_t>(g.n);
-    if (!t.sc) return fail(FFR_ENOMEM, "arena exhausted (tables)");
-    FFR_CUDA(cudaMemcpyAsync(t.dxv, h.dxv.data(), 8 * g.nx, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.dyv, h.dyv.data(), 8 * g.ny, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.dzv, h.dzv.data(), 8 * g.nz, cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.scale, scale.data(), 8 * scale.size(), cudaMemcpyHostToDevice, s));
-    FFR_CUDA(cudaMemcpyAsync(t.fanvel, fan.data(), 8 * fan.size(), cudaMemcpyHostToDevice, s));
-    int rc = staged_copy(t.ct, h.ct.data(), g.n, false, s);
-    if (!rc) rc = build_codes(h, t.ct, t.sc, t.fcu, t.fcv, t.fcw, s);
-    if (rc) return rc;
-    // The host vectors die at return: wait for the copies.
-    FFR_CUDA(cudaStreamSynchronize(s));
-    R.nx = g.nx; R.ny = g.ny; R.nz = g.nz;
-    R.n = (int)g.n; R.nu = (int)g.nu; R.nv = (int)g.nv; R.nw = (int)g.nw;
-    R.dxv = t.dxv; R.dyv = t.dyv; R.dzv = t.dzv;
-    R.ct = t.ct; R.fcu = t.fcu; R.fcv = t.fcv; R.fcw = t.fcw;
-    R.sc = t.sc; R.scale = t.scale; R.fanvel = t.fanvel;
-    return FFR_OK;
+    int rc;
+    if ((rc = hs.put(t.dxv, h.dxv.data(), 8 * g.nx, s)) || (rc = hs.put(t.dyv, h.dyv.data(), 8 * g.ny, s)) ||
+        (rc = hs.put(t.dzv, h.dzv.data(), 8 * g.nz, s)) || (rc = hs.put(t.scale, scale.data(), 8 * scale.size(), s)) ||
+        (rc = hs.put(t.fanvel, fan.data(), 8 * fan.size(), s)))
+        return rc;
+    return build_codes(h, t.ct, t.sc, t.fcu, t.fcv, t.fcw, s);
 }
 
 // CG launch geometry: as many co-resident blocks as the room can use.
@@ -1058,6 +1077,7 @@ struct ffr_fluid {
     cudaStream_t body_stream = nullptr;
     int split_mode = -1;           // multigrid schedule: -1 split in graphs only, 0 never, 1 always
     SplitHost split_host;          // host pacing of the eager split solve
+    HostStage stage;               // page-locked source of the set-up copies
 };
 
 namespace {
@@ -1242,11 +1262,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
                          al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (s->mg ? mg_bytes(s->room, s->mgh) : 0);
     rc = s->arena.alloc(bytes, s->stream);
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
-    rc = upload_tables(s->room, s->arena, s->stream, s->tab, s->R);
-    if (!rc && s->mg) {
-        rc = mg_upload(s->room, s->mgh, s->R, s->arena, s->stream, s->M);
-        s->M.vol_x = s->R.dxv; s->M.vol_y = s->R.dyv; s->M.vol_z = s->R.dzv;
-    }
+    rc = carve_tables(s->room, s->arena, s->tab, s->R);
     Arena &a = s->arena;
     s->u = a.take<double>(g.nu); s->v = a.take<double>(g.nv); s->w = a.take<double>(g.nw);
     s->us = a.take<double>(g.nu); s->vs = a.take<double>(g.nv); s->ws = a.take<double>(g.nw);
@@ -1282,20 +1298,36 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
         return fail(FFR_ECUDA, "cudaEventCreate");
     }
     cudaStream_t st = s->stream;
-#define UP(dst, src, cnt)                                                                      \
-    do {                                                                                       \
-        if (src) {                                                                             \
-            rc = staged_copy(dst, src, 8 * (cnt), false, st);                                  \
-            if (rc) { ffr_fluid_destroy(s); return rc; }                                       \
-        } else {                                                                               \
-            FFR_CUDA(cudaMemsetAsync(dst, 0, 8 * (cnt), st));                                  \
-        }                                                                                      \
-    } while (0)
-    UP(s->u, init ? init->u : nullptr, g.nu);
-    UP(s->v, init ? init->v : nullptr, g.nv);
-    UP(s->w, init ? init->w : nullptr, g.nw);
-    UP(s->p, init ? init->p : nullptr, g.n);
-#undef UP
+    // Synchronous copies first, while nothing is queued on the stream (so
+    // they wait for the link only, not for other rooms' kernels); then the
+    // rest of the set-up is queued and create returns without waiting.
+    rc = upload_cell_types(s->room, s->tab, st);
+    if (rc) { ffr_fluid_destroy(s); return rc; }
+    if (init) {
+        const double *src[4] = {init->u, init->v, init->w, init->p};
+        double *dst[4] = {s->u, s->v, s->w, s->p};
+        const long long cnt[4] = {g.nu, g.nv, g.nw, g.n};
+        for (int f = 0; f < 4; f++)
+            if (src[f] && (rc = staged_copy(dst[f], src[f], 8 * cnt[f], false, st))) {
+                ffr_fluid_destroy(s);
+                return rc;
+            }
+    }
+    {
+        const double *src[4] = {init ? init->u : nullptr, init ? init->v : nullptr, init ? init->w : nullptr,
+                                init ? init->p : nullptr};
+        double *dst[4] = {s->u, s->v, s->w, s->p};
+        const long long cnt[4] = {g.nu, g.nv, g.nw, g.n};
+        for (int f = 0; f < 4; f++)
+            if (!src[f]) FFR_CUDA(cudaMemsetAsync(dst[f], 0, 8 * cnt[f], st));
+    }
+    rc = s->stage.reserve(tables_stage_bytes(s->room) + (s->mg ? mg_stage_bytes(s->room) : 0));
+    if (!rc) rc = queue_tables(s->room, s->tab, s->stage, st);
+    if (!rc && s->mg) {
+        rc = mg_upload(s->room, s->mgh, s->R, s->arena, s->stage, st, s->M);
+        s->M.vol_x = s->R.dxv; s->M.vol_y = s->R.dyv; s->M.vol_z = s->R.dzv;
+    }
+    if (rc) { ffr_fluid_destroy(s); return rc; }
     FFR_CUDA(cudaMemsetAsync(s->st, 0, sizeof(StepState), st));
     FFR_CUDA(cudaMemsetAsync(s->split_state, 0, 256, st));
     k_fill<<<stream_blocks(g.n), kThreads, 0, st>>>(s->T0, (int)g.n, params->T_initial);
@@ -1308,7 +1340,6 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
             FFR_LAUNCHED(1);
         }
     }
-    FFR_CUDA(cudaStreamSynchronize(st));
     *out = s;
     return FFR_OK;
 }
@@ -1323,6 +1354,7 @@ int ffr_fluid_destroy(ffr_fluid *s)
     if (s->body_stream) cudaStreamDestroy(s->body_stream);
     s->split_host.release();
     if (s->done_ev) cudaEventDestroy(s->done_ev);
+    s->stage.release();
     s->arena.release();
     pinned_put(s->ring_host, sizeof(ffr_step_result) * kRing);
     pinned_put(s->st_host, sizeof(StepState));
@@ -1923,6 +1955,7 @@ struct ffr_poisson {
     GridSync *gs;
     CGScalars *sc;
     unsigned blocks;
+    HostStage stage;
 };
 
 extern "C" {
@@ -1949,7 +1982,10 @@ int ffr_poisson_create(const ffr_room_desc *room, int max_iter, double tol, ffr_
                          al(sizeof(GridSync)) + al(sizeof(CGScalars)) + 4 * 256;
     rc = s->arena.alloc(bytes);
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
-    rc = upload_tables(s->room, s->arena, s->stream, s->tab, s->R);
+    rc = carve_tables(s->room, s->arena, s->tab, s->R);
+    if (!rc) rc = upload_cell_types(s->room, s->tab, s->stream);
+    if (!rc) rc = s->stage.reserve(tables_stage_bytes(s->room));
+    if (!rc) rc = queue_tables(s->room, s->tab, s->stage, s->stream);
     Arena &a = s->arena;
     s->r = a.take<double>(g.n); s->da = a.take<double>(g.n); s->db = a.take<double>(g.n);
     s->ad = a.take<double>(g.n); s->x_tmp = a.take<double>(g.n); s->b_tmp = a.take<double>(g.n);
@@ -1964,6 +2000,11 @@ int ffr_poisson_create(const ffr_room_desc *room, int max_iter, double tol, ffr_
         ffr_poisson_destroy(s);
         return rc;
     }
+    // a solve may run on the caller's stream: the set-up must be complete
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        ffr_poisson_destroy(s);
+        return fail(FFR_ECUDA, "poisson set-up");
+    }
     *out = s;
     return FFR_OK;
 }
@@ -1972,6 +2013,7 @@ int ffr_poisson_destroy(ffr_poisson *s)
 {
     if (!s) return FFR_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
+    s->stage.release();
     s->arena.release();
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;

@@ -111,6 +111,34 @@ void pinned_put(void *p, size_t bytes)
     g_pinned[bytes].push_back(p);
 }
 
+int HostStage::reserve(size_t bytes)
+{
+    size_t sz = 64u << 10;           // power-of-two sizes keep the pinned cache reusable
+    while (sz < bytes) sz <<= 1;
+    base = static_cast<char *>(pinned_get(sz));
+    if (!base) return fail(FFR_ENOMEM, "pinned staging block");
+    size = sz;
+    used = 0;
+    return FFR_OK;
+}
+
+int HostStage::put(void *dev, const void *src, size_t bytes, cudaStream_t s)
+{
+    const size_t b = (bytes + 15) & ~size_t(15);
+    if (!base || used + b > size) return fail(FFR_ENOMEM, "set-up staging block exhausted");
+    std::memcpy(base + used, src, bytes);
+    FFR_CUDA(cudaMemcpyAsync(dev, base + used, bytes, cudaMemcpyHostToDevice, s));
+    used += b;
+    return FFR_OK;
+}
+
+void HostStage::release()
+{
+    pinned_put(base, size);
+    base = nullptr;
+    size = used = 0;
+}
+
 namespace {
 // One host thread's slice of a staged copy: chunks through two page-locked
 // bounce buffers on the thread's own stream, so the DMA of one chunk
