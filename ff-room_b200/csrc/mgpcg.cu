@@ -742,6 +742,47 @@ __device__ __forceinline__ void pass_redpost_dot(const PCGArgs &A, int start, in
     float *z = M.lv[0].x;
     const bool sweep = M.nlev_grid >= 1;
     const int n = R.n, ny = R.ny, nz = R.nz, plane = ny * nz, pk = (nz + 1) >> 1;
+    if ((nz & 1) == 0) {
+        // even rows: pair loads (see pass_direction); the red cell's x and y
+        // neighbours are one half of the neighbouring pairs, its z neighbours
+        // the other cell of the pair and one single load
+        for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
+            const int i = w.i, j = w.j, k0 = 2 * w.k;
+            const int c0 = (i * ny + j) * nz + k0;
+            const bool red0 = ((i + j + k0) & 1) == 0;
+            const ushort2 cd = *reinterpret_cast<const ushort2 *>(R.sc + c0);
+            const double2 r = *reinterpret_cast<const double2 *>(A.r + c0);
+            const float2 zc = *reinterpret_cast<const float2 *>(z + c0);
+            float z0 = zc.x, z1 = zc.y;
+            const int cr = red0 ? c0 : c0 + 1;
+            const float br = M.r32[cr];
+            const int ox[4] = {max(c0 - plane, 0), min(c0 + plane, n - 2), max(c0 - nz, 0), min(c0 + nz, n - 2)};
+            float zn[6];
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+                const float2 zv = *reinterpret_cast<const float2 *>(z + ox[a]);
+                zn[a] = red0 ? zv.x : zv.y;
+            }
+            const float zo = z[red0 ? max(c0 - 1, 0) : min(c0 + 2, n - 1)];
+            zn[4] = red0 ? zo : zc.x;
+            zn[5] = red0 ? zc.y : zo;
+            const unsigned coder = red0 ? cd.x : cd.y;
+            if (sweep && active_code(coder)) {
+                float t[6], D;
+                fine_coefs(M, coder, i, j, red0 ? k0 : k0 + 1, t, D);
+                float sum = 0.0f;
+#pragma unroll
+                for (int a = 0; a < 6; a++)
+                    if (t[a] != 0.0f) sum += t[a] * zn[a];
+                const float zr = (br + sum) / D;
+                z[cr] = zr;
+                if (red0) z0 = zr; else z1 = zr;
+            }
+            if (active_code(cd.x)) acc += r.x * (double)z0;
+            if (active_code(cd.y)) acc += r.y * (double)z1;
+        }
+        return;
+    }
     for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
         const CellPair P(w, ny, nz);
         const unsigned code0 = R.sc[P.c0], code1 = R.sc[P.c1];
@@ -780,6 +821,63 @@ __device__ __forceinline__ void pass_direction(const PCGArgs &A, int start, int 
     const MGDev &M = A.M;
     const float *z = M.lv[0].x;
     const int n = R.n, ny = R.ny, nz = R.nz, plane = ny * nz, pk = (nz + 1) >> 1;
+    if ((nz & 1) == 0) {
+        // Even rows: both cells of every pair, and the pairs of its x and y
+        // neighbours, sit at even indices, so each pair moves with one
+        // 16-byte (8-byte for FP32, 4-byte for codes) load or store.  A
+        // neighbour pair outside the grid is clamped to a pair inside it;
+        // its values get weight 0, exactly as the clamped single loads of
+        // the general loop below.
+        for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
+            const int i = w.i, j = w.j, k0 = 2 * w.k;
+            const int c0 = (i * ny + j) * nz + k0;
+            const ushort2 cd = *reinterpret_cast<const ushort2 *>(R.sc + c0);
+            const double2 dp = *reinterpret_cast<const double2 *>(dold + c0);
+            const float2 zc = *reinterpret_cast<const float2 *>(z + c0);
+            const double2 xo = update_x ? *reinterpret_cast<const double2 *>(A.x + c0) : make_double2(0.0, 0.0);
+            const int ox[4] = {max(c0 - plane, 0), min(c0 + plane, n - 2), max(c0 - nz, 0), min(c0 + nz, n - 2)};
+            double n0[6], n1[6];
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+                const double2 dv = *reinterpret_cast<const double2 *>(dold + ox[a]);
+                const float2 zv = *reinterpret_cast<const float2 *>(z + ox[a]);
+                n0[a] = fma(beta, dv.x, (double)zv.x);
+                n1[a] = fma(beta, dv.y, (double)zv.y);
+            }
+            const int zm = max(c0 - 1, 0), zp = min(c0 + 2, n - 1);
+            n0[4] = fma(beta, dold[zm], (double)z[zm]);
+            n1[5] = fma(beta, dold[zp], (double)z[zp]);
+            const double d0 = fma(beta, dp.x, (double)zc.x), d1 = fma(beta, dp.y, (double)zc.y);
+            n0[5] = d1;
+            n1[4] = d0;
+            auto cell = [&](unsigned code, int k, double dp_, double dc, double xo_, const double (&dn)[6],
+                            double &dout, double &qout, double &xout) {
+                xout = xo_;
+                if (!active_code(code)) {
+                    dout = 0.0;
+                    qout = 0.0;
+                    return;
+                }
+                if (update_x) xout = fma(alpha_prev, dp_, xo_);
+                dout = dc;
+                double wt[6], diag;
+                ref_weights(R, M, code, i, j, k, wt, diag);
+                double o = 0.0;
+#pragma unroll
+                for (int a = 0; a < 6; a++) o += wt[a] * dn[a];
+                const double qc = cell_vol(M, i, j, k) * (diag * dc - o);
+                qout = qc;
+                acc += dc * qc;
+            };
+            double2 dn2, q2, xn2;
+            cell(cd.x, k0, dp.x, d0, xo.x, n0, dn2.x, q2.x, xn2.x);
+            cell(cd.y, k0 + 1, dp.y, d1, xo.y, n1, dn2.y, q2.y, xn2.y);
+            *reinterpret_cast<double2 *>(dnew + c0) = dn2;
+            *reinterpret_cast<double2 *>(A.q + c0) = q2;
+            if (update_x) *reinterpret_cast<double2 *>(A.x + c0) = xn2;
+        }
+        return;
+    }
     for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
         const CellPair P(w, ny, nz);
         const int c0 = P.c0, c1 = P.c1;
@@ -834,6 +932,40 @@ __device__ __forceinline__ void pass_residual(const PCGArgs &A, int start, int s
     const MGDev &M = A.M;
     float *z = M.lv[0].x;
     const int ny = R.ny, nz = R.nz, pk = (nz + 1) >> 1;
+    if ((nz & 1) == 0) {
+        // even rows: pair loads and stores (see pass_direction).  A cell
+        // that is not an unknown keeps r (stored back unchanged) and its
+        // r32 and z, which the solve's set-up pass made 0.
+        for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
+            const int i = w.i, j = w.j, k0 = 2 * w.k;
+            const int c0 = (i * ny + j) * nz + k0;
+            const bool red0 = ((i + j + k0) & 1) == 0;
+            const ushort2 cd = *reinterpret_cast<const ushort2 *>(R.sc + c0);
+            const double2 rq = *reinterpret_cast<const double2 *>(A.r + c0);
+            const double2 qq = *reinterpret_cast<const double2 *>(A.q + c0);
+            float tt[6], D;
+            fine_coefs(M, red0 ? cd.x : cd.y, i, j, red0 ? k0 : k0 + 1, tt, D);
+            double2 rn = rq;
+            float2 r32v = make_float2(0.0f, 0.0f), zv = make_float2(0.0f, 0.0f);
+            auto cell = [&](unsigned code, int k, double r0, double q0, bool red, double &rout, float &r32out,
+                            float &zout) {
+                if (!active_code(code)) return;
+                const double rv = r0 - alpha * q0;
+                rout = rv;
+                const double ru = rv / cell_vol(M, i, j, k);
+                acc += ru * ru;
+                const float r32 = (float)rv;
+                r32out = r32;
+                zout = red ? r32 / D : 0.0f;
+            };
+            cell(cd.x, k0, rq.x, qq.x, red0, rn.x, r32v.x, zv.x);
+            cell(cd.y, k0 + 1, rq.y, qq.y, !red0, rn.y, r32v.y, zv.y);
+            *reinterpret_cast<double2 *>(A.r + c0) = rn;
+            *reinterpret_cast<float2 *>(M.r32 + c0) = r32v;
+            *reinterpret_cast<float2 *>(z + c0) = zv;
+        }
+        return;
+    }
     for (Walk w(start, stride, ny, pk, R.nx * ny * pk); w.ok(); w.next()) {
         const CellPair P(w, ny, nz);
         const unsigned code0 = R.sc[P.c0], code1 = R.sc[P.c1];
