@@ -751,7 +751,7 @@ __device__ __forceinline__ void pass_redpost_dot(const PCGArgs &A, int start, in
             const int c0 = (i * ny + j) * nz + k0;
             const bool red0 = ((i + j + k0) & 1) == 0;
             const ushort2 cd = *reinterpret_cast<const ushort2 *>(R.sc + c0);
-            const double2 r = *reinterpret_cast<const double2 *>(A.r + c0);
+            const double2 r = __ldcs(reinterpret_cast<const double2 *>(A.r + c0));
             const float2 zc = *reinterpret_cast<const float2 *>(z + c0);
             float z0 = zc.x, z1 = zc.y;
             const int cr = red0 ? c0 : c0 + 1;
@@ -834,7 +834,7 @@ __device__ __forceinline__ void pass_direction(const PCGArgs &A, int start, int 
             const ushort2 cd = *reinterpret_cast<const ushort2 *>(R.sc + c0);
             const double2 dp = *reinterpret_cast<const double2 *>(dold + c0);
             const float2 zc = *reinterpret_cast<const float2 *>(z + c0);
-            const double2 xo = update_x ? *reinterpret_cast<const double2 *>(A.x + c0) : make_double2(0.0, 0.0);
+            const double2 xo = update_x ? __ldcs(reinterpret_cast<const double2 *>(A.x + c0)) : make_double2(0.0, 0.0);
             const int ox[4] = {max(c0 - plane, 0), min(c0 + plane, n - 2), max(c0 - nz, 0), min(c0 + nz, n - 2)};
             double n0[6], n1[6];
 #pragma unroll
@@ -873,8 +873,8 @@ __device__ __forceinline__ void pass_direction(const PCGArgs &A, int start, int 
             cell(cd.x, k0, dp.x, d0, xo.x, n0, dn2.x, q2.x, xn2.x);
             cell(cd.y, k0 + 1, dp.y, d1, xo.y, n1, dn2.y, q2.y, xn2.y);
             *reinterpret_cast<double2 *>(dnew + c0) = dn2;
-            *reinterpret_cast<double2 *>(A.q + c0) = q2;
-            if (update_x) *reinterpret_cast<double2 *>(A.x + c0) = xn2;
+            __stcs(reinterpret_cast<double2 *>(A.q + c0), q2);
+            if (update_x) __stcs(reinterpret_cast<double2 *>(A.x + c0), xn2);
         }
         return;
     }
@@ -941,8 +941,8 @@ __device__ __forceinline__ void pass_residual(const PCGArgs &A, int start, int s
             const int c0 = (i * ny + j) * nz + k0;
             const bool red0 = ((i + j + k0) & 1) == 0;
             const ushort2 cd = *reinterpret_cast<const ushort2 *>(R.sc + c0);
-            const double2 rq = *reinterpret_cast<const double2 *>(A.r + c0);
-            const double2 qq = *reinterpret_cast<const double2 *>(A.q + c0);
+            const double2 rq = __ldcs(reinterpret_cast<const double2 *>(A.r + c0));
+            const double2 qq = __ldcs(reinterpret_cast<const double2 *>(A.q + c0));
             float tt[6], D;
             fine_coefs(M, red0 ? cd.x : cd.y, i, j, red0 ? k0 : k0 + 1, tt, D);
             double2 rn = rq;
@@ -960,7 +960,7 @@ __device__ __forceinline__ void pass_residual(const PCGArgs &A, int start, int s
             };
             cell(cd.x, k0, rq.x, qq.x, red0, rn.x, r32v.x, zv.x);
             cell(cd.y, k0 + 1, rq.y, qq.y, !red0, rn.y, r32v.y, zv.y);
-            *reinterpret_cast<double2 *>(A.r + c0) = rn;
+            __stcs(reinterpret_cast<double2 *>(A.r + c0), rn);
             *reinterpret_cast<float2 *>(M.r32 + c0) = r32v;
             *reinterpret_cast<float2 *>(z + c0) = zv;
         }
