@@ -680,16 +680,20 @@ struct ClusterGroup {
 // start, start + stride, ... (a persistent group or one item per thread)
 
 // rhs, r = V*rhs on the unknowns, x = 0, d = 0, z = red sweep from 0;
-// acc = {||b||^2 over non-SOLID rows, ||b||^2 over unknowns}
+// acc = {||b||^2 over non-SOLID rows, ||b||^2 over unknowns}.  Warm start
+// (A.warm): x keeps its values (the previous step's pressure) and
+// r = V*(rhs - A x) on the unknowns, A the reference's row (the operator
+// of the direction pass); OUTFLOW values of x do not enter these rows.
 __device__ __forceinline__ void pass_init(const PCGArgs &A, int start, int stride, double (&acc)[2])
 {
     const RoomDev &R = A.R;
     const MGDev &M = A.M;
     float *z = M.lv[0].x;
+    const int n = R.n, plane = R.ny * R.nz, nz = R.nz;
     for (Walk wk(start, stride, R.ny, R.nz, R.n); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
         const unsigned code = R.sc[c];
-        A.x[c] = 0.0;
+        if (!A.warm) A.x[c] = 0.0;
         A.da[c] = 0.0;
         A.db[c] = 0.0;
         double rv = 0.0;
@@ -700,6 +704,15 @@ __device__ __forceinline__ void pass_init(const PCGArgs &A, int start, int strid
             if (active_code(code)) {
                 acc[1] += b * b;
                 rv = b * cell_vol(M, i, j, k);
+                if (A.warm) {
+                    int idx[6];
+                    nb_index(c, plane, nz, n, idx);
+                    double wt[6], diag, o = 0.0;
+                    ref_weights(R, M, code, i, j, k, wt, diag);
+#pragma unroll
+                    for (int a = 0; a < 6; a++) o += wt[a] * A.x[idx[a]];
+                    rv -= cell_vol(M, i, j, k) * (diag * A.x[c] - o);
+                }
                 if (((i + j + k) & 1) == 0) {
                     float tt[6], D;
                     fine_coefs(M, code, i, j, k, tt, D);

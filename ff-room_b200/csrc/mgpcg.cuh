@@ -62,6 +62,7 @@ struct PCGArgs {
     const double *us, *vs, *ws;    // rhs from predicted faces when from_faces
     double rhs_factor;
     int from_faces;
+    int warm;                      // start from x as it is (else from x = 0)
     const double *rhs;
     double *x, *r, *da, *db, *q;
     double *partials;

@@ -1078,6 +1078,9 @@ struct ffr_fluid {
     int split_mode = -1;           // multigrid schedule: -1 split in graphs only, 0 never, 1 always
     SplitHost split_host;          // host pacing of the eager split solve
     HostStage stage;               // page-locked source of the set-up copies
+    bool warm_start = true;        // multigrid solve starts from the previous step's pressure
+    double *p0 = nullptr;          // multigrid: the pressure the last solve started from
+    bool p0_valid = false;         // p0 belongs to the last step (taken by this handle's own launches)
 };
 
 namespace {
@@ -1086,15 +1089,23 @@ namespace {
 // is being captured and the multigrid solve is recorded in its split form
 // (WHILE node); 1 = the stream is being captured (no host-paced launches);
 // 0 = eager launch.
-int enqueue_pressure(ffr_fluid *s, cudaStream_t st, int capture, unsigned *body_kernels)
+int enqueue_pressure(ffr_fluid *s, cudaStream_t st, int capture, unsigned *body_kernels, bool restore = false)
 {
     const ffr_fluid_params &P = s->prm;
+    if (s->mg && s->warm_start) {
+        // the starting pressure of this solve, kept so that a re-solve of the
+        // same system (restore: ffr_fluid_time_pressure) starts from it too
+        const size_t bytes = 8 * (size_t)s->room.g.n;
+        FFR_CUDA(restore ? cudaMemcpyAsync(s->p, s->p0, bytes, cudaMemcpyDeviceToDevice, st)
+                         : cudaMemcpyAsync(s->p0, s->p, bytes, cudaMemcpyDeviceToDevice, st));
+    }
     if (s->mg) {
         PCGArgs pa2{};
         pa2.R = s->R; pa2.M = s->M;
         pa2.us = s->us; pa2.vs = s->vs; pa2.ws = s->ws;
         pa2.rhs_factor = -(P.rho / P.dt);
         pa2.from_faces = 1;
+        pa2.warm = s->warm_start ? 1 : 0;
         pa2.x = s->p; pa2.r = s->r; pa2.da = s->da; pa2.db = s->db; pa2.q = s->ad;
         pa2.partials = s->partials; pa2.gs = s->gs; pa2.sc = s->sc;
         pa2.max_iter = P.poisson_max_iter; pa2.tol = P.poisson_tol;
@@ -1136,6 +1147,7 @@ int fluid_enqueue_step(ffr_fluid *s)
     s->prof.begin(FFR_PROF_PRESSURE, st);
     int rc = enqueue_pressure(s, st, s->capturing_split ? 2 : 0, &s->split_body);
     if (rc) return rc;
+    s->p0_valid = true;
     s->prof.end(st, 1);
     CorrArgs co{P.dt / P.rho};
     s->prof.begin(FFR_PROF_CORRECT, st);
@@ -1256,7 +1268,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     s->blocks_cells = stream_blocks(g.n);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = tables_bytes(s->room) + 2 * (al(8 * g.nu) + al(8 * g.nv) + al(8 * g.nw)) +
-                         7 * al(8 * g.n) + al(8 * std::max<size_t>(s->cg_blocks * 4, 2 * 2368)) + al(8 * s->blocks_cells) +
+                         (s->mg ? 8 : 7) * al(8 * g.n) + al(8 * std::max<size_t>(s->cg_blocks * 4, 2 * 2368)) + al(8 * s->blocks_cells) +
                          al(256) +
                          al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
                          al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (s->mg ? mg_bytes(s->room, s->mgh) : 0);
@@ -1269,6 +1281,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     s->p = a.take<double>(g.n); s->T0 = a.take<double>(g.n); s->T1 = a.take<double>(g.n);
     s->r = a.take<double>(g.n); s->da = a.take<double>(g.n); s->db = a.take<double>(g.n);
     s->ad = a.take<double>(g.n);
+    if (s->mg) s->p0 = a.take<double>(g.n);
     s->partials = a.take<double>(std::max<size_t>(s->cg_blocks * 4, 2 * 2368));
     s->tpart = a.take<double>(s->blocks_cells);
     s->split_state = a.take<char>(256);
@@ -1458,6 +1471,8 @@ int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *i
 {
     if (!s || nrep <= 0 || !ms_per_solve) return fail(FFR_EINVAL, "bad arguments");
     if (s->pending) return fail(FFR_EINVAL, "a queued chunk has not been polled yet");
+    if (s->mg && s->warm_start && !s->p0_valid)
+        return fail(FFR_EINVAL, "no step of this handle's own launches to re-solve (warm-started solve)");
     cudaStream_t st = s->stream;
     FFR_CUDA(cudaStreamSynchronize(st));
     // the solve reads the predicted faces and halt flag of the last step
@@ -1477,7 +1492,7 @@ int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *i
         const bool split = s->mg && s->cluster_ctas == 0 && s->block_override == 0 && s->split_mode != 0;
         if (split && !s->body_stream) FFR_CUDA(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
         FFR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-        rc = enqueue_pressure(s, st, split ? 2 : 1, &body);
+        rc = enqueue_pressure(s, st, split ? 2 : 1, &body, true);
         cudaError_t e = cudaStreamEndCapture(st, &g);
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture(pressure)");
@@ -1493,7 +1508,7 @@ int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *i
         if (ge) {
             FFR_CUDA(cudaGraphLaunch(ge, st));
         } else {
-            rc = enqueue_pressure(s, st, 0, nullptr);
+            rc = enqueue_pressure(s, st, 0, nullptr, true);
         }
     }
     FFR_CUDA(cudaEventRecord(b, st));
@@ -1515,6 +1530,16 @@ int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *i
         count_launch(per_solve * (unsigned)(nrep + 1) - captured);
     }
     return rc;
+}
+
+int ffr_fluid_set_warm_start(ffr_fluid *s, int enable)
+{
+    if (!s) return fail(FFR_EINVAL, "NULL handle");
+    if (s->pending) return fail(FFR_EINVAL, "a queued chunk has not been polled yet");
+    if (s->use_graph || s->graph_exec) return fail(FFR_EINVAL, "choose the start before capturing the step graph");
+    s->warm_start = enable != 0;
+    s->p0_valid = false;
+    return FFR_OK;
 }
 
 int ffr_fluid_set_split(ffr_fluid *s, int mode)
@@ -1727,6 +1752,7 @@ PCGArgs room_pcg_args(ffr_fluid *s)
     a.us = s->us; a.vs = s->vs; a.ws = s->ws;
     a.rhs_factor = -(P.rho / P.dt);
     a.from_faces = 1;
+    a.warm = s->warm_start ? 1 : 0;
     a.x = s->p; a.r = s->r; a.da = s->da; a.db = s->db; a.q = s->ad;
     a.partials = s->partials; a.gs = s->gs; a.sc = s->sc;
     a.max_iter = P.poisson_max_iter; a.tol = P.poisson_tol;
@@ -1895,6 +1921,7 @@ int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge)
         // the batch stream follows everything queued on the room's own stream
         FFR_CUDA(cudaEventRecord(b->ev, s->stream));
         FFR_CUDA(cudaStreamWaitEvent(st, b->ev, 0));
+        s->p0_valid = false;      // batched steps keep no starting pressure
     }
     const int n = (int)b->rooms.size();
     k_b_begin<<<1, 256, 0, st>>>(b->broom, n, stop_on_converge ? 1 : 0);

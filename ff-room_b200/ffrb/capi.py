@@ -137,6 +137,7 @@ def lib():
             "ffr_fluid_set_cluster": ([vp, C.c_int], C.c_int),
             "ffr_fluid_time_pressure": ([vp, C.c_int, _dp, C.POINTER(C.c_int)], C.c_int),
             "ffr_fluid_set_split": ([vp, C.c_int], C.c_int),
+            "ffr_fluid_set_warm_start": ([vp, C.c_int], C.c_int),
             "ffr_fluid_snapshot": ([vp, _dp, _dp, _dp, _dp], C.c_int),
             "ffr_batch_create": ([C.POINTER(vp), C.c_int, C.POINTER(vp)], C.c_int),
             "ffr_batch_destroy": ([vp], C.c_int),
@@ -297,6 +298,10 @@ class FluidHandle:
     def set_split(self, mode: int) -> None:
         """Multigrid schedule: 1 kernel per pass, 0 persistent, -1 split in graphs."""
         check(lib().ffr_fluid_set_split(self.h, mode))
+
+    def set_warm_start(self, enable: bool) -> None:
+        """Multigrid-PCG start: the previous step's pressure (default) or zero."""
+        check(lib().ffr_fluid_set_warm_start(self.h, int(enable)))
 
     def time_pressure(self, nrep: int = 3):
         """(mean ms per pressure solve, iterations) re-solving the last step."""

@@ -189,9 +189,18 @@ int ffr_fluid_device_bytes(ffr_fluid *s, size_t *bytes);
 int ffr_fluid_use_graph(ffr_fluid *s, int enable);
 /* Benchmark aid (no counterpart in the reference): solves the pressure
  * system of the last step again `nrep` times from a pressure-only CUDA graph
- * (the same kernels the step runs, the same result each time) and returns
- * the mean milliseconds per solve and its iteration count. */
+ * (the same kernels the step runs, from the same starting pressure, the
+ * same result each time) and returns the mean milliseconds per solve and its
+ * iteration count.  With a warm-started multigrid solve the last step must
+ * have been taken by this handle's own launches (not by a batch). */
 int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *iterations);
+/* Starting pressure of the multigrid-PCG solve: 1 (default) = the previous
+ * step's pressure, 0 = zero, as PoissonSolver::solve starts
+ * (PoissonSolver.cpp:93-158).  Either way the solve stops on the
+ * reference's ||b - A x|| / ||b|| < tol, so the solution lies within the same
+ * tolerance of the exact one; the warm start needs fewer iterations.  The
+ * plain FP64 CG always starts from zero.  Set before ffr_fluid_use_graph. */
+int ffr_fluid_set_warm_start(ffr_fluid *s, int enable);
 /* Multigrid-PCG schedule (no counterpart in the reference): 1 = one kernel
  * per multigrid pass, also outside graphs (the host paces the iterations and
  * ffr_fluid_enqueue returns only after the last step's solve is queued);

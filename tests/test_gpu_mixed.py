@@ -122,3 +122,54 @@ def test_split_eager_matches_split_graph(name):
     assert np.array_equal(a.get("p"), b.get("p"))
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("name", ["c1_upwind_10", "summer_cooling_10", "oblique_stretch_10", "thermal_small_10",
+                                  "vent_quick_10"])
+def test_warm_start_tracks_reference(name):
+    """The multigrid solve started from the previous step's pressure (the
+    default) and from zero (the reference's start) both stay within the
+    mixed bound of the FP64 fixtures; the first step (zero pressure before
+    it) is bit-identical, and the warm start takes no more iterations."""
+    from ffrb import capi
+    g = Golden(name)
+    p = g.params.with_(poisson="mgpcg", precision="mixed")
+    warm = capi.FluidHandle(g.room, p)
+    cold = capi.FluidHandle(g.room, p)
+    cold.set_warm_start(False)
+    for h in (warm, cold):
+        h.set_split(1)
+    rw, rc = warm.advance(1), cold.advance(1)
+    assert rw[0]["cg_iterations"] == rc[0]["cg_iterations"]
+    for k in "uvwpT":
+        assert np.array_equal(warm.get(k), cold.get(k)), k
+    rw += warm.advance(g.nsteps - 1)
+    rc += cold.advance(g.nsteps - 1)
+    for h in (warm, cold):
+        for k in "uvwpT":
+            err = rel_err(h.get(k), g.fields[k])
+            assert err <= 1e-4, (k, err)
+    assert all(r["pressure_residual"] < g.params.poisson_tol for r in rw if r["cg_iterations"] > 0)
+    assert sum(r["cg_iterations"] for r in rw) <= sum(r["cg_iterations"] for r in rc)
+    warm.close()
+    cold.close()
+
+
+def test_time_pressure_after_batched_step_is_refused():
+    """A warm-started re-solve needs the starting pressure of the last step,
+    which batched steps do not keep."""
+    from ffrb import capi
+    g = Golden("c1_upwind_10")
+    h = capi.FluidHandle(g.room, g.params.with_(poisson="mgpcg", precision="mixed"))
+    h.set_split(1)
+    h.advance(2)
+    ms, it = h.time_pressure(2)
+    assert ms > 0 and it > 0
+    b = capi.BatchHandle([h])
+    b.advance(1)
+    with pytest.raises(capi.FfrError):
+        h.time_pressure(2)
+    b.close()
+    h.advance(1)
+    assert h.time_pressure(1)[1] > 0
+    h.close()
