@@ -65,6 +65,7 @@ struct PCGArgs {
     int warm;                      // start from x as it is (else from x = 0)
     const double *rhs;
     double *x, *r, *da, *db, *q;
+    double *xprev, *x0;            // warm start: the previous solution, the start kept
     double *partials;
     GridSync *gs;
     CGScalars *sc;
@@ -75,6 +76,10 @@ struct PCGArgs {
     int *out_iters;
     int *out_flags;
 };
+// Warm start of the next solve, queued before it: x0 = x + (x - xprev) / 2
+// (x the previous step's solution, xprev the one before) from the room's
+// third step on, x itself before; xprev = x; the start is also kept in a.x0.
+int launch_extrapolate(const PCGArgs &a, cudaStream_t s);
 // Cooperative launch of the whole preconditioned solve.
 int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned override_blocks = 0);
 unsigned pcg_max_blocks();

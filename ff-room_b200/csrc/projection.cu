@@ -1080,6 +1080,7 @@ struct ffr_fluid {
     HostStage stage;               // page-locked source of the set-up copies
     bool warm_start = true;        // multigrid solve starts from the previous step's pressure
     double *p0 = nullptr;          // multigrid: the pressure the last solve started from
+    double *pprev = nullptr;       // multigrid: the solution of the step before the last
     bool p0_valid = false;         // p0 belongs to the last step (taken by this handle's own launches)
 };
 
@@ -1092,13 +1093,6 @@ namespace {
 int enqueue_pressure(ffr_fluid *s, cudaStream_t st, int capture, unsigned *body_kernels, bool restore = false)
 {
     const ffr_fluid_params &P = s->prm;
-    if (s->mg && s->warm_start) {
-        // the starting pressure of this solve, kept so that a re-solve of the
-        // same system (restore: ffr_fluid_time_pressure) starts from it too
-        const size_t bytes = 8 * (size_t)s->room.g.n;
-        FFR_CUDA(restore ? cudaMemcpyAsync(s->p, s->p0, bytes, cudaMemcpyDeviceToDevice, st)
-                         : cudaMemcpyAsync(s->p0, s->p, bytes, cudaMemcpyDeviceToDevice, st));
-    }
     if (s->mg) {
         PCGArgs pa2{};
         pa2.R = s->R; pa2.M = s->M;
@@ -1107,9 +1101,18 @@ int enqueue_pressure(ffr_fluid *s, cudaStream_t st, int capture, unsigned *body_
         pa2.from_faces = 1;
         pa2.warm = s->warm_start ? 1 : 0;
         pa2.x = s->p; pa2.r = s->r; pa2.da = s->da; pa2.db = s->db; pa2.q = s->ad;
+        pa2.xprev = s->pprev; pa2.x0 = s->p0;
         pa2.partials = s->partials; pa2.gs = s->gs; pa2.sc = s->sc;
         pa2.max_iter = P.poisson_max_iter; pa2.tol = P.poisson_tol;
         pa2.st = s->st;
+        if (s->warm_start) {
+            // the start of this solve; a re-solve of the same system
+            // (restore: ffr_fluid_time_pressure) starts from the kept copy
+            if (restore)
+                FFR_CUDA(cudaMemcpyAsync(s->p, s->p0, 8 * (size_t)s->room.g.n, cudaMemcpyDeviceToDevice, st));
+            else if (int rc = launch_extrapolate(pa2, st))
+                return rc;
+        }
         const bool plain_grid = s->cluster_ctas == 0 && s->block_override == 0;
         if (capture == 2) return capture_split_pcg(pa2, s->split_state, st, s->body_stream, body_kernels);
         if (capture == 0 && plain_grid && s->split_mode == 1)
@@ -1268,7 +1271,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     s->blocks_cells = stream_blocks(g.n);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = tables_bytes(s->room) + 2 * (al(8 * g.nu) + al(8 * g.nv) + al(8 * g.nw)) +
-                         (s->mg ? 8 : 7) * al(8 * g.n) + al(8 * std::max<size_t>(s->cg_blocks * 4, 2 * 2368)) + al(8 * s->blocks_cells) +
+                         (s->mg ? 9 : 7) * al(8 * g.n) + al(8 * std::max<size_t>(s->cg_blocks * 4, 2 * 2368)) + al(8 * s->blocks_cells) +
                          al(256) +
                          al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
                          al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (s->mg ? mg_bytes(s->room, s->mgh) : 0);
@@ -1281,7 +1284,10 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     s->p = a.take<double>(g.n); s->T0 = a.take<double>(g.n); s->T1 = a.take<double>(g.n);
     s->r = a.take<double>(g.n); s->da = a.take<double>(g.n); s->db = a.take<double>(g.n);
     s->ad = a.take<double>(g.n);
-    if (s->mg) s->p0 = a.take<double>(g.n);
+    if (s->mg) {
+        s->p0 = a.take<double>(g.n);
+        s->pprev = a.take<double>(g.n);
+    }
     s->partials = a.take<double>(std::max<size_t>(s->cg_blocks * 4, 2 * 2368));
     s->tpart = a.take<double>(s->blocks_cells);
     s->split_state = a.take<char>(256);
@@ -1343,6 +1349,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
     if (rc) { ffr_fluid_destroy(s); return rc; }
     FFR_CUDA(cudaMemsetAsync(s->st, 0, sizeof(StepState), st));
     FFR_CUDA(cudaMemsetAsync(s->split_state, 0, 256, st));
+    if (s->mg) FFR_CUDA(cudaMemsetAsync(s->pprev, 0, 8 * g.n, st));
     k_fill<<<stream_blocks(g.n), kThreads, 0, st>>>(s->T0, (int)g.n, params->T_initial);
     FFR_LAUNCHED(1);
     if (params->thermal) {
@@ -1754,6 +1761,7 @@ PCGArgs room_pcg_args(ffr_fluid *s)
     a.from_faces = 1;
     a.warm = s->warm_start ? 1 : 0;
     a.x = s->p; a.r = s->r; a.da = s->da; a.db = s->db; a.q = s->ad;
+    a.xprev = s->pprev; a.x0 = s->p0;
     a.partials = s->partials; a.gs = s->gs; a.sc = s->sc;
     a.max_iter = P.poisson_max_iter; a.tol = P.poisson_tol;
     a.st = s->st;

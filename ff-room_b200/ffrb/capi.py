@@ -300,7 +300,7 @@ class FluidHandle:
         check(lib().ffr_fluid_set_split(self.h, mode))
 
     def set_warm_start(self, enable: bool) -> None:
-        """Multigrid-PCG start: the previous step's pressure (default) or zero."""
+        """Multigrid-PCG start: extrapolated from the last two pressures (default) or zero."""
         check(lib().ffr_fluid_set_warm_start(self.h, int(enable)))
 
     def time_pressure(self, nrep: int = 3):
