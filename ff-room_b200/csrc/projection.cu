@@ -59,6 +59,36 @@ __device__ __forceinline__ F adv_lw(F pm, F pc, F pp, F a, F dt, F h)
     return (flr - fll) / h;
 }
 
+// The three schemes with the reciprocal spacing ih = 1/h (mixed precision).
+template <class F>
+__device__ __forceinline__ F adv_up_r(F pm, F pc, F pp, F a, F ih)
+{
+    return (a > F(0)) ? a * (pc - pm) * ih : a * (pp - pc) * ih;
+}
+
+template <class F>
+__device__ __forceinline__ F adv_quick_r(F pmm, F pm, F pc, F pp, F a, F ih)
+{
+    F fr, fl;
+    if (a >= F(0)) {
+        fr = (F(6) * pc + F(3) * pp - pm) * F(0.125);
+        fl = (F(6) * pm + F(3) * pc - pmm) * F(0.125);
+    } else {
+        fr = (F(6) * pp + F(3) * pc - pmm) * F(0.125);
+        fl = (F(6) * pc + F(3) * pp - pm) * F(0.125);
+    }
+    return a * (fr - fl) * ih;
+}
+
+template <class F>
+__device__ __forceinline__ F adv_lw_r(F pm, F pc, F pp, F a, F dt, F ih)
+{
+    const F cr = a * dt * ih;
+    const F flr = a * (F(0.5) * (pc + pp) - F(0.5) * cr * (pp - pc));
+    const F fll = a * (F(0.5) * (pm + pc) - F(0.5) * cr * (pc - pm));
+    return (flr - fll) * ih;
+}
+
 // The predicted increment dt*(-adv + dif) of one face from its stencil
 // values (FluidSolver.cpp:132-162), in arithmetic F.  ax is the advecting
 // velocity along x for this face, etc.; scheme 1 = QUICK (the caller has
@@ -67,6 +97,23 @@ template <class F>
 __device__ __forceinline__ F face_increment(int use_quick, int lw, F c, F xmm, F xm, F xp, F ymm, F ym, F yp,
                                             F zmm, F zm, F zp, F ax, F ay, F az, F hx, F hy, F hz, F nu, F dt)
 {
+    if constexpr (sizeof(F) == 4) {
+        // mixed precision: one correctly rounded reciprocal per axis and
+        // products in place of the six divisions (well inside the mixed bound)
+        const F ix = __frcp_rn(hx), iy = __frcp_rn(hy), iz = __frcp_rn(hz);
+        F adv;
+        if (use_quick) {
+            adv = adv_quick_r(xmm, xm, c, xp, ax, ix) + adv_quick_r(ymm, ym, c, yp, ay, iy) +
+                  adv_quick_r(zmm, zm, c, zp, az, iz);
+        } else if (lw) {
+            adv = adv_lw_r(xm, c, xp, ax, dt, ix) + adv_lw_r(ym, c, yp, ay, dt, iy) + adv_lw_r(zm, c, zp, az, dt, iz);
+        } else {
+            adv = adv_up_r(xm, c, xp, ax, ix) + adv_up_r(ym, c, yp, ay, iy) + adv_up_r(zm, c, zp, az, iz);
+        }
+        const F dif = nu * ((ix * ix) * (xm - F(2) * c + xp) + (iy * iy) * (ym - F(2) * c + yp) +
+                            (iz * iz) * (zm - F(2) * c + zp));
+        return dt * (-adv + dif);
+    }
     F adv;
     if (use_quick) {
         adv = adv_quick(xmm, xm, c, xp, ax, hx) + adv_quick(ymm, ym, c, yp, ay, hy) + adv_quick(zmm, zm, c, zp, az, hz);
@@ -120,104 +167,111 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
     // as in the reference); the advecting-velocity pairs are always inside
     // for an interior face.
     const int pu = ny * nz, lastu = R.nu - 1;
-    for (Walk wk(start, stride, ny, nz, R.nu); wk.ok(); wk.next()) {
-        const int t = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        const uint8_t code = R.fcu[t];
-        double val = u[t];
-        if (i > 0 && i < nx) {
-            const double uc = val;
-            const double xm0 = u[max(t - pu, 0)], xp0 = u[min(t + pu, lastu)];
-            const double ym0 = u[max(t - nz, 0)], yp0 = u[min(t + nz, lastu)];
-            const double zm0 = u[max(t - 1, 0)], zp0 = u[min(t + 1, lastu)];
-            const double v0 = v[VIX(i - 1, j, k)], v1 = v[VIX(i, j, k)];
-            const double w0 = w[WIX(i - 1, j, k)], w1 = w[WIX(i, j, k)];
-            const int q = quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
-            // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1
-            // (k=1) they fall into the previous row of the flat array
-            double xmm = 0.0, ymm = 0.0, zmm = 0.0;
-            if (quick) {
-                const double a = u[max(t - 2 * pu, 0)], b = u[max(t - 2 * nz, 0)], c = u[max(t - 2, 0)];
-                xmm = q ? a : 0.0; ymm = q ? b : 0.0; zmm = q ? c : 0.0;
-            }
-            const double xm = (i > 1) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
-            const double av = (j > 0 && j < ny) ? 0.5 * (v0 + v1) : 0.0;
-            const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
-            const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
-            const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
-            val = uc + (double)face_increment<F>(q, lw, F(uc), F(xmm), F(xm), F(xp), F(ymm), F(ym), F(yp),
-                                                 F(zmm), F(zm), F(zp), F(uc), F(av), F(aw), F(R.dxv[i]),
-                                                 F(R.dyv[j]), F(R.dzv[k]), nu, dt);
-        }
-        us[t] = face_code(code, val, R.fanvel, 0);
-    }
     const int pv = (ny + 1) * nz, lastv = R.nv - 1;
-    for (Walk wk(start, stride, ny + 1, nz, R.nv); wk.ok(); wk.next()) {
-        const int f = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        const uint8_t code = R.fcv[f];
-        double val = v[f];
-        if (j > 0 && j < ny) {
-            const double vc = val;
-            const double u0 = u[UIX(i, j - 1, k)], u1 = u[UIX(i, j, k)];
-            const double xm0 = v[max(f - pv, 0)], xp0 = v[min(f + pv, lastv)];
-            const double ym0 = v[max(f - nz, 0)], yp0 = v[min(f + nz, lastv)];
-            const double w0 = w[WIX(i, j - 1, k)], w1 = w[WIX(i, j, k)];
-            const double zm0 = v[max(f - 1, 0)], zp0 = v[min(f + 1, lastv)];
-            const int q = quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2;
-            // v's x and z "far" neighbours are the near ones
-            // (FluidSolver.cpp:208,211)
-            double ymm = 0.0;
-            if (quick) {
-                const double a = v[max(f - 2 * nz, 0)];
-                ymm = q ? a : 0.0;
-            }
-            const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
-            const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
-            const double ym = (j > 1) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
-            const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
-            const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
-            val = vc + (double)face_increment<F>(q, lw, F(vc), F(xm), F(xm), F(xp), F(ymm), F(ym), F(yp),
-                                                 F(zm), F(zm), F(zp), F(au), F(vc), F(aw), F(R.dxv[i]),
-                                                 F(R.dyv[j]), F(R.dzv[k]), nu, dt);
-        }
-        vs[f] = face_code(code, val, R.fanvel, 1);
-    }
     const int pw = ny * (nz + 1), lastw = R.nw - 1;
-    for (Walk wk(start, stride, ny, nz + 1, R.nw); wk.ok(); wk.next()) {
-        const int f = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        const uint8_t code = R.fcw[f];
-        double val = w[f];
-        if (k > 0 && k < nz) {
-            const double wc = val;
-            const double u0 = u[UIX(i, j, k - 1)], u1 = u[UIX(i, j, k)];
-            const double xm0 = w[max(f - pw, 0)], xp0 = w[min(f + pw, lastw)];
-            const double v0 = v[VIX(i, j, k - 1)], v1 = v[VIX(i, j, k)];
-            const double ym0 = w[max(f - (nz + 1), 0)], yp0 = w[min(f + (nz + 1), lastw)];
-            const double zm0 = w[max(f - 1, 0)], zp0 = w[min(f + 1, lastw)];
-            double tb = 0.0, tc = 0.0;
-            if (A.buoyancy) {
-                const int c = UIX(i, j, k);
-                tb = T[c - 1];
-                tc = T[c];
+    // One pass over the corners (i, j, k) of the extended grid
+    // (nx+1)(ny+1)(nz+1): the u, v and w faces with that lower corner, so the
+    // three components are streamed once between them (three passes, one
+    // per component, each re-read the other two after L2 had dropped them).
+    for (Walk wk(start, stride, ny + 1, nz + 1, (nx + 1) * (ny + 1) * (nz + 1)); wk.ok(); wk.next()) {
+        const int i = wk.i, j = wk.j, k = wk.k;
+        if (j < ny && k < nz) {
+            const int t = UIX(i, j, k);
+            const uint8_t code = R.fcu[t];
+            double val = u[t];
+            if (i > 0 && i < nx) {
+                const double uc = val;
+                const double xm0 = u[max(t - pu, 0)], xp0 = u[min(t + pu, lastu)];
+                const double ym0 = u[max(t - nz, 0)], yp0 = u[min(t + nz, lastu)];
+                const double zm0 = u[max(t - 1, 0)], zp0 = u[min(t + 1, lastu)];
+                const double v0 = v[VIX(i - 1, j, k)], v1 = v[VIX(i, j, k)];
+                const double w0 = w[WIX(i - 1, j, k)], w1 = w[WIX(i, j, k)];
+                const int q = quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+                // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1
+                // (k=1) they fall into the previous row of the flat array
+                double xmm = 0.0, ymm = 0.0, zmm = 0.0;
+                if (quick) {
+                    const double a = u[max(t - 2 * pu, 0)], b = u[max(t - 2 * nz, 0)], c = u[max(t - 2, 0)];
+                    xmm = q ? a : 0.0; ymm = q ? b : 0.0; zmm = q ? c : 0.0;
+                }
+                const double xm = (i > 1) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+                const double av = (j > 0 && j < ny) ? 0.5 * (v0 + v1) : 0.0;
+                const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+                const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
+                const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+                val = uc + (double)face_increment<F>(q, lw, F(uc), F(xmm), F(xm), F(xp), F(ymm), F(ym), F(yp),
+                                                     F(zmm), F(zm), F(zp), F(uc), F(av), F(aw), F(R.dxv[i]),
+                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
             }
-            const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2;
-            // w's x and y "far" neighbours are the near ones
-            // (FluidSolver.cpp:275-276)
-            double zmm = 0.0;
-            if (quick) {
-                const double a = w[max(f - 2, 0)];
-                zmm = q ? a : 0.0;
-            }
-            const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
-            const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
-            const double av = (j > 0) ? 0.5 * (v0 + v1) : 0.0;
-            const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
-            const double zm = (k > 1) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
-            val = wc + (double)face_increment<F>(q, lw, F(wc), F(xm), F(xm), F(xp), F(ym), F(ym), F(yp),
-                                                 F(zmm), F(zm), F(zp), F(au), F(av), F(wc), F(R.dxv[i]),
-                                                 F(R.dyv[j]), F(R.dzv[k]), nu, dt);
-            if (A.buoyancy) val += (double)(F(A.bcoeff) * (F(0.5) * (F(tb) + F(tc)) - F(A.T_ref)));
+            us[t] = face_code(code, val, R.fanvel, 0);
         }
-        ws[f] = face_code(code, val, R.fanvel, 2);
+        if (i < nx && k < nz) {
+            const int f = VIX(i, j, k);
+            const uint8_t code = R.fcv[f];
+            double val = v[f];
+            if (j > 0 && j < ny) {
+                const double vc = val;
+                const double u0 = u[UIX(i, j - 1, k)], u1 = u[UIX(i, j, k)];
+                const double xm0 = v[max(f - pv, 0)], xp0 = v[min(f + pv, lastv)];
+                const double ym0 = v[max(f - nz, 0)], yp0 = v[min(f + nz, lastv)];
+                const double w0 = w[WIX(i, j - 1, k)], w1 = w[WIX(i, j, k)];
+                const double zm0 = v[max(f - 1, 0)], zp0 = v[min(f + 1, lastv)];
+                const int q = quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+                // v's x and z "far" neighbours are the near ones
+                // (FluidSolver.cpp:208,211)
+                double ymm = 0.0;
+                if (quick) {
+                    const double a = v[max(f - 2 * nz, 0)];
+                    ymm = q ? a : 0.0;
+                }
+                const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
+                const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+                const double ym = (j > 1) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+                const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
+                const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+                val = vc + (double)face_increment<F>(q, lw, F(vc), F(xm), F(xm), F(xp), F(ymm), F(ym), F(yp),
+                                                     F(zm), F(zm), F(zp), F(au), F(vc), F(aw), F(R.dxv[i]),
+                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
+            }
+            vs[f] = face_code(code, val, R.fanvel, 1);
+        }
+        if (i < nx && j < ny) {
+            const int f = WIX(i, j, k);
+            const uint8_t code = R.fcw[f];
+            double val = w[f];
+            if (k > 0 && k < nz) {
+                const double wc = val;
+                const double u0 = u[UIX(i, j, k - 1)], u1 = u[UIX(i, j, k)];
+                const double xm0 = w[max(f - pw, 0)], xp0 = w[min(f + pw, lastw)];
+                const double v0 = v[VIX(i, j, k - 1)], v1 = v[VIX(i, j, k)];
+                const double ym0 = w[max(f - (nz + 1), 0)], yp0 = w[min(f + (nz + 1), lastw)];
+                const double zm0 = w[max(f - 1, 0)], zp0 = w[min(f + 1, lastw)];
+                double tb = 0.0, tc = 0.0;
+                if (A.buoyancy) {
+                    const int c = UIX(i, j, k);
+                    tb = T[c - 1];
+                    tc = T[c];
+                }
+                const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2;
+                // w's x and y "far" neighbours are the near ones
+                // (FluidSolver.cpp:275-276)
+                double zmm = 0.0;
+                if (quick) {
+                    const double a = w[max(f - 2, 0)];
+                    zmm = q ? a : 0.0;
+                }
+                const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
+                const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+                const double av = (j > 0) ? 0.5 * (v0 + v1) : 0.0;
+                const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+                const double zm = (k > 1) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+                val = wc + (double)face_increment<F>(q, lw, F(wc), F(xm), F(xm), F(xp), F(ym), F(ym), F(yp),
+                                                     F(zmm), F(zm), F(zp), F(au), F(av), F(wc), F(R.dxv[i]),
+                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
+                if (A.buoyancy) val += (double)(F(A.bcoeff) * (F(0.5) * (F(tb) + F(tc)) - F(A.T_ref)));
+            }
+            ws[f] = face_code(code, val, R.fanvel, 2);
+        }
     }
 }
 
@@ -627,20 +681,39 @@ __device__ __forceinline__ void advect_T_body(const RoomDev &R, const ThermArgs 
         const double xmm = q ? tat(i - 2, j, k) : 0.0, ymm = q ? tat(i, j - 2, k) : 0.0,
                      zmm = q ? tat(i, j, k - 2) : 0.0;
         const F hx = F(R.dxv[i]), hy = F(R.dyv[j]), hz = F(R.dzv[k]), dt = F(A.dt);
-        F adv;
-        if (q) {
-            adv = adv_quick(F(xmm), F(xm), F(tc), F(xp), F(ac), hx) + adv_quick(F(ymm), F(ym), F(tc), F(yp), F(bc), hy)
-                + adv_quick(F(zmm), F(zm), F(tc), F(zp), F(cc), hz);
-        } else if (lw) {
-            adv = adv_lw(F(xm), F(tc), F(xp), F(ac), dt, hx) + adv_lw(F(ym), F(tc), F(yp), F(bc), dt, hy)
-                + adv_lw(F(zm), F(tc), F(zp), F(cc), dt, hz);
-        } else {
-            adv = adv_up(F(xm), F(tc), F(xp), F(ac), hx) + adv_up(F(ym), F(tc), F(yp), F(bc), hy)
-                + adv_up(F(zm), F(tc), F(zp), F(cc), hz);
-        }
+        F adv, dif;
         const F ftc = F(tc);
-        const F dif = F(A.alpha) * ((F(xm) - F(2) * ftc + F(xp)) / (hx * hx) + (F(ym) - F(2) * ftc + F(yp)) / (hy * hy)
-                                    + (F(zm) - F(2) * ftc + F(zp)) / (hz * hz));
+        if constexpr (sizeof(F) == 4) {
+            // mixed precision: reciprocal spacings in place of the divisions
+            const F ix = __frcp_rn(hx), iy = __frcp_rn(hy), iz = __frcp_rn(hz);
+            if (q) {
+                adv = adv_quick_r(F(xmm), F(xm), ftc, F(xp), F(ac), ix) +
+                      adv_quick_r(F(ymm), F(ym), ftc, F(yp), F(bc), iy) +
+                      adv_quick_r(F(zmm), F(zm), ftc, F(zp), F(cc), iz);
+            } else if (lw) {
+                adv = adv_lw_r(F(xm), ftc, F(xp), F(ac), dt, ix) + adv_lw_r(F(ym), ftc, F(yp), F(bc), dt, iy) +
+                      adv_lw_r(F(zm), ftc, F(zp), F(cc), dt, iz);
+            } else {
+                adv = adv_up_r(F(xm), ftc, F(xp), F(ac), ix) + adv_up_r(F(ym), ftc, F(yp), F(bc), iy) +
+                      adv_up_r(F(zm), ftc, F(zp), F(cc), iz);
+            }
+            dif = F(A.alpha) * ((F(xm) - F(2) * ftc + F(xp)) * (ix * ix) + (F(ym) - F(2) * ftc + F(yp)) * (iy * iy) +
+                                (F(zm) - F(2) * ftc + F(zp)) * (iz * iz));
+        } else {
+            if (q) {
+                adv = adv_quick(F(xmm), F(xm), F(tc), F(xp), F(ac), hx) +
+                      adv_quick(F(ymm), F(ym), F(tc), F(yp), F(bc), hy) +
+                      adv_quick(F(zmm), F(zm), F(tc), F(zp), F(cc), hz);
+            } else if (lw) {
+                adv = adv_lw(F(xm), F(tc), F(xp), F(ac), dt, hx) + adv_lw(F(ym), F(tc), F(yp), F(bc), dt, hy) +
+                      adv_lw(F(zm), F(tc), F(zp), F(cc), dt, hz);
+            } else {
+                adv = adv_up(F(xm), F(tc), F(xp), F(ac), hx) + adv_up(F(ym), F(tc), F(yp), F(bc), hy) +
+                      adv_up(F(zm), F(tc), F(zp), F(cc), hz);
+            }
+            dif = F(A.alpha) * ((F(xm) - F(2) * ftc + F(xp)) / (hx * hx) + (F(ym) - F(2) * ftc + F(yp)) / (hy * hy) +
+                                (F(zm) - F(2) * ftc + F(zp)) / (hz * hz));
+        }
         const double tn = tc + (double)(dt * (-adv + dif));
         Tn[c] = tn;
         sum += tn;

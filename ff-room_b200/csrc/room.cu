@@ -252,7 +252,8 @@ int load_room(const ffr_room_desc *d, HostRoom &r)
     if (d->nx <= 0 || d->ny <= 0 || d->nz <= 0)
         return fail(FFR_EINVAL, "Grid dimensions must be positive");
     const long long n = (long long)d->nx * d->ny * d->nz;
-    if (n > (1ll << 31) - 1 - 4ll * d->nx * d->ny)
+    if (n > (1ll << 31) - 1 - 4ll * d->nx * d->ny ||
+        (long long)(d->nx + 1) * (d->ny + 1) * (d->nz + 1) > (1ll << 31) - 1)
         return fail(FFR_ERANGE, "grid too large for 32-bit face indexing");
     if (!d->dxv || !d->dyv || !d->dzv || !d->cell_type)
         return fail(FFR_EINVAL, "room spacing or cell_type pointer is NULL");
