@@ -166,6 +166,8 @@ def run_ours(args, rank: int, world: int, dist):
     if kind == "fluid":
         h = capi.FluidHandle(room, params)
         h.set_split(args.split)
+        if not args.warm_start and getattr(params, "poisson", "") == "mgpcg":
+            h.set_warm_start(False)
         if args.graph:
             h.use_graph(True)
     else:
@@ -263,6 +265,8 @@ def run_e2e(args, kind, room, params):
     if kind == "fluid":
         h = capi.FluidHandle(room, params, init)
         h.set_split(args.split)
+        if not args.warm_start and getattr(params, "poisson", "") == "mgpcg":
+            h.set_warm_start(False)
         if args.graph:
             h.use_graph(True)
         recs = h.advance(args.steps)
@@ -346,7 +350,9 @@ def config_of(args, room, kind, params):
     if kind == "fluid":
         c.update({"precision": params.precision, "poisson": params.poisson, "poisson_tol": params.poisson_tol,
                   "dt": params.dt, "advection": params.advection, "thermal": params.thermal,
-                  "buoyancy": params.buoyancy})
+                  "buoyancy": params.buoyancy,
+                  "pressure_start": ("extrapolated previous pressures" if args.warm_start and params.poisson == "mgpcg"
+                                     else "zero")})
     else:
         c.update(params)
     return c
@@ -372,7 +378,8 @@ def serving_requests(kind: str, n: int, max_cells: int, max_steps: int):
     return requests_from_configs(rooms, [params_from_scene(c) for c in rooms], [0.0] * len(rooms), max_steps)
 
 
-def run_serving(kind: str, n: int, max_cells: int, max_steps: int, batched: bool = True, chunk: int = 10):
+def run_serving(kind: str, n: int, max_cells: int, max_steps: int, batched: bool = True, chunk: int = 10,
+                warm_start: bool = True):
     """The serving sample through the continuous-batching server: batched
     (every active room in one launch per stage, rooms joining and leaving
     between chunks) or one stream per room with tuned schedules."""
@@ -381,7 +388,8 @@ def run_serving(kind: str, n: int, max_cells: int, max_steps: int, batched: bool
     reqs = serving_requests(kind, n, max_cells, max_steps)
     tuner = Tuner()   # default schedules: one 16-block cluster per room up to 1 M cells
     free, total = torch.cuda.mem_get_info()
-    srv = Server(mem_budget=int(free * 0.6), max_active=64, tuner=tuner, batched=batched, chunk=chunk)
+    srv = Server(mem_budget=int(free * 0.6), max_active=64, tuner=tuner, batched=batched, chunk=chunk,
+                 warm_start=warm_start)
     # untimed warm-up of both arms on a few short requests (module loading,
     # memory-pool growth, pinned-buffer cache)
     warm = [Request(r.rid, 0.0, r.room, r.params, 2) for r in reqs[:4]]
@@ -410,12 +418,14 @@ def run_serving(kind: str, n: int, max_cells: int, max_steps: int, batched: bool
 def serving_arm(args):
     import torch
     torch.cuda.set_device(0)
-    rep = run_serving(args.workload, args.requests, args.max_cells, args.max_steps, bool(args.batched), args.chunk)
+    rep = run_serving(args.workload, args.requests, args.max_cells, args.max_steps, bool(args.batched), args.chunk,
+                      bool(args.warm_start))
     line = {"metric": METRIC, "value": rep["room_solves_per_s"], "unit": "room-solves/s", "n_gpus": 1,
             "steps": args.max_steps, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
             "config": {"workload": args.workload, "requests": rep["requests"], "max_cells": args.max_cells,
-                       "max_steps": args.max_steps, "precision": "mixed", "poisson": "mgpcg"},
+                       "max_steps": args.max_steps, "precision": "mixed", "poisson": "mgpcg",
+                       "pressure_start": "extrapolated previous pressures" if args.warm_start else "zero"},
             "serving": rep, "gpu_launches": rep["gpu_launches"], "clocks": rep["clocks"]}
     print(json.dumps(line))
 
@@ -442,6 +452,8 @@ def main():
     ap.add_argument("--chunk", type=int, default=10, help="serving/batch: steps between membership changes")
     ap.add_argument("--graph", type=int, default=1,
                     help="replay each step as a CUDA graph (the multigrid solve then runs one kernel per pass)")
+    ap.add_argument("--warm-start", type=int, default=1, choices=[0, 1],
+                    help="multigrid solve from the extrapolated previous pressures (1) or from zero (0)")
     ap.add_argument("--split", type=int, default=-1, choices=[-1, 0, 1],
                     help="multigrid schedule: 1 one kernel per pass (host-paced outside graphs), "
                          "0 one persistent kernel, -1 split in graphs only")
@@ -474,8 +486,8 @@ def main():
         dtype = {"fp64": "f64", "mixed": "f32/f64", "fp32": "f32", "fp16": "f16/f32"}.get(args.precision, args.precision)
         serving = None
         if not args.no_serving and args.workload == "large_thermal" and world == 1:
-            serving = run_serving("serving", 48, 600_000, 40, batched=False)
-            alt = run_serving("serving", 48, 600_000, 40, batched=True)
+            serving = run_serving("serving", 48, 600_000, 40, batched=False, warm_start=bool(args.warm_start))
+            alt = run_serving("serving", 48, 600_000, 40, batched=True, warm_start=bool(args.warm_start))
             serving["batched_mode"] = {k: alt[k] for k in ("room_solves_per_s", "p50_s", "p99_s",
                                                           "speedup_vs_serial_fp64", "gpu_launches")}
         line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,

@@ -172,12 +172,15 @@ class Outcome:
 
 
 class _Active:
-    def __init__(self, req: Request, sched: Schedule, t_admit: float, keep_fields: bool, split: int = -1):
+    def __init__(self, req: Request, sched: Schedule, t_admit: float, keep_fields: bool, split: int = -1,
+                 warm_start: bool = True):
         self.req = req
         self.sched = sched
         self.t_admit = t_admit
         self.keep_fields = keep_fields
         self.h = capi.FluidHandle(req.room, req.params)
+        if not warm_start and req.params.poisson == "mgpcg":
+            self.h.set_warm_start(False)
         if split != -1:
             self.h.set_split(split)
         else:
@@ -214,13 +217,14 @@ class Server:
     in chunks of `chunk` steps; rooms join and leave between chunks."""
 
     def __init__(self, mem_budget: int, max_active: int = 64, tuner: Optional[Tuner] = None,
-                 keep_fields: bool = False, batched: bool = False, chunk: int = 10):
+                 keep_fields: bool = False, batched: bool = False, chunk: int = 10, warm_start: bool = True):
         self.mem_budget = mem_budget
         self.max_active = max_active
         self.tuner = tuner or Tuner()
         self.keep_fields = keep_fields
         self.batched = batched
         self.chunk = chunk
+        self.warm_start = warm_start
 
     def run(self, requests: List[Request], realtime: bool = True) -> List[Outcome]:
         if self.batched:
@@ -256,7 +260,8 @@ class Server:
                 need = estimate_bytes(req.room, req.params)
                 if active and used + need > self.mem_budget:
                     break
-                a = _Active(req, Schedule(0, self.chunk, False, 0), now, self.keep_fields, split=1)
+                a = _Active(req, Schedule(0, self.chunk, False, 0), now, self.keep_fields, split=1,
+                            warm_start=self.warm_start)
                 a.charge = need
                 used += need
                 active.append(a)
@@ -306,7 +311,7 @@ class Server:
                 need = estimate_bytes(req.room, req.params)
                 if active and used + need > self.mem_budget:
                     break
-                a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields)
+                a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields, warm_start=self.warm_start)
                 a.charge = need
                 used += need
                 a.launch()
