@@ -145,7 +145,11 @@ typedef struct ffr_fluid ffr_fluid;
 
 /* FluidSolver::FluidSolver (cpp/src/core/FluidSolver.cpp:18-32): uploads the
  * room and the initial fields, sets T := T_initial and, when thermal,
- * applies the opening temperature BC. */
+ * applies the opening temperature BC.  The cell types and fields are copied
+ * before it returns; the tables derived from them (stencil and face codes,
+ * multigrid coefficients) are built by kernels queued on the handle's
+ * stream, which every later call on the handle follows, so a server
+ * creating rooms never waits for a busy GPU here. */
 int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
                      const ffr_fields *init, ffr_fluid **out);
 int ffr_fluid_destroy(ffr_fluid *s);
