@@ -749,16 +749,18 @@ struct CellPair {
 
 // Warm-start extrapolation (see launch_extrapolate): elementwise, so every
 // launch shape gives the same values.  The state of a halted room is kept.
-// Half a step of linear extrapolation: through the early transient of the
-// rooms measured it starts several times closer to the solution than the
-// previous pressure, and closer than a full step until the flow settles.
+// Half a step of linear extrapolation through a room's first ten steps (the
+// early transient, where it starts several times closer to the solution
+// than the previous pressure and than a full step), a full step after that
+// (closer than half a step once the flow evolves smoothly).
 __device__ __forceinline__ void pass_extrapolate(const PCGArgs &A, int start, int stride)
 {
     if (!A.warm || (A.st && A.st->halt)) return;
-    const bool ex = A.st && A.st->step >= 2;
+    const int step = A.st ? A.st->step : 0;
+    const double theta = step >= 10 ? 1.0 : (step >= 2 ? 0.5 : 0.0);
     for (int c = start; c < A.R.n; c += stride) {
         const double a = __ldcs(A.x + c), b = __ldcs(A.xprev + c);
-        const double x0 = ex ? a + 0.5 * (a - b) : a;
+        const double x0 = a + theta * (a - b);
         __stcs(A.x + c, x0);
         __stcs(A.xprev + c, a);
         __stcs(A.x0 + c, x0);

@@ -76,9 +76,10 @@ struct PCGArgs {
     int *out_iters;
     int *out_flags;
 };
-// Warm start of the next solve, queued before it: x0 = x + (x - xprev) / 2
-// (x the previous step's solution, xprev the one before) from the room's
-// third step on, x itself before; xprev = x; the start is also kept in a.x0.
+// Warm start of the next solve, queued before it: x0 = x + theta (x - xprev)
+// (x the previous step's solution, xprev the one before; theta 0 on a
+// room's first two steps, 1/2 up to its tenth, 1 after); xprev = x; the
+// start is also kept in a.x0.
 int launch_extrapolate(const PCGArgs &a, cudaStream_t s);
 // Cooperative launch of the whole preconditioned solve.
 int launch_pcg(const PCGArgs &a, cudaStream_t s, unsigned *blocks_used, unsigned override_blocks = 0);

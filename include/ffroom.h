@@ -198,9 +198,10 @@ int ffr_fluid_use_graph(ffr_fluid *s, int enable);
  * iteration count.  With a warm-started multigrid solve the last step must
  * have been taken by this handle's own launches (not by a batch). */
 int ffr_fluid_time_pressure(ffr_fluid *s, int nrep, double *ms_per_solve, int *iterations);
-/* Starting pressure of the multigrid-PCG solve: 1 (default) = half a step
- * of linear extrapolation of the last two pressures (the previous pressure
- * on a room's first two steps), 0 = zero, as PoissonSolver::solve starts
+/* Starting pressure of the multigrid-PCG solve: 1 (default) = linear
+ * extrapolation of the last two pressures (half a step through a room's
+ * first ten steps, a full step after; the previous pressure on its first
+ * two steps), 0 = zero, as PoissonSolver::solve starts
  * (PoissonSolver.cpp:93-158).  Either way the solve stops on the
  * reference's ||b - A x|| / ||b|| < tol, so the solution lies within the same
  * tolerance of the exact one; the warm start needs fewer iterations.  The
