@@ -2,7 +2,7 @@
 
 The golden fixtures come from the compiled reference (tests/golden/
 make_golden.py).  The oracle must reproduce every field and every step
-result, including the CG iteration counts, before it may judge the GPU.
+result, including the CG iteration counts, before it may check the GPU.
 Tolerances: 1e-11 max-norm relative for short runs (only the FMA contraction
 of the reference's -O3 build differs), 1e-8 for the 500-step run.
 """
