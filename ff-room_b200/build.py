@@ -19,7 +19,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INC = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-CUDA_SOURCES = ["room.cu", "projection.cu", "mgpcg.cu", "lbm.cu", "noalloc.cu"]
+CUDA_SOURCES = ["room.cu", "projection.cu", "mgpcg.cu", "lbm.cu", "noalloc.cu", "server.cu"]
 HEADERS = ["common.cuh", "projection.cuh", "mgpcg.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1114,6 +1114,24 @@ int launch_cg(const CGArgs &a, unsigned blocks, cudaStream_t s)
 
 // ------------------------------------------------------- fluid handle
 
+// Pressure-solve grid of a room: as many co-resident blocks as it can use.
+unsigned fluid_cg_blocks(const RoomGeom &g)
+{
+    return std::max(1u, std::min(std::max(cg_max_blocks(), pcg_max_blocks()),
+                                 (unsigned)((g.n + kThreads - 1) / kThreads)));
+}
+
+// Device bytes of one projection handle (its single arena).
+size_t fluid_arena_bytes(const HostRoom &room, bool mg, const MGHost &mgh)
+{
+    const RoomGeom &g = room.g;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    return tables_bytes(room) + 2 * (al(8 * g.nu) + al(8 * g.nv) + al(8 * g.nw)) + (mg ? 9 : 7) * al(8 * g.n) +
+           al(8 * std::max<size_t>(fluid_cg_blocks(g) * 4, 2 * 2368)) + al(8 * stream_blocks(g.n)) + al(256) +
+           al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
+           al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (mg ? mg_bytes(room, mgh) : 0);
+}
+
 struct ffr_fluid {
     HostRoom room;
     ffr_fluid_params prm;
@@ -1338,17 +1356,10 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
         delete s;
         return fail(FFR_ECUDA, "cudaStreamCreate");
     }
-    s->cg_blocks = std::max(1u, std::min(std::max(cg_max_blocks(), pcg_max_blocks()),
-                                         (unsigned)((g.n + kThreads - 1) / kThreads)));
+    s->cg_blocks = fluid_cg_blocks(g);
     s->blocks_faces = stream_blocks(g.nu + g.nv + g.nw);
     s->blocks_cells = stream_blocks(g.n);
-    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-    const size_t bytes = tables_bytes(s->room) + 2 * (al(8 * g.nu) + al(8 * g.nv) + al(8 * g.nw)) +
-                         (s->mg ? 9 : 7) * al(8 * g.n) + al(8 * std::max<size_t>(s->cg_blocks * 4, 2 * 2368)) + al(8 * s->blocks_cells) +
-                         al(256) +
-                         al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
-                         al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (s->mg ? mg_bytes(s->room, s->mgh) : 0);
-    rc = s->arena.alloc(bytes, s->stream);
+    rc = s->arena.alloc(fluid_arena_bytes(s->room, s->mg, s->mgh), s->stream);
     if (rc) { cudaStreamDestroy(s->stream); delete s; return rc; }
     rc = carve_tables(s->room, s->arena, s->tab, s->R);
     Arena &a = s->arena;
@@ -1666,6 +1677,25 @@ int ffr_fluid_use_graph(ffr_fluid *s, int enable)
     s->graph = g;
     s->graph_launches = (unsigned)(ffr_launch_count() - l0);
     s->use_graph = true;
+    return FFR_OK;
+}
+
+int ffr_fluid_estimate_bytes(const ffr_room_desc *room, const ffr_fluid_params *params, size_t *bytes)
+{
+    if (!params || !bytes) return fail(FFR_EINVAL, "NULL params or bytes");
+    HostRoom r;
+    int rc = load_room(room, r);
+    if (rc) return rc;
+    MGHost mgh;
+    const bool mg = params->poisson == FFR_POISSON_MGPCG || params->use_multigrid;
+    if (mg) build_mg_levels(r, mgh);
+    // the arena plus the transient scratch of the multigrid coefficient build
+    size_t scratch = 0;
+    if (mg && mgh.nx.size() > 1) {
+        const size_t m1 = (size_t)mgh.nx[1] * mgh.ny[1] * mgh.nz[1];
+        scratch = 2 * (48 * m1 + ((m1 + 255) & ~size_t(255)));
+    }
+    *bytes = fluid_arena_bytes(r, mg, mgh) + scratch;
     return FFR_OK;
 }
 

@@ -85,6 +85,15 @@ class Fields(C.Structure):
 _lib = None
 
 
+class OutcomeC(C.Structure):
+    _fields_ = [("id", C.c_longlong), ("cells", C.c_longlong), ("status", C.c_int), ("steps", C.c_int),
+                ("converged", C.c_int), ("velocity_change", C.c_double), ("divergence_max", C.c_double),
+                ("T_mean", C.c_double), ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def lib():
     """Loads the library once; raises when it is missing (no CPU fallback)."""
     global _lib
@@ -144,6 +153,15 @@ def lib():
             "ffr_batch_set_rooms": ([vp, C.POINTER(vp), C.c_int], C.c_int),
             "ffr_batch_size": ([vp, C.POINTER(C.c_int)], C.c_int),
             "ffr_batch_enqueue": ([vp, C.c_int, C.c_int], C.c_int),
+            "ffr_fluid_estimate_bytes": ([C.POINTER(RoomDesc), C.POINTER(FluidParamsC), C.POINTER(C.c_size_t)],
+                                         C.c_int),
+            "ffr_server_create": ([C.c_size_t, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+            "ffr_server_destroy": ([vp], C.c_int),
+            "ffr_server_submit": ([vp, C.c_longlong, C.POINTER(RoomDesc), C.POINTER(FluidParamsC), C.c_int],
+                                  C.c_int),
+            "ffr_server_progress": ([vp, C.POINTER(OutcomeC), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+                                    C.c_int),
+            "ffr_server_drain": ([vp, C.POINTER(OutcomeC), C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
                                            C.c_double, vp, _dp, C.POINTER(C.c_int)], C.c_int),
         }
@@ -517,3 +535,58 @@ def poisson_solve_noalloc(room: RoomSpec, cell_type_ptr: int, rhs_ptr: int, p_pt
                                           max_iter, tol, C.c_void_p(stream) if stream else None,
                                           C.byref(res), C.byref(it)))
     return res.value, it.value
+
+
+def estimate_bytes(room: RoomSpec, params: FluidParams) -> int:
+    """Device bytes a FluidHandle of this room would take (ffr_fluid_estimate_bytes)."""
+    m = _RoomMarshal(room)
+    pc = _params(params)
+    b = C.c_size_t()
+    check(lib().ffr_fluid_estimate_bytes(C.byref(m.desc), C.byref(pc), C.byref(b)))
+    return int(b.value)
+
+
+class NativeServer:
+    """The continuous-batching server of the C ABI (ffr_server_*): rooms are
+    submitted, admitted by device memory, advanced in chunks on their own
+    streams and returned as outcome dicts by progress() / drain()."""
+
+    def __init__(self, mem_budget: int, max_active: int = 64, chunk: int = 20):
+        h = C.c_void_p()
+        check(lib().ffr_server_create(int(mem_budget), int(max_active), int(chunk), C.byref(h)))
+        self.h = h
+        self._buf = (OutcomeC * 256)()
+
+    def submit(self, rid: int, room: RoomSpec, params: FluidParams, max_steps: int) -> None:
+        m = _RoomMarshal(room)          # the server copies the arrays
+        pc = _params(params)
+        check(lib().ffr_server_submit(self.h, int(rid), C.byref(m.desc), C.byref(pc), int(max_steps)))
+
+    def progress(self):
+        """One non-blocking round: (finished outcomes, requests still pending)."""
+        n, pend = C.c_int(), C.c_int()
+        check(lib().ffr_server_progress(self.h, self._buf, len(self._buf), C.byref(n), C.byref(pend)))
+        return [self._buf[i].as_dict() for i in range(n.value)], pend.value
+
+    def drain(self):
+        """Runs every submitted request to the end; all their outcomes."""
+        out = []
+        while True:
+            n = C.c_int()
+            check(lib().ffr_server_drain(self.h, self._buf, len(self._buf), C.byref(n)))
+            out += [self._buf[i].as_dict() for i in range(n.value)]
+            if n.value < len(self._buf):
+                break
+        rest, pend = self.progress()
+        return out + rest
+
+    def close(self) -> None:
+        if self.h:
+            lib().ffr_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -186,6 +186,10 @@ int ffr_fluid_set_blocks(ffr_fluid *s, int blocks);
 int ffr_fluid_set_cluster(ffr_fluid *s, int ctas);
 /* Device memory the handle holds (one allocation, made at create). */
 int ffr_fluid_device_bytes(ffr_fluid *s, size_t *bytes);
+/* Device memory ffr_fluid_create would take for this room and parameters
+ * (its allocation plus the transient scratch of the multigrid set-up),
+ * without creating anything: admission control for servers. */
+int ffr_fluid_estimate_bytes(const ffr_room_desc *room, const ffr_fluid_params *params, size_t *bytes);
 /* Captures one step (all its kernels) as a CUDA graph and replays it for
  * every later step of ffr_fluid_enqueue/advance/step (enable = 1), or goes
  * back to direct launches (0).  The kernels read their per-step state from
@@ -267,6 +271,47 @@ enum { FFR_PROF_PREDICT = 0, FFR_PROF_PRESSURE = 1, FFR_PROF_CORRECT = 2, FFR_PR
        FFR_PROF_N = 4 };
 int ffr_fluid_profile(ffr_fluid *s, int enable);
 int ffr_fluid_profile_read(ffr_fluid *s, double *ms, long long *launches);
+
+/* ------------------------------------------------------------ server */
+/* Continuous-batching server over one GPU (no counterpart in the
+ * reference, which solves one room per call): rooms are submitted as
+ * requests, admitted while a slot and the device-memory budget allow
+ * (each charged ffr_fluid_estimate_bytes), advanced on their own streams in
+ * chunks of steps (ffr_fluid_enqueue / ffr_fluid_poll, no host wait between
+ * chunks), and leave on convergence (stop_on_converge) or at their step
+ * cap, when the next queued room is admitted.  A room's schedule follows
+ * its size: up to 2^20 cells the multigrid solve runs in one 16-block
+ * thread-block cluster (many rooms side by side), above that on the whole
+ * GPU; every step replays a captured CUDA graph.  The server lives on the
+ * calling thread: it advances only inside ffr_server_progress/drain. */
+typedef struct ffr_server ffr_server;
+
+/* One finished request.  Times are seconds since ffr_server_create. */
+typedef struct ffr_outcome {
+    long long id;
+    long long cells;
+    int status;            /* FFR_OK, or the error that ended the request */
+    int steps;
+    int converged;
+    double velocity_change, divergence_max, T_mean;
+    double t_submit, t_admit, t_done;
+} ffr_outcome;
+
+/* max_active: rooms in flight at once; chunk: steps per queued chunk. */
+int ffr_server_create(size_t mem_budget, int max_active, int chunk, ffr_server **out);
+int ffr_server_destroy(ffr_server *s);
+/* Queues one room (its arrays are copied); it runs up to max_steps steps.
+ * FFR_ERANGE when the room alone exceeds the memory budget. */
+int ffr_server_submit(ffr_server *s, long long id, const ffr_room_desc *room, const ffr_fluid_params *params,
+                      int max_steps);
+/* One non-blocking round: admits queued rooms, collects finished chunks,
+ * queues the next ones; copies up to max_out finished requests to `out`
+ * (*nout of them; the rest wait for the next call) and sets *pending to the
+ * requests not yet returned. */
+int ffr_server_progress(ffr_server *s, ffr_outcome *out, int max_out, int *nout, int *pending);
+/* Rounds until every submitted request has finished; returns up to max_out
+ * of them as ffr_server_progress does. */
+int ffr_server_drain(ffr_server *s, ffr_outcome *out, int max_out, int *nout);
 
 /* ------------------------------------------------------ pressure solve */
 typedef struct ffr_poisson ffr_poisson;

@@ -163,3 +163,35 @@ def test_cooling_sweep_stops_on_the_reference_steps(precision, poisson):
         assert abs(r.T_mean - want["T_mean"][-1]) <= tol * abs(want["T_mean"][-1]), (want["label"], r.T_mean)
         if r.reached:
             assert r.time_to_target_s == pytest.approx(want["steps"] * base.solver.dt)
+
+
+def test_native_server_matches_rooms_alone():
+    """The C-ABI server (ffr_server_*): every room ends on exactly the step
+    results of the same room run alone with the server's schedule (one
+    16-block cluster, CUDA-graph steps), whatever else ran beside it and
+    however its steps were chunked; a tight budget admits fewer rooms at a
+    time and changes nothing."""
+    from ffrb import capi
+    reqs = _small_requests(n=6, steps=12)
+    reqs = [type(r)(r.rid, r.t_arrival, r.room, r.params.with_(poisson="mgpcg", precision="mixed"), r.max_steps)
+            for r in reqs]
+    alone = {}
+    for rq in reqs:
+        h = capi.FluidHandle(rq.room, rq.params)
+        h.set_cluster(16)
+        h.use_graph(True)
+        alone[rq.rid] = h.advance(rq.max_steps, stop_on_converge=True)
+        h.close()
+    need = max(capi.estimate_bytes(rq.room, rq.params) for rq in reqs)
+    for budget, active in ((64 * need, 8), (2 * need, 8)):
+        srv = capi.NativeServer(budget, active, 5)
+        for rq in reqs:
+            srv.submit(rq.rid, rq.room, rq.params, rq.max_steps)
+        out = {o["id"]: o for o in srv.drain()}
+        srv.close()
+        assert sorted(out) == sorted(alone)
+        for rid, recs in alone.items():
+            o = out[rid]
+            assert o["status"] == 0 and o["steps"] == len(recs), (rid, o)
+            assert o["velocity_change"] == recs[-1]["velocity_change"] and o["T_mean"] == recs[-1]["T_mean"]
+            assert bool(o["converged"]) == bool(recs[-1]["converged"])

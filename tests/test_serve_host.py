@@ -107,3 +107,33 @@ def test_batched_server_chunks_membership_and_admission(monkeypatch):
     sizes = [n for kind, n in _FakeBatch.log if kind in ("create", "set")]
     assert max(sizes) <= 3                       # memory admission: three rooms at a time
     assert all(n <= 4 for kind, n in _FakeBatch.log if kind == "enqueue")
+
+
+def test_native_server_host_paths():
+    """The C-ABI server without a GPU: footprint estimates, the budget
+    check at submit, argument errors, and every request coming back as an
+    outcome (on a box without a GPU, with the handle's CUDA error as its
+    status) instead of a hang."""
+    import pytest
+    from ffrb import capi
+    small, big = empty_room(8, 8, 8, 1, 1, 1), empty_room(32, 32, 32, 1, 1, 1)
+    p = FluidParams(poisson="mgpcg", precision="mixed")
+    assert capi.estimate_bytes(big, p) > capi.estimate_bytes(small, p)
+    assert capi.estimate_bytes(big, p) > capi.estimate_bytes(big, p.with_(poisson="cg"))
+    with pytest.raises(capi.FfrError) as e:
+        capi.NativeServer(0, 4, 5)
+    assert e.value.status == capi.FFR_EINVAL
+    tiny = capi.NativeServer(capi.estimate_bytes(small, p), 4, 5)
+    with pytest.raises(capi.FfrError) as e:
+        tiny.submit(1, big, p, 3)
+    assert e.value.status == 6                      # FFR_ERANGE: alone over the budget
+    tiny.close()
+    srv = capi.NativeServer(1 << 30, 2, 5)
+    for i in range(3):
+        srv.submit(10 + i, small, p, 4)
+    out = srv.drain()
+    assert sorted(o["id"] for o in out) == [10, 11, 12]
+    for o in out:
+        assert o["cells"] == 512 and 0 <= o["steps"] <= 4 and o["t_done"] >= o["t_admit"] >= o["t_submit"]
+        assert o["status"] == 0 or o["steps"] == 0
+    srv.close()
