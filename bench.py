@@ -286,11 +286,12 @@ def run_e2e(args, kind, room, params):
 
 # ------------------------------------------------- CPU reference timing
 
-def cpu_reference(kind, room, params, nsteps=20, budget_s=15.0):
+def cpu_reference(kind, room, params, nsteps=20, budget_s=15.0, single_thread=True):
     """The reference solver (oracle/_ref driver) on a bounded sample of the
     workload: the first steps of the room from rest, stopping at the first
     step that starts after `budget_s` seconds of stepping; the value is the
-    cells divided by the median wall time of one step() call."""
+    cells divided by the median wall time of one step() call.  With
+    single_thread, a one-thread estimate is added beside it."""
     import oracle as orc
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
@@ -310,12 +311,35 @@ def cpu_reference(kind, room, params, nsteps=20, budget_s=15.0):
     _, _, recs = drv.fluid_run(room, p, nsteps, use_openmp=True, time_budget=budget_s)
     t = statistics.median(r.seconds for r in recs)
     its = [r.cg_iterations for r in recs]
-    return {"value": cells / t, "unit": "cell-steps/s", "cores": threads, "kind": "reference",
-            "sample": (f"first {len(recs)} steps of the {room.nx}x{room.ny}x{room.nz} room from rest through the "
-                       f"reference FluidSolver (OpenMP, {threads} threads; plain FP64 CG to tol "
-                       f"{params.poisson_tol:g}, {min(its)}-{max(its)} iterations per step); median step() "
-                       f"wall time {t * 1e3:.1f} ms"),
-            "cg_iterations": its}
+    out = {"value": cells / t, "unit": "cell-steps/s", "cores": threads, "kind": "reference",
+           "sample": (f"first {len(recs)} steps of the {room.nx}x{room.ny}x{room.nz} room from rest through the "
+                      f"reference FluidSolver (OpenMP, {threads} threads; plain FP64 CG to tol "
+                      f"{params.poisson_tol:g}, {min(its)}-{max(its)} iterations per step); value = cells / "
+                      f"median step() wall time ({t * 1e3:.1f} ms)"),
+           "steps_timed": len(recs), "seconds_stepping": round(sum(r.seconds for r in recs), 2),
+           "cg_iterations": its}
+    if single_thread:
+        out["single_thread"] = cpu_reference_single_thread(drv, room, p, float(np.median(its)))
+    return out
+
+
+def cpu_reference_single_thread(drv, room, p, cg_its: float, m: int = 40):
+    """The reference solver on one host thread (use_openmp off), estimated
+    from two capped first steps: one step with the CG capped at m iterations
+    and one capped at 2m give the time per CG iteration and the rest of the
+    step; the estimate is that rest plus cg_its iterations (the iteration
+    count the multi-threaded sample needed).  A full single-thread step of a
+    large room takes about a minute, so it is not run whole."""
+    _, _, r1 = drv.fluid_run(room, p.with_(poisson_max_iter=m), 1, use_openmp=False)
+    _, _, r2 = drv.fluid_run(room, p.with_(poisson_max_iter=2 * m), 1, use_openmp=False)
+    t_it = max(0.0, (r2[0].seconds - r1[0].seconds) / m)
+    t_rest = max(0.0, r1[0].seconds - m * t_it)
+    t_step = t_rest + cg_its * t_it
+    return {"value": room.n_cells / t_step, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
+            "sample": (f"first step from rest with the CG capped at {m} and {2 * m} iterations "
+                       f"({r1[0].seconds:.2f} s, {r2[0].seconds:.2f} s): {t_it * 1e3:.2f} ms per CG iteration, "
+                       f"{t_rest:.2f} s for the rest of the step, extrapolated to {cg_its:.0f} iterations "
+                       f"= {t_step:.1f} s per step (an extrapolation, not a timed full step)")}
 
 
 def reference_arm(args):
@@ -330,31 +354,42 @@ def reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}))
         return
     # one run of up to warmup + steps reference steps, bounded in time so the
-    # whole arm ends within a few minutes
+    # whole arm ends within a few minutes; the reference steps from rest
+    # with no separate warm-up, and every step it took is a timed sample
     cb = cpu_reference(kind, room, params, nsteps=max(1, args.warmup + args.steps),
-                       budget_s=float(args.ref_budget))
+                       budget_s=float(args.ref_budget), single_thread=False)
     v = cb["value"]
+    nsteps = cb.get("steps_timed", args.steps)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": room.n_cells / v * 1e3,
+            "steps": nsteps, "warmup": 0, "steps_requested": args.steps, "warmup_requested": args.warmup,
+            "ms_per_step": room.n_cells / v * 1e3, "value_is": "cells / median wall time of one step()",
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": config_of(args, room, kind, params),
+            "data": "synthetic", "config": config_of(args, room, kind, params, reference=True),
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def config_of(args, room, kind, params):
+def config_of(args, room, kind, params, reference=False):
+    """The workload keys (identical for both arms) and the method that ran:
+    for the reference arm, the reference's own method (FP64 fields, plain
+    CG from a zero pressure, OpenMP on the host cores)."""
     c = {"workload": args.workload, "grid": [room.nx, room.ny, room.nz], "cells": room.n_cells,
          "l2": "inputs larger than L2 (no flush)" if room.n_cells * 8 * 5 > 126e6 else "L2 flush not applied",
-         "parallelism": f"replicas x{args.gpus}"}
+         "parallelism": "host cores (OpenMP)" if reference else f"replicas x{args.gpus}"}
     if kind == "fluid":
         c.update({"precision": params.precision, "poisson": params.poisson, "poisson_tol": params.poisson_tol,
                   "dt": params.dt, "advection": params.advection, "thermal": params.thermal,
                   "buoyancy": params.buoyancy,
                   "pressure_start": ("extrapolated previous pressures" if args.warm_start and params.poisson == "mgpcg"
                                      else "zero")})
+        if reference:
+            c.update({"precision": "fp64", "poisson": "cg", "pressure_start": "zero",
+                      "method": "reference FluidSolver (unpreconditioned FP64 CG)"})
     else:
         c.update(params)
+        if reference:
+            c.update({"storage": "fp64", "method": "reference LBMSolver (FP64, one thread)"})
     return c
 
 

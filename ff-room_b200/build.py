@@ -39,13 +39,28 @@ def _run(cmd) -> None:
     subprocess.check_call(cmd)
 
 
+OBJ_DIR = os.path.join(PKG, "_build")
+
+
 def build_cuda(force: bool = False) -> str:
+    """Each .cu compiles to its own object (in parallel), then one link."""
+    from concurrent.futures import ThreadPoolExecutor
     srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
-    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INC, "ffroom.h"), __file__]
-    if force or _stale(LIB, deps):
-        _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+    common = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INC, "ffroom.h"), __file__]
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    objs = [os.path.join(OBJ_DIR, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    todo = [(s, o) for s, o in zip(srcs, objs) if force or _stale(o, [s] + common)]
+
+    def compile_one(so):
+        src, obj = so
+        _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-c",
               "-Xptxas", "-v" if os.environ.get("FFR_PTXAS_VERBOSE") else "-O3",
-              "-I", INC, "-I", CSRC, *srcs, "-o", LIB])
+              "-I", INC, "-I", CSRC, src, "-o", obj])
+
+    with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        list(ex.map(compile_one, todo))
+    if force or todo or _stale(LIB, objs):
+        _run([NVCC, *ARCH, "-shared", *objs, "-o", LIB])
     return LIB
 
 

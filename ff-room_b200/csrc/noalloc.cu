@@ -14,7 +14,12 @@
 // different host threads on one device) race on it and must be serialised
 // by the caller.  The first call on a device looks the array's device
 // address up with cudaGetSymbolAddress (set-up, once per device); make that
-// first call before any stream capture.
+// first call before any stream capture.  Each call waits for its stream to
+// finish the solve before it returns (the residual and the iteration count
+// come back through the array).  The stream must belong to the current
+// device, and the cached address lives as long as the process: a caller that
+// resets the device (cudaDeviceReset) must reload the library before calling
+// this again on that device.
 #include "projection.cuh"
 
 #include <cstring>

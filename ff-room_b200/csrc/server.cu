@@ -2,7 +2,12 @@
 //
 // Requests wait in arrival order; a request is admitted while fewer than
 // max_active rooms are in flight and its device bytes (ffr_fluid_estimate_
-// bytes) fit the budget next to the rooms in flight.  An admitted room gets
+// bytes) fit the budget next to the rooms in flight.  A request that does
+// not fit does not block the ones behind it: later, smaller requests that
+// fit are admitted past it, but each waiting request can be passed at most
+// kMaxPassed times; once the oldest blocked request reaches that bound no
+// one passes it any more, so the rooms in flight drain until it fits
+// (bounded waiting for large rooms).  An admitted room gets
 // its own ffr_fluid handle (own stream, CUDA-graph steps, the size-class
 // schedule below) and advances in chunks: ffr_fluid_enqueue queues a chunk,
 // ffr_fluid_poll collects it without blocking, and the next chunk is queued
@@ -23,6 +28,8 @@ namespace {
 
 constexpr long long kClusterMaxCells = 1ll << 20;   // one 16-block cluster per room up to this size
 constexpr int kClusterCtas = 16;
+constexpr int kMaxPassed = 16;      // admissions past one waiting request before it blocks the queue
+constexpr size_t kScanDepth = 256;  // queued requests looked at per admission round
 
 double now_s(std::chrono::steady_clock::time_point t0)
 {
@@ -64,6 +71,7 @@ struct Request {
     int max_steps = 0;
     size_t bytes = 0;
     double t_submit = 0.0;
+    int passed = 0;     // later requests admitted while this one waited
 };
 
 struct Active {
@@ -195,11 +203,18 @@ int ffr_server_progress(ffr_server *s, ffr_outcome *out, int max_out, int *nout,
 {
     if (!s || (max_out > 0 && !out) || max_out < 0) return fail(FFR_EINVAL, "bad server progress arguments");
     // admission: arrival order, a free slot and room in the budget (the
-    // first room is always admitted when nothing runs)
-    while (!s->queue.empty() && (int)s->active.size() < s->max_active) {
-        Request *r = s->queue.front();
-        if (!s->active.empty() && s->used + r->bytes > s->budget) break;
-        s->queue.pop_front();
+    // first room is always admitted when nothing runs); requests that fit
+    // may pass ones that do not, up to kMaxPassed times each
+    size_t qi = 0;
+    while (qi < s->queue.size() && qi < kScanDepth && (int)s->active.size() < s->max_active) {
+        Request *r = s->queue[qi];
+        if (!s->active.empty() && s->used + r->bytes > s->budget) {
+            if (r->passed >= kMaxPassed) break;   // this one waits longest: let the GPU drain for it
+            qi++;
+            continue;
+        }
+        for (size_t b = 0; b < qi; b++) s->queue[b]->passed++;
+        s->queue.erase(s->queue.begin() + (long)qi);
         s->used += r->bytes;
         s->active.emplace_back();
         Active &a = s->active.back();

@@ -208,6 +208,43 @@ class _Active:
         return done
 
 
+MAX_PASSED = 16       # admissions past one waiting request before it blocks the queue
+SCAN_DEPTH = 256      # queued requests looked at per admission round
+
+
+class _Admission:
+    """Arrival-order admission in which a request that does not fit the
+    memory budget lets later requests that fit pass it, at most MAX_PASSED
+    of them; after that it blocks the queue until the rooms in flight
+    drain enough for it (the same rule as the native server, server.cu)."""
+
+    def __init__(self, requests: List["Request"]):
+        self.queue = sorted(requests, key=lambda r: r.t_arrival)
+        self.passed = [0] * len(self.queue)
+        self.need = [estimate_bytes(r.room, r.params) for r in self.queue]
+        self.order = list(range(len(self.queue)))
+
+    def __bool__(self) -> bool:
+        return bool(self.order)
+
+    def next_fit(self, now: float, realtime: bool, used: int, budget: int, any_active: bool):
+        """The request to admit now, or None (removed from the queue)."""
+        for pos, qi in enumerate(self.order[:SCAN_DEPTH]):
+            req = self.queue[qi]
+            if realtime and req.t_arrival > now:
+                return None
+            need = self.need[qi]
+            if any_active and used + need > budget:
+                if self.passed[qi] >= MAX_PASSED:
+                    return None
+                continue
+            for earlier in self.order[:pos]:
+                self.passed[earlier] += 1
+            del self.order[pos]
+            return req, need
+        return None
+
+
 class Server:
     """Continuous-batching server over one GPU.
 
@@ -243,29 +280,25 @@ class Server:
         return o
 
     def _run_batched(self, requests: List[Request], realtime: bool) -> List[Outcome]:
-        queue = sorted(requests, key=lambda r: r.t_arrival)
+        adm = _Admission(requests)
         active: List[_Active] = []
         used = 0
         out: List[Outcome] = []
         t0 = time.perf_counter()
-        qi = 0
         batch = None
         members: List[int] = []
-        while qi < len(queue) or active:
+        while adm or active:
             now = time.perf_counter() - t0
-            while qi < len(queue) and len(active) < self.max_active:
-                req = queue[qi]
-                if realtime and req.t_arrival > now:
+            while adm and len(active) < self.max_active:
+                pick = adm.next_fit(now, realtime, used, self.mem_budget, bool(active))
+                if pick is None:
                     break
-                need = estimate_bytes(req.room, req.params)
-                if active and used + need > self.mem_budget:
-                    break
+                req, need = pick
                 a = _Active(req, Schedule(0, self.chunk, False, 0), now, self.keep_fields, split=1,
                             warm_start=self.warm_start)
                 a.charge = need
                 used += need
                 active.append(a)
-                qi += 1
             if not active:
                 time.sleep(0.0002)
                 continue
@@ -295,28 +328,25 @@ class Server:
         return out
 
     def _run_streams(self, requests: List[Request], realtime: bool = True) -> List[Outcome]:
-        queue = sorted(requests, key=lambda r: r.t_arrival)
+        adm = _Admission(requests)
         active: List[_Active] = []
         used = 0
         out: List[Outcome] = []
         t0 = time.perf_counter()
-        qi = 0
-        while qi < len(queue) or active:
+        while adm or active:
             now = time.perf_counter() - t0
             # admission: arrived, a free slot, and room in the memory budget
-            while qi < len(queue) and len(active) < self.max_active:
-                req = queue[qi]
-                if realtime and req.t_arrival > now:
+            # (smaller requests may pass a waiting large one, boundedly)
+            while adm and len(active) < self.max_active:
+                pick = adm.next_fit(now, realtime, used, self.mem_budget, bool(active))
+                if pick is None:
                     break
-                need = estimate_bytes(req.room, req.params)
-                if active and used + need > self.mem_budget:
-                    break
+                req, need = pick
                 a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields, warm_start=self.warm_start)
                 a.charge = need
                 used += need
                 a.launch()
                 active.append(a)
-                qi += 1
             progressed = False
             still = []
             for a in active:

@@ -279,7 +279,13 @@ int ffr_fluid_profile_read(ffr_fluid *s, double *ms, long long *launches);
  * (each charged ffr_fluid_estimate_bytes), advanced on their own streams in
  * chunks of steps (ffr_fluid_enqueue / ffr_fluid_poll, no host wait between
  * chunks), and leave on convergence (stop_on_converge) or at their step
- * cap, when the next queued room is admitted.  A room's schedule follows
+ * cap, when the next queued room is admitted.  Admission goes in arrival
+ * order, except that a request which does not fit the budget lets later
+ * requests that do fit pass it, at most 16 of them; then it blocks the
+ * queue until the rooms in flight leave room for it.  The budget is charged
+ * with each room's arena bytes (ffr_fluid_estimate_bytes); the CUDA-graph
+ * executables, streams and events of a handle come on top of it, so leave
+ * a margin of device memory beyond the budget.  A room's schedule follows
  * its size: up to 2^20 cells the multigrid solve runs in one 16-block
  * thread-block cluster (many rooms side by side), above that on the whole
  * GPU; every step replays a captured CUDA graph.  The server lives on the
@@ -346,9 +352,14 @@ int ffr_poisson_apply(ffr_poisson *s, const double *x, double *ax);
  * library until exit) sized for at most FFR_NOALLOC_MAX_CELLS cells and
  * FFR_NOALLOC_MAX_DIM cells per axis; larger rooms get FFR_ERANGE.  The
  * caller passes the spacings on the host and the cell types, rhs and
- * pressure on the device.  All calls on a device share that array, so calls
- * that overlap on the GPU race; the first call on a device looks the array
- * up (once per device) and should come before any stream capture. */
+ * pressure on the device; the stream must belong to the current device.
+ * The call returns only after the solve has finished on that stream (it
+ * reads the residual and iteration count back).  All calls on a device
+ * share that array, so calls that overlap on the GPU race; the first call on
+ * a device looks the array up (once per device) and should come before any
+ * stream capture.  The looked-up address is kept for the life of the
+ * process: after cudaDeviceReset the library must be unloaded and loaded
+ * again before this entry point is used on that device. */
 #define FFR_NOALLOC_MAX_CELLS (64 * 64 * 64)
 #define FFR_NOALLOC_MAX_DIM 4096
 int ffr_poisson_solve_noalloc(int nx, int ny, int nz, const double *dxv, const double *dyv,

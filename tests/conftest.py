@@ -16,7 +16,24 @@ for p in (PKG, os.path.join(ROOT, "oracle")):
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = os.environ.get("FFR_REFERENCE", "/root/reference")
+
+
+def _reference_checkout() -> str:
+    """The reference checkout the checker was built from: $FFR_REFERENCE, or
+    the path oracle/Makefile recorded in oracle/_ref/reference_path.  Empty
+    when neither is known; tests that read the reference's own Python
+    sources skip then (and wherever the recorded path does not exist)."""
+    env = os.environ.get("FFR_REFERENCE")
+    if env:
+        return env
+    try:
+        with open(os.path.join(ROOT, "oracle", "_ref", "reference_path")) as fh:
+            return fh.read().strip()
+    except OSError:
+        return ""
+
+
+REFERENCE = _reference_checkout()
 
 
 def pytest_configure(config):

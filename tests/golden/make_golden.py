@@ -1,9 +1,9 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container that has the reference sources (default /root/reference)
-after ``make -C oracle`` has built oracle/_ref:
+Run in a container that has the reference sources, after
+``make -C oracle REF=<reference checkout>`` has built oracle/_ref:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>
 
 For every case the reference's own Python ``Scene`` builds the masks on the
 reference's compiled ``_ffroom_core`` (oracle/_ref), the reference
@@ -80,6 +80,13 @@ def cases():
     cfg, prm = workloads.large_thermal(grid=(40, 32, 12))
     prm = prm.with_(precision="fp64", poisson="cg", poisson_tol=1e-8, poisson_max_iter=5000)
     out.append(("thermal_small_10", cfg, 10, {"params": prm, "driver_only": True}))
+    # the large thermal room scaled down to 80x64x24 (same room, fans, boxes,
+    # heat patches, dt and pressure tolerance 1e-8) over its full 2000 steps;
+    # generated with the reference's OpenMP loops on (its parallel
+    # reductions), the same method
+    cfg, prm = workloads.large_thermal(grid=(80, 64, 24))
+    prm = prm.with_(precision="fp64", poisson="cg", poisson_tol=1e-8, poisson_max_iter=20000, use_openmp=True)
+    out.append(("thermal_80x64x24_2000", cfg, 2000, {"params": prm, "driver_only": True}))
     # LBM
     out.append(("lbm_basic_10", SceneConfig.load_yaml(os.path.join(REF, "examples", "basic_room.yaml")), 10,
                 {"lbm": (0.8, 0.01, 1.0)}))
@@ -252,7 +259,7 @@ def mask_hashes():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="the reference checkout (its python/ and examples/)")
     ap.add_argument("--only", default="", help="comma-separated case names (also cooling_sweep, mask_hashes)")
     args = ap.parse_args()
     REF = args.ref

@@ -137,3 +137,33 @@ def test_native_server_host_paths():
         assert o["cells"] == 512 and 0 <= o["steps"] <= 4 and o["t_done"] >= o["t_admit"] >= o["t_submit"]
         assert o["status"] == 0 or o["steps"] == 0
     srv.close()
+
+
+def test_admission_lets_small_rooms_pass_a_waiting_large_one_boundedly():
+    """A request that does not fit lets later ones that fit pass it, at most
+    MAX_PASSED of them; then admission stops until memory frees up."""
+    from ffrb.serve import MAX_PASSED, Request, _Admission
+    p = FluidParams()
+    small, big = empty_room(8, 8, 8, 1, 1, 1), empty_room(64, 64, 64, 1, 1, 1)
+    reqs = [Request(0, 0.0, small, p, 1), Request(1, 0.1, big, p, 1)]
+    reqs += [Request(2 + i, 0.2 + 0.01 * i, small, p, 1) for i in range(MAX_PASSED + 4)]
+    adm = _Admission(reqs)
+    nb, ns = estimate_bytes(big, p), estimate_bytes(small, p)
+    budget = nb + ns - 1          # the big room cannot run beside anything
+    used = 0
+    got = []
+    while True:
+        pick = adm.next_fit(1e9, True, used, budget, any_active=True)
+        if pick is None:
+            break
+        got.append(pick[0].rid)
+        used = ns                 # one small room in flight at a time
+    assert got[0] == 0 and 1 not in got
+    assert len(got) == 1 + MAX_PASSED
+    # with nothing in flight the waiting big room is next
+    pick = adm.next_fit(1e9, True, 0, budget, any_active=False)
+    assert pick[0].rid == 1
+    # realtime: requests that have not arrived are not admitted
+    adm2 = _Admission(reqs)
+    assert adm2.next_fit(0.05, True, 0, budget, any_active=False)[0].rid == 0
+    assert adm2.next_fit(0.05, True, 0, budget, any_active=False) is None

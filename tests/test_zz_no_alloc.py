@@ -41,6 +41,32 @@ def test_noalloc_matches_allocating_solve(name):
     h.close()
 
 
+def test_noalloc_takes_no_device_memory():
+    """A solve through the allocation-free entry point must not take device
+    memory: after a first call (which may do its one-time set-up), a second
+    call leaves the free device memory no lower and torch's pool unchanged.
+    Every tensor is made before the first call."""
+    import torch
+    from ffrb import capi
+    g = Golden("c1_upwind_10")
+    stream = torch.cuda.current_stream().cuda_stream
+    ct = torch.tensor(g.room.cell_type, device="cuda", dtype=torch.uint8)
+    rhs = np.random.default_rng(3).standard_normal(g.room.n_cells)
+    rhs[g.room.cell_type == 1] = 0.0
+    b = torch.tensor(rhs, device="cuda", dtype=torch.float64)
+    x = torch.zeros_like(b)
+    capi.poisson_solve_noalloc(g.room, ct.data_ptr(), b.data_ptr(), x.data_ptr(), 3000, 1e-8, stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    reserved0, allocated0 = torch.cuda.memory_reserved(), torch.cuda.memory_allocated()
+    capi.poisson_solve_noalloc(g.room, ct.data_ptr(), b.data_ptr(), x.data_ptr(), 3000, 1e-8, stream)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 >= free0, (free0, free1)
+    assert torch.cuda.memory_reserved() == reserved0
+    assert torch.cuda.memory_allocated() == allocated0
+
+
 def test_noalloc_rejects_rooms_beyond_its_capacity():
     import torch
     from ffrb import capi
