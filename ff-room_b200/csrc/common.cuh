@@ -157,7 +157,7 @@ void pinned_put(void *p, size_t bytes);
 // ------------------------------------------------ grid-wide barrier
 
 // Counter barrier for a cooperative launch (all blocks co-resident).  Every
-// wait is bounded by `kBarrierTimeoutNs`; a block that gives up sets `err`
+// wait is bounded by the wait limit below; a block that gives up sets `err`
 // and returns false so that the kernel can unwind.
 struct GridSync {
     unsigned int count;
@@ -165,7 +165,23 @@ struct GridSync {
     int err;
     int pad;
 };
-constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;  // 4 s
+constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;  // 4 s, the default wait limit
+
+// The bound of every device-side wait of this translation unit's kernels
+// (one copy per .cu file and device).  ffr_set_device_wait_limit sets every
+// copy on the current device; a test shortens it to make a wait run out.
+static __device__ unsigned long long g_wait_limit_ns = kBarrierTimeoutNs;
+
+// Host side: sets this translation unit's copy on the current device.  Each
+// .cu file with device waits exports one wrapper (set_wait_limit_<file>).
+#define FFR_DEFINE_WAIT_LIMIT_SETTER(NAME)                                                 \
+    int NAME(unsigned long long ns)                                                        \
+    {                                                                                      \
+        const cudaError_t e = cudaMemcpyToSymbol(g_wait_limit_ns, &ns, sizeof(ns));        \
+        return e == cudaSuccess ? FFR_OK : cuda_fail(e, "cudaMemcpyToSymbol(wait limit)"); \
+    }
+int set_wait_limit_projection(unsigned long long ns);
+int set_wait_limit_mgpcg(unsigned long long ns);
 
 __device__ __forceinline__ unsigned long long global_ns()
 {
@@ -254,7 +270,7 @@ __device__ bool grid_allreduce(GridSync *gs, double *partials, double *out, doub
             const unsigned long long t0 = global_ns();
             while (ld_acquire(&gs->gen) == g) {
                 __nanosleep(64);
-                if (global_ns() - t0 > kBarrierTimeoutNs || *(volatile int *)&gs->err) {
+                if (global_ns() - t0 > g_wait_limit_ns || *(volatile int *)&gs->err) {
                     atomicExch(&gs->err, 1);
                     s_ok = 0;
                     break;

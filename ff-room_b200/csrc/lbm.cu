@@ -498,6 +498,35 @@ __global__ void k_lbm_fan_of(const uint8_t *__restrict__ ct, int nx, int ny, int
     }
 }
 
+// Checkpoint conversion between the stored populations and FP64 f in the
+// reference's layout f[q*N + c] (LBMSolver.hpp:77-82): FP64 storage holds f
+// itself, the narrow modes the shifted g = f - w_q.
+template <int MODE>
+__global__ void k_lbm_export(int n, const typename Store<MODE>::T *__restrict__ f, double *__restrict__ out)
+{
+    const long long total = 19ll * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(t / n);
+        const double v = (double)Store<MODE>::ld(f + t);
+        out[t] = MODE == 0 ? v : v + lbm_w(q);
+    }
+}
+
+template <int MODE>
+__global__ void k_lbm_import(int n, const double *__restrict__ in, typename Store<MODE>::T *__restrict__ f)
+{
+    const long long total = 19ll * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(t / n);
+        const double v = in[t];
+        if (MODE == 0) Store<0>::st(reinterpret_cast<double *>(f) + t, v);
+        else if (MODE == 1) reinterpret_cast<float *>(f)[t] = (float)(v - lbm_w(q));
+        else reinterpret_cast<__half *>(f)[t] = __double2half(v - lbm_w(q));
+    }
+}
+
 }  // namespace ffr
 
 using namespace ffr;
@@ -838,6 +867,63 @@ int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host)
     double *d = s && host ? lbm_field(s, field, &len) : nullptr;
     if (!d) return fail(FFR_EINVAL, "bad LBM set_field arguments");
     return staged_copy(d, host, 8 * len, false, s->stream);
+}
+
+// Populations of the current buffer (the post-collision state the step
+// keeps) through a device staging array of 19*N doubles and the staged
+// host copy.
+static int lbm_state_io(ffr_lbm *s, double *host_out, const double *host_in, int *step_io)
+{
+    const long long total = 19ll * s->room.g.n;
+    int rc = lbm_pull(s);
+    if (rc) return rc;
+    LbmState hs = *s->st_host;
+    void *cur = hs.par ? s->f1 : s->f0;
+    double *tmp = nullptr;
+    FFR_CUDA(cudaMallocAsync((void **)&tmp, 8 * total, s->stream));
+    const unsigned nb = blocks_for(total);
+    const int n = (int)s->room.g.n;
+    if (host_out) {
+        switch (s->storage) {
+        case FFR_LBM_FP64: k_lbm_export<0><<<nb, kThr, 0, s->stream>>>(n, (const double *)cur, tmp); break;
+        case FFR_LBM_FP32: k_lbm_export<1><<<nb, kThr, 0, s->stream>>>(n, (const float *)cur, tmp); break;
+        default: k_lbm_export<2><<<nb, kThr, 0, s->stream>>>(n, (const __half *)cur, tmp);
+        }
+        FFR_LAUNCHED(1);
+        rc = staged_copy(host_out, tmp, 8 * total, true, s->stream);
+        if (step_io) *step_io = hs.step;
+    } else {
+        rc = staged_copy(tmp, host_in, 8 * total, false, s->stream);
+        if (!rc) {
+            switch (s->storage) {
+            case FFR_LBM_FP64: k_lbm_import<0><<<nb, kThr, 0, s->stream>>>(n, tmp, (double *)cur); break;
+            case FFR_LBM_FP32: k_lbm_import<1><<<nb, kThr, 0, s->stream>>>(n, tmp, (float *)cur); break;
+            default: k_lbm_import<2><<<nb, kThr, 0, s->stream>>>(n, tmp, (__half *)cur);
+            }
+            FFR_LAUNCHED(1);
+            if (step_io) {
+                hs.step = *step_io;
+                FFR_CUDA(cudaMemcpyAsync(s->st, &hs, sizeof(LbmState), cudaMemcpyHostToDevice, s->stream));
+            }
+        }
+    }
+    cudaFreeAsync(tmp, s->stream);
+    if (!rc) FFR_CUDA(cudaStreamSynchronize(s->stream));
+    if (!rc) rc = lbm_pull(s);
+    return rc;
+}
+
+int ffr_lbm_get_populations(ffr_lbm *s, double *f_host, int *step)
+{
+    if (!s || !f_host) return fail(FFR_EINVAL, "NULL handle or buffer");
+    return lbm_state_io(s, f_host, nullptr, step);
+}
+
+int ffr_lbm_set_populations(ffr_lbm *s, const double *f_host, int step)
+{
+    if (!s || !f_host) return fail(FFR_EINVAL, "NULL handle or buffer");
+    if (step < 0) return fail(FFR_EINVAL, "negative step");
+    return lbm_state_io(s, nullptr, f_host, &step);
 }
 
 int ffr_lbm_synchronize(ffr_lbm *s)

@@ -227,7 +227,7 @@ __device__ bool grid_barrier(GridSync *gs)
             const unsigned long long t0 = global_ns();
             while (ld_acquire(&gs->gen) == g) {
                 __nanosleep(32);
-                if (global_ns() - t0 > kBarrierTimeoutNs || *(volatile int *)&gs->err) {
+                if (global_ns() - t0 > g_wait_limit_ns || *(volatile int *)&gs->err) {
                     atomicExch(&gs->err, 1);
                     s_ok = 0;
                     break;
@@ -2196,5 +2196,7 @@ int batch_split_solve(BatchSplit &B, cudaStream_t s, int max_iter)
     FFR_LAUNCHED(1);
     return FFR_OK;
 }
+
+FFR_DEFINE_WAIT_LIMIT_SETTER(set_wait_limit_mgpcg)
 
 }  // namespace ffr

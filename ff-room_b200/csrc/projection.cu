@@ -973,11 +973,76 @@ __global__ void k_b_finalize(const BRoom *rooms)
 #undef VIX
 #undef WIX
 
+// Self-test of the bounded device waits: every block but block 0 enters the
+// library's grid reduction, which block 0 never joins, so nothing releases
+// it; each waiting block gives up after the wait limit, records
+// FFR_FLAG_TIMEOUT and returns.  No wait is unbounded and no access leaves
+// the buffers (partials holds gridDim.x values).
+__global__ void k_wait_selftest(GridSync *gs, double *partials, double *out, int *flags)
+{
+    __shared__ double sh[32];
+    if (blockIdx.x == 0) return;
+    double v[1] = {1.0};
+    if (!grid_allreduce<1>(gs, partials, out, v, sh) && threadIdx.x == 0) atomicOr(flags, FFR_FLAG_TIMEOUT);
+}
+
+FFR_DEFINE_WAIT_LIMIT_SETTER(set_wait_limit_projection)
+
 }  // namespace ffr
 
 // =================================================================== host
 
 using namespace ffr;
+
+extern "C" int ffr_set_device_wait_limit(double seconds)
+{
+    if (!(seconds >= 0.0) || seconds > 60.0) return fail(FFR_EINVAL, "wait limit must be in [0, 60] s");
+    const unsigned long long ns =
+        seconds == 0.0 ? kBarrierTimeoutNs : (unsigned long long)(seconds * 1e9 + 0.5);
+    int rc = set_wait_limit_projection(ns);
+    if (!rc) rc = set_wait_limit_mgpcg(ns);
+    return rc;
+}
+
+extern "C" int ffr_selftest_device_wait(int blocks, double *elapsed_ms)
+{
+    if (blocks < 2 || blocks > 64) return fail(FFR_EINVAL, "blocks must be in [2, 64]");
+    cudaStream_t st = nullptr;
+    FFR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const size_t bytes = 256 + 8 * 64 + 256 + 256;
+    unsigned char *buf = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&buf, bytes, st);
+    if (e != cudaSuccess) { cudaStreamDestroy(st); return cuda_fail(e, "cudaMallocAsync(self-test)"); }
+    GridSync *gs = reinterpret_cast<GridSync *>(buf);
+    double *partials = reinterpret_cast<double *>(buf + 256);
+    double *out = reinterpret_cast<double *>(buf + 256 + 8 * 64);
+    int *flags = reinterpret_cast<int *>(buf + 256 + 8 * 64 + 256);
+    int host_flags = 0;
+    cudaEvent_t ev[2];
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    e = cudaMemsetAsync(buf, 0, bytes, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], st);
+    if (e == cudaSuccess) {
+        k_wait_selftest<<<blocks, 128, 0, st>>>(gs, partials, out, flags);
+        e = cudaGetLastError();
+        count_launch(1);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&host_flags, flags, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    float ms = 0.0f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    cudaFreeAsync(buf, st);
+    cudaStreamSynchronize(st);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return cuda_fail(e, "device wait self-test");
+    if (elapsed_ms) *elapsed_ms = ms;
+    if (host_flags & FFR_FLAG_TIMEOUT) return fail(FFR_ETIMEDOUT, "self-test wait gave up at the wait limit");
+    return FFR_OK;
+}
 
 namespace {
 

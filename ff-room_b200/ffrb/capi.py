@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(PKG, "libffroom_cuda.so")
 
 FFR_OK, FFR_EINVAL, FFR_ENOMEM, FFR_ECUDA, FFR_ETIMEDOUT, FFR_ENOTSUP, FFR_ERANGE = range(7)
 FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "T": 4}
+FFR_FLAG_NAN, FFR_FLAG_CG_MAXITER, FFR_FLAG_CG_BREAKDOWN, FFR_FLAG_TIMEOUT = 1, 2, 4, 8
 PREC = {"fp64": 0, "mixed": 1}
 POISSON = {"cg": 0, "mgpcg": 1}
 LBM_STORAGE = {"fp64": 0, "fp32": 1, "fp16": 2}
@@ -162,6 +163,10 @@ def lib():
             "ffr_server_progress": ([vp, C.POINTER(OutcomeC), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
                                     C.c_int),
             "ffr_server_drain": ([vp, C.POINTER(OutcomeC), C.c_int, C.POINTER(C.c_int)], C.c_int),
+            "ffr_set_device_wait_limit": ([C.c_double], C.c_int),
+            "ffr_selftest_device_wait": ([C.c_int, _dp], C.c_int),
+            "ffr_lbm_get_populations": ([vp, _dp, C.POINTER(C.c_int)], C.c_int),
+            "ffr_lbm_set_populations": ([vp, _dp, C.c_int], C.c_int),
             "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
                                            C.c_double, vp, _dp, C.POINTER(C.c_int)], C.c_int),
         }
@@ -181,6 +186,18 @@ def check(status: int) -> None:
 
 def launch_count() -> int:
     return int(lib().ffr_launch_count())
+
+
+def set_device_wait_limit(seconds: float) -> None:
+    """Bound of the device-side waits on the current device (0: 4 s)."""
+    check(lib().ffr_set_device_wait_limit(float(seconds)))
+
+
+def selftest_device_wait(blocks: int = 8):
+    """(status, elapsed_ms) of the bounded-wait self-test kernel."""
+    ms = C.c_double(0.0)
+    st = lib().ffr_selftest_device_wait(int(blocks), C.byref(ms))
+    return st, ms.value
 
 
 class _RoomMarshal:
@@ -512,6 +529,18 @@ class LbmHandle:
         out = np.empty(int(np.prod(shape)), dtype=np.float64)
         check(lib().ffr_lbm_get_field(self.h, FIELD[field], out.ctypes.data_as(_dp)))
         return out
+
+    def get_populations(self):
+        """(f, step): the kept populations as FP64 f[q*N + c] and the step counter."""
+        f = np.empty(19 * self.room.n_cells, dtype=np.float64)
+        step = C.c_int(0)
+        check(lib().ffr_lbm_get_populations(self.h, f.ctypes.data_as(_dp), C.byref(step)))
+        return f, step.value
+
+    def set_populations(self, f, step: int) -> None:
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        assert f.size == 19 * self.room.n_cells
+        check(lib().ffr_lbm_set_populations(self.h, f.ctypes.data_as(_dp), int(step)))
 
     def divergence_max(self) -> float:
         d = C.c_double()

@@ -45,6 +45,17 @@ typedef enum ffr_status {
 const char *ffr_status_string(int status);
 /* Detail of the most recent failure on the calling thread ("" if none). */
 const char *ffr_last_error(void);
+/* Upper bound of every bounded device-side wait (the grid barriers of the
+ * persistent solves), in seconds on the current device; 0 restores the
+ * default of 4 s.  For tests of the failure path; no counterpart in the
+ * reference. */
+int ffr_set_device_wait_limit(double seconds);
+/* Self-test of that bound: a kernel whose blocks wait at a grid barrier
+ * that one block never reaches.  Every wait gives up at the limit, the
+ * kernel returns and this returns FFR_ETIMEDOUT with the kernel's duration
+ * in *elapsed_ms; the CUDA context stays usable.  No counterpart in the
+ * reference. */
+int ffr_selftest_device_wait(int blocks, double *elapsed_ms);
 /* Library version, e.g. "0.1.0 sm_100a". */
 const char *ffr_version(void);
 /* Kernels this library has launched since load (all handles). */
@@ -391,6 +402,17 @@ int ffr_lbm_get_field(ffr_lbm *s, int field, double *host);
 int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host);
 int ffr_lbm_synchronize(ffr_lbm *s);
 int ffr_lbm_stream(ffr_lbm *s, void **stream);
+/* Checkpoint and resume of an LBM room (the reference keeps its populations
+ * private: LBMSolver.hpp:77-82 f_, laid out f[q*N + c]).  get copies the
+ * populations the handle keeps between steps (post-collision, ready to
+ * stream) into f_host as 19*N FP64 values in that layout, with the step
+ * counter; set loads them (narrow storage rounds them to its type) and sets
+ * the counter.  Together with the u, v, w, p fields (ffr_lbm_get_field /
+ * ffr_lbm_set_field) they are the whole state of a room: a handle created
+ * for the same room and parameters and loaded this way continues exactly
+ * as the saved one would (bit-identically in FP64 storage). */
+int ffr_lbm_get_populations(ffr_lbm *s, double *f_host, int *step);
+int ffr_lbm_set_populations(ffr_lbm *s, const double *f_host, int step);
 /* Kernel-group timing as for ffr_fluid_profile; groups FFR_LPROF_*. */
 enum { FFR_LPROF_STREAM_COLLIDE = 0, FFR_LPROF_FACES = 1, FFR_LPROF_N = 2 };
 int ffr_lbm_profile(ffr_lbm *s, int enable);
