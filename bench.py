@@ -7,7 +7,7 @@ floor / cooled ceiling patches, four seeded boxes, dt = 0.005 s, pressure to
 than L2 (u, v, w, p, T alone are 315 MB), so no flush is needed.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload large_thermal|lbm_room|basic_room]
+                    [--workload large_thermal|lbm_room|basic_room|batch256|serving_c5|lbm_c4]
                     [--precision mixed|fp64|fp32|fp16] [--graph 1|0]
 
 The default is the mixed-precision path (FP32 increments and FP32 multigrid
@@ -450,6 +450,179 @@ def run_serving(kind: str, n: int, max_cells: int, max_steps: int, batched: bool
     return rep
 
 
+# ------------------------------------- C3: 256 uneven rooms in one batch
+
+def _serial_fp64_estimate(reqs, sample: int = 8, steps: int = 20):
+    """Serial plain FP64 GPU solve time of `reqs` (each to its own step
+    count), estimated from a stratified sample: `sample` rooms spread over
+    the size range each run `steps` steps from rest with the reference's
+    method (FP64, unpreconditioned CG); every request is charged the
+    per-cell-step time of the sampled room nearest in size, times its cells
+    and steps.  Returns (seconds, description)."""
+    from ffrb import capi
+    order = sorted(range(len(reqs)), key=lambda i: reqs[i].room.n_cells)
+    pick = [order[int(round(k * (len(order) - 1) / max(1, sample - 1)))] for k in range(sample)]
+    rates = []
+    for i in pick:
+        rq = reqs[i]
+        p = rq.params.with_(precision="fp64", poisson="cg", use_multigrid=False)
+        h = capi.FluidHandle(rq.room, p)
+        h.advance(1)
+        h.synchronize()
+        t0 = time.perf_counter()
+        h.advance(steps)
+        h.synchronize()
+        dt = time.perf_counter() - t0
+        h.close()
+        rates.append((rq.room.n_cells, rq.room.n_cells * steps / dt))
+    total = 0.0
+    for rq, st in ((r, getattr(r, "steps_done", r.max_steps)) for r in reqs):
+        rate = min(rates, key=lambda cr: abs(np.log(cr[0] / rq.room.n_cells)))[1]
+        total += rq.room.n_cells * st / rate
+    desc = (f"plain FP64 CG on the GPU, one room at a time: {sample} rooms spread over the size range each timed "
+            f"for {steps} steps after one untimed step; every request charged the per-cell-step time of the "
+            f"sampled room nearest in size times its cells and steps (an extrapolation)")
+    return total, desc
+
+
+def run_batch256(steps: int = 500, engines=("batched", "streams")):
+    """The 256 uneven rooms (seed 7, dims U{32..128} per axis, 500 steps,
+    mixed precision) advanced as one batch: every stage one launch for all
+    rooms, each step one CUDA-graph replay with the multigrid solve in a
+    WHILE node; beside it the same rooms on one stream per room."""
+    import torch
+    from ffrb import capi, workloads
+    from ffrb.params import params_from_scene
+    from ffrb.serve import Server, requests_from_configs
+    cfgs = workloads.batch_rooms(steps=steps)
+    reqs = requests_from_configs(cfgs, [params_from_scene(c) for c in cfgs], [0.0] * len(cfgs), steps)
+    cells = sum(r.room.n_cells for r in reqs)
+    free, _ = torch.cuda.mem_get_info()
+    out = {"rooms": len(reqs), "cells": cells, "steps_per_room": steps,
+           "sample": "all 256 rooms of the seed-7 batch, 500 steps each, all at t = 0 (no convergence stop)"}
+    # untimed warm-up: a few small rooms through both engines
+    small = sorted(reqs, key=lambda r: r.room.n_cells)[:4]
+    from ffrb.serve import Request
+    warm = [Request(r.rid, 0.0, r.room, r.params, 2) for r in small]
+    for eng in engines:
+        Server(mem_budget=int(free * 0.5), max_active=len(reqs), batched=(eng == "batched"), chunk=2).run(
+            warm, realtime=False)
+    for eng in engines:
+        l0 = capi.launch_count()
+        srv = Server(mem_budget=int(free * 0.6), max_active=len(reqs), batched=(eng == "batched"), chunk=50)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            t0 = time.perf_counter()
+            res = srv.run(reqs, realtime=False)
+            span = time.perf_counter() - t0
+        done_steps = sum(o.steps for o in res)
+        by_cells = {o.rid: o for o in res}
+        out[eng] = {"room_solves_per_s": len(res) / span, "makespan_s": span,
+                    "cell_steps_per_s": sum(by_cells[r.rid].steps * r.room.n_cells for r in reqs) / span,
+                    "steps_done": done_steps, "gpu_launches": capi.launch_count() - l0,
+                    "clocks": clk.summary()}
+    for r in reqs:
+        r.steps_done = steps
+    t_serial, desc = _serial_fp64_estimate(reqs)
+    out["serial_fp64_room_solves_per_s"] = len(reqs) / t_serial
+    out["serial_fp64_estimate"] = desc
+    for eng in engines:
+        out[eng]["speedup_vs_serial_fp64"] = out[eng]["room_solves_per_s"] * t_serial / len(reqs)
+    return out
+
+
+# ------------------------------------------------ C4: the LBM lattice
+
+def run_lbm_c4(steps: int = 200, warmup: int = 10):
+    """The 384x320x128 D3Q19 lattice (fan inlet at lattice speed 0.05, six
+    boxes, tau 0.52) with FP64, FP32 and FP16 population storage: lattice
+    cell-steps/s over `steps` steps (CUDA events on the solver's stream) and
+    the step kernel against the HBM roofline."""
+    import torch
+    from ffrb import capi, workloads
+    from ffrb.scene import build_room
+    cfg, tau, dt = workloads.lbm_room()
+    room = build_room(cfg)
+    peak, peak_kind = measured_peak()
+    out = {"grid": [room.nx, room.ny, room.nz], "cells": room.n_cells, "tau": tau, "steps": steps}
+    for storage in ("fp64", "fp32", "fp16"):
+        h = capi.LbmHandle(room, tau, steps + warmup, 0.0, dt, storage)
+        h.advance(warmup)
+        h.synchronize()
+        stream = torch.cuda.ExternalStream(h.stream())
+        h.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        recs = h.advance(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        prof = h.profile_read()
+        h.close()
+        t_k = prof["stream_collide"][0] / 1e3
+        b = LBM_STEP_B[storage] * room.n_cells * len(recs)
+        out[storage] = {"lattice_cell_steps_per_s": room.n_cells * len(recs) / (ms / 1e3),
+                        "ms_per_step": ms / len(recs),
+                        "step_kernel_GBps": round(b / t_k / 1e9, 1),
+                        "step_kernel_frac": round(b / t_k / 1e9 / peak, 4),
+                        "step_kernel_share": round(prof["stream_collide"][0] / ms, 4),
+                        "algorithmic_bytes_per_cell": LBM_STEP_B[storage],
+                        "traffic_bytes_per_cell": load_traffic("lbm_step_bytes_per_cell", storage)}
+    out["peak_GBps"] = peak
+    out["peak_source"] = peak_kind
+    return out
+
+
+# ------------------------------------------------ C5: the serving stream
+
+def run_serving_c5(n: int = 96, max_steps: int = 200, tol: float = 1e-4, max_cells: int = None,
+                   engines=("streams", "batched")):
+    """A time-bounded prefix of the serving stream (seed 11, Poisson
+    arrivals at 200/s, log-uniform sizes up to 256x256x96): the first n
+    requests, arriving in real time, each solved in mixed precision until
+    max|du|/dt < tol or max_steps, through the continuous-batching server."""
+    import torch
+    from ffrb import capi, workloads
+    from ffrb.serve import Request, Server, report, requests_from_configs
+    stream = workloads.serving_stream()
+    pick = [rq for rq in stream if max_cells is None or np.prod(rq.cfg.room.grid) <= max_cells][:n]
+    reqs = requests_from_configs([rq.cfg for rq in pick],
+                                 [rq.params.with_(convergence_tol=tol) for rq in pick],
+                                 [rq.t_arrival - pick[0].t_arrival for rq in pick], max_steps)
+    free, _ = torch.cuda.mem_get_info()
+    warm = [Request(r.rid, 0.0, r.room, r.params, 2) for r in sorted(reqs, key=lambda r: r.room.n_cells)[:4]]
+    out = {"requests": len(reqs), "cells_max": max(r.room.n_cells for r in reqs),
+           "cells_min": min(r.room.n_cells for r in reqs), "stop_rule": f"max|du|/dt < {tol:g} or {max_steps} steps",
+           "sample": (f"the first {len(reqs)} requests of the seed-11 stream"
+                      + (f" with <= {max_cells} cells" if max_cells else " (full size mix)")
+                      + f", arriving in real time over {reqs[-1].t_arrival:.2f} s")}
+    results = {}
+    for eng in engines:
+        srv = Server(mem_budget=int(free * 0.6), max_active=64, batched=(eng == "batched"), chunk=10)
+        srv.run(warm, realtime=False)
+        l0 = capi.launch_count()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            res = srv.run(reqs, realtime=True)
+        rep = report(res)
+        conv = [o for o in res if o.converged]
+        rep["p50_time_to_converged_s"] = float(np.percentile([o.latency for o in conv], 50)) if conv else None
+        rep["p99_time_to_converged_s"] = float(np.percentile([o.latency for o in conv], 99)) if conv else None
+        rep["median_final_velocity_change"] = float(np.median([o.velocity_change for o in res]))
+        rep["gpu_launches"] = capi.launch_count() - l0
+        rep["clocks"] = clk.summary()
+        results[eng] = (rep, res)
+        out[eng] = rep
+    # the serial baseline solves the same requests to the same step counts
+    steps_of = {o.rid: o.steps for o in results[engines[0]][1]}
+    for r in reqs:
+        r.steps_done = steps_of[r.rid]
+    t_serial, desc = _serial_fp64_estimate(reqs)
+    out["serial_fp64_room_solves_per_s"] = len(reqs) / t_serial
+    out["serial_fp64_estimate"] = desc
+    for eng in engines:
+        out[eng]["speedup_vs_serial_fp64"] = out[eng]["room_solves_per_s"] * t_serial / len(reqs)
+    return out
+
+
 def serving_arm(args):
     import torch
     torch.cuda.set_device(0)
@@ -481,7 +654,9 @@ def main():
     ap.add_argument("--requests", type=int, default=48, help="serving/batch sample size")
     ap.add_argument("--max-cells", type=int, default=600_000, help="serving/batch: largest room in the sample")
     ap.add_argument("--max-steps", type=int, default=40, help="serving/batch: step cap per room")
-    ap.add_argument("--no-serving", action="store_true", help="default run: skip the serving sample")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="default run: skip the serving, batch and lattice samples")
+    ap.add_argument("--tol", type=float, default=1e-4, help="serving_c5: the stop rule's max|du|/dt")
     ap.add_argument("--batched", type=int, default=0,
                     help="serving/batch: 1 = one launch per stage for all active rooms, 0 = one stream per room")
     ap.add_argument("--chunk", type=int, default=10, help="serving/batch: steps between membership changes")
@@ -498,6 +673,22 @@ def main():
         return
     if args.workload in ("serving", "batch"):
         serving_arm(args)
+        return
+    if args.workload in ("batch256", "serving_c5", "lbm_c4"):
+        import torch
+        torch.cuda.set_device(0)
+        if args.workload == "batch256":
+            rep = run_batch256(args.max_steps if args.max_steps != 40 else 500)
+            value, unit = rep["batched"]["room_solves_per_s"], "room-solves/s"
+        elif args.workload == "serving_c5":
+            rep = run_serving_c5(args.requests, args.max_steps, args.tol)
+            value, unit = rep["streams"]["room_solves_per_s"], "room-solves/s"
+        else:
+            rep = run_lbm_c4(args.steps)
+            value, unit = rep["fp32"]["lattice_cell_steps_per_s"], "lattice-cell-steps/s"
+        print(json.dumps({"metric": METRIC, "value": value, "unit": unit, "n_gpus": 1, "dtype": "f32/f64",
+                          "data": "synthetic", "higher_is_better": True, "config": {"workload": args.workload},
+                          args.workload: rep}))
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -519,19 +710,21 @@ def main():
         if not args.no_cpu_baseline:
             cb = cpu_reference(kind, room, params)
         dtype = {"fp64": "f64", "mixed": "f32/f64", "fp32": "f32", "fp16": "f16/f32"}.get(args.precision, args.precision)
-        serving = None
+        extra_blocks = {}
         if not args.no_serving and args.workload == "large_thermal" and world == 1:
-            serving = run_serving("serving", 48, 600_000, 40, batched=False, warm_start=bool(args.warm_start))
-            alt = run_serving("serving", 48, 600_000, 40, batched=True, warm_start=bool(args.warm_start))
-            serving["batched_mode"] = {k: alt[k] for k in ("room_solves_per_s", "p50_s", "p99_s",
-                                                          "speedup_vs_serial_fp64", "gpu_launches")}
+            # the other benchmark configurations, each a bounded sample
+            extra_blocks["serving"] = run_serving_c5(96, 200, 1e-4)
+            extra_blocks["serving_reference_tol"] = run_serving_c5(48, 2000, 1.0, max_cells=600_000,
+                                                                   engines=("streams",))
+            extra_blocks["batch256"] = run_batch256()
+            extra_blocks["lbm_c4"] = run_lbm_c4()
         line = {"metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
                 "steps": res["steps"], "warmup": args.warmup, "ms_per_step": res["ms"] / max(1, res["steps"]),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
                 "data": "synthetic", "config": config_of(args, room, kind, params),
                 "roofline": res["roofline"], "cpu_baseline": cb, "e2e": res["e2e"],
-                "gpu_launches": res["launches"], "clocks": res["clocks"], "detail": res["extra"],
-                "serving": serving}
+                "gpu_launches": res["launches"], "clocks": res["clocks"], "detail": res["extra"]}
+        line.update(extra_blocks)
         print(json.dumps(line))
     if dist:
         dist.barrier()

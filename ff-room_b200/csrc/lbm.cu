@@ -500,16 +500,25 @@ __global__ void k_lbm_fan_of(const uint8_t *__restrict__ ct, int nx, int ny, int
 
 // Checkpoint conversion between the stored populations and FP64 f in the
 // reference's layout f[q*N + c] (LBMSolver.hpp:77-82): FP64 storage holds f
-// itself, the narrow modes the shifted g = f - w_q.
+// itself, the narrow modes the shifted g = f - w_q.  SOLID cells stream
+// nothing and their slots of the second buffer are never written; they are
+// exported as 0, the value the reference's push streaming leaves in them
+// (LBMSolver.cpp:151-190), and never read by a step.
 template <int MODE>
-__global__ void k_lbm_export(int n, const typename Store<MODE>::T *__restrict__ f, double *__restrict__ out)
+__global__ void k_lbm_export(int n, const uint8_t *__restrict__ ct, const typename Store<MODE>::T *__restrict__ f,
+                             double *__restrict__ out)
 {
     const long long total = 19ll * n;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int q = (int)(t / n);
-        const double v = (double)Store<MODE>::ld(f + t);
-        out[t] = MODE == 0 ? v : v + lbm_w(q);
+        const int c = (int)(t - (long long)q * n);
+        double v = 0.0;
+        if (ct[c] != CT_SOLID) {
+            v = (double)Store<MODE>::ld(f + t);
+            if (MODE != 0) v += lbm_w(q);
+        }
+        out[t] = v;
     }
 }
 
@@ -861,6 +870,15 @@ int ffr_lbm_get_field(ffr_lbm *s, int field, double *host)
     return staged_copy(host, d, 8 * len, true, s->stream);
 }
 
+int ffr_lbm_field_dev(ffr_lbm *s, int field, double **dev)
+{
+    long long len = 0;
+    double *d = s && dev ? lbm_field(s, field, &len) : nullptr;
+    if (!d) return fail(FFR_EINVAL, "bad LBM field_dev arguments");
+    *dev = d;
+    return FFR_OK;
+}
+
 int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host)
 {
     long long len = 0;
@@ -885,9 +903,9 @@ static int lbm_state_io(ffr_lbm *s, double *host_out, const double *host_in, int
     const int n = (int)s->room.g.n;
     if (host_out) {
         switch (s->storage) {
-        case FFR_LBM_FP64: k_lbm_export<0><<<nb, kThr, 0, s->stream>>>(n, (const double *)cur, tmp); break;
-        case FFR_LBM_FP32: k_lbm_export<1><<<nb, kThr, 0, s->stream>>>(n, (const float *)cur, tmp); break;
-        default: k_lbm_export<2><<<nb, kThr, 0, s->stream>>>(n, (const __half *)cur, tmp);
+        case FFR_LBM_FP64: k_lbm_export<0><<<nb, kThr, 0, s->stream>>>(n, s->L.ct, (const double *)cur, tmp); break;
+        case FFR_LBM_FP32: k_lbm_export<1><<<nb, kThr, 0, s->stream>>>(n, s->L.ct, (const float *)cur, tmp); break;
+        default: k_lbm_export<2><<<nb, kThr, 0, s->stream>>>(n, s->L.ct, (const __half *)cur, tmp);
         }
         FFR_LAUNCHED(1);
         rc = staged_copy(host_out, tmp, 8 * total, true, s->stream);

@@ -1496,6 +1496,13 @@ __global__ void __launch_bounds__(256) k_bsp_residual(BatchDev D, BMap m)
     sp_residual_body(A, D.ss[r], P, D.active, cudaGraphConditionalHandle{}, 0);
 }
 
+// Condition of the batched solve's WHILE node: iterate while any room of
+// the batch is still iterating (the count its init and residual passes keep).
+__global__ void k_bsp_cond(const int *active, cudaGraphConditionalHandle cond)
+{
+    if (threadIdx.x == 0) cudaGraphSetConditional(cond, *(volatile const int *)active > 0 ? 1u : 0u);
+}
+
 __global__ void __launch_bounds__(256) k_bsp_final(BatchDev D, BMap m)
 {
     __shared__ __align__(16) PCGArgs A;
@@ -2190,6 +2197,55 @@ int batch_split_solve(BatchSplit &B, cudaStream_t s, int max_iter)
             if (!more) break;
         }
     }
+    k_bsp_final<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    FFR_LAUNCHED(1);
+    k_bsp_backsub<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    FFR_LAUNCHED(1);
+    return FFR_OK;
+}
+
+int capture_batch_split(BatchSplit &B, cudaStream_t s, cudaStream_t bs)
+{
+    if (B.nrooms == 0) return FFR_OK;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    FFR_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return fail(FFR_EINVAL, "batched solve must be captured");
+    FFR_CUDA(cudaMemsetAsync(B.D.active, 0, sizeof(int), s));
+    k_bsp_extrapolate<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    FFR_LAUNCHED(1);
+    k_bsp_init<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    FFR_LAUNCHED(1);
+    FFR_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphConditionalHandle cond;
+    FFR_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    k_bsp_cond<<<1, 32, 0, s>>>(B.D.active, cond);
+    FFR_LAUNCHED(1);
+    FFR_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    FFR_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    FFR_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    // one iteration of every room still iterating, then the condition; a
+    // room that finished returns at once from every pass, and each room
+    // stops itself at its own poisson_max_iter, so the loop ends
+    FFR_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    int rc = batch_iteration(B, bs);
+    if (!rc) {
+        k_bsp_cond<<<1, 32, 0, bs>>>(B.D.active, cond);
+        FFR_LAUNCHED(1);
+    }
+    cudaGraph_t body_out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(bs, &body_out);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture(batched PCG iteration)");
     k_bsp_final<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
     FFR_LAUNCHED(1);
     k_bsp_backsub<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);

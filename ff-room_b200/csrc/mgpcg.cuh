@@ -174,6 +174,11 @@ void batch_split_release(BatchSplit &B);
 // max_iter bounds the batches queued (the largest poisson_max_iter of the
 // rooms; every room also stops itself at its own).
 int batch_split_solve(BatchSplit &B, cudaStream_t s, int max_iter);
+// The same solve recorded into the graph being captured on s: a WHILE node
+// whose body (captured on bs) is one iteration of every room, repeated while
+// any room is still iterating, so a batched step replays with no host
+// involvement.
+int capture_batch_split(BatchSplit &B, cudaStream_t s, cudaStream_t bs);
 
 // The split solve launched kernel by kernel outside any graph.  The host
 // queues iterations in batches and stops at the first batch whose copy of

@@ -1901,6 +1901,14 @@ struct ffr_batch {
     const HeatItem *heat = nullptr;
     bool any_thermal = false;
     int max_iter = 0;
+    // one captured batched step (predictor, the solve's WHILE node,
+    // correction, thermal, finalize), replayed per step when use_graph;
+    // recaptured after a membership change
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t body_stream = nullptr;
+    unsigned graph_launches = 0;
 };
 
 namespace {
@@ -1909,6 +1917,9 @@ void batch_free(ffr_batch *b)
 {
     if (!b) return;
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->body_stream) cudaStreamDestroy(b->body_stream);
     batch_split_release(b->split);
     if (b->split.active_host) cudaFreeHost(b->split.active_host);
     for (int k = 0; k < 2; k++)
@@ -1973,6 +1984,11 @@ int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms)
     }
     // the tables of the previous membership may still be read by its launches
     FFR_CUDA(cudaStreamSynchronize(b->stream));
+    // a captured step holds the previous tables' addresses
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
     b->rooms.assign(rooms, rooms + nrooms);
     b->any_thermal = false;
     b->max_iter = 0;
@@ -2088,6 +2104,79 @@ int ffr_batch_size(const ffr_batch *b, int *nrooms)
     return FFR_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// One batched step: every stage one launch for all rooms.  capturing: the
+// pressure solve is recorded as a WHILE node (the batch stream is being
+// captured), else it is paced by the host.
+int batch_enqueue_step(ffr_batch *b, bool capturing)
+{
+    cudaStream_t st = b->stream;
+    const int n = (int)b->rooms.size();
+    k_b_predict<<<b->nb_faces, kThreads, 0, st>>>(b->broom, b->faces);
+    FFR_LAUNCHED(1);
+    int rc = capturing ? capture_batch_split(b->split, st, b->body_stream)
+                       : batch_split_solve(b->split, st, b->max_iter);
+    if (rc) return rc;
+    k_b_correct<<<b->nb_cells, kThreads, 0, st>>>(b->broom, b->cells);
+    FFR_LAUNCHED(1);
+    if (b->any_thermal) {
+        if (b->nb_open) {
+            k_b_opening<<<b->nb_open, kThreads, 0, st>>>(b->broom, b->open, b->openm, 0);
+            FFR_LAUNCHED(1);
+        }
+        k_b_advect_T<<<b->nb_cells, kThreads, 0, st>>>(b->broom, b->cells);
+        FFR_LAUNCHED(1);
+        if (b->nb_open) {
+            k_b_opening<<<b->nb_open, kThreads, 0, st>>>(b->broom, b->open, b->openm, 1);
+            FFR_LAUNCHED(1);
+        }
+    }
+    if (b->nb_heat) {
+        k_b_heat<<<b->nb_heat, kThreads, 0, st>>>(b->broom, b->heat, b->heatm);
+        FFR_LAUNCHED(1);
+    }
+    k_b_finalize<<<n, kThreads, 0, st>>>(b->broom);
+    FFR_LAUNCHED(1);
+    return FFR_OK;
+}
+
+int batch_capture(ffr_batch *b)
+{
+    if (!b->body_stream) FFR_CUDA(cudaStreamCreateWithFlags(&b->body_stream, cudaStreamNonBlocking));
+    const unsigned long long l0 = ffr_launch_count();
+    FFR_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+    int rc = batch_enqueue_step(b, true);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture(batched step)");
+    e = cudaGraphInstantiate(&b->graph_exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(e, "cudaGraphInstantiate(batched step)");
+    }
+    b->graph = g;
+    b->graph_launches = (unsigned)(ffr_launch_count() - l0);
+    return FFR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ffr_batch_use_graph(ffr_batch *b, int enable)
+{
+    if (!b) return fail(FFR_EINVAL, "NULL batch");
+    b->use_graph = enable != 0;
+    return FFR_OK;
+}
+
 int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge)
 {
     if (!b || nsteps < 0 || nsteps > kRing) return fail(FFR_EINVAL, "bad handle or nsteps (0..1024)");
@@ -2100,33 +2189,20 @@ int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge)
         s->p0_valid = false;      // batched steps keep no starting pressure
     }
     const int n = (int)b->rooms.size();
+    if (b->use_graph && nsteps > 0 && !b->graph_exec) {
+        int rc = batch_capture(b);
+        if (rc) return rc;
+    }
     k_b_begin<<<1, 256, 0, st>>>(b->broom, n, stop_on_converge ? 1 : 0);
     FFR_LAUNCHED(1);
     for (int k = 0; k < nsteps; k++) {
-        k_b_predict<<<b->nb_faces, kThreads, 0, st>>>(b->broom, b->faces);
-        FFR_LAUNCHED(1);
-        int rc = batch_split_solve(b->split, st, b->max_iter);
+        if (b->use_graph) {
+            FFR_CUDA(cudaGraphLaunch(b->graph_exec, st));
+            count_launch(b->graph_launches);
+            continue;
+        }
+        int rc = batch_enqueue_step(b, false);
         if (rc) return rc;
-        k_b_correct<<<b->nb_cells, kThreads, 0, st>>>(b->broom, b->cells);
-        FFR_LAUNCHED(1);
-        if (b->any_thermal) {
-            if (b->nb_open) {
-                k_b_opening<<<b->nb_open, kThreads, 0, st>>>(b->broom, b->open, b->openm, 0);
-                FFR_LAUNCHED(1);
-            }
-            k_b_advect_T<<<b->nb_cells, kThreads, 0, st>>>(b->broom, b->cells);
-            FFR_LAUNCHED(1);
-            if (b->nb_open) {
-                k_b_opening<<<b->nb_open, kThreads, 0, st>>>(b->broom, b->open, b->openm, 1);
-                FFR_LAUNCHED(1);
-            }
-        }
-        if (b->nb_heat) {
-            k_b_heat<<<b->nb_heat, kThreads, 0, st>>>(b->broom, b->heat, b->heatm);
-            FFR_LAUNCHED(1);
-        }
-        k_b_finalize<<<n, kThreads, 0, st>>>(b->broom);
-        FFR_LAUNCHED(1);
     }
     // each room's results as ffr_fluid_enqueue leaves them, for ffr_fluid_poll
     for (ffr_fluid *s : b->rooms) {

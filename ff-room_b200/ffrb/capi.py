@@ -154,6 +154,7 @@ def lib():
             "ffr_batch_set_rooms": ([vp, C.POINTER(vp), C.c_int], C.c_int),
             "ffr_batch_size": ([vp, C.POINTER(C.c_int)], C.c_int),
             "ffr_batch_enqueue": ([vp, C.c_int, C.c_int], C.c_int),
+            "ffr_batch_use_graph": ([vp, C.c_int], C.c_int),
             "ffr_fluid_estimate_bytes": ([C.POINTER(RoomDesc), C.POINTER(FluidParamsC), C.POINTER(C.c_size_t)],
                                          C.c_int),
             "ffr_server_create": ([C.c_size_t, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
@@ -166,6 +167,7 @@ def lib():
             "ffr_set_device_wait_limit": ([C.c_double], C.c_int),
             "ffr_selftest_device_wait": ([C.c_int, _dp], C.c_int),
             "ffr_lbm_get_populations": ([vp, _dp, C.POINTER(C.c_int)], C.c_int),
+            "ffr_lbm_field_dev": ([vp, C.c_int, C.POINTER(vp)], C.c_int),
             "ffr_lbm_set_populations": ([vp, _dp, C.c_int], C.c_int),
             "ffr_poisson_solve_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, vp, vp, vp, C.c_int,
                                            C.c_double, vp, _dp, C.POINTER(C.c_int)], C.c_int),
@@ -182,6 +184,16 @@ def check(status: int) -> None:
     if status != FFR_OK:
         L = lib()
         raise FfrError(status, f"{L.ffr_status_string(status).decode()}: {L.ffr_last_error().decode()}")
+
+
+class DeviceArray:
+    """A device buffer of this library seen through __cuda_array_interface__
+    (torch.as_tensor(DeviceArray(ptr, n), device="cuda") wraps it without a
+    copy); the owning handle must outlive the view."""
+
+    def __init__(self, ptr: int, n: int, typestr: str = "<f8"):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3}
 
 
 def launch_count() -> int:
@@ -400,6 +412,9 @@ class BatchHandle:
         check(lib().ffr_batch_set_rooms(self.h, arr, len(rooms)))
         self.rooms = list(rooms)
 
+    def use_graph(self, enable: bool = True) -> None:
+        check(lib().ffr_batch_use_graph(self.h, int(enable)))
+
     def enqueue(self, nsteps: int, stop_on_converge: bool = True) -> None:
         check(lib().ffr_batch_enqueue(self.h, nsteps, int(stop_on_converge)))
         for r in self.rooms:
@@ -529,6 +544,11 @@ class LbmHandle:
         out = np.empty(int(np.prod(shape)), dtype=np.float64)
         check(lib().ffr_lbm_get_field(self.h, FIELD[field], out.ctypes.data_as(_dp)))
         return out
+
+    def field_dev(self, field: str) -> int:
+        p = C.c_void_p()
+        check(lib().ffr_lbm_field_dev(self.h, FIELD[field], C.byref(p)))
+        return p.value
 
     def get_populations(self):
         """(f, step): the kept populations as FP64 f[q*N + c] and the step counter."""

@@ -251,10 +251,14 @@ class Server:
     batched=False: every room runs on its own stream with its own launches
     (the tuner's schedule per size class); batched=True: all active rooms
     advance together, one launch per stage for the whole set (ffr_batch),
-    in chunks of `chunk` steps; rooms join and leave between chunks."""
+    in chunks of `chunk` steps; rooms join and leave between chunks.  With
+    batch_graph (default) each batched step replays one captured CUDA graph
+    (recaptured when the membership changes)."""
 
     def __init__(self, mem_budget: int, max_active: int = 64, tuner: Optional[Tuner] = None,
-                 keep_fields: bool = False, batched: bool = False, chunk: int = 10, warm_start: bool = True):
+                 keep_fields: bool = False, batched: bool = False, chunk: int = 10, warm_start: bool = True,
+                 batch_graph: bool = True):
+        self.batch_graph = batch_graph
         self.mem_budget = mem_budget
         self.max_active = max_active
         self.tuner = tuner or Tuner()
@@ -305,6 +309,8 @@ class Server:
             ids = [id(a) for a in active]
             if batch is None:
                 batch = capi.BatchHandle([a.h for a in active])
+                if self.batch_graph:
+                    batch.use_graph(True)
                 members = ids
             elif ids != members:
                 batch.set_rooms([a.h for a in active])

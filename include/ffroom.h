@@ -248,8 +248,16 @@ int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms);
 int ffr_batch_destroy(ffr_batch *b);
 int ffr_batch_size(const ffr_batch *b, int *nrooms);
 /* Queues nsteps (0..1024) steps of every room; returns once the last
- * step's pressure solve is queued (the solves are paced by the host). */
+ * step's pressure solve is queued (the solves are paced by the host, or,
+ * with ffr_batch_use_graph, replayed from the captured step graph). */
 int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge);
+/* enable != 0: the next ffr_batch_enqueue captures one batched step as a
+ * CUDA graph (every stage one launch for all rooms; the pressure solve a
+ * WHILE node that iterates while any room is still iterating) and each step
+ * replays it, so the host queues one graph launch per step and never waits
+ * inside a chunk.  Results are identical to the host-paced form.  A
+ * membership change (ffr_batch_set_rooms) recaptures it. */
+int ffr_batch_use_graph(ffr_batch *b, int enable);
 
 /* FluidSolver::compute_divergence_max (FluidSolver.cpp:470-484). */
 int ffr_fluid_divergence_max(ffr_fluid *s, double *out);
@@ -400,6 +408,9 @@ int ffr_lbm_current_step(ffr_lbm *s, int *out);
  * (extract_macroscopic, LBMSolver.cpp:288-376): u, v, w faces and p. */
 int ffr_lbm_get_field(ffr_lbm *s, int field, double *host);
 int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host);
+/* Device pointer of the u, v, w or p field (valid until destroy; written in
+ * place by every step, so read it in stream order). */
+int ffr_lbm_field_dev(ffr_lbm *s, int field, double **dev);
 int ffr_lbm_synchronize(ffr_lbm *s);
 int ffr_lbm_stream(ffr_lbm *s, void **stream);
 /* Checkpoint and resume of an LBM room (the reference keeps its populations

@@ -102,3 +102,32 @@ def test_batch_rejects_rooms_it_cannot_take():
     h2 = _handle(g)
     with pytest.raises(capi.FfrError):
         capi.BatchHandle([h2, h2])
+
+
+def test_batch_graph_matches_host_paced_batch():
+    """The batched step captured as one CUDA graph (the solve a WHILE node
+    over the count of rooms still iterating) gives exactly the host-paced
+    batch's results, across a membership change (which recaptures it)."""
+    from ffrb import capi
+    gs = [Golden(n) for n in NAMES]
+    steps = min(g.nsteps for g in gs)
+    out = {}
+    for graph in (False, True):
+        hs = [_handle(g) for g in gs]
+        b = capi.BatchHandle(hs)
+        if graph:
+            b.use_graph(True)
+        first = b.advance(steps // 2)
+        b.set_rooms(hs[::-1])
+        second = b.advance(steps - steps // 2)[::-1]
+        out[graph] = ([f + s for f, s in zip(first, second)], [{k: h.get(k) for k in "uvwpT"} for h in hs])
+        b.close()
+        for h in hs:
+            h.close()
+    for g, ra, rb, fa, fb in zip(gs, out[False][0], out[True][0], out[False][1], out[True][1]):
+        assert len(ra) == len(rb) == steps
+        for x, y in zip(ra, rb):
+            for k in HIST:
+                assert x[k] == y[k], (g.name, k, x[k], y[k])
+        for k in "uvwpT":
+            assert np.array_equal(fa[k], fb[k]), (g.name, k)
