@@ -69,6 +69,9 @@ class _FakeBatch:
         self.rooms = list(rooms)
         _FakeBatch.log.append(("create", len(self.rooms)))
 
+    def use_graph(self, enable=True):
+        _FakeBatch.log.append(("graph", bool(enable)))
+
     def set_rooms(self, rooms):
         assert all(not r.closed for r in rooms)
         self.rooms = list(rooms)
