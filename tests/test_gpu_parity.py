@@ -88,6 +88,26 @@ def test_basic_room_lbm_converges_at_published_step():
     assert len(recs) == 119 and recs[-1]["converged"]
 
 
+@pytest.mark.parametrize("storage,tol", [("fp32", 2e-6), ("fp16", 2e-3)])
+@pytest.mark.parametrize("name", ["lbm_basic_10", "lbm_small_20", "lbm_openings_10"])
+def test_lbm_narrow_storage_tracks_reference(name, storage, tol):
+    """FP32 / FP16 population storage (shifted populations, FP32 collision)
+    against the reference's FP64 LBM fixtures.  Bound per storage: an FP32
+    population carries a relative rounding of 6e-8 and an FP16 one 4.9e-4
+    of the shifted value; over 10-20 steps the fields stay within about 5e-7
+    (FP32) and 5e-4 (FP16) of the reference, and the bound is four times
+    that."""
+    from ffrb import capi
+    g = Golden(name)
+    L = g.lbm
+    h = capi.LbmHandle(g.room, L["tau"], g.nsteps, L["tol"], L["dt"], storage)
+    h.advance(g.nsteps)
+    for k in "uvwp":
+        err = rel_err(h.get(k), g.fields[k])
+        assert err <= tol, (storage, k, err)
+    h.close()
+
+
 @pytest.mark.parametrize("storage,tol", [("fp32", 2e-3), ("fp16", 5e-2)])
 def test_lbm_narrow_storage_tracks_fp64(storage, tol):
     """FP32 / FP16 populations (shifted, FP32 collision) against the FP64
