@@ -232,6 +232,49 @@ def cooling_sweep(drv):
         json.dump(out, fh, indent=1)
 
 
+def bridge_traces(core):
+    """tests/golden/bridge_*.json/.npz: every call the reference's own
+    SolverBridge.run / run_animated make into `_ffroom_core`, recorded on the
+    reference's compiled module (tests/bridge_trace.py), for the GPU test
+    that replays them on this repository's drop-in module.  A progress
+    callback reads each step's (step, vel_change, div_max, T_mean), as the
+    documented callback does."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from bridge_trace import Recorder
+
+    def progress(step, vc, dm, tm):
+        pass
+
+    def basic():
+        return RefSceneConfig.load_yaml(os.path.join(REF, "examples", "basic_room.yaml"))
+
+    def cooling():
+        c = RefSceneConfig.load_yaml(os.path.join(REF, "examples", "summer_cooling.yaml"))
+        c.solver.max_steps = 120          # a bounded prefix of its 5000 steps
+        return c
+
+    def basic_lbm():
+        c = basic()
+        c.solver.method = "lbm"
+        return c
+
+    jobs = [("bridge_basic_room_run", basic, "run"), ("bridge_basic_room_animated", basic, "animated"),
+            ("bridge_summer_cooling_run", cooling, "run"), ("bridge_basic_room_lbm_run", basic_lbm, "run")]
+    for name, make, how in jobs:
+        rec = Recorder(core)
+        sys.modules["_ffroom_core"] = rec
+        try:
+            bridge = ref_bridge.SolverBridge(make())
+            if how == "run":
+                res = bridge.run(progress_callback=progress, print_interval=0)
+            else:
+                res, snaps = bridge.run_animated(save_every=100, progress_callback=progress, print_interval=0)
+        finally:
+            sys.modules["_ffroom_core"] = core
+        rec.save(os.path.join(HERE, name + ".json"), os.path.join(HERE, name + ".npz"))
+        print(name, "ops", len(rec.ops), "arrays", len(rec.arrays), "steps", res.steps, "converged", res.converged)
+
+
 def mask_hashes():
     """sha256 of the masks of the synthetic workloads, built by the
     reference Scene, so that CPU tests can pin the restated scene builder
@@ -282,4 +325,6 @@ if __name__ == "__main__":
         cooling_sweep(drv)
     if only is None or "mask_hashes" in only:
         mask_hashes()
+    if only is None or "bridge_traces" in only:
+        bridge_traces(core)
     print("done")
