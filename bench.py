@@ -532,18 +532,29 @@ def run_batch256(steps: int = 500, engines=("batched", "streams")):
 
 # ------------------------------------------------ C4: the LBM lattice
 
+LBM_STABLE_TAU = 0.6
+
+
 def run_lbm_c4(steps: int = 200, warmup: int = 10):
     """The 384x320x128 D3Q19 lattice (fan inlet at lattice speed 0.05, six
-    boxes, tau 0.52) with FP64, FP32 and FP16 population storage: lattice
-    cell-steps/s over `steps` steps (CUDA events on the solver's stream) and
-    the step kernel against the HBM roofline."""
+    boxes) with FP64, FP32 and FP16 population storage: lattice cell-steps/s
+    over `steps` steps (CUDA events on the solver's stream) and the step
+    kernel against the HBM roofline.  The configuration's tau = 0.52 drives
+    this lattice to NaN within 250 steps (in FP64, whose arithmetic matches
+    the reference's bit for bit; 0.55 within 500), so the timing runs at
+    tau = 0.6, which stays finite over 10000 steps; the work per step does
+    not depend on tau."""
     import torch
     from ffrb import capi, workloads
     from ffrb.scene import build_room
-    cfg, tau, dt = workloads.lbm_room()
+    cfg, tau_cfg, dt = workloads.lbm_room()
+    tau = LBM_STABLE_TAU
     room = build_room(cfg)
     peak, peak_kind = measured_peak()
-    out = {"grid": [room.nx, room.ny, room.nz], "cells": room.n_cells, "tau": tau, "steps": steps}
+    out = {"grid": [room.nx, room.ny, room.nz], "cells": room.n_cells, "tau": tau, "tau_configured": tau_cfg,
+           "steps": steps,
+           "note": "tau 0.52 diverges to NaN within 250 steps on this lattice (FP64, the reference's arithmetic); "
+                   "timed at tau 0.6 (finite over 10000 steps)"}
     for storage in ("fp64", "fp32", "fp16"):
         h = capi.LbmHandle(room, tau, steps + warmup, 0.0, dt, storage)
         h.advance(warmup)

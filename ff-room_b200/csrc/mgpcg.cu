@@ -1048,8 +1048,10 @@ __device__ __forceinline__ void pass_backsub(const PCGArgs &A, int start, int st
 // blocks must still hold enough warps per SM to hide memory latency.
 constexpr int kClusterThreads = 512;
 
-template <class G, int NT = 256>
-__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_pcg(PCGArgs A)
+// The whole solve on the blocks of group G (a cooperative grid or one
+// thread-block cluster).
+template <class G>
+__device__ __forceinline__ void pcg_body(const PCGArgs &A)
 {
     __shared__ double sh[32];
     if (A.st && A.st->halt) return;
@@ -1136,6 +1138,27 @@ finish:
             atomicOr(&A.st->flags, flags);
         }
     }
+}
+
+template <class G, int NT = 256>
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_pcg(PCGArgs A)
+{
+    pcg_body<G>(A);
+}
+
+// Batched rooms, one thread-block cluster per room: cluster c (blocks
+// c*ctas .. c*ctas + ctas - 1) runs the whole solve of room c, exactly as
+// that room's own one-cluster launch (k_pcg<ClusterGroup>) does, so many
+// rooms' solves run side by side in one launch with no host pacing.
+__global__ void __launch_bounds__(kClusterThreads, 1) k_bpcg_cluster(BatchDev D, int ctas)
+{
+    __shared__ __align__(16) PCGArgs A;
+    const int r = (int)(blockIdx.x / (unsigned)ctas);
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(D.args + r);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(&A);
+    for (int i = threadIdx.x; i < (int)(sizeof(PCGArgs) / 8); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    pcg_body<ClusterGroup>(A);
 }
 
 // ================================================================ split
@@ -2201,6 +2224,32 @@ int batch_split_solve(BatchSplit &B, cudaStream_t s, int max_iter)
     FFR_LAUNCHED(1);
     k_bsp_backsub<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
     FFR_LAUNCHED(1);
+    return FFR_OK;
+}
+
+int launch_batch_cluster(BatchSplit &B, cudaStream_t s, int ctas)
+{
+    if (B.nrooms == 0) return FFR_OK;
+    static bool attr_set = false;
+    if (!attr_set) {
+        FFR_CUDA(cudaFuncSetAttribute(k_bpcg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr_set = true;
+    }
+    k_bsp_extrapolate<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    FFR_LAUNCHED(1);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(B.nrooms * ctas));
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    FFR_CUDA(cudaLaunchKernelEx(&cfg, k_bpcg_cluster, B.D, ctas));
+    count_launch(1);
     return FFR_OK;
 }
 

@@ -179,6 +179,11 @@ int batch_split_solve(BatchSplit &B, cudaStream_t s, int max_iter);
 // any room is still iterating, so a batched step replays with no host
 // involvement.
 int capture_batch_split(BatchSplit &B, cudaStream_t s, cudaStream_t bs);
+// Every room's whole solve in one launch, one thread-block cluster of `ctas`
+// blocks per room (each room's own one-cluster schedule, ffr_fluid_set_
+// cluster), after the batched warm-start extrapolation.  No host pacing and
+// nothing to capture specially.
+int launch_batch_cluster(BatchSplit &B, cudaStream_t s, int ctas);
 
 // The split solve launched kernel by kernel outside any graph.  The host
 // queues iterations in batches and stops at the first batch whose copy of

@@ -558,6 +558,37 @@ struct FluidSolver : DeviceSolver {
         check(ffr_fluid_divergence_max(h, &d));
         return d;
     }
+
+    // The cell-centred velocity and speed of SolverBridge.run_animated's
+    // snapshots (python/ff_room/solver_bridge.py:222-238), formed on the
+    // device: {"speed": (Nx, Ny, Nz), "vel": (Nx, Ny, Nz, 3)}.  No
+    // counterpart in the reference module; run_animated may call it in place
+    // of reading the three face arrays back (the fields stay on the GPU).
+    py::dict snapshot()
+    {
+        acquire();
+        const size_t n = (size_t)grid.Nx * grid.Ny * grid.Nz;
+        std::vector<double> uc(n), vc(n), wc(n);
+        py::array_t<double> speed({(py::ssize_t)grid.Nx, (py::ssize_t)grid.Ny, (py::ssize_t)grid.Nz});
+        py::array_t<double> vel({(py::ssize_t)grid.Nx, (py::ssize_t)grid.Ny, (py::ssize_t)grid.Nz, (py::ssize_t)3});
+        double *sp = speed.mutable_data();
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = ffr_fluid_snapshot(h, uc.data(), vc.data(), wc.data(), sp);
+        }
+        check(rc);
+        double *vp = vel.mutable_data();
+        for (size_t c = 0; c < n; c++) {
+            vp[3 * c] = uc[c];
+            vp[3 * c + 1] = vc[c];
+            vp[3 * c + 2] = wc[c];
+        }
+        py::dict d;
+        d["speed"] = speed;
+        d["vel"] = vel;
+        return d;
+    }
     int current_step()
     {
         int c = 0;
@@ -832,6 +863,7 @@ PYBIND11_MODULE(_ffroom_core, m)
         .def("step", &FluidSolver::step)
         .def("run", &FluidSolver::run, py::arg("callback") = py::none())
         .def("compute_divergence_max", &FluidSolver::compute_divergence_max)
+        .def("snapshot", &FluidSolver::snapshot)
         .def_property_readonly("current_step", &FluidSolver::current_step);
 
     py::class_<LBMSolver>(m, "LBMSolver")

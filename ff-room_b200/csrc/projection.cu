@@ -1901,6 +1901,7 @@ struct ffr_batch {
     const HeatItem *heat = nullptr;
     bool any_thermal = false;
     int max_iter = 0;
+    int cluster_ctas = 0;         // > 0: every room's whole solve on one cluster of this size
     // one captured batched step (predictor, the solve's WHILE node,
     // correction, thermal, finalize), replayed per step when use_graph;
     // recaptured after a membership change
@@ -1978,7 +1979,9 @@ int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms)
         if (!s) return fail(FFR_EINVAL, "NULL room handle");
         if (!s->mg) return fail(FFR_EINVAL, "a batch takes rooms with the multigrid pressure solve");
         if (s->pending) return fail(FFR_EINVAL, "a room has a queued chunk that was not polled");
-        if (s->cluster_ctas || s->block_override) return fail(FFR_EINVAL, "a batched room keeps the default grid");
+        if (s->block_override) return fail(FFR_EINVAL, "a batched room keeps the default grid");
+        if (s->cluster_ctas != rooms[0]->cluster_ctas)
+            return fail(FFR_EINVAL, "the rooms of a batch share one schedule (all split, or one cluster size)");
         for (int q = 0; q < r; q++)
             if (rooms[q] == s) return fail(FFR_EINVAL, "a room appears twice in the batch");
     }
@@ -1990,6 +1993,7 @@ int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms)
     b->graph_exec = nullptr;
     b->graph = nullptr;
     b->rooms.assign(rooms, rooms + nrooms);
+    b->cluster_ctas = rooms[0]->cluster_ctas;
     b->any_thermal = false;
     b->max_iter = 0;
     // per-room arguments, block tables of the step kernels, patch items
@@ -2117,8 +2121,9 @@ int batch_enqueue_step(ffr_batch *b, bool capturing)
     const int n = (int)b->rooms.size();
     k_b_predict<<<b->nb_faces, kThreads, 0, st>>>(b->broom, b->faces);
     FFR_LAUNCHED(1);
-    int rc = capturing ? capture_batch_split(b->split, st, b->body_stream)
-                       : batch_split_solve(b->split, st, b->max_iter);
+    int rc = b->cluster_ctas > 0 ? launch_batch_cluster(b->split, st, b->cluster_ctas)
+             : capturing           ? capture_batch_split(b->split, st, b->body_stream)
+                                   : batch_split_solve(b->split, st, b->max_iter);
     if (rc) return rc;
     k_b_correct<<<b->nb_cells, kThreads, 0, st>>>(b->broom, b->cells);
     FFR_LAUNCHED(1);

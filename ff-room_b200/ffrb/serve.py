@@ -253,12 +253,18 @@ class Server:
     advance together, one launch per stage for the whole set (ffr_batch),
     in chunks of `chunk` steps; rooms join and leave between chunks.  With
     batch_graph (default) each batched step replays one captured CUDA graph
-    (recaptured when the membership changes)."""
+    (recaptured when the membership changes).  batch_cluster (default 16):
+    each batched room's whole pressure solve runs on its own thread-block
+    cluster of that size, every room's in one launch, and rooms above
+    Tuner.CLUSTER_MAX_CELLS run beside the batch on their own streams;
+    batch_cluster=0: every room joins the batch with the one-kernel-per-pass
+    solve."""
 
     def __init__(self, mem_budget: int, max_active: int = 64, tuner: Optional[Tuner] = None,
                  keep_fields: bool = False, batched: bool = False, chunk: int = 10, warm_start: bool = True,
-                 batch_graph: bool = True):
+                 batch_graph: bool = True, batch_cluster: int = 16):
         self.batch_graph = batch_graph
+        self.batch_cluster = batch_cluster
         self.mem_budget = mem_budget
         self.max_active = max_active
         self.tuner = tuner or Tuner()
@@ -284,51 +290,92 @@ class Server:
         return o
 
     def _run_batched(self, requests: List[Request], realtime: bool) -> List[Outcome]:
+        """Batch members advance together in chunks (one launch per stage);
+        with batch_cluster, rooms above the one-cluster size run beside the
+        batch on their own streams with the tuner's schedule.  Members join
+        and leave only between batch chunks."""
         adm = _Admission(requests)
-        active: List[_Active] = []
+        members: List[_Active] = []
+        solo: List[_Active] = []
         used = 0
         out: List[Outcome] = []
         t0 = time.perf_counter()
         batch = None
-        members: List[int] = []
-        while adm or active:
+        batch_ids: List[int] = []
+        in_flight = False
+        while adm or members or solo:
             now = time.perf_counter() - t0
-            while adm and len(active) < self.max_active:
-                pick = adm.next_fit(now, realtime, used, self.mem_budget, bool(active))
-                if pick is None:
-                    break
-                req, need = pick
-                a = _Active(req, Schedule(0, self.chunk, False, 0), now, self.keep_fields, split=1,
-                            warm_start=self.warm_start)
-                a.charge = need
-                used += need
-                active.append(a)
-            if not active:
-                time.sleep(0.0002)
-                continue
-            ids = [id(a) for a in active]
-            if batch is None:
-                batch = capi.BatchHandle([a.h for a in active])
-                if self.batch_graph:
-                    batch.use_graph(True)
-                members = ids
-            elif ids != members:
-                batch.set_rooms([a.h for a in active])
-                members = ids
-            nsteps = min([self.chunk] + [a.req.max_steps - a.steps for a in active])
-            batch.enqueue(nsteps, True)
+            if not in_flight:
+                while adm and len(members) + len(solo) < self.max_active:
+                    pick = adm.next_fit(now, realtime, used, self.mem_budget, bool(members or solo))
+                    if pick is None:
+                        break
+                    req, need = pick
+                    small = req.room.n_cells <= Tuner.CLUSTER_MAX_CELLS and req.params.poisson == "mgpcg"
+                    if self.batch_cluster and small:
+                        a = _Active(req, Schedule(0, self.chunk, False, self.batch_cluster), now, self.keep_fields,
+                                    warm_start=self.warm_start)
+                        members.append(a)
+                    elif self.batch_cluster:
+                        a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields,
+                                    warm_start=self.warm_start)
+                        a.launch()
+                        solo.append(a)
+                    else:
+                        a = _Active(req, Schedule(0, self.chunk, False, 0), now, self.keep_fields, split=1,
+                                    warm_start=self.warm_start)
+                        members.append(a)
+                    a.charge = need
+                    used += need
+                if members:
+                    ids = [id(a) for a in members]
+                    if batch is None:
+                        batch = capi.BatchHandle([a.h for a in members])
+                        if self.batch_graph:
+                            batch.use_graph(True)
+                    elif ids != batch_ids:
+                        batch.set_rooms([a.h for a in members])
+                    batch_ids = ids
+                    nsteps = min([self.chunk] + [a.req.max_steps - a.steps for a in members])
+                    batch.enqueue(nsteps, True)
+                    for a in members:
+                        a.queued = nsteps
+                        a.result = None
+                    in_flight = True
+            progressed = False
+            if in_flight:
+                waiting = False
+                for a in members:
+                    if a.result is None:
+                        a.result = a.poll()
+                        waiting |= a.result is None
+                if not waiting:
+                    in_flight = False
+                    progressed = True
+                    still = []
+                    for a in members:
+                        if a.result:
+                            out.append(self._finish(a, t0))
+                            used -= a.charge
+                        else:
+                            still.append(a)
+                    members = still
             still = []
-            for a in active:
-                a.queued = nsteps
-                done = None
-                while done is None:
-                    done = a.poll()
-                if done:
+            for a in solo:
+                st = a.poll()
+                if st is None:
+                    still.append(a)
+                    continue
+                progressed = True
+                if st:
                     out.append(self._finish(a, t0))
                     used -= a.charge
                 else:
+                    a.launch()
                     still.append(a)
-            active = still
+            solo = still
+            if not progressed:
+                time.sleep(0.0002)
         if batch is not None:
             batch.close()
         return out

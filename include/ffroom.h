@@ -236,7 +236,12 @@ int ffr_fluid_set_split(ffr_fluid *s, int mode);
  * room solved alone with the one-kernel-per-pass multigrid schedule).  The
  * rooms stay ordinary handles: after ffr_batch_enqueue each room's results
  * are collected with ffr_fluid_poll, and fields are read as usual.  Rooms
- * must use the multigrid pressure solve and the default grid; a room may
+ * must use the multigrid pressure solve and one common schedule: either the
+ * default grid (the solve runs one batched kernel per pass, paced by the
+ * host or by a WHILE node of the step graph) or one cluster size set with
+ * ffr_fluid_set_cluster (every room's whole solve runs on its own cluster of
+ * that size, all rooms in one launch; results identical to the room solved
+ * alone with that cluster size); a room may
  * belong to several batches but only one may run at a time.  A batch keeps
  * pointers to its rooms: after destroying a member, replace the members
  * (ffr_batch_set_rooms) before the next ffr_batch_enqueue. */

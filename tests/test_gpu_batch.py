@@ -131,3 +131,42 @@ def test_batch_graph_matches_host_paced_batch():
                 assert x[k] == y[k], (g.name, k, x[k], y[k])
         for k in "uvwpT":
             assert np.array_equal(fa[k], fb[k]), (g.name, k)
+
+
+def test_batch_of_cluster_rooms_matches_rooms_alone():
+    """Rooms on the one-cluster schedule (ffr_fluid_set_cluster(16)) batched:
+    every room's whole solve runs on its own cluster, all rooms in one
+    launch, and each room ends exactly as when solved alone on that
+    schedule, with the step graph and without it."""
+    from ffrb import capi
+    gs = [Golden(n) for n in NAMES]
+    steps = min(g.nsteps for g in gs)
+
+    def cl(g):
+        from ffrb import capi as c
+        h = c.FluidHandle(g.room, g.params.with_(poisson="mgpcg", precision="mixed"))
+        h.set_cluster(16)
+        return h
+
+    alone = []
+    for g in gs:
+        h = cl(g)
+        recs = h.advance(steps)
+        alone.append((recs, {k: h.get(k) for k in "uvwpT"}))
+        h.close()
+    for graph in (False, True):
+        hs = [cl(g) for g in gs]
+        b = capi.BatchHandle(hs)
+        if graph:
+            b.use_graph(True)
+        out = b.advance(steps)
+        for g, h, recs, (recs_a, fa) in zip(gs, hs, out, alone):
+            assert len(recs) == steps
+            for ra, rb in zip(recs_a, recs):
+                for k in HIST:
+                    assert ra[k] == rb[k], (g.name, graph, k, ra[k], rb[k])
+            for k in "uvwpT":
+                assert np.array_equal(h.get(k), fa[k]), (g.name, graph, k)
+        b.close()
+        for h in hs:
+            h.close()

@@ -246,3 +246,26 @@ def test_result_files_from_a_device_room(tmp_path):
     rows = np.loadtxt(tmp_path / "v.csv", delimiter=",", skiprows=1)
     assert np.array_equal(rows[:, 6], h.snapshot(with_velocity=False)["speed"].ravel())
     h.close()
+
+
+def test_dropin_snapshot_matches_run_animated_arithmetic():
+    """FluidSolver.snapshot() (device-side) gives run_animated's cell-centred
+    velocity and speed (solver_bridge.py:222-238) from the same fields."""
+    import _ffroom_core as c
+    from ffrb.scene import build_on_core, solver_params
+    g = Golden("summer_cooling_10")
+    grid, bm = build_on_core(c, g.room)
+    params = solver_params(c, g.cfg)
+    s = c.FluidSolver(grid, bm, params)
+    for _ in range(5):
+        s.step()
+    snap = s.snapshot()
+    u, v, w = np.array(grid.u_shaped()), np.array(grid.v_shaped()), np.array(grid.w_shaped())
+    uc = 0.5 * (u[:-1, :, :] + u[1:, :, :])
+    vc = 0.5 * (v[:, :-1, :] + v[:, 1:, :])
+    wc = 0.5 * (w[:, :, :-1] + w[:, :, 1:])
+    assert np.allclose(snap["vel"], np.stack([uc, vc, wc], axis=-1), rtol=0, atol=1e-14)
+    assert np.allclose(snap["speed"], np.sqrt(uc ** 2 + vc ** 2 + wc ** 2), rtol=1e-14, atol=1e-14)
+    # the snapshot leaves the run unchanged
+    r = s.step()
+    assert r.step == 6

@@ -112,10 +112,12 @@ def test_cluster_schedule_tracks_reference(ctas):
         h.close()
 
 
-def test_batched_server_results_identical_alone_and_in_mix():
+@pytest.mark.parametrize("cluster", [0, 16])
+def test_batched_server_results_identical_alone_and_in_mix(cluster):
     """The batched engine: rooms arriving at different times join and leave
     the batch between chunks; each room's fields equal those of the room
-    solved alone (split multigrid form) bit for bit."""
+    solved alone with the same pressure schedule (the split multigrid form,
+    or one 16-block cluster per room) bit for bit."""
     from ffrb import capi
     from ffrb.serve import Server
     reqs = _small_requests(6, steps=9)
@@ -125,11 +127,14 @@ def test_batched_server_results_identical_alone_and_in_mix():
     alone = {}
     for rq in reqs:
         h = capi.FluidHandle(rq.room, rq.params)
-        h.set_split(1)
+        if cluster:
+            h.set_cluster(cluster)
+        else:
+            h.set_split(1)
         h.advance(rq.max_steps, stop_on_converge=True)
         alone[rq.rid] = {k: h.get(k) for k in "uvwpT"}
         h.close()
-    srv = Server(mem_budget=8 << 30, max_active=4, keep_fields=True, batched=True, chunk=3)
+    srv = Server(mem_budget=8 << 30, max_active=4, keep_fields=True, batched=True, chunk=3, batch_cluster=cluster)
     out = srv.run(reqs, realtime=True)
     assert len(out) == len(reqs)
     for o in out:

@@ -45,6 +45,18 @@ class _FakeRoom:
     def set_split(self, mode):
         self.split = mode
 
+    def set_cluster(self, ctas):
+        self.cluster = ctas
+
+    def set_blocks(self, blocks):
+        self.blocks = blocks
+
+    def use_graph(self, enable=True):
+        self.graph = enable
+
+    def enqueue(self, n, stop=True):
+        self.pending = n
+
     def poll(self):
         n, self.pending = self.pending, 0
         out = [{"step": self.steps + i + 1, "converged": False, "velocity_change": 1.0, "T_mean": 20.0,
@@ -102,14 +114,16 @@ def test_batched_server_chunks_membership_and_admission(monkeypatch):
     caps = [5, 12, 7, 20, 3, 9]
     reqs = [Request(i, 0.0, rooms[i], p, caps[i]) for i in range(6)]
     need = max(estimate_bytes(r, p) for r in rooms)
-    srv = Server(mem_budget=3 * need, max_active=8, batched=True, chunk=4)
-    out = srv.run(reqs, realtime=False)
-    assert sorted(o.rid for o in out) == list(range(6))
-    for o in out:
-        assert o.steps == caps[o.rid]
-    sizes = [n for kind, n in _FakeBatch.log if kind in ("create", "set")]
-    assert max(sizes) <= 3                       # memory admission: three rooms at a time
-    assert all(n <= 4 for kind, n in _FakeBatch.log if kind == "enqueue")
+    for cluster in (0, 16):
+        _FakeBatch.log = []
+        srv = Server(mem_budget=3 * need, max_active=8, batched=True, chunk=4, batch_cluster=cluster)
+        out = srv.run(reqs, realtime=False)
+        assert sorted(o.rid for o in out) == list(range(6))
+        for o in out:
+            assert o.steps == caps[o.rid]
+        sizes = [n for kind, n in _FakeBatch.log if kind in ("create", "set")]
+        assert max(sizes) <= 3                       # memory admission: three rooms at a time
+        assert all(n <= 4 for kind, n in _FakeBatch.log if kind == "enqueue")
 
 
 def test_native_server_host_paths():
