@@ -1147,13 +1147,13 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_pcg(PCGArgs A)
 }
 
 // Batched rooms, one thread-block cluster per room: cluster c (blocks
-// c*ctas .. c*ctas + ctas - 1) runs the whole solve of room c, exactly as
+// c*ctas .. c*ctas + ctas - 1) runs the whole solve of room order[c], exactly as
 // that room's own one-cluster launch (k_pcg<ClusterGroup>) does, so many
 // rooms' solves run side by side in one launch with no host pacing.
-__global__ void __launch_bounds__(kClusterThreads, 1) k_bpcg_cluster(BatchDev D, int ctas)
+__global__ void __launch_bounds__(kClusterThreads, 1) k_bpcg_cluster(BatchDev D, const int *order, int ctas)
 {
     __shared__ __align__(16) PCGArgs A;
-    const int r = (int)(blockIdx.x / (unsigned)ctas);
+    const int r = order[blockIdx.x / (unsigned)ctas];
     const unsigned long long *src = reinterpret_cast<const unsigned long long *>(D.args + r);
     unsigned long long *dst = reinterpret_cast<unsigned long long *>(&A);
     for (int i = threadIdx.x; i < (int)(sizeof(PCGArgs) / 8); i += blockDim.x) dst[i] = src[i];
@@ -1170,7 +1170,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_bpcg_cluster(BatchDev D,
 // and the residual kernel sets the conditional handle of the graph's WHILE
 // node to 0 once the solve is over.
 
-constexpr int kSplitMaxBlocks = 2368;   // 16 per SM
+#ifndef FFR_L0_BLOCKS
+#define FFR_L0_BLOCKS 2368
+#endif
+constexpr int kSplitMaxBlocks = FFR_L0_BLOCKS;   // level-0 pass grid cap (a multiple of the 148 SMs)
 
 struct SplitState {
     double bnorm, rz_old, beta, alpha, alpha_prev, res;
@@ -2075,9 +2078,15 @@ int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std
     std::vector<int> mids;
     for (int r = 0; r < n; r++)
         if (sh[r].mid) mids.push_back(r);
+    // the one-cluster-per-room launch takes the rooms largest first, so the
+    // last clusters to start are the shortest (less tail at the stage end)
+    std::vector<int> order(n);
+    for (int r = 0; r < n; r++) order[r] = r;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return args[a].R.n > args[b].R.n; });
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     size_t bytes = al(sizeof(PCGArgs) * n) + al(sizeof(void *) * n) + al(sizeof(int)) +
-                   al(4 * (t_cells0.room.size() + t_cells0.first.size())) + al(4 * (mids.size() + 1));
+                   al(4 * (t_cells0.room.size() + t_cells0.first.size())) + al(4 * (mids.size() + 1)) +
+                   al(4 * n);
     for (int l = 0; l < nlev; l++)
         bytes += al(4 * (t_pairs[l].room.size() + t_pairs[l].first.size())) +
                  al(4 * (t_coarse[l].room.size() + t_coarse[l].first.size()));
@@ -2122,6 +2131,7 @@ int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std
     mids.push_back(0);
     B.mid_rooms = reinterpret_cast<const int *>(put(mids.data(), 4 * mids.size()));
     B.nmid = (int)mids.size() - 1;
+    B.cluster_order = reinterpret_cast<const int *>(put(order.data(), 4 * order.size()));
     FFR_CUDA(cudaMemcpy(B.dev, host.data(), bytes, cudaMemcpyHostToDevice));
     return FFR_OK;
 }
@@ -2248,7 +2258,7 @@ int launch_batch_cluster(BatchSplit &B, cudaStream_t s, int ctas)
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    FFR_CUDA(cudaLaunchKernelEx(&cfg, k_bpcg_cluster, B.D, ctas));
+    FFR_CUDA(cudaLaunchKernelEx(&cfg, k_bpcg_cluster, B.D, B.cluster_order, ctas));
     count_launch(1);
     return FFR_OK;
 }

@@ -155,6 +155,7 @@ struct BatchSplit {
     BMap post0{};                     // level-0 black post-smoothing
     unsigned nb_post0 = 0;
     const int *mid_rooms = nullptr;   // rooms with levels small enough for one block
+    const int *cluster_order = nullptr;   // rooms largest first (one-cluster-per-room launch)
     int nmid = 0;
     void *dev = nullptr;              // device allocation holding all tables
     size_t cap = 0;                   // its size (reused while large enough)
