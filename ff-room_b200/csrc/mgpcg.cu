@@ -1171,7 +1171,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_bpcg_cluster(BatchDev D,
 // node to 0 once the solve is over.
 
 #ifndef FFR_L0_BLOCKS
-#define FFR_L0_BLOCKS 2368
+#define FFR_L0_BLOCKS 1184
 #endif
 constexpr int kSplitMaxBlocks = FFR_L0_BLOCKS;   // level-0 pass grid cap (a multiple of the 148 SMs)
 

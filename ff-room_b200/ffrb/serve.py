@@ -208,6 +208,56 @@ class _Active:
         return done
 
 
+class _Group:
+    """One batch of the batched engine: its members, its BatchHandle (own
+    stream) and whether a chunk of it is in flight."""
+
+    def __init__(self):
+        self.members: List["_Active"] = []
+        self.batch = None
+        self.ids: List[int] = []
+        self.in_flight = False
+
+    def cells(self) -> int:
+        return sum(a.req.room.n_cells for a in self.members)
+
+    def launch(self, chunk: int, graph: bool) -> None:
+        ids = [id(a) for a in self.members]
+        if self.batch is None:
+            self.batch = capi.BatchHandle([a.h for a in self.members])
+            if graph:
+                self.batch.use_graph(True)
+        elif ids != self.ids:
+            self.batch.set_rooms([a.h for a in self.members])
+        self.ids = ids
+        nsteps = min([chunk] + [a.req.max_steps - a.steps for a in self.members])
+        self.batch.enqueue(nsteps, True)
+        for a in self.members:
+            a.queued = nsteps
+            a.result = None
+        self.in_flight = True
+
+    def poll(self):
+        """None while the chunk runs; else the members that finished (they
+        leave the group)."""
+        waiting = False
+        for a in self.members:
+            if a.result is None:
+                a.result = a.poll()
+                waiting |= a.result is None
+        if waiting:
+            return None
+        self.in_flight = False
+        done = [a for a in self.members if a.result]
+        self.members = [a for a in self.members if not a.result]
+        return done
+
+    def close(self) -> None:
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
+
+
 MAX_PASSED = 16       # admissions past one waiting request before it blocks the queue
 SCAN_DEPTH = 256      # queued requests looked at per admission round
 
@@ -258,13 +308,15 @@ class Server:
     cluster of that size, every room's in one launch, and rooms above
     Tuner.CLUSTER_MAX_CELLS run beside the batch on their own streams;
     batch_cluster=0: every room joins the batch with the one-kernel-per-pass
-    solve."""
+    solve.  batch_groups (default 2): the batched rooms are spread over that
+    many batches, each with its own stream and chunks."""
 
     def __init__(self, mem_budget: int, max_active: int = 64, tuner: Optional[Tuner] = None,
                  keep_fields: bool = False, batched: bool = False, chunk: int = 10, warm_start: bool = True,
-                 batch_graph: bool = True, batch_cluster: int = 16):
+                 batch_graph: bool = True, batch_cluster: int = 16, batch_groups: int = 2):
         self.batch_graph = batch_graph
         self.batch_cluster = batch_cluster
+        self.batch_groups = batch_groups
         self.mem_budget = mem_budget
         self.max_active = max_active
         self.tuner = tuner or Tuner()
@@ -292,74 +344,57 @@ class Server:
     def _run_batched(self, requests: List[Request], realtime: bool) -> List[Outcome]:
         """Batch members advance together in chunks (one launch per stage);
         with batch_cluster, rooms above the one-cluster size run beside the
-        batch on their own streams with the tuner's schedule.  Members join
-        and leave only between batch chunks."""
+        batch on their own streams with the tuner's schedule.  Members are
+        spread over `batch_groups` batches (each on its own stream, so one
+        group's predictor and correction overlap another's solve); a member
+        joins or leaves its group only between that group's chunks."""
         adm = _Admission(requests)
-        members: List[_Active] = []
+        groups = [_Group() for _ in range(max(1, self.batch_groups))]
         solo: List[_Active] = []
         used = 0
         out: List[Outcome] = []
         t0 = time.perf_counter()
-        batch = None
-        batch_ids: List[int] = []
-        in_flight = False
-        while adm or members or solo:
+
+        def n_active():
+            return len(solo) + sum(len(g.members) for g in groups)
+
+        while adm or solo or any(g.members for g in groups):
             now = time.perf_counter() - t0
-            if not in_flight:
-                while adm and len(members) + len(solo) < self.max_active:
-                    pick = adm.next_fit(now, realtime, used, self.mem_budget, bool(members or solo))
-                    if pick is None:
-                        break
-                    req, need = pick
-                    small = req.room.n_cells <= Tuner.CLUSTER_MAX_CELLS and req.params.poisson == "mgpcg"
-                    if self.batch_cluster and small:
+            idle = [g for g in groups if not g.in_flight]
+            while adm and idle and n_active() < self.max_active:
+                pick = adm.next_fit(now, realtime, used, self.mem_budget, n_active() > 0)
+                if pick is None:
+                    break
+                req, need = pick
+                small = req.room.n_cells <= Tuner.CLUSTER_MAX_CELLS and req.params.poisson == "mgpcg"
+                if self.batch_cluster and not small:
+                    a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields, warm_start=self.warm_start)
+                    a.launch()
+                    solo.append(a)
+                else:
+                    if self.batch_cluster:
                         a = _Active(req, Schedule(0, self.chunk, False, self.batch_cluster), now, self.keep_fields,
                                     warm_start=self.warm_start)
-                        members.append(a)
-                    elif self.batch_cluster:
-                        a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields,
-                                    warm_start=self.warm_start)
-                        a.launch()
-                        solo.append(a)
                     else:
                         a = _Active(req, Schedule(0, self.chunk, False, 0), now, self.keep_fields, split=1,
                                     warm_start=self.warm_start)
-                        members.append(a)
-                    a.charge = need
-                    used += need
-                if members:
-                    ids = [id(a) for a in members]
-                    if batch is None:
-                        batch = capi.BatchHandle([a.h for a in members])
-                        if self.batch_graph:
-                            batch.use_graph(True)
-                    elif ids != batch_ids:
-                        batch.set_rooms([a.h for a in members])
-                    batch_ids = ids
-                    nsteps = min([self.chunk] + [a.req.max_steps - a.steps for a in members])
-                    batch.enqueue(nsteps, True)
-                    for a in members:
-                        a.queued = nsteps
-                        a.result = None
-                    in_flight = True
+                    min(idle, key=lambda g: g.cells()).members.append(a)
+                a.charge = need
+                used += need
+            for g in idle:
+                if g.members:
+                    g.launch(self.chunk, self.batch_graph)
             progressed = False
-            if in_flight:
-                waiting = False
-                for a in members:
-                    if a.result is None:
-                        a.result = a.poll()
-                        waiting |= a.result is None
-                if not waiting:
-                    in_flight = False
-                    progressed = True
-                    still = []
-                    for a in members:
-                        if a.result:
-                            out.append(self._finish(a, t0))
-                            used -= a.charge
-                        else:
-                            still.append(a)
-                    members = still
+            for g in groups:
+                if not g.in_flight:
+                    continue
+                done = g.poll()
+                if done is None:
+                    continue
+                progressed = True
+                for a in done:
+                    out.append(self._finish(a, t0))
+                    used -= a.charge
             still = []
             for a in solo:
                 st = a.poll()
@@ -376,8 +411,8 @@ class Server:
             solo = still
             if not progressed:
                 time.sleep(0.0002)
-        if batch is not None:
-            batch.close()
+        for g in groups:
+            g.close()
         return out
 
     def _run_streams(self, requests: List[Request], realtime: bool = True) -> List[Outcome]:
