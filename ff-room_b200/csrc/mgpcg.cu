@@ -845,271 +845,14 @@ __device__ __forceinline__ void pass_redpost_dot(const PCGArgs &A, int start, in
     }
 }
 
-// ---- fused level-0 post-smoothing (split and batched forms)
-//
-// The black half-sweep with the coarse correction (smooth_color<true> on
-// level 0) and the red half-sweep with r.z (pass_redpost_dot) in one pass:
-// a block owns a tile of kPT_J x kPT_K cells of the (j, k) plane and marches
-// along i over kPT_I-ish planes.  For each plane it first updates the black
-// cells of the next plane over the tile and a one-cell halo into a ring of
-// three planes in shared memory (each value by the very expression the
-// black sweep uses), then the red cells of the current plane from the ring
-// (the expression of the red sweep), so the black values never go through
-// DRAM.  Outputs go to z2, not z: other blocks still read the red values of
-// z (pre-smoothing) for their own halo blocks.  Every cell of z2 is written
-// (cells that are not unknowns keep z's value, zero), so the direction pass
-// can read z2 everywhere.
-constexpr int kPT_J = 8, kPT_K = 32, kPT_I = 16;
-constexpr int kPT_HJ = kPT_J + 2, kPT_HK = kPT_K + 2, kPT_PLANE = kPT_HJ * kPT_HK;
-constexpr int kPostMaxBlocks = 2048;    // partials hold at least this many block sums
-
-struct PostTiles {
-    int nj, nk, ni, ci;     // tiles along j, k, i; planes per i-chunk
-};
-
-__host__ __device__ inline PostTiles post_tiles(int nx, int ny, int nz)
-{
-    PostTiles t;
-    t.nj = (ny + kPT_J - 1) / kPT_J;
-    t.nk = (nz + kPT_K - 1) / kPT_K;
-    int ni = (nx + kPT_I - 1) / kPT_I;
-    const int cap = kPostMaxBlocks / (t.nj * t.nk > 0 ? t.nj * t.nk : 1);
-    if (ni > cap) ni = cap > 0 ? cap : 1;
-    t.ci = (nx + ni - 1) / ni;
-    t.ni = (nx + t.ci - 1) / t.ci;
-    return t;
-}
-
-// The fused pass applies when level 0 is smoothed by grid passes and the
-// tiles fit the partial-sum buffer.
-__host__ __device__ inline bool use_post0(const MGDev &M, int nx, int ny, int nz)
-{
-    const PostTiles t = post_tiles(nx, ny, nz);
-    return M.nlev > 1 && M.nlev_grid >= 1 && M.z2 != nullptr && t.nj * t.nk * t.ni <= kPostMaxBlocks;
-}
-
-__device__ __forceinline__ int post0_blocks_dev(int nx, int ny, int nz)
-{
-    const PostTiles t = post_tiles(nx, ny, nz);
-    return t.nj * t.nk * t.ni;
-}
-
-// Black value of cell (i, j, k) after the level-0 post-smoothing half-sweep
-// (smooth_color<true>, l = 0, colour 1): the same loads and expression.
-__device__ __forceinline__ float post0_black(const PCGArgs &A, int i, int j, int k)
-{
-    const MGDev &M = A.M;
-    const MGLevel &L = M.lv[0];
-    const MGLevel &Lc = M.lv[1 < M.nlev ? 1 : 0];
-    const int c = (i * A.R.ny + j) * A.R.nz + k;
-    const float bc = L.b[c];
-    const unsigned code = A.R.sc[c];
-    float D;
-    const float s = fine_nbsum<true>(A.R, M, L, Lc, code, c, i, j, k, D);
-    if (!active_code(code)) return L.x[c];
-    return (bc + s) / D;
-}
-
-__device__ __forceinline__ void pass_post0(const PCGArgs &A, int lb, double &acc)
-{
-    __shared__ float ring[3][kPT_PLANE];
-    const RoomDev &R = A.R;
-    const MGDev &M = A.M;
-    const float *z = M.lv[0].x;
-    float *z2 = M.z2;
-    const int nx = R.nx, ny = R.ny, nz = R.nz;
-    const PostTiles T = post_tiles(nx, ny, nz);
-    const int tk = lb % T.nk, tj = (lb / T.nk) % T.nj, ti = lb / (T.nk * T.nj);
-    const int j0 = tj * kPT_J, k0 = tk * kPT_K;
-    const int i0 = ti * T.ci, i1 = min(i0 + T.ci, nx);
-    // this thread's column of the tile
-    const int cj = threadIdx.x / kPT_K, ck = threadIdx.x % kPT_K;
-    const int j = j0 + cj, k = k0 + ck;
-    const bool mine = cj < kPT_J && j < ny && k < nz;
-    // black values of plane p over the tile and its halo into ring slot p % 3
-    auto black_plane = [&](int p) {
-        float *dst = ring[(p + 3) % 3];
-        for (int h = threadIdx.x; h < kPT_PLANE; h += blockDim.x) {
-            const int hj = h / kPT_HK, hk = h % kPT_HK;
-            const int jj = j0 - 1 + hj, kk = k0 - 1 + hk;
-            float v = 0.0f;
-            if (p >= 0 && p < nx && jj >= 0 && jj < ny && kk >= 0 && kk < nz && ((p + jj + kk) & 1))
-                v = post0_black(A, p, jj, kk);
-            dst[h] = v;
-        }
-    };
-    black_plane(i0 - 1);
-    black_plane(i0);
-    for (int i = i0; i < i1; i++) {
-        black_plane(i + 1);
-        __syncthreads();
-        if (mine) {
-            const int c = (i * ny + j) * nz + k;
-            const unsigned code = R.sc[c];
-            const int hc = (cj + 1) * kPT_HK + (ck + 1);
-            float zc;
-            if ((i + j + k) & 1) {
-                zc = ring[(i + 3) % 3][hc];
-            } else if (active_code(code)) {
-                const float zn[6] = {ring[(i + 2) % 3][hc], ring[(i + 1) % 3][hc], ring[i % 3][hc - kPT_HK],
-                                     ring[i % 3][hc + kPT_HK], ring[i % 3][hc - 1], ring[i % 3][hc + 1]};
-                float t[6], D;
-                fine_coefs(M, code, i, j, k, t, D);
-                float sum = 0.0f;
-#pragma unroll
-                for (int a = 0; a < 6; a++)
-                    if (t[a] != 0.0f) sum += t[a] * zn[a];
-                zc = (M.r32[c] + sum) / D;
-            } else {
-                zc = z[c];
-            }
-            z2[c] = zc;
-            if (active_code(code)) acc += __ldcs(A.r + c) * (double)zc;
-        }
-        __syncthreads();
-    }
-}
-
-// ---- fused level-0 pre-smoothing and restriction (split and batched forms)
-//
-// The black half-sweep from the red start (smooth_color<false> on level 0)
-// and the restriction of the red residuals to level 1 (restrict_level,
-// l = 0) in one pass, for a level 0 that halves every axis: a block owns a
-// tile of kPT_J x kPT_K cells (even-aligned, so each coarse cell's children
-// lie in one tile) and marches along i in plane pairs.  Black values of the
-// tile and a one-cell halo go to a four-plane ring in shared memory, the red
-// residuals of a plane pair to a second buffer, and one thread per coarse
-// cell sums its red children in restrict_level's order.  The black values
-// are used by the restriction only (the post-smoothing recomputes them), so
-// they never go through DRAM.
-constexpr int kPre_Slots = 4;
-
-__host__ __device__ inline PostTiles pre_tiles(int nx, int ny, int nz)
-{
-    PostTiles t = post_tiles(nx, ny, nz);
-    t.ci = (t.ci + 1) & ~1;                 // even chunks: coarse cells never straddle two
-    t.ni = (nx + t.ci - 1) / t.ci;
-    return t;
-}
-
-__host__ __device__ inline bool use_pre0(const MGDev &M, int nx, int ny, int nz)
-{
-    const PostTiles t = pre_tiles(nx, ny, nz);
-    const int top = M.nlev_grid < M.nlev - 1 ? M.nlev_grid : M.nlev - 1;
-    const int gdown = M.nlev_mid < top ? M.nlev_mid : top;
-    return M.nlev > 1 && gdown >= 1 && M.lv[0].sx && M.lv[0].sy && M.lv[0].sz &&
-           t.nj * t.nk * t.ni <= kPostMaxBlocks;
-}
-
-// Black value of cell (i, j, k) after the level-0 pre-smoothing half-sweep
-// (smooth_color<false>, l = 0, colour 1).
-__device__ __forceinline__ float pre0_black(const PCGArgs &A, int i, int j, int k)
-{
-    const MGDev &M = A.M;
-    const MGLevel &L = M.lv[0];
-    const MGLevel &Lc = M.lv[1 < M.nlev ? 1 : 0];
-    const int c = (i * A.R.ny + j) * A.R.nz + k;
-    const float bc = L.b[c];
-    const unsigned code = A.R.sc[c];
-    float D;
-    const float s = fine_nbsum<false>(A.R, M, L, Lc, code, c, i, j, k, D);
-    if (!active_code(code)) return L.x[c];
-    return (bc + s) / D;
-}
-
-__device__ __forceinline__ void pass_pre0(const PCGArgs &A, int lb)
-{
-    __shared__ float ring[kPre_Slots][kPT_PLANE];
-    __shared__ float rres[2][kPT_J][kPT_K];
-    __shared__ unsigned char ract[2][kPT_J][kPT_K];
-    const RoomDev &R = A.R;
-    const MGDev &M = A.M;
-    const MGLevel &L = M.lv[0];
-    const MGLevel &C = M.lv[1];
-    const int nx = R.nx, ny = R.ny, nz = R.nz;
-    const PostTiles T = pre_tiles(nx, ny, nz);
-    const int tk = lb % T.nk, tj = (lb / T.nk) % T.nj, ti = lb / (T.nk * T.nj);
-    const int j0 = tj * kPT_J, k0 = tk * kPT_K;
-    const int i0 = ti * T.ci, i1 = min(i0 + T.ci, nx);
-    const int cj = threadIdx.x / kPT_K, ck = threadIdx.x % kPT_K;
-    auto black_plane = [&](int p) {
-        float *dst = ring[(p + kPre_Slots) % kPre_Slots];
-        for (int h = threadIdx.x; h < kPT_PLANE; h += blockDim.x) {
-            const int hj = h / kPT_HK, hk = h % kPT_HK;
-            const int jj = j0 - 1 + hj, kk = k0 - 1 + hk;
-            float v = 0.0f;
-            if (p >= 0 && p < nx && jj >= 0 && jj < ny && kk >= 0 && kk < nz && ((p + jj + kk) & 1))
-                v = pre0_black(A, p, jj, kk);
-            dst[h] = v;
-        }
-    };
-    black_plane(i0 - 1);
-    black_plane(i0);
-    black_plane(i0 + 1);
-    black_plane(i0 + 2);
-    for (int i = i0; i < i1; i += 2) {
-        __syncthreads();
-        // red residuals b - (D x - sum t x_nb) of the plane pair (restrict_level's expression)
-        for (int a = 0; a < 2; a++) {
-            const int ii = i + a, j = j0 + cj, k = k0 + ck;
-            bool act = false;
-            float rv = 0.0f;
-            if (ii < i1 && j < ny && k < nz && ((ii + j + k) & 1) == 0) {
-                const int c = (ii * ny + j) * nz + k;
-                const unsigned code = R.sc[c];
-                const int hc = (cj + 1) * kPT_HK + (ck + 1);
-                const float v[6] = {ring[(ii + kPre_Slots - 1) % kPre_Slots][hc], ring[(ii + 1) % kPre_Slots][hc],
-                                    ring[ii % kPre_Slots][hc - kPT_HK], ring[ii % kPre_Slots][hc + kPT_HK],
-                                    ring[ii % kPre_Slots][hc - 1], ring[ii % kPre_Slots][hc + 1]};
-                float t[6], D;
-                fine_coefs(M, code, ii, j, k, t, D);
-                float s = 0.0f;
-#pragma unroll
-                for (int q = 0; q < 6; q++)
-                    if (t[q] != 0.0f) s += t[q] * v[q];
-                act = active_code(code);
-                rv = L.b[c] - (D * L.x[c] - s);
-            }
-            rres[a][cj][ck] = rv;
-            ract[a][cj][ck] = act ? 1 : 0;
-        }
-        __syncthreads();
-        // one thread per coarse cell of the pair: children in the order a, b, e
-        if (threadIdx.x < (kPT_J / 2) * (kPT_K / 2)) {
-            const int pj = threadIdx.x / (kPT_K / 2), pk = threadIdx.x % (kPT_K / 2);
-            const int I = i >> 1, J = (j0 >> 1) + pj, K = (k0 >> 1) + pk;
-            if (I < C.nx && J < C.ny && K < C.nz) {
-                float sum = 0.0f;
-#pragma unroll
-                for (int a = 0; a < 2; a++)
-#pragma unroll
-                    for (int b = 0; b < 2; b++)
-#pragma unroll
-                        for (int e = 0; e < 2; e++)
-                            if (ract[a][2 * pj + b][2 * pk + e]) sum += rres[a][2 * pj + b][2 * pk + e];
-                const int P = (I * C.ny + J) * C.nz + K;
-                const float DP = C.coef[P].w;
-                C.b[P] = sum;
-                C.x[P] = (((I + J + K) & 1) == 0 && DP != 0.0f) ? sum / DP : 0.0f;
-            }
-        }
-        // the next pair's black planes replace the two this pair no longer needs
-        if (i + 2 < i1) {
-            black_plane(i + 3);
-            black_plane(i + 4);
-        }
-    }
-}
-
 // d = z + beta d_old, the deferred x += alpha_prev d_old, q = M d; acc = d.q
 __device__ __forceinline__ void pass_direction(const PCGArgs &A, int start, int stride, double beta,
                                                double alpha_prev, bool update_x, const double *__restrict__ dold,
-                                               double *__restrict__ dnew, double &acc,
-                                               const float *__restrict__ zsrc = nullptr)
+                                               double *__restrict__ dnew, double &acc)
 {
     const RoomDev &R = A.R;
     const MGDev &M = A.M;
-    const float *z = zsrc ? zsrc : M.lv[0].x;
+    const float *z = M.lv[0].x;
     const int n = R.n, ny = R.ny, nz = R.nz, plane = ny * nz, pk = (nz + 1) >> 1;
     if ((nz & 1) == 0) {
         // Even rows: both cells of every pair, and the pairs of its x and y
@@ -1508,28 +1251,14 @@ __device__ __forceinline__ void sp_redpost_body(const PCGArgs &A, SplitState *ss
     }
 }
 
-__device__ __forceinline__ void sp_post0_body(const PCGArgs &A, SplitState *ss, BPos P)
-{
-    __shared__ double sh[32];
-    double acc[1] = {0.0};
-    pass_post0(A, P.lb, acc[0]);
-    if (last_block_total<1>(acc, A.partials, &ss->ticket, sh, P) && threadIdx.x == 0) {
-        ss->beta = ss->it == 0 ? 0.0 : acc[0] / ss->rz_old;
-        ss->rz_old = acc[0];
-    }
-}
-
-__device__ __forceinline__ void sp_pre0_body(const PCGArgs &A, BPos P) { pass_pre0(A, P.lb); }
-
 __device__ __forceinline__ void sp_direction_body(const PCGArgs &A, SplitState *ss, BPos P, int *active)
 {
     __shared__ double sh[32];
     const double *dold = ss->dpar ? A.db : A.da;
     double *dnew = ss->dpar ? A.da : A.db;
     double acc[1] = {0.0};
-    const float *zsrc = use_post0(A.M, A.R.nx, A.R.ny, A.R.nz) ? A.M.z2 : nullptr;
     pass_direction(A, P.lb * blockDim.x + threadIdx.x, P.nb * blockDim.x, ss->beta, ss->alpha_prev, ss->it > 0,
-                   dold, dnew, acc[0], zsrc);
+                   dold, dnew, acc[0]);
     if (last_block_total<1>(acc, A.partials, &ss->ticket, sh, P) && threadIdx.x == 0) {
         ss->dpar ^= 1;            // the new direction is current from here on
         ss->pending = 0;
@@ -1666,18 +1395,6 @@ __global__ void __launch_bounds__(256) k_sp_redpost(PCGArgs A, SplitState *ss)
     sp_redpost_body(A, ss, grid_pos());
 }
 
-__global__ void __launch_bounds__(256) k_sp_pre0(PCGArgs A, const SplitState *ss)
-{
-    if (ss->done) return;
-    sp_pre0_body(A, grid_pos());
-}
-
-__global__ void __launch_bounds__(256) k_sp_post0(PCGArgs A, SplitState *ss)
-{
-    if (ss->done) return;
-    sp_post0_body(A, ss, grid_pos());
-}
-
 __global__ void __launch_bounds__(256, 3) k_sp_direction(PCGArgs A, SplitState *ss)
 {
     if (ss->done) return;
@@ -1785,26 +1502,6 @@ __global__ void __launch_bounds__(256) k_bsp_redpost(BatchDev D, BMap m)
     sp_redpost_body(A, D.ss[r], P);
 }
 
-__global__ void __launch_bounds__(256) k_bsp_pre0(BatchDev D, BMap m)
-{
-    __shared__ __align__(16) PCGArgs A;
-    BPos P;
-    const int r = bmap(m, P);
-    if (D.ss[r]->done) return;
-    load_args(A, D.args + r);
-    sp_pre0_body(A, P);
-}
-
-__global__ void __launch_bounds__(256) k_bsp_post0(BatchDev D, BMap m)
-{
-    __shared__ __align__(16) PCGArgs A;
-    BPos P;
-    const int r = bmap(m, P);
-    if (D.ss[r]->done) return;
-    load_args(A, D.args + r);
-    sp_post0_body(A, D.ss[r], P);
-}
-
 __global__ void __launch_bounds__(256, 3) k_bsp_direction(BatchDev D, BMap m)
 {
     __shared__ __align__(16) PCGArgs A;
@@ -1862,7 +1559,7 @@ size_t mg_bytes(const HostRoom &r, const MGHost &h)
 {
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const RoomGeom &g = r.g;
-    size_t b = 3 * al(4 * g.n) + 9 * al(4 * std::max(g.nx, std::max(g.ny, g.nz)));
+    size_t b = 2 * al(4 * g.n) + 9 * al(4 * std::max(g.nx, std::max(g.ny, g.nz)));
     for (size_t l = 1; l < h.nx.size(); l++) {
         const size_t m = (size_t)h.nx[l] * h.ny[l] * h.nz[l];
         b += al(16 * m) + 2 * al(4 * m);
@@ -1914,9 +1611,8 @@ int mg_upload(const HostRoom &r, const MGHost &h, const RoomDev &R, Arena &ar, H
     M.lv[0].coef = nullptr;
     M.lv[0].x = ar.take<float>(g.n);
     M.r32 = ar.take<float>(g.n);
-    M.z2 = ar.take<float>(g.n);
     M.lv[0].b = M.r32;
-    if (!M.r32 || !M.z2 || !fzr) return fail(FFR_ENOMEM, "arena exhausted (multigrid)");
+    if (!M.r32 || !fzr) return fail(FFR_ENOMEM, "arena exhausted (multigrid)");
     {
         float *dev[9] = {fx, fxl, fxr, fy, fyl, fyr, fz, fzl, fzr};
         const std::vector<float> *src[9] = {&dx, &ixl, &ixr, &dy, &iyl, &iyr, &dz, &izl, &izr};
@@ -2116,11 +1812,8 @@ unsigned split_body_kernels(const MGDev &M)
     const int top = std::min(M.nlev_grid, M.nlev - 1);
     const int gdown = std::min(M.nlev_mid, top);
     unsigned k = 2u * (unsigned)gdown;                        // grid levels: smooth + restrict
-    if (use_pre0(M, M.lv[0].nx, M.lv[0].ny, M.lv[0].nz)) k -= 1;  // level 0: one fused pass
     if (M.nlev_mid < top || M.nlev_grid < M.nlev) k += 1;     // k_sp_mid
     k += 2u * (unsigned)std::max(0, gdown - 1);               // grid levels gdown-1 .. 1 post-smooth
-    if (use_post0(M, M.lv[0].nx, M.lv[0].ny, M.lv[0].nz))
-        return k + 3;                                         // fused post-smooth + r.z, direction, residual
     if (M.nlev_grid >= 1) k += 1;                             // level-0 black post-smooth
     return k + 3;                                             // red post + r.z, direction, residual
 }
@@ -2131,7 +1824,6 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
 {
     const MGDev &M = a.M;
     const unsigned cb = split_blocks_level0(a.R.n);
-    const bool fused = use_post0(M, a.R.nx, a.R.ny, a.R.nz);
     int rc = FFR_OK;
     auto chk = [&]() {
         cudaError_t e = cudaGetLastError();
@@ -2141,14 +1833,7 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
     if (M.nlev > 1) {
         const int top = std::min(M.nlev_grid, M.nlev - 1);
         const int gdown = std::min(M.nlev_mid, top);
-        const bool pre0 = use_pre0(M, a.R.nx, a.R.ny, a.R.nz);
         for (int l = 0; l < gdown; l++) {
-            if (l == 0 && pre0) {
-                const PostTiles T = pre_tiles(a.R.nx, a.R.ny, a.R.nz);
-                k_sp_pre0<<<(unsigned)(T.nj * T.nk * T.ni), kPT_J * kPT_K, 0, bs>>>(a, ss);
-                chk();
-                continue;
-            }
             k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
             chk();
             k_sp_restrict<<<split_blocks_cells(M, l + 1), 256, 0, bs>>>(a, ss, l);
@@ -2177,17 +1862,12 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
             k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 0);
             chk();
         }
-        if (M.nlev_grid >= 1 && !fused) {
+        if (M.nlev_grid >= 1) {
             k_sp_smooth<true><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 1);
             chk();
         }
     }
-    if (fused) {
-        const PostTiles T = post_tiles(a.R.nx, a.R.ny, a.R.nz);
-        k_sp_post0<<<(unsigned)(T.nj * T.nk * T.ni), kPT_J * kPT_K, 0, bs>>>(a, ss);
-    } else {
-        k_sp_redpost<<<cb, 256, 0, bs>>>(a, ss);
-    }
+    k_sp_redpost<<<cb, 256, 0, bs>>>(a, ss);
     chk();
     k_sp_direction<<<cb, 256, 0, bs>>>(a, ss);
     chk();
@@ -2329,8 +2009,6 @@ struct RoomShape {
     int gdown;                    // grid levels smoothed and restricted on the way down
     unsigned pairs[kMaxLevels], coarse[kMaxLevels];
     bool mid;                     // has levels small enough for one block
-    unsigned post0;               // blocks of the fused level-0 post-smoothing (0: separate passes)
-    unsigned pre0;                // blocks of the fused level-0 pre-smoothing + restriction (0: separate)
 };
 
 RoomShape room_shape(const PCGArgs &a)
@@ -2350,14 +2028,6 @@ RoomShape room_shape(const PCGArgs &a)
             r.coarse[l] = split_blocks_cells(M, l + 1);
         }
         r.mid = M.nlev_grid < M.nlev;
-    }
-    if (use_post0(M, a.R.nx, a.R.ny, a.R.nz)) {
-        const PostTiles T = post_tiles(a.R.nx, a.R.ny, a.R.nz);
-        r.post0 = (unsigned)(T.nj * T.nk * T.ni);
-    }
-    if (use_pre0(M, a.R.nx, a.R.ny, a.R.nz)) {
-        const PostTiles T = pre_tiles(a.R.nx, a.R.ny, a.R.nz);
-        r.pre0 = (unsigned)(T.nj * T.nk * T.ni);
     }
     return r;
 }
@@ -2395,29 +2065,16 @@ int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std
         std::vector<int> room, first;
         unsigned total = 0;
     };
-    Tab t_cells0, t_pairs[kMaxLevels], t_coarse[kMaxLevels], t_post0, t_bpost0, t_redpost;
+    Tab t_cells0, t_pairs[kMaxLevels], t_coarse[kMaxLevels];
     std::vector<unsigned> nb(n);
     for (int r = 0; r < n; r++) nb[r] = sh[r].cb;
     t_cells0.total = build_map(t_cells0.room, t_cells0.first, nb);
-    // level-0 post-smoothing: fused for the rooms that take it, the black
-    // sweep and the red sweep + r.z as separate passes for the others
-    for (int r = 0; r < n; r++) nb[r] = sh[r].post0;
-    t_post0.total = build_map(t_post0.room, t_post0.first, nb);
-    for (int r = 0; r < n; r++) nb[r] = (!sh[r].post0 && sh[r].gdown >= 1) ? sh[r].pairs[0] : 0;
-    t_bpost0.total = build_map(t_bpost0.room, t_bpost0.first, nb);
-    for (int r = 0; r < n; r++) nb[r] = sh[r].post0 ? 0 : sh[r].cb;
-    t_redpost.total = build_map(t_redpost.room, t_redpost.first, nb);
-    // level 0 on the way down: rooms with the fused pre-smoothing +
-    // restriction take it (pre0), the others the two passes
     for (int l = 0; l < nlev; l++) {
-        for (int r = 0; r < n; r++) nb[r] = (l < sh[r].gdown && !(l == 0 && sh[r].pre0)) ? sh[r].pairs[l] : 0;
+        for (int r = 0; r < n; r++) nb[r] = l < sh[r].gdown ? sh[r].pairs[l] : 0;
         t_pairs[l].total = build_map(t_pairs[l].room, t_pairs[l].first, nb);
-        for (int r = 0; r < n; r++) nb[r] = (l < sh[r].gdown && !(l == 0 && sh[r].pre0)) ? sh[r].coarse[l] : 0;
+        for (int r = 0; r < n; r++) nb[r] = l < sh[r].gdown ? sh[r].coarse[l] : 0;
         t_coarse[l].total = build_map(t_coarse[l].room, t_coarse[l].first, nb);
     }
-    Tab t_pre0;
-    for (int r = 0; r < n; r++) nb[r] = sh[r].pre0;
-    t_pre0.total = build_map(t_pre0.room, t_pre0.first, nb);
     std::vector<int> mids;
     for (int r = 0; r < n; r++)
         if (sh[r].mid) mids.push_back(r);
@@ -2430,8 +2087,6 @@ int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std
     size_t bytes = al(sizeof(PCGArgs) * n) + al(sizeof(void *) * n) + al(sizeof(int)) +
                    al(4 * (t_cells0.room.size() + t_cells0.first.size())) + al(4 * (mids.size() + 1)) +
                    al(4 * n);
-    for (const Tab *t : {&t_post0, &t_bpost0, &t_redpost, &t_pre0})
-        bytes += al(4 * (t->room.size() + t->first.size()));
     for (int l = 0; l < nlev; l++)
         bytes += al(4 * (t_pairs[l].room.size() + t_pairs[l].first.size())) +
                  al(4 * (t_coarse[l].room.size() + t_coarse[l].first.size()));
@@ -2467,14 +2122,6 @@ int batch_split_build(BatchSplit &B, const std::vector<PCGArgs> &args, const std
     };
     put_map(t_cells0, B.cells0);
     B.nb_cells0 = t_cells0.total;
-    put_map(t_post0, B.post0);
-    B.nb_post0 = t_post0.total;
-    put_map(t_bpost0, B.bpost0);
-    B.nb_bpost0 = t_bpost0.total;
-    put_map(t_redpost, B.redpost);
-    B.nb_redpost = t_redpost.total;
-    put_map(t_pre0, B.pre0);
-    B.nb_pre0 = t_pre0.total;
     for (int l = 0; l < nlev; l++) {
         put_map(t_pairs[l], B.pairs[l]);
         B.nb_pairs[l] = t_pairs[l].total;
@@ -2509,10 +2156,6 @@ int batch_iteration(BatchSplit &B, cudaStream_t s)
         if (e != cudaSuccess && rc == FFR_OK) rc = cuda_fail(e, what);
         count_launch(1);
     };
-    if (B.nb_pre0) {
-        k_bsp_pre0<<<B.nb_pre0, kPT_J * kPT_K, 0, s>>>(B.D, B.pre0);
-        chk("k_bsp_pre0");
-    }
     for (int l = 0; l < B.nlev; l++) {
         if (!B.nb_pairs[l]) continue;
         k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 1);
@@ -2531,18 +2174,12 @@ int batch_iteration(BatchSplit &B, cudaStream_t s)
         k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 0);
         chk("k_bsp_smooth");
     }
-    if (B.nb_bpost0) {
-        k_bsp_smooth<true><<<B.nb_bpost0, 256, 0, s>>>(B.D, B.bpost0, 0, 1);
+    if (B.nlev >= 1 && B.nb_pairs[0]) {
+        k_bsp_smooth<true><<<B.nb_pairs[0], 256, 0, s>>>(B.D, B.pairs[0], 0, 1);
         chk("k_bsp_smooth");
     }
-    if (B.nb_redpost) {
-        k_bsp_redpost<<<B.nb_redpost, 256, 0, s>>>(B.D, B.redpost);
-        chk("k_bsp_redpost");
-    }
-    if (B.nb_post0) {
-        k_bsp_post0<<<B.nb_post0, kPT_J * kPT_K, 0, s>>>(B.D, B.post0);
-        chk("k_bsp_post0");
-    }
+    k_bsp_redpost<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
+    chk("k_bsp_redpost");
     k_bsp_direction<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
     chk("k_bsp_direction");
     k_bsp_residual<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);

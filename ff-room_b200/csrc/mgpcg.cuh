@@ -37,8 +37,6 @@ struct MGDev {
     double s64x, s64y, s64z, vol64;   // uniform: FP64 stencil scales 1/h^2 and cell volume
     double diag64;                    // uniform: FP64 diagonal of an all-interior row
     float *r32;           // FP32 copy of the scaled CG residual (level-0 rhs)
-    float *z2;            // level-0 preconditioned residual after the fused post-smoothing
-                          // (split and batched forms; the direction pass reads it)
 };
 
 // Host side: the level sizes of a room's hierarchy.
@@ -154,12 +152,8 @@ struct BatchSplit {
     unsigned nb_pairs[kMaxLevels]{}, nb_coarse[kMaxLevels]{};
     BMap post[kMaxLevels]{};          // up-sweep smoothing of level l >= 1
     unsigned nb_post[kMaxLevels]{};
-    BMap post0{};                     // fused level-0 post-smoothing (rooms that take it)
+    BMap post0{};                     // level-0 black post-smoothing
     unsigned nb_post0 = 0;
-    BMap bpost0{}, redpost{};         // the separate level-0 post passes of the other rooms
-    unsigned nb_bpost0 = 0, nb_redpost = 0;
-    BMap pre0{};                      // fused level-0 pre-smoothing + restriction
-    unsigned nb_pre0 = 0;
     const int *mid_rooms = nullptr;   // rooms with levels small enough for one block
     const int *cluster_order = nullptr;   // rooms largest first (one-cluster-per-room launch)
     int nmid = 0;

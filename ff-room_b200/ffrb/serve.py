@@ -34,7 +34,7 @@ from .scene import RoomSpec, SceneConfig, build_room
 # the multigrid extra (FP32 z and residual, coarse levels, about 1/7 of the
 # fine level at 24 bytes per cell)
 BYTES_PER_CELL = 6 * 8 + 3 * 8 + 4 * 8 + 2 + 3 + 1
-MG_BYTES_PER_CELL = 8 + 4 + 4
+MG_BYTES_PER_CELL = 8 + 4
 
 
 def estimate_bytes(room: RoomSpec, params: FluidParams) -> int:
