@@ -45,13 +45,20 @@ FALLBACK_HBM = 6650.0
 CG_INIT_B = 50.0       # read u*,v*,w* + code, write r, d, x
 CG_ITER_B = 74.0       # phase A (r, d_old, x, code -> d, Ad, x) + phase B (r, Ad -> r)
 CG_FINAL_B = 24.0      # x += alpha d
-# Multigrid-preconditioned CG (k_pcg), per fine cell.  Per iteration: the
-# level-0 passes (black pre-smooth 15, restriction 11, black post-smooth
-# 15.5, red post-smooth + r.z 23, direction/operator 47, residual update 35)
-# plus ~16 for the coarse levels (16-byte coefficients, 1/8 the cells per
-# level); once per solve: set-up 60 and the final x update 24.
-PCG_ITER_B = 163.0
-PCG_ONCE_B = 84.0
+# Multigrid-preconditioned CG, split form (the bench path), per fine cell:
+# the level-0 arrays each pass must move through DRAM, counted once per pass
+# (level 1 and below, 24 MB and less for the large room, stay in L2 and
+# count nothing).  Per iteration: residual update 34 (r read and written, q,
+# code; r32 and z written), black pre-smoothing 14 (z, r32, code read, z
+# written; the colours share DRAM sectors), restriction 11 (z, r32, code;
+# the level-1 rhs), black post-smoothing 14.5 (the same plus the level-1
+# correction), red post-smoothing + r.z 22 (z, r32, code, r; z written),
+# direction + operator 46 (z, d_old, x, code; d, q, x written).  Once per
+# solve: the warm-start extrapolation 40, the set-up 68 (predicted faces,
+# code, the previous pressure; r, two directions, r32, z written) and the
+# final x update 24.
+PCG_ITER_B = 141.5
+PCG_ONCE_B = 132.0
 # LBM step kernel per lattice cell: read and write 19 populations, the
 # flag byte, the cell velocity (FP64 with FP64 populations, else FP32) and
 # p (FP64); boundary cells also read a 4-byte blocked-direction mask.
@@ -233,6 +240,10 @@ def run_ours(args, rank: int, world: int, dist):
                 "algorithmic_bytes_per_launch": bytes_cg / launches_cg,
                 "share_of_step": round(prof.get("pressure", prof.get("pressure_estimate"))[0] / ms, 4),
                 "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}
+        if roof["traffic"]:
+            # the same launch judged by the DRAM bytes ncu measured for it
+            t_launch = (ms_solve / 1e3) if args.graph else (prof["pressure"][0] / 1e3 / launches_cg)
+            roof["frac_by_traffic"] = round(roof["traffic"] / t_launch / 1e9 / peak, 4)
         if args.graph:
             roof["timing"] = "pressure solve of the last step re-run 3x from its own CUDA graph"
         extra = {"cg_iterations_mean": float(np.mean(iters)), "velocity_change_last": recs[-1]["velocity_change"]}

@@ -309,7 +309,7 @@ __device__ __forceinline__ void stencil_term(unsigned cls, double s, double xn, 
 // the block partials of d.Ad; phase B does r -= alpha*Ad and ||r||^2.  Each
 // phase ends in a deterministic grid-wide sum.  Stopping rules, the
 // |d.Ad| < 1e-30 break and the returned residual follow the reference.
-__global__ void __launch_bounds__(256) k_cg(CGArgs A)
+__global__ void __launch_bounds__(256, 4) k_cg(CGArgs A)
 {
     __shared__ double sh[32];
     if (A.st && A.st->halt) return;
@@ -354,14 +354,26 @@ __global__ void __launch_bounds__(256) k_cg(CGArgs A)
         int it = 0;
         for (; it < A.max_iter; it++) {
             double dacc[1] = {0.0};
-            for (int c = t0; c < n; c += nth) {
+            // the cells of this thread in the same order as before (so every
+            // partial sum is unchanged); coordinates carried by the walk, and
+            // every load issued before the stencil code is tested (neighbour
+            // indices clamped into the array; a clamped value is only ever
+            // used for a neighbour that is an unknown, i.e. inside the room)
+            for (Walk w(t0, nth, ny, nz, n); w.ok(); w.next()) {
+                const int c = w.c, i = w.i, j = w.j, k = w.k;
                 const unsigned code = R.sc[c];
-                double dc;
+                const int nb[6] = {max(c - plane, 0), min(c + plane, n - 1), max(c - nz, 0), min(c + nz, n - 1),
+                                   max(c - 1, 0), min(c + 1, n - 1)};
+                const double dp = dold[c];
+                double dc, dn[6];
                 if (first) {
-                    dc = dold[c];
+                    dc = dp;
+#pragma unroll
+                    for (int q = 0; q < 6; q++) dn[q] = dold[nb[q]];
                 } else {
-                    const double dp = dold[c];
                     dc = fma(beta, dp, r[c]);
+#pragma unroll
+                    for (int q = 0; q < 6; q++) dn[q] = fma(beta, dold[nb[q]], r[nb[q]]);
                     x[c] = fma(alpha_prev, dp, x[c]);
                     dnew[c] = dc;
                 }
@@ -369,16 +381,13 @@ __global__ void __launch_bounds__(256) k_cg(CGArgs A)
                 if (code & SC_SOLID) {
                     a = dc;
                 } else {
-                    const int i = c / plane, rem = c - i * plane, j = rem / nz, k = rem - j * nz;
+                    const double sc6[6] = {sxl[i], sxr[i], syl[j], syr[j], szl[k], szr[k]};
                     double diag = 0.0, off = 0.0;
-#define DIRN(o) (first ? dold[c + (o)] : fma(beta, dold[c + (o)], r[c + (o)]))
-                    if ((code >> 0) & 3) stencil_term((code >> 0) & 3, sxl[i], ((code >> 0) & 3) == SC_IN ? DIRN(-plane) : 0.0, diag, off);
-                    if ((code >> 2) & 3) stencil_term((code >> 2) & 3, sxr[i], ((code >> 2) & 3) == SC_IN ? DIRN(plane) : 0.0, diag, off);
-                    if ((code >> 4) & 3) stencil_term((code >> 4) & 3, syl[j], ((code >> 4) & 3) == SC_IN ? DIRN(-nz) : 0.0, diag, off);
-                    if ((code >> 6) & 3) stencil_term((code >> 6) & 3, syr[j], ((code >> 6) & 3) == SC_IN ? DIRN(nz) : 0.0, diag, off);
-                    if ((code >> 8) & 3) stencil_term((code >> 8) & 3, szl[k], ((code >> 8) & 3) == SC_IN ? DIRN(-1) : 0.0, diag, off);
-                    if ((code >> 10) & 3) stencil_term((code >> 10) & 3, szr[k], ((code >> 10) & 3) == SC_IN ? DIRN(1) : 0.0, diag, off);
-#undef DIRN
+#pragma unroll
+                    for (int q = 0; q < 6; q++) {
+                        const unsigned cls = (code >> (2 * q)) & 3u;
+                        if (cls) stencil_term(cls, sc6[q], cls == SC_IN ? dn[q] : 0.0, diag, off);
+                    }
                     if (diag < 1e-30) diag = 1.0;
                     a = diag * dc - off;
                 }
@@ -1180,10 +1189,18 @@ int launch_cg(const CGArgs &a, unsigned blocks, cudaStream_t s)
 // ------------------------------------------------------- fluid handle
 
 // Pressure-solve grid of a room: as many co-resident blocks as it can use.
+// Blocks of the persistent CG launch: co-resident (a cooperative launch).
 unsigned fluid_cg_blocks(const RoomGeom &g)
 {
-    return std::max(1u, std::min(std::max(cg_max_blocks(), pcg_max_blocks()),
-                                 (unsigned)((g.n + kThreads - 1) / kThreads)));
+    return std::max(1u, std::min(cg_max_blocks(), (unsigned)((g.n + kThreads - 1) / kThreads)));
+}
+
+// Block partials both persistent solves may write (four per block).
+size_t fluid_partials(const RoomGeom &g)
+{
+    const unsigned want = (unsigned)((g.n + kThreads - 1) / kThreads);
+    const unsigned most = std::max(1u, std::min(std::max(cg_max_blocks(), pcg_max_blocks()), want));
+    return std::max<size_t>((size_t)most * 4, 2 * 2368);
 }
 
 // Device bytes of one projection handle (its single arena).
@@ -1192,7 +1209,7 @@ size_t fluid_arena_bytes(const HostRoom &room, bool mg, const MGHost &mgh)
     const RoomGeom &g = room.g;
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     return tables_bytes(room) + 2 * (al(8 * g.nu) + al(8 * g.nv) + al(8 * g.nw)) + (mg ? 9 : 7) * al(8 * g.n) +
-           al(8 * std::max<size_t>(fluid_cg_blocks(g) * 4, 2 * 2368)) + al(8 * stream_blocks(g.n)) + al(256) +
+           al(8 * fluid_partials(g)) + al(8 * stream_blocks(g.n)) + al(256) +
            al(sizeof(GridSync)) + al(sizeof(CGScalars)) + al(sizeof(StepState)) +
            al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (mg ? mg_bytes(room, mgh) : 0);
 }
@@ -1437,7 +1454,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
         s->p0 = a.take<double>(g.n);
         s->pprev = a.take<double>(g.n);
     }
-    s->partials = a.take<double>(std::max<size_t>(s->cg_blocks * 4, 2 * 2368));
+    s->partials = a.take<double>(fluid_partials(g));
     s->tpart = a.take<double>(s->blocks_cells);
     s->split_state = a.take<char>(256);
     s->gs = a.take<GridSync>(1);
