@@ -141,6 +141,17 @@ def scaled_traffic(per_unit, units):
     return None if per_unit is None else per_unit * units
 
 
+def solve_traffic(mg: bool, cells: int, iters: float):
+    """DRAM bytes of one pressure solve from the measured per-cell figures:
+    per iteration, plus once per solve (set-up, warm start, final update)
+    for the multigrid solve."""
+    if not mg:
+        return scaled_traffic(load_traffic("cg_bytes_per_cell_iter"), cells * iters)
+    it = load_traffic("pcg_split_bytes_per_cell_iter")
+    once = load_traffic("pcg_split_bytes_per_cell_once") or 0.0
+    return None if it is None else cells * (once + it * iters)
+
+
 # ------------------------------------------------------------- workloads
 
 def make_workload(name: str, precision: str, grid=None):
@@ -234,9 +245,7 @@ def run_ours(args, rank: int, world: int, dist):
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 # measured DRAM bytes per cell and iteration (ncu, full-size
                 # room) times the cells and iterations of one launch
-                "traffic": scaled_traffic(load_traffic("pcg_split_bytes_per_cell_iter" if mg else
-                                                       "cg_bytes_per_cell_iter"),
-                                          cells * (it_solve if args.graph else float(np.mean(iters)))),
+                "traffic": solve_traffic(mg, cells, it_solve if args.graph else float(np.mean(iters))),
                 "algorithmic_bytes_per_launch": bytes_cg / launches_cg,
                 "share_of_step": round(prof.get("pressure", prof.get("pressure_estimate"))[0] / ms, 4),
                 "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}
