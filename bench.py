@@ -527,9 +527,14 @@ def run_batch256(steps: int = 500, engines=("batched", "streams")):
     for eng in engines:
         Server(mem_budget=int(free * 0.5), max_active=len(reqs), batched=(eng == "batched"), chunk=2).run(
             warm, realtime=False)
+    from ffrb.tune import TUNED_TABLE, load_tuned
+    tuner = load_tuned()
+    out["schedules"] = ("streams engine: the tuned per-size-class table (ffrb/tuned_b200.json)"
+                        if os.path.exists(TUNED_TABLE) else "streams engine: default schedules")
     for eng in engines:
         l0 = capi.launch_count()
-        srv = Server(mem_budget=int(free * 0.6), max_active=len(reqs), batched=(eng == "batched"), chunk=50)
+        srv = Server(mem_budget=int(free * 0.6), max_active=len(reqs), batched=(eng == "batched"), chunk=50,
+                     tuner=tuner)
         with ClockSampler(torch.cuda.current_device()) as clk:
             t0 = time.perf_counter()
             res = srv.run(reqs, realtime=False)
@@ -627,8 +632,13 @@ def run_serving_c5(n: int = 96, max_steps: int = 200, tol: float = 1e-4, max_cel
                       + (f" with <= {max_cells} cells" if max_cells else " (full size mix)")
                       + f", arriving in real time over {reqs[-1].t_arrival:.2f} s")}
     results = {}
+    from ffrb.tune import TUNED_TABLE, load_tuned
+    tuner = load_tuned()
+    out["schedules"] = ("streams engine: the tuned per-size-class table (ffrb/tuned_b200.json)"
+                        if os.path.exists(TUNED_TABLE) else "streams engine: default schedules")
     for eng in engines:
-        srv = Server(mem_budget=int(free * 0.6), max_active=64, batched=(eng == "batched"), chunk=10)
+        srv = Server(mem_budget=int(free * 0.6), max_active=64, batched=(eng == "batched"), chunk=10,
+                     tuner=tuner)
         srv.run(warm, realtime=False)
         l0 = capi.launch_count()
         with ClockSampler(torch.cuda.current_device()) as clk:
