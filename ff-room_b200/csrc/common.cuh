@@ -312,43 +312,6 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *slot, doub
 
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
-// Programmatic dependent launch.  A kernel launched with launch_pdl may be
-// scheduled while the kernel before it on the stream drains; pdl_wait()
-// blocks until that kernel has completed and its memory is visible, so it
-// comes before the first access to anything the predecessor writes (a no-op
-// for a kernel launched without the attribute).  pdl_trigger() lets the
-// next kernel start launching once every block of this one has started.
-#ifndef FFR_PDL
-#define FFR_PDL 1
-#endif
-__device__ __forceinline__ void pdl_wait()
-{
-#if FFR_PDL
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-#endif
-}
-__device__ __forceinline__ void pdl_trigger()
-{
-#if FFR_PDL
-    asm volatile("griddepcontrol.launch_dependents;" :::);
-#endif
-}
-
-template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = FFR_PDL;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
-}
-
 // Event-pair timing of kernel groups on one stream (host side).
 struct GroupTimer {
     bool on = false;

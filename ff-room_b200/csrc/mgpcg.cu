@@ -1372,24 +1372,18 @@ __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
 __global__ void __launch_bounds__(256) k_sp_init(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
                                                  int use_cond)
 {
-    pdl_wait();
-    pdl_trigger();
     sp_init_body(A, ss, grid_pos(), nullptr, cond, use_cond);
 }
 
 template <bool CORR>
 __global__ void __launch_bounds__(256, FFR_LB_SMOOTH) k_sp_smooth(PCGArgs A, const SplitState *ss, int l, int color)
 {
-    pdl_wait();
-    pdl_trigger();
     if (ss->done) return;
     smooth_color<CORR>(A, A.M.lv, A.M.nlev, l, color, gtid(), gthreads());
 }
 
 __global__ void __launch_bounds__(256, FFR_LB_SMOOTH) k_sp_restrict(PCGArgs A, const SplitState *ss, int l)
 {
-    pdl_wait();
-    pdl_trigger();
     if (ss->done) return;
     restrict_level(A, A.M.lv, l, gtid(), gthreads());
 }
@@ -1402,24 +1396,18 @@ __global__ void __launch_bounds__(1024) k_sp_coarse(PCGArgs A, const SplitState 
 
 __global__ void __launch_bounds__(kMidThreads, 1) k_sp_mid(PCGArgs A, const SplitState *ss, int mid)
 {
-    pdl_wait();
-    pdl_trigger();
     if (ss->done) return;   // the same value in every block of the cluster
     sp_mid_body(A, mid);
 }
 
 __global__ void __launch_bounds__(256, FFR_LB_RES) k_sp_redpost(PCGArgs A, SplitState *ss)
 {
-    pdl_wait();
-    pdl_trigger();
     if (ss->done) return;
     sp_redpost_body(A, ss, grid_pos());
 }
 
 __global__ void __launch_bounds__(256, FFR_LB_DIR) k_sp_direction(PCGArgs A, SplitState *ss)
 {
-    pdl_wait();
-    pdl_trigger();
     if (ss->done) return;
     sp_direction_body(A, ss, grid_pos(), nullptr);
 }
@@ -1427,8 +1415,6 @@ __global__ void __launch_bounds__(256, FFR_LB_DIR) k_sp_direction(PCGArgs A, Spl
 __global__ void __launch_bounds__(256, FFR_LB_RES) k_sp_residual(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
                                                      int use_cond)
 {
-    pdl_wait();
-    pdl_trigger();
     if (ss->done) {
         if (use_cond && gtid() == 0) cudaGraphSetConditional(cond, 0);
         return;
@@ -1443,16 +1429,12 @@ __global__ void __launch_bounds__(256) k_sp_extrapolate(PCGArgs A)
 
 __global__ void __launch_bounds__(256) k_sp_final(PCGArgs A, const SplitState *ss)
 {
-    pdl_wait();
-    pdl_trigger();
     if (A.st && A.st->halt) return;
     sp_final_body(A, ss, grid_pos());
 }
 
 __global__ void __launch_bounds__(256) k_sp_backsub(PCGArgs A, const SplitState *ss)
 {
-    pdl_wait();
-    pdl_trigger();
     if (A.st && A.st->halt) return;
     sp_backsub_body(A, ss, grid_pos());
 }
@@ -1863,9 +1845,9 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
         const int top = std::min(M.nlev_grid, M.nlev - 1);
         const int gdown = std::min(M.nlev_mid, top);
         for (int l = 0; l < gdown; l++) {
-            launch_pdl(k_sp_smooth<false>, split_blocks_pairs(M, l), 256, bs, a, ss, l, 1);
+            k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
             chk();
-            launch_pdl(k_sp_restrict, split_blocks_cells(M, l + 1), 256, bs, a, ss, l);
+            k_sp_restrict<<<split_blocks_cells(M, l + 1), 256, 0, bs>>>(a, ss, l);
             chk();
         }
         if (M.nlev_mid < top || M.nlev_grid < M.nlev) {
@@ -1874,35 +1856,33 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
             cfg.gridDim = dim3((unsigned)ctas);
             cfg.blockDim = dim3(kMidThreads);
             cfg.stream = bs;
-            cudaLaunchAttribute attr[2];
+            cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
             attr[0].val.clusterDim.x = (unsigned)ctas;
             attr[0].val.clusterDim.y = 1;
             attr[0].val.clusterDim.z = 1;
-            attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-            attr[1].val.programmaticStreamSerializationAllowed = FFR_PDL;
             cfg.attrs = attr;
-            cfg.numAttrs = 2;
+            cfg.numAttrs = 1;
             cudaError_t e = cudaLaunchKernelEx(&cfg, k_sp_mid, a, (const SplitState *)ss, M.nlev_mid);
             if (e != cudaSuccess && rc == FFR_OK) rc = cuda_fail(e, "cudaLaunchKernelEx(k_sp_mid)");
             chk();
         }
         for (int l = gdown - 1; l >= 1; l--) {
-            launch_pdl(k_sp_smooth<true>, split_blocks_pairs(M, l), 256, bs, a, ss, l, 1);
+            k_sp_smooth<true><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
             chk();
-            launch_pdl(k_sp_smooth<false>, split_blocks_pairs(M, l), 256, bs, a, ss, l, 0);
+            k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 0);
             chk();
         }
         if (M.nlev_grid >= 1) {
-            launch_pdl(k_sp_smooth<true>, split_blocks_pairs(M, 0), 256, bs, a, ss, 0, 1);
+            k_sp_smooth<true><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 1);
             chk();
         }
     }
-    launch_pdl(k_sp_redpost, cb, 256, bs, a, ss);
+    k_sp_redpost<<<cb, 256, 0, bs>>>(a, ss);
     chk();
-    launch_pdl(k_sp_direction, cb, 256, bs, a, ss);
+    k_sp_direction<<<cb, 256, 0, bs>>>(a, ss);
     chk();
-    launch_pdl(k_sp_residual, cb, 256, bs, a, ss, cond, use_cond);
+    k_sp_residual<<<cb, 256, 0, bs>>>(a, ss, cond, use_cond);
     chk();
     return rc;
 }
