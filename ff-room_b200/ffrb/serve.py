@@ -67,8 +67,13 @@ class Tuner:
     saved and loaded.
     """
 
-    CANDIDATES = [Schedule(0, 20, False), Schedule(0, 20, True), Schedule(-4, 20, True),
-                  Schedule(-8, 20, True), Schedule(0, 20, True, 16), Schedule(0, 20, True, 8),
+    # Candidates for a server, where a room shares the GPU with others: the
+    # split solve on the whole GPU, or one thread-block cluster of 4-16
+    # blocks per room, each step a graph replay.  The persistent grid-wide
+    # solve is left out: a cooperative grid beside other rooms' kernels is
+    # only co-resident once they leave room for it, and its grid barriers
+    # then wait (up to the device wait limit) on blocks that are not running.
+    CANDIDATES = [Schedule(0, 20, True), Schedule(0, 20, True, 16), Schedule(0, 20, True, 8),
                   Schedule(0, 20, True, 4)]
 
     def __init__(self, table: Optional[Dict[int, Schedule]] = None):

@@ -39,9 +39,9 @@ def load_tuned(path: str = TUNED_TABLE) -> Tuner:
     return Tuner.from_json(d.get("table", d))
 
 
-def sample_rooms(n_stream: int = 64, n_batch: int = 32):
+def sample_rooms(n_stream: int = 400, n_batch: int = 128, per_class: int = 12):
     """Rooms of the serving stream (seed 11) and of the 256-room batch
-    (seed 7): up to four per size class from each."""
+    (seed 7): up to per_class of each size class."""
     from . import workloads
     from .params import params_from_scene
     from .scene import build_room
@@ -52,7 +52,7 @@ def sample_rooms(n_stream: int = 64, n_batch: int = 32):
         picked.setdefault(size_class(int(np.prod(c.room.grid))), []).append((c, params_from_scene(c)))
     rooms, params = [], []
     for cls in sorted(picked):
-        for cfg, p in picked[cls][:4]:
+        for cfg, p in picked[cls][:per_class]:
             rooms.append(build_room(cfg))
             params.append(p)
     return rooms, params
@@ -62,7 +62,8 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=TUNED_TABLE)
     ap.add_argument("--steps", type=int, default=6)
-    ap.add_argument("--concurrent", type=int, default=4)
+    ap.add_argument("--concurrent", type=int, default=12,
+                    help="rooms of a class timed side by side (a served GPU holds many)")
     args = ap.parse_args()
     rooms, params = sample_rooms()
     t = Tuner()
@@ -71,8 +72,9 @@ def main() -> None:
     took = time.perf_counter() - t0
     out = {"table": t.to_json(), "tuned_seconds": round(took, 1),
            "classes": sorted(int(k) for k in t.to_json()),
-           "how": (f"Tuner.tune over {len(rooms)} rooms (serving stream seed 11, batch seed 7; up to 4 per "
-                   f"size class side by side), {args.steps} steps per candidate, fastest aggregate cell-steps/s")}
+           "how": (f"Tuner.tune over {len(rooms)} rooms (serving stream seed 11, batch seed 7), up to "
+                   f"{args.concurrent} rooms of a size class side by side, {args.steps} steps per candidate, "
+                   f"fastest aggregate cell-steps/s")}
     with open(args.out, "w") as fh:
         json.dump(out, fh, indent=1)
     print(json.dumps(out))
