@@ -611,7 +611,7 @@ def run_lbm_c4(steps: int = 200, warmup: int = 10):
 # ------------------------------------------------ C5: the serving stream
 
 def run_serving_c5(n: int = 96, max_steps: int = 200, tol: float = 1e-4, max_cells: int = None,
-                   engines=("streams", "batched")):
+                   engines=("streams",)):
     """A time-bounded prefix of the serving stream (seed 11, Poisson
     arrivals at 200/s, log-uniform sizes up to 256x256x96): the first n
     requests, arriving in real time, each solved in mixed precision until

@@ -1353,16 +1353,6 @@ __device__ __forceinline__ void sp_mid_body(const PCGArgs &A, int mid)
 
 // ---- one-room kernels (the grid is the room's)
 
-// Minimum resident blocks per SM asked of the level-0 passes (register caps).
-#ifndef FFR_LB_DIR
-#define FFR_LB_DIR 3
-#endif
-#ifndef FFR_LB_RES
-#define FFR_LB_RES 1
-#endif
-#ifndef FFR_LB_SMOOTH
-#define FFR_LB_SMOOTH 1
-#endif
 
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
@@ -1376,13 +1366,13 @@ __global__ void __launch_bounds__(256) k_sp_init(PCGArgs A, SplitState *ss, cuda
 }
 
 template <bool CORR>
-__global__ void __launch_bounds__(256, FFR_LB_SMOOTH) k_sp_smooth(PCGArgs A, const SplitState *ss, int l, int color)
+__global__ void __launch_bounds__(256) k_sp_smooth(PCGArgs A, const SplitState *ss, int l, int color)
 {
     if (ss->done) return;
     smooth_color<CORR>(A, A.M.lv, A.M.nlev, l, color, gtid(), gthreads());
 }
 
-__global__ void __launch_bounds__(256, FFR_LB_SMOOTH) k_sp_restrict(PCGArgs A, const SplitState *ss, int l)
+__global__ void __launch_bounds__(256) k_sp_restrict(PCGArgs A, const SplitState *ss, int l)
 {
     if (ss->done) return;
     restrict_level(A, A.M.lv, l, gtid(), gthreads());
@@ -1400,19 +1390,19 @@ __global__ void __launch_bounds__(kMidThreads, 1) k_sp_mid(PCGArgs A, const Spli
     sp_mid_body(A, mid);
 }
 
-__global__ void __launch_bounds__(256, FFR_LB_RES) k_sp_redpost(PCGArgs A, SplitState *ss)
+__global__ void __launch_bounds__(256) k_sp_redpost(PCGArgs A, SplitState *ss)
 {
     if (ss->done) return;
     sp_redpost_body(A, ss, grid_pos());
 }
 
-__global__ void __launch_bounds__(256, FFR_LB_DIR) k_sp_direction(PCGArgs A, SplitState *ss)
+__global__ void __launch_bounds__(256, 3) k_sp_direction(PCGArgs A, SplitState *ss)
 {
     if (ss->done) return;
     sp_direction_body(A, ss, grid_pos(), nullptr);
 }
 
-__global__ void __launch_bounds__(256, FFR_LB_RES) k_sp_residual(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
+__global__ void __launch_bounds__(256) k_sp_residual(PCGArgs A, SplitState *ss, cudaGraphConditionalHandle cond,
                                                      int use_cond)
 {
     if (ss->done) {

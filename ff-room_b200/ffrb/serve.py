@@ -220,21 +220,21 @@ class _Group:
     def __init__(self):
         self.members: List["_Active"] = []
         self.batch = None
-        self.ids: List[int] = []
+        self.launched: List["_Active"] = []   # the members of the last chunk (held, so never confused with new ones)
         self.in_flight = False
 
     def cells(self) -> int:
         return sum(a.req.room.n_cells for a in self.members)
 
     def launch(self, chunk: int, graph: bool) -> None:
-        ids = [id(a) for a in self.members]
+        same = len(self.members) == len(self.launched) and all(a is b for a, b in zip(self.members, self.launched))
         if self.batch is None:
             self.batch = capi.BatchHandle([a.h for a in self.members])
             if graph:
                 self.batch.use_graph(True)
-        elif ids != self.ids:
+        elif not same:
             self.batch.set_rooms([a.h for a in self.members])
-        self.ids = ids
+        self.launched = list(self.members)
         nsteps = min([chunk] + [a.req.max_steps - a.steps for a in self.members])
         self.batch.enqueue(nsteps, True)
         for a in self.members:
@@ -313,12 +313,12 @@ class Server:
     cluster of that size, every room's in one launch, and rooms above
     Tuner.CLUSTER_MAX_CELLS run beside the batch on their own streams;
     batch_cluster=0: every room joins the batch with the one-kernel-per-pass
-    solve.  batch_groups (default 2): the batched rooms are spread over that
-    many batches, each with its own stream and chunks."""
+    solve.  batch_groups (default 1): the batched rooms may be spread over
+    that many batches, each with its own stream and chunks."""
 
     def __init__(self, mem_budget: int, max_active: int = 64, tuner: Optional[Tuner] = None,
                  keep_fields: bool = False, batched: bool = False, chunk: int = 10, warm_start: bool = True,
-                 batch_graph: bool = True, batch_cluster: int = 16, batch_groups: int = 2):
+                 batch_graph: bool = True, batch_cluster: int = 16, batch_groups: int = 1):
         self.batch_graph = batch_graph
         self.batch_cluster = batch_cluster
         self.batch_groups = batch_groups
