@@ -89,18 +89,29 @@ __device__ __forceinline__ F adv_lw_r(F pm, F pc, F pp, F a, F dt, F ih)
     return (flr - fll) * ih;
 }
 
+// The spacing argument of face_increment along one axis: the cell width
+// for FP64 arithmetic, its correctly rounded FP32 reciprocal (a table of
+// the room) for the mixed-precision mode.
+template <class F>
+__device__ __forceinline__ F axis_spacing(const double *width, const float *rwidth, int i)
+{
+    if constexpr (sizeof(F) == 4) return rwidth[i];
+    else return width[i];
+}
+
 // The predicted increment dt*(-adv + dif) of one face from its stencil
 // values (FluidSolver.cpp:132-162), in arithmetic F.  ax is the advecting
-// velocity along x for this face, etc.; scheme 1 = QUICK (the caller has
+// velocity along x for this face, etc.; hx, hy, hz are axis_spacing<F>
+// values (widths in FP64, reciprocal widths in FP32); scheme 1 = QUICK (the caller has
 // checked its activation range and passes the far neighbours), 2 = LW.
 template <class F>
 __device__ __forceinline__ F face_increment(int use_quick, int lw, F c, F xmm, F xm, F xp, F ymm, F ym, F yp,
                                             F zmm, F zm, F zp, F ax, F ay, F az, F hx, F hy, F hz, F nu, F dt)
 {
     if constexpr (sizeof(F) == 4) {
-        // mixed precision: one correctly rounded reciprocal per axis and
-        // products in place of the six divisions (well inside the mixed bound)
-        const F ix = __frcp_rn(hx), iy = __frcp_rn(hy), iz = __frcp_rn(hz);
+        // mixed precision: products with the correctly rounded reciprocal
+        // widths in place of the six divisions (well inside the mixed bound)
+        const F ix = hx, iy = hy, iz = hz;
         F adv;
         if (use_quick) {
             adv = adv_quick_r(xmm, xm, c, xp, ax, ix) + adv_quick_r(ymm, ym, c, yp, ay, iy) +
@@ -169,12 +180,18 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
     const int pu = ny * nz, lastu = R.nu - 1;
     const int pv = (ny + 1) * nz, lastv = R.nv - 1;
     const int pw = ny * (nz + 1), lastw = R.nw - 1;
+    const InvSpacing I(R);
     // One pass over the corners (i, j, k) of the extended grid
     // (nx+1)(ny+1)(nz+1): the u, v and w faces with that lower corner, so the
     // three components are streamed once between them (three passes, one
     // per component, each re-read the other two after L2 had dropped them).
     for (Walk wk(start, stride, ny + 1, nz + 1, (nx + 1) * (ny + 1) * (nz + 1)); wk.ok(); wk.next()) {
         const int i = wk.i, j = wk.j, k = wk.k;
+        // spacings of the corner's cell (entries past the last cell of an
+        // axis are read only by faces that take no increment)
+        const F hx = axis_spacing<F>(R.dxv, I.fx, min(i, nx - 1));
+        const F hy = axis_spacing<F>(R.dyv, I.fy, min(j, ny - 1));
+        const F hz = axis_spacing<F>(R.dzv, I.fz, min(k, nz - 1));
         if (j < ny && k < nz) {
             const int t = UIX(i, j, k);
             const uint8_t code = R.fcu[t];
@@ -200,8 +217,7 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
                 const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
                 const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
                 val = uc + (double)face_increment<F>(q, lw, F(uc), F(xmm), F(xm), F(xp), F(ymm), F(ym), F(yp),
-                                                     F(zmm), F(zm), F(zp), F(uc), F(av), F(aw), F(R.dxv[i]),
-                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
+                                                     F(zmm), F(zm), F(zp), F(uc), F(av), F(aw), hx, hy, hz, nu, dt);
             }
             us[t] = face_code(code, val, R.fanvel, 0);
         }
@@ -230,8 +246,7 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
                 const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
                 const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
                 val = vc + (double)face_increment<F>(q, lw, F(vc), F(xm), F(xm), F(xp), F(ymm), F(ym), F(yp),
-                                                     F(zm), F(zm), F(zp), F(au), F(vc), F(aw), F(R.dxv[i]),
-                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
+                                                     F(zm), F(zm), F(zp), F(au), F(vc), F(aw), hx, hy, hz, nu, dt);
             }
             vs[f] = face_code(code, val, R.fanvel, 1);
         }
@@ -266,8 +281,7 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
                 const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
                 const double zm = (k > 1) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
                 val = wc + (double)face_increment<F>(q, lw, F(wc), F(xm), F(xm), F(xp), F(ym), F(ym), F(yp),
-                                                     F(zmm), F(zm), F(zp), F(au), F(av), F(wc), F(R.dxv[i]),
-                                                     F(R.dyv[j]), F(R.dzv[k]), nu, dt);
+                                                     F(zmm), F(zm), F(zp), F(au), F(av), F(wc), hx, hy, hz, nu, dt);
                 if (A.buoyancy) val += (double)(F(A.bcoeff) * (F(0.5) * (F(tb) + F(tc)) - F(A.T_ref)));
             }
             ws[f] = face_code(code, val, R.fanvel, 2);
@@ -480,7 +494,106 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
     double dmax = 0.0, divmax = 0.0;
     int nan = 0;
     const int last = R.n - 1;
-    for (Walk wk(start, stride, ny, nz, R.n); wk.ok(); wk.next()) {
+    const InvSpacing I(R);
+    // One face along an axis: the correction where the face is interior
+    // (lo/hi flags), then its code.  The same arithmetic for every face
+    // whichever cell forms it, so a face two cells share comes out the same.
+    auto xface = [&](double f, bool interior, double pd, double rc) {
+        return interior ? f - c0 * (pd * rc) : f;
+    };
+    if ((nz & 1) == 0) {
+        // Even rows: the cells (i, j, k0) and (i, j, k0 + 1) of a pair.  The
+        // pressure, the x and y face arrays and the codes hold both at an
+        // even index, so each pair of values moves with one 16-byte (2-byte
+        // for codes) load or store; the z face between the two cells is
+        // formed once (an interior face carries no outflow copy, so both
+        // cells would form it alike).  A neighbour pair outside the grid is
+        // clamped to a pair inside it and not used, as in the general loop.
+        const int pk = nz >> 1;
+        for (Walk wk(start, stride, ny, pk, nx * ny * pk); wk.ok(); wk.next()) {
+            const int i = wk.i, j = wk.j, k0 = 2 * wk.k;
+            const int c = (i * ny + j) * nz + k0;
+            const double2 pc = *reinterpret_cast<const double2 *>(p + c);
+            const double2 pxm = *reinterpret_cast<const double2 *>(p + max(c - plane, 0));
+            const double2 pxp = *reinterpret_cast<const double2 *>(p + min(c + plane, last - 1));
+            const double2 pym = *reinterpret_cast<const double2 *>(p + max(c - nz, 0));
+            const double2 pyp = *reinterpret_cast<const double2 *>(p + min(c + nz, last - 1));
+            const double pzm = p[max(c - 1, 0)], pzp = p[min(c + 2, last)];
+            const int vl = VIX(i, j, k0), wl = WIX(i, j, k0);
+            const double2 usl = *reinterpret_cast<const double2 *>(us + c);
+            const double2 ush = *reinterpret_cast<const double2 *>(us + c + plane);
+            const double2 vsl = *reinterpret_cast<const double2 *>(vs + vl);
+            const double2 vsh = *reinterpret_cast<const double2 *>(vs + vl + nz);
+            const double ws0 = ws[wl], ws1 = ws[wl + 1], ws2 = ws[wl + 2];
+            const uchar2 cul = *reinterpret_cast<const uchar2 *>(R.fcu + c);
+            const uchar2 cuh = *reinterpret_cast<const uchar2 *>(R.fcu + c + plane);
+            const uchar2 cvl = *reinterpret_cast<const uchar2 *>(R.fcv + vl);
+            const uchar2 cvh = *reinterpret_cast<const uchar2 *>(R.fcv + vl + nz);
+            const uint8_t cw0 = R.fcw[wl], cw1 = R.fcw[wl + 1], cw2 = R.fcw[wl + 2];
+            const double2 uo = *reinterpret_cast<const double2 *>(u + c);
+            const double2 vo = *reinterpret_cast<const double2 *>(v + vl);
+            const double wo0 = w[wl], wo1 = w[wl + 1];
+            const uchar2 ctp = *reinterpret_cast<const uchar2 *>(R.ct + c);
+            const double rxl = I.cx[i], rxh = I.cx[min(i + 1, nx - 1)];
+            const double ryl = I.cy[j], ryh = I.cy[min(j + 1, ny - 1)];
+            const bool xl = i >= 1, xh = i + 1 <= nx - 1, yl = j >= 1, yh = j + 1 <= ny - 1;
+            // faces of one cell along x or y: corrected, coded, outflow copies
+            auto pair_faces = [&](double lo, double hi, uint8_t cl, uint8_t ch, bool il, bool ih, double pdl,
+                                  double pdh, double rl, double rh, int comp, double &flo, double &fhi) {
+                lo = face_code(cl, xface(lo, il, pdl, rl), R.fanvel, comp);
+                hi = face_code(ch, xface(hi, ih, pdh, rh), R.fanvel, comp);
+                if (cl & FC_OUTCOPY) lo = hi;
+                if (ch & FC_OUTCOPY) hi = lo;
+                flo = lo;
+                fhi = hi;
+            };
+            double ulo0, uhi0, ulo1, uhi1, vlo0, vhi0, vlo1, vhi1;
+            pair_faces(usl.x, ush.x, cul.x, cuh.x, xl, xh, pc.x - pxm.x, pxp.x - pc.x, rxl, rxh, 0, ulo0, uhi0);
+            pair_faces(usl.y, ush.y, cul.y, cuh.y, xl, xh, pc.y - pxm.y, pxp.y - pc.y, rxl, rxh, 0, ulo1, uhi1);
+            pair_faces(vsl.x, vsh.x, cvl.x, cvh.x, yl, yh, pc.x - pym.x, pyp.x - pc.x, ryl, ryh, 1, vlo0, vhi0);
+            pair_faces(vsl.y, vsh.y, cvl.y, cvh.y, yl, yh, pc.y - pym.y, pyp.y - pc.y, ryl, ryh, 1, vlo1, vhi1);
+            // z faces k0, k0 + 1 (shared, always interior), k0 + 2
+            const double f0 = face_code(cw0, xface(ws0, k0 >= 1, pc.x - pzm, I.cz[k0]), R.fanvel, 2);
+            const double f1 = face_code(cw1, xface(ws1, true, pc.y - pc.x, I.cz[k0 + 1]), R.fanvel, 2);
+            const double f2 = face_code(cw2, xface(ws2, k0 + 2 <= nz - 1, pzp - pc.y, I.cz[min(k0 + 2, nz - 1)]),
+                                        R.fanvel, 2);
+            double wlo0 = f0, whi0 = f1, wlo1 = f1, whi1 = f2;
+            if (cw0 & FC_OUTCOPY) wlo0 = whi0;
+            if (cw1 & FC_OUTCOPY) whi0 = wlo0;
+            if (cw1 & FC_OUTCOPY) wlo1 = whi1;
+            if (cw2 & FC_OUTCOPY) whi1 = wlo1;
+            dmax = fmax(dmax, fmax(fabs(ulo0 - uo.x), fabs(ulo1 - uo.y)));
+            dmax = fmax(dmax, fmax(fabs(vlo0 - vo.x), fabs(vlo1 - vo.y)));
+            dmax = fmax(dmax, fmax(fabs(wlo0 - wo0), fabs(wlo1 - wo1)));
+            *reinterpret_cast<double2 *>(u + c) = make_double2(ulo0, ulo1);
+            *reinterpret_cast<double2 *>(v + vl) = make_double2(vlo0, vlo1);
+            w[wl] = wlo0;
+            w[wl + 1] = wlo1;
+            if (i == nx - 1) {
+                const double2 o = *reinterpret_cast<const double2 *>(u + c + plane);
+                dmax = fmax(dmax, fmax(fabs(uhi0 - o.x), fabs(uhi1 - o.y)));
+                *reinterpret_cast<double2 *>(u + c + plane) = make_double2(uhi0, uhi1);
+            }
+            if (j == ny - 1) {
+                const double2 o = *reinterpret_cast<const double2 *>(v + vl + nz);
+                dmax = fmax(dmax, fmax(fabs(vhi0 - o.x), fabs(vhi1 - o.y)));
+                *reinterpret_cast<double2 *>(v + vl + nz) = make_double2(vhi0, vhi1);
+            }
+            if (k0 + 2 == nz) {
+                dmax = fmax(dmax, fabs(whi1 - w[wl + 2]));
+                w[wl + 2] = whi1;
+            }
+            if (isnan(ulo0) || isnan(uhi0) || isnan(vlo0) || isnan(vhi0) || isnan(wlo0) || isnan(whi0) ||
+                isnan(ulo1) || isnan(uhi1) || isnan(vlo1) || isnan(vhi1) || isnan(wlo1) || isnan(whi1))
+                nan = 1;
+            const double rwx = I.wx[i], rwy = I.wy[j];
+            if (ctp.x == CT_FLUID)
+                divmax = fmax(divmax, fabs((uhi0 - ulo0) * rwx + (vhi0 - vlo0) * rwy + (whi0 - wlo0) * I.wz[k0]));
+            if (ctp.y == CT_FLUID)
+                divmax = fmax(divmax, fabs((uhi1 - ulo1) * rwx + (vhi1 - vlo1) * rwy + (whi1 - wlo1) * I.wz[k0 + 1]));
+        }
+    }
+    for (Walk wk(start, stride, ny, nz, (nz & 1) ? R.n : 0); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
         // the pressure stencil and the old low faces, loaded before any test
         const double pc = p[c];
@@ -490,8 +603,8 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
         // x faces
         const int ul = c, uh = c + plane;
         double lo = us[ul], hi = us[uh];
-        if (i >= 1) lo = lo - c0 * ((pc - pxm) / (0.5 * (R.dxv[i - 1] + R.dxv[i])));
-        if (i + 1 <= nx - 1) hi = hi - c0 * ((pxp - pc) / (0.5 * (R.dxv[i] + R.dxv[i + 1])));
+        if (i >= 1) lo = lo - c0 * ((pc - pxm) * I.cx[i]);
+        if (i + 1 <= nx - 1) hi = hi - c0 * ((pxp - pc) * I.cx[i + 1]);
         uint8_t cl = R.fcu[ul], ch = R.fcu[uh];
         lo = face_code(cl, lo, R.fanvel, 0);
         hi = face_code(ch, hi, R.fanvel, 0);
@@ -507,8 +620,8 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
         // y faces
         const int vl = VIX(i, j, k), vh = vl + nz;
         lo = vs[vl]; hi = vs[vh];
-        if (j >= 1) lo = lo - c0 * ((pc - pym) / (0.5 * (R.dyv[j - 1] + R.dyv[j])));
-        if (j + 1 <= ny - 1) hi = hi - c0 * ((pyp - pc) / (0.5 * (R.dyv[j] + R.dyv[j + 1])));
+        if (j >= 1) lo = lo - c0 * ((pc - pym) * I.cy[j]);
+        if (j + 1 <= ny - 1) hi = hi - c0 * ((pyp - pc) * I.cy[j + 1]);
         cl = R.fcv[vl]; ch = R.fcv[vh];
         lo = face_code(cl, lo, R.fanvel, 1);
         hi = face_code(ch, hi, R.fanvel, 1);
@@ -524,8 +637,8 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
         // z faces
         const int wl = WIX(i, j, k), wh = wl + 1;
         lo = ws[wl]; hi = ws[wh];
-        if (k >= 1) lo = lo - c0 * ((pc - pzm) / (0.5 * (R.dzv[k - 1] + R.dzv[k])));
-        if (k + 1 <= nz - 1) hi = hi - c0 * ((pzp - pc) / (0.5 * (R.dzv[k] + R.dzv[k + 1])));
+        if (k >= 1) lo = lo - c0 * ((pc - pzm) * I.cz[k]);
+        if (k + 1 <= nz - 1) hi = hi - c0 * ((pzp - pc) * I.cz[k + 1]);
         cl = R.fcw[wl]; ch = R.fcw[wh];
         lo = face_code(cl, lo, R.fanvel, 2);
         hi = face_code(ch, hi, R.fanvel, 2);
@@ -540,7 +653,7 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
         }
         if (isnan(ulo) || isnan(uhi) || isnan(vlo) || isnan(vhi) || isnan(wlo) || isnan(whi)) nan = 1;
         if (R.ct[c] == CT_FLUID) {
-            const double d = fabs((uhi - ulo) / R.dxv[i] + (vhi - vlo) / R.dyv[j] + (whi - wlo) / R.dzv[k]);
+            const double d = fabs((uhi - ulo) * I.wx[i] + (vhi - vlo) * I.wy[j] + (whi - wlo) * I.wz[k]);
             divmax = fmax(divmax, d);
         }
     }
@@ -631,6 +744,75 @@ struct ThermArgs {
     int scheme;
 };
 
+// The new temperature of one FLUID cell (FluidSolver::advect_temperature,
+// FluidSolver.cpp:388-456) from its value tc, its six neighbours' types and
+// values in the order x-, x+, y-, y+, z-, z+ and its six face velocities.
+// F as for k_predict.
+template <class F>
+__device__ __forceinline__ double temp_cell(const RoomDev &R, const ThermArgs &A, const InvSpacing &I,
+                                            const double *T, int i, int j, int k, double tc, const uint8_t (&nct)[6],
+                                            const double (&nT)[6], double u0, double u1, double v0, double v1,
+                                            double w0, double w1)
+{
+    const int nx = R.nx, ny = R.ny, nz = R.nz;
+    const int quick = A.scheme == 1, lw = A.scheme == 2;
+    const double ac = 0.5 * (u0 + u1);
+    const double bc = 0.5 * (v0 + v1);
+    const double cc = 0.5 * (w0 + w1);
+    // Neumann at the domain edge and at SOLID cells (FluidSolver.cpp:417-422)
+    const bool inside[6] = {i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
+    double tn6[6];
+#pragma unroll
+    for (int a = 0; a < 6; a++) tn6[a] = (inside[a] && nct[a] != CT_SOLID) ? nT[a] : tc;
+    auto tat = [&](int ii, int jj, int kk) -> double {
+        if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) return tc;
+        const int qq = UIX(ii, jj, kk);
+        return R.ct[qq] == CT_SOLID ? tc : T[qq];
+    };
+    const double xm = tn6[0], xp = tn6[1];
+    const double ym = tn6[2], yp = tn6[3];
+    const double zm = tn6[4], zp = tn6[5];
+    const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+    const double xmm = q ? tat(i - 2, j, k) : 0.0, ymm = q ? tat(i, j - 2, k) : 0.0,
+                 zmm = q ? tat(i, j, k - 2) : 0.0;
+    const F hx = axis_spacing<F>(R.dxv, I.fx, i), hy = axis_spacing<F>(R.dyv, I.fy, j),
+            hz = axis_spacing<F>(R.dzv, I.fz, k), dt = F(A.dt);
+    F adv, dif;
+    const F ftc = F(tc);
+    if constexpr (sizeof(F) == 4) {
+        // mixed precision: reciprocal spacings in place of the divisions
+        const F ix = hx, iy = hy, iz = hz;
+        if (q) {
+            adv = adv_quick_r(F(xmm), F(xm), ftc, F(xp), F(ac), ix) +
+                  adv_quick_r(F(ymm), F(ym), ftc, F(yp), F(bc), iy) +
+                  adv_quick_r(F(zmm), F(zm), ftc, F(zp), F(cc), iz);
+        } else if (lw) {
+            adv = adv_lw_r(F(xm), ftc, F(xp), F(ac), dt, ix) + adv_lw_r(F(ym), ftc, F(yp), F(bc), dt, iy) +
+                  adv_lw_r(F(zm), ftc, F(zp), F(cc), dt, iz);
+        } else {
+            adv = adv_up_r(F(xm), ftc, F(xp), F(ac), ix) + adv_up_r(F(ym), ftc, F(yp), F(bc), iy) +
+                  adv_up_r(F(zm), ftc, F(zp), F(cc), iz);
+        }
+        dif = F(A.alpha) * ((F(xm) - F(2) * ftc + F(xp)) * (ix * ix) + (F(ym) - F(2) * ftc + F(yp)) * (iy * iy) +
+                            (F(zm) - F(2) * ftc + F(zp)) * (iz * iz));
+    } else {
+        if (q) {
+            adv = adv_quick(F(xmm), F(xm), F(tc), F(xp), F(ac), hx) +
+                  adv_quick(F(ymm), F(ym), F(tc), F(yp), F(bc), hy) +
+                  adv_quick(F(zmm), F(zm), F(tc), F(zp), F(cc), hz);
+        } else if (lw) {
+            adv = adv_lw(F(xm), F(tc), F(xp), F(ac), dt, hx) + adv_lw(F(ym), F(tc), F(yp), F(bc), dt, hy) +
+                  adv_lw(F(zm), F(tc), F(zp), F(cc), dt, hz);
+        } else {
+            adv = adv_up(F(xm), F(tc), F(xp), F(ac), hx) + adv_up(F(ym), F(tc), F(yp), F(bc), hy) +
+                  adv_up(F(zm), F(tc), F(zp), F(cc), hz);
+        }
+        dif = F(A.alpha) * ((F(xm) - F(2) * ftc + F(xp)) / (hx * hx) + (F(ym) - F(2) * ftc + F(yp)) / (hy * hy) +
+                            (F(zm) - F(2) * ftc + F(zp)) / (hz * hz));
+    }
+    return tc + (double)(dt * (-adv + dif));
+}
+
 // FluidSolver::advect_temperature (FluidSolver.cpp:388-456) with the block
 // partial sums of the new T over FLUID cells for compute_T_mean
 // (FluidSolver.cpp:458-468).  F as for k_predict.
@@ -645,10 +827,55 @@ __device__ __forceinline__ void advect_T_body(const RoomDev &R, const ThermArgs 
     const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
     const double *T = st->tpar ? T1 : T0;
     double *Tn = st->tpar ? T0 : T1;
-    const int quick = A.scheme == 1, lw = A.scheme == 2;
     double sum = 0.0;
     const int last = R.n - 1;
-    for (Walk wk(start, stride, ny, nz, R.n); wk.ok(); wk.next()) {
+    const InvSpacing I(R);
+    if ((nz & 1) == 0) {
+        // Even rows: the cells (i, j, k0), (i, j, k0 + 1) of a pair, with
+        // 16-byte loads of T and of the x and y faces and 2-byte loads of
+        // the cell types at even indices (a neighbour pair outside the grid
+        // is clamped to a pair inside it and not used); the z face between
+        // the two cells is read once.
+        const int pk = nz >> 1;
+        for (Walk wk(start, stride, ny, pk, nx * ny * pk); wk.ok(); wk.next()) {
+            const int i = wk.i, j = wk.j, k0 = 2 * wk.k;
+            const int c = (i * ny + j) * nz + k0;
+            const uchar2 tcell = *reinterpret_cast<const uchar2 *>(R.ct + c);
+            const double2 tc = *reinterpret_cast<const double2 *>(T + c);
+            const int nb[4] = {max(c - plane, 0), min(c + plane, last - 1), max(c - nz, 0), min(c + nz, last - 1)};
+            uint8_t nct0[6], nct1[6];
+            double nT0[6], nT1[6];
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+                const uchar2 t2 = *reinterpret_cast<const uchar2 *>(R.ct + nb[a]);
+                const double2 v2 = *reinterpret_cast<const double2 *>(T + nb[a]);
+                nct0[a] = t2.x; nct1[a] = t2.y;
+                nT0[a] = v2.x; nT1[a] = v2.y;
+            }
+            const int zm = max(c - 1, 0), zp = min(c + 2, last);
+            nct0[4] = R.ct[zm]; nT0[4] = T[zm];
+            nct0[5] = tcell.y; nT0[5] = tc.y;
+            nct1[4] = tcell.x; nT1[4] = tc.x;
+            nct1[5] = R.ct[zp]; nT1[5] = T[zp];
+            const double2 ul = *reinterpret_cast<const double2 *>(u + c);
+            const double2 uh = *reinterpret_cast<const double2 *>(u + c + plane);
+            const int vl = VIX(i, j, k0), wl = WIX(i, j, k0);
+            const double2 vlo = *reinterpret_cast<const double2 *>(v + vl);
+            const double2 vhi = *reinterpret_cast<const double2 *>(v + vl + nz);
+            const double w0 = w[wl], w1 = w[wl + 1], w2 = w[wl + 2];
+            double t0 = tc.x, t1 = tc.y;
+            if (tcell.x == CT_FLUID) {
+                t0 = temp_cell<F>(R, A, I, T, i, j, k0, tc.x, nct0, nT0, ul.x, uh.x, vlo.x, vhi.x, w0, w1);
+                sum += t0;
+            }
+            if (tcell.y == CT_FLUID) {
+                t1 = temp_cell<F>(R, A, I, T, i, j, k0 + 1, tc.y, nct1, nT1, ul.y, uh.y, vlo.y, vhi.y, w1, w2);
+                sum += t1;
+            }
+            *reinterpret_cast<double2 *>(Tn + c) = make_double2(t0, t1);
+        }
+    }
+    for (Walk wk(start, stride, ny, nz, (nz & 1) ? R.n : 0); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
         const uint8_t tcell = R.ct[c];
         const double tc = T[c];
@@ -670,60 +897,7 @@ __device__ __forceinline__ void advect_T_body(const RoomDev &R, const ThermArgs 
             Tn[c] = tc;
             continue;
         }
-        const double ac = 0.5 * (u0 + u1);
-        const double bc = 0.5 * (v0 + v1);
-        const double cc = 0.5 * (w0 + w1);
-        // Neumann at the domain edge and at SOLID cells (FluidSolver.cpp:417-422)
-        const bool inside[6] = {i > 0, i < nx - 1, j > 0, j < ny - 1, k > 0, k < nz - 1};
-        double tn6[6];
-#pragma unroll
-        for (int a = 0; a < 6; a++) tn6[a] = (inside[a] && nct[a] != CT_SOLID) ? nT[a] : tc;
-        auto tat = [&](int ii, int jj, int kk) -> double {
-            if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) return tc;
-            const int qq = UIX(ii, jj, kk);
-            return R.ct[qq] == CT_SOLID ? tc : T[qq];
-        };
-        const double xm = tn6[0], xp = tn6[1];
-        const double ym = tn6[2], yp = tn6[3];
-        const double zm = tn6[4], zp = tn6[5];
-        const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
-        const double xmm = q ? tat(i - 2, j, k) : 0.0, ymm = q ? tat(i, j - 2, k) : 0.0,
-                     zmm = q ? tat(i, j, k - 2) : 0.0;
-        const F hx = F(R.dxv[i]), hy = F(R.dyv[j]), hz = F(R.dzv[k]), dt = F(A.dt);
-        F adv, dif;
-        const F ftc = F(tc);
-        if constexpr (sizeof(F) == 4) {
-            // mixed precision: reciprocal spacings in place of the divisions
-            const F ix = __frcp_rn(hx), iy = __frcp_rn(hy), iz = __frcp_rn(hz);
-            if (q) {
-                adv = adv_quick_r(F(xmm), F(xm), ftc, F(xp), F(ac), ix) +
-                      adv_quick_r(F(ymm), F(ym), ftc, F(yp), F(bc), iy) +
-                      adv_quick_r(F(zmm), F(zm), ftc, F(zp), F(cc), iz);
-            } else if (lw) {
-                adv = adv_lw_r(F(xm), ftc, F(xp), F(ac), dt, ix) + adv_lw_r(F(ym), ftc, F(yp), F(bc), dt, iy) +
-                      adv_lw_r(F(zm), ftc, F(zp), F(cc), dt, iz);
-            } else {
-                adv = adv_up_r(F(xm), ftc, F(xp), F(ac), ix) + adv_up_r(F(ym), ftc, F(yp), F(bc), iy) +
-                      adv_up_r(F(zm), ftc, F(zp), F(cc), iz);
-            }
-            dif = F(A.alpha) * ((F(xm) - F(2) * ftc + F(xp)) * (ix * ix) + (F(ym) - F(2) * ftc + F(yp)) * (iy * iy) +
-                                (F(zm) - F(2) * ftc + F(zp)) * (iz * iz));
-        } else {
-            if (q) {
-                adv = adv_quick(F(xmm), F(xm), F(tc), F(xp), F(ac), hx) +
-                      adv_quick(F(ymm), F(ym), F(tc), F(yp), F(bc), hy) +
-                      adv_quick(F(zmm), F(zm), F(tc), F(zp), F(cc), hz);
-            } else if (lw) {
-                adv = adv_lw(F(xm), F(tc), F(xp), F(ac), dt, hx) + adv_lw(F(ym), F(tc), F(yp), F(bc), dt, hy) +
-                      adv_lw(F(zm), F(tc), F(zp), F(cc), dt, hz);
-            } else {
-                adv = adv_up(F(xm), F(tc), F(xp), F(ac), hx) + adv_up(F(ym), F(tc), F(yp), F(bc), hy) +
-                      adv_up(F(zm), F(tc), F(zp), F(cc), hz);
-            }
-            dif = F(A.alpha) * ((F(xm) - F(2) * ftc + F(xp)) / (hx * hx) + (F(ym) - F(2) * ftc + F(yp)) / (hy * hy) +
-                                (F(zm) - F(2) * ftc + F(zp)) / (hz * hz));
-        }
-        const double tn = tc + (double)(dt * (-adv + dif));
+        const double tn = temp_cell<F>(R, A, I, T, i, j, k, tc, nct, nT, u0, u1, v0, v1, w0, w1);
         Tn[c] = tn;
         sum += tn;
     }
@@ -1080,7 +1254,7 @@ unsigned stream_blocks(long long work)
 
 // Device copy of the room-derived tables shared by a solver and its CG.
 struct RoomTables {
-    double *dxv, *dyv, *dzv, *scale, *fanvel;
+    double *dxv, *dyv, *dzv, *scale, *fanvel, *inv;
     uint8_t *ct, *fcu, *fcv, *fcw;
     uint16_t *sc;
 };
@@ -1090,7 +1264,8 @@ size_t tables_bytes(const HostRoom &h)
     const RoomGeom &g = h.g;
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     return al(8 * g.nx) + al(8 * g.ny) + al(8 * g.nz) + al(8 * 2 * (g.nx + g.ny + g.nz)) +
-           al(8 * 3 * kMaxFans) + al(g.n) + al(g.nu) + al(g.nv) + al(g.nw) + al(2 * g.n);
+           al(8 * 3 * kMaxFans) + al(g.n) + al(g.nu) + al(g.nv) + al(g.nw) + al(2 * g.n) +
+           al(20 * (size_t)(g.nx + g.ny + g.nz) + 8);
 }
 
 // Carves the tables from the arena and points R at them (no device work).
@@ -1107,12 +1282,13 @@ int carve_tables(const HostRoom &h, Arena &ar, RoomTables &t, RoomDev &R)
     t.fcv = ar.take<uint8_t>(g.nv);
     t.fcw = ar.take<uint8_t>(g.nw);
     t.sc = ar.take<uint16_t>(g.n);
-    if (!t.sc) return fail(FFR_ENOMEM, "arena exhausted (tables)");
+    t.inv = ar.take<double>((size_t)(5 * (g.nx + g.ny + g.nz) + 1) / 2);
+    if (!t.inv) return fail(FFR_ENOMEM, "arena exhausted (tables)");
     R.nx = g.nx; R.ny = g.ny; R.nz = g.nz;
     R.n = (int)g.n; R.nu = (int)g.nu; R.nv = (int)g.nv; R.nw = (int)g.nw;
     R.dxv = t.dxv; R.dyv = t.dyv; R.dzv = t.dzv;
     R.ct = t.ct; R.fcu = t.fcu; R.fcv = t.fcv; R.fcw = t.fcw;
-    R.sc = t.sc; R.scale = t.scale; R.fanvel = t.fanvel;
+    R.sc = t.sc; R.scale = t.scale; R.fanvel = t.fanvel; R.inv = t.inv;
     return FFR_OK;
 }
 
@@ -1120,7 +1296,8 @@ int carve_tables(const HostRoom &h, Arena &ar, RoomTables &t, RoomDev &R)
 size_t tables_stage_bytes(const HostRoom &h)
 {
     const RoomGeom &g = h.g;
-    return 8 * 3 * (size_t)(g.nx + g.ny + g.nz) + 8 * 3 * kMaxFans + 5 * 16;
+    return 8 * 3 * (size_t)(g.nx + g.ny + g.nz) + 8 * 3 * kMaxFans + 5 * 16 +
+           20 * (size_t)(g.nx + g.ny + g.nz) + 32;
 }
 
 // The cell types, by a synchronous staged copy.  Made before any kernel is
@@ -1141,10 +1318,26 @@ int queue_tables(const HostRoom &h, const RoomTables &t, HostStage &hs, cudaStre
     std::vector<double> fan(3 * kMaxFans, 0.0);
     for (size_t f = 0; f < h.fans.size(); f++)
         for (int c = 0; c < 3; c++) fan[3 * f + c] = h.fans[f].vel[c];
+    // Reciprocal spacings (RoomDev::inv): the centre distance is formed as
+    // the kernels formed it, 0.5 * (d[i-1] + d[i]); the FP32 entry is the
+    // correctly rounded reciprocal of the rounded width, the value
+    // __frcp_rn((float)d[i]) gives on the device.
+    const int S = g.nx + g.ny + g.nz;
+    std::vector<double> inv((5 * (size_t)S + 1) / 2, 0.0);
+    float *finv = reinterpret_cast<float *>(inv.data() + 2 * S);
+    const std::vector<double> *d3[3] = {&h.dxv, &h.dyv, &h.dzv};
+    for (int a = 0, off = 0; a < 3; off += (int)d3[a]->size(), a++) {
+        const std::vector<double> &d = *d3[a];
+        for (size_t i = 0; i < d.size(); i++) {
+            if (i > 0) inv[off + i] = 1.0 / (0.5 * (d[i - 1] + d[i]));
+            inv[S + off + i] = 1.0 / d[i];
+            finv[off + i] = 1.0f / (float)d[i];
+        }
+    }
     int rc;
     if ((rc = hs.put(t.dxv, h.dxv.data(), 8 * g.nx, s)) || (rc = hs.put(t.dyv, h.dyv.data(), 8 * g.ny, s)) ||
         (rc = hs.put(t.dzv, h.dzv.data(), 8 * g.nz, s)) || (rc = hs.put(t.scale, scale.data(), 8 * scale.size(), s)) ||
-        (rc = hs.put(t.fanvel, fan.data(), 8 * fan.size(), s)))
+        (rc = hs.put(t.fanvel, fan.data(), 8 * fan.size(), s)) || (rc = hs.put(t.inv, inv.data(), 8 * inv.size(), s)))
         return rc;
     return build_codes(h, t.ct, t.sc, t.fcu, t.fcv, t.fcw, s);
 }

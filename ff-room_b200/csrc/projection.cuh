@@ -34,6 +34,24 @@ struct RoomDev {
     const uint16_t *sc;
     const double *scale;   // sxl sxr syl syr szl szr
     const double *fanvel;  // 3 per fan
+    // Reciprocal spacings, S = nx + ny + nz entries per table, axes in
+    // turn: [0, S) 1/(cell-centre distance below the cell) (entry 0 of an
+    // axis unused), [S, 2S) 1/(cell width) in FP64, then S floats holding
+    // the correctly rounded FP32 reciprocal of the FP32 cell width.
+    const double *inv;
+};
+
+// The reciprocal-spacing tables of a room (RoomDev::inv).
+struct InvSpacing {
+    const double *cx, *cy, *cz, *wx, *wy, *wz;
+    const float *fx, *fy, *fz;
+    __device__ __forceinline__ InvSpacing(const RoomDev &R)
+    {
+        const int S = R.nx + R.ny + R.nz;
+        cx = R.inv; cy = cx + R.nx; cz = cy + R.ny;
+        wx = R.inv + S; wy = wx + R.nx; wz = wy + R.ny;
+        fx = reinterpret_cast<const float *>(R.inv + 2 * S); fy = fx + R.nx; fz = fy + R.ny;
+    }
 };
 
 struct CGArgs {
