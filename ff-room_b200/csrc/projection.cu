@@ -154,13 +154,86 @@ struct PredArgs {
     double T_ref;
 };
 
-// Predictor for every face of u, v and w (one thread per face, flat over
-// the three arrays): FluidSolver::compute_intermediate (FluidSolver.cpp:
-// 83-309), then apply_buoyancy on interior w faces (FluidSolver.cpp:373-386),
-// then the no-slip / inflow codes (BoundaryManager.cpp:60-130).  F is the
-// arithmetic of the increment: double reproduces the reference; float is
-// the mixed-precision mode (FP32 increment added to the FP64 state).
-// The body over faces start, start + stride, ... (all blocks of one room).
+// The predicted value of one interior face from its loaded neighbourhood
+// (compute_intermediate, FluidSolver.cpp:83-309): the boundary selects (a
+// neighbour outside reads as 0, as in the reference), the far-neighbour
+// selection of QUICK, then the increment in arithmetic F.  c is the face's
+// own value, xm0 .. zp0 its six neighbours, xmm0 .. zmm0 the far ones (read
+// only under QUICK), a0/a1 and b0/b1 the two pairs of the other components
+// averaged into the advecting velocities.
+template <class F>
+__device__ __forceinline__ double pred_u(int quick, int lw, int nx, int ny, int nz, int i, int j, int k, double c,
+                                         double xmm0, double xm0, double xp0, double ymm0, double ym0, double yp0,
+                                         double zmm0, double zm0, double zp0, double v0, double v1, double w0,
+                                         double w1, F hx, F hy, F hz, F nu, F dt)
+{
+    const int q = quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+    // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1 (k=1)
+    // they fall into the previous row of the flat array
+    const double xmm = q ? xmm0 : 0.0, ymm = q ? ymm0 : 0.0, zmm = q ? zmm0 : 0.0;
+    const double xm = (i > 1) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+    const double av = (j > 0 && j < ny) ? 0.5 * (v0 + v1) : 0.0;
+    const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+    const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
+    const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+    return c + (double)face_increment<F>(q, lw, F(c), F(xmm), F(xm), F(xp), F(ymm), F(ym), F(yp), F(zmm), F(zm),
+                                         F(zp), F(c), F(av), F(aw), hx, hy, hz, nu, dt);
+}
+
+template <class F>
+__device__ __forceinline__ double pred_v(int quick, int lw, int nx, int ny, int nz, int i, int j, int k, double c,
+                                         double xm0, double xp0, double ymm0, double ym0, double yp0, double zm0,
+                                         double zp0, double u0, double u1, double w0, double w1, F hx, F hy, F hz,
+                                         F nu, F dt)
+{
+    const int q = quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+    // v's x and z "far" neighbours are the near ones (FluidSolver.cpp:208,211)
+    const double ymm = q ? ymm0 : 0.0;
+    const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
+    const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+    const double ym = (j > 1) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+    const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
+    const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+    return c + (double)face_increment<F>(q, lw, F(c), F(xm), F(xm), F(xp), F(ymm), F(ym), F(yp), F(zm), F(zm),
+                                         F(zp), F(au), F(c), F(aw), hx, hy, hz, nu, dt);
+}
+
+// w additionally takes apply_buoyancy (FluidSolver.cpp:373-386) from the
+// temperatures tb, tc of the cells below and above the face.
+template <class F>
+__device__ __forceinline__ double pred_w(const PredArgs &A, int quick, int lw, int nx, int ny, int nz, int i, int j,
+                                         int k, double c, double xm0, double xp0, double ym0, double yp0,
+                                         double zmm0, double zm0, double zp0, double u0, double u1, double v0,
+                                         double v1, double tb, double tc, F hx, F hy, F hz, F nu, F dt)
+{
+    const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2;
+    // w's x and y "far" neighbours are the near ones (FluidSolver.cpp:275-276)
+    const double zmm = q ? zmm0 : 0.0;
+    const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
+    const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
+    const double av = (j > 0) ? 0.5 * (v0 + v1) : 0.0;
+    const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
+    const double zm = (k > 1) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
+    double val = c + (double)face_increment<F>(q, lw, F(c), F(xm), F(xm), F(xp), F(ym), F(ym), F(yp), F(zmm),
+                                               F(zm), F(zp), F(au), F(av), F(c), hx, hy, hz, nu, dt);
+    if (A.buoyancy) val += (double)(F(A.bcoeff) * (F(0.5) * (F(tb) + F(tc)) - F(A.T_ref)));
+    return val;
+}
+
+// Predictor for every face of u, v and w: FluidSolver::compute_intermediate
+// (FluidSolver.cpp:83-309), then apply_buoyancy on interior w faces
+// (FluidSolver.cpp:373-386), then the no-slip / inflow codes
+// (BoundaryManager.cpp:60-130).  F is the arithmetic of the increment:
+// double reproduces the reference; float is the mixed-precision mode (FP32
+// increment added to the FP64 state).  The body over work items start,
+// start + stride, ... (all blocks of one room).
+//
+// One pass over the corners (i, j, k) of the extended grid
+// (nx+1)(ny+1)(nz+1): the u, v and w faces with that lower corner, so the
+// three components are streamed once between them (three passes, one per
+// component, each re-read the other two after L2 had dropped them).
+// Neighbour loads go through indices clamped into their array and are
+// issued before the boundary tests select them.
 template <class F>
 __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A, const double *__restrict__ u,
                                              const double *__restrict__ v, const double *__restrict__ w,
@@ -172,19 +245,10 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
     const int quick = A.scheme == 1, lw = A.scheme == 2;
     const F dt = F(A.dt), nu = F(A.nu);
     const double *T = st->tpar ? T1 : T0;
-    // The three face arrays in turn, each with carried (i, j, k).  Neighbour
-    // loads go through indices clamped into the array and are all issued
-    // before the boundary tests select them (a neighbour outside reads as 0,
-    // as in the reference); the advecting-velocity pairs are always inside
-    // for an interior face.
     const int pu = ny * nz, lastu = R.nu - 1;
     const int pv = (ny + 1) * nz, lastv = R.nv - 1;
     const int pw = ny * (nz + 1), lastw = R.nw - 1;
     const InvSpacing I(R);
-    // One pass over the corners (i, j, k) of the extended grid
-    // (nx+1)(ny+1)(nz+1): the u, v and w faces with that lower corner, so the
-    // three components are streamed once between them (three passes, one
-    // per component, each re-read the other two after L2 had dropped them).
     for (Walk wk(start, stride, ny + 1, nz + 1, (nx + 1) * (ny + 1) * (nz + 1)); wk.ok(); wk.next()) {
         const int i = wk.i, j = wk.j, k = wk.k;
         // spacings of the corner's cell (entries past the last cell of an
@@ -197,27 +261,19 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
             const uint8_t code = R.fcu[t];
             double val = u[t];
             if (i > 0 && i < nx) {
-                const double uc = val;
                 const double xm0 = u[max(t - pu, 0)], xp0 = u[min(t + pu, lastu)];
                 const double ym0 = u[max(t - nz, 0)], yp0 = u[min(t + nz, lastu)];
                 const double zm0 = u[max(t - 1, 0)], zp0 = u[min(t + 1, lastu)];
                 const double v0 = v[VIX(i - 1, j, k)], v1 = v[VIX(i, j, k)];
                 const double w0 = w[WIX(i - 1, j, k)], w1 = w[WIX(i, j, k)];
-                const int q = quick && i >= 2 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
-                // flat-index far neighbours (FluidSolver.cpp:137-141): at j=1
-                // (k=1) they fall into the previous row of the flat array
                 double xmm = 0.0, ymm = 0.0, zmm = 0.0;
                 if (quick) {
-                    const double a = u[max(t - 2 * pu, 0)], b = u[max(t - 2 * nz, 0)], c = u[max(t - 2, 0)];
-                    xmm = q ? a : 0.0; ymm = q ? b : 0.0; zmm = q ? c : 0.0;
+                    xmm = u[max(t - 2 * pu, 0)];
+                    ymm = u[max(t - 2 * nz, 0)];
+                    zmm = u[max(t - 2, 0)];
                 }
-                const double xm = (i > 1) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
-                const double av = (j > 0 && j < ny) ? 0.5 * (v0 + v1) : 0.0;
-                const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
-                const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
-                const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
-                val = uc + (double)face_increment<F>(q, lw, F(uc), F(xmm), F(xm), F(xp), F(ymm), F(ym), F(yp),
-                                                     F(zmm), F(zm), F(zp), F(uc), F(av), F(aw), hx, hy, hz, nu, dt);
+                val = pred_u<F>(quick, lw, nx, ny, nz, i, j, k, val, xmm, xm0, xp0, ymm, ym0, yp0, zmm, zm0, zp0,
+                                v0, v1, w0, w1, hx, hy, hz, nu, dt);
             }
             us[t] = face_code(code, val, R.fanvel, 0);
         }
@@ -226,27 +282,14 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
             const uint8_t code = R.fcv[f];
             double val = v[f];
             if (j > 0 && j < ny) {
-                const double vc = val;
                 const double u0 = u[UIX(i, j - 1, k)], u1 = u[UIX(i, j, k)];
                 const double xm0 = v[max(f - pv, 0)], xp0 = v[min(f + pv, lastv)];
                 const double ym0 = v[max(f - nz, 0)], yp0 = v[min(f + nz, lastv)];
                 const double w0 = w[WIX(i, j - 1, k)], w1 = w[WIX(i, j, k)];
                 const double zm0 = v[max(f - 1, 0)], zp0 = v[min(f + 1, lastv)];
-                const int q = quick && i >= 1 && i <= nx - 2 && j >= 2 && j <= ny - 2 && k >= 1 && k <= nz - 2;
-                // v's x and z "far" neighbours are the near ones
-                // (FluidSolver.cpp:208,211)
-                double ymm = 0.0;
-                if (quick) {
-                    const double a = v[max(f - 2 * nz, 0)];
-                    ymm = q ? a : 0.0;
-                }
-                const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
-                const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
-                const double ym = (j > 1) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
-                const double aw = (k > 0 && k < nz) ? 0.5 * (w0 + w1) : 0.0;
-                const double zm = (k > 0) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
-                val = vc + (double)face_increment<F>(q, lw, F(vc), F(xm), F(xm), F(xp), F(ymm), F(ym), F(yp),
-                                                     F(zm), F(zm), F(zp), F(au), F(vc), F(aw), hx, hy, hz, nu, dt);
+                const double ymm = quick ? v[max(f - 2 * nz, 0)] : 0.0;
+                val = pred_v<F>(quick, lw, nx, ny, nz, i, j, k, val, xm0, xp0, ymm, ym0, yp0, zm0, zp0, u0, u1, w0,
+                                w1, hx, hy, hz, nu, dt);
             }
             vs[f] = face_code(code, val, R.fanvel, 1);
         }
@@ -255,7 +298,6 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
             const uint8_t code = R.fcw[f];
             double val = w[f];
             if (k > 0 && k < nz) {
-                const double wc = val;
                 const double u0 = u[UIX(i, j, k - 1)], u1 = u[UIX(i, j, k)];
                 const double xm0 = w[max(f - pw, 0)], xp0 = w[min(f + pw, lastw)];
                 const double v0 = v[VIX(i, j, k - 1)], v1 = v[VIX(i, j, k)];
@@ -267,22 +309,9 @@ __device__ __forceinline__ void predict_body(const RoomDev &R, const PredArgs &A
                     tb = T[c - 1];
                     tc = T[c];
                 }
-                const int q = quick && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 2 && k <= nz - 2;
-                // w's x and y "far" neighbours are the near ones
-                // (FluidSolver.cpp:275-276)
-                double zmm = 0.0;
-                if (quick) {
-                    const double a = w[max(f - 2, 0)];
-                    zmm = q ? a : 0.0;
-                }
-                const double au = (i > 0) ? 0.5 * (u0 + u1) : 0.0;
-                const double xm = (i > 0) ? xm0 : 0.0, xp = (i < nx - 1) ? xp0 : 0.0;
-                const double av = (j > 0) ? 0.5 * (v0 + v1) : 0.0;
-                const double ym = (j > 0) ? ym0 : 0.0, yp = (j < ny - 1) ? yp0 : 0.0;
-                const double zm = (k > 1) ? zm0 : 0.0, zp = (k < nz - 1) ? zp0 : 0.0;
-                val = wc + (double)face_increment<F>(q, lw, F(wc), F(xm), F(xm), F(xp), F(ym), F(ym), F(yp),
-                                                     F(zmm), F(zm), F(zp), F(au), F(av), F(wc), hx, hy, hz, nu, dt);
-                if (A.buoyancy) val += (double)(F(A.bcoeff) * (F(0.5) * (F(tb) + F(tc)) - F(A.T_ref)));
+                const double zmm = quick ? w[max(f - 2, 0)] : 0.0;
+                val = pred_w<F>(A, quick, lw, nx, ny, nz, i, j, k, val, xm0, xp0, ym0, yp0, zmm, zm0, zp0, u0, u1,
+                                v0, v1, tb, tc, hx, hy, hz, nu, dt);
             }
             ws[f] = face_code(code, val, R.fanvel, 2);
         }
@@ -482,6 +511,7 @@ struct CorrArgs {
 // recomputes the three high faces, so it can also fold max |u_new - u_old|
 // (FluidSolver.cpp:527-534) and, for FLUID cells, |div u|
 // (compute_divergence_max, FluidSolver.cpp:470-484) in the same pass.
+template <bool PAIRS>
 __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A, double *__restrict__ u,
                                              double *__restrict__ v, double *__restrict__ w,
                                              const double *__restrict__ us, const double *__restrict__ vs,
@@ -501,8 +531,9 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
     auto xface = [&](double f, bool interior, double pd, double rc) {
         return interior ? f - c0 * (pd * rc) : f;
     };
-    if ((nz & 1) == 0) {
-        // Even rows: the cells (i, j, k0) and (i, j, k0 + 1) of a pair.  The
+    if constexpr (PAIRS) {
+        // Even rows (PAIRS needs nz even): the cells (i, j, k0) and
+        // (i, j, k0 + 1) of a pair.  The
         // pressure, the x and y face arrays and the codes hold both at an
         // even index, so each pair of values moves with one 16-byte (2-byte
         // for codes) load or store; the z face between the two cells is
@@ -592,69 +623,73 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
             if (ctp.y == CT_FLUID)
                 divmax = fmax(divmax, fabs((uhi1 - ulo1) * rwx + (vhi1 - vlo1) * rwy + (whi1 - wlo1) * I.wz[k0 + 1]));
         }
-    }
-    for (Walk wk(start, stride, ny, nz, (nz & 1) ? R.n : 0); wk.ok(); wk.next()) {
-        const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
-        // the pressure stencil and the old low faces, loaded before any test
-        const double pc = p[c];
-        const double pxm = p[max(c - plane, 0)], pxp = p[min(c + plane, last)];
-        const double pym = p[max(c - nz, 0)], pyp = p[min(c + nz, last)];
-        const double pzm = p[max(c - 1, 0)], pzp = p[min(c + 1, last)];
-        // x faces
-        const int ul = c, uh = c + plane;
-        double lo = us[ul], hi = us[uh];
-        if (i >= 1) lo = lo - c0 * ((pc - pxm) * I.cx[i]);
-        if (i + 1 <= nx - 1) hi = hi - c0 * ((pxp - pc) * I.cx[i + 1]);
-        uint8_t cl = R.fcu[ul], ch = R.fcu[uh];
-        lo = face_code(cl, lo, R.fanvel, 0);
-        hi = face_code(ch, hi, R.fanvel, 0);
-        if (cl & FC_OUTCOPY) lo = hi;
-        if (ch & FC_OUTCOPY) hi = lo;
-        const double ulo = lo, uhi = hi;
-        dmax = fmax(dmax, fabs(lo - u[ul]));
-        u[ul] = lo;
-        if (i == nx - 1) {
-            dmax = fmax(dmax, fabs(hi - u[uh]));
-            u[uh] = hi;
-        }
-        // y faces
-        const int vl = VIX(i, j, k), vh = vl + nz;
-        lo = vs[vl]; hi = vs[vh];
-        if (j >= 1) lo = lo - c0 * ((pc - pym) * I.cy[j]);
-        if (j + 1 <= ny - 1) hi = hi - c0 * ((pyp - pc) * I.cy[j + 1]);
-        cl = R.fcv[vl]; ch = R.fcv[vh];
-        lo = face_code(cl, lo, R.fanvel, 1);
-        hi = face_code(ch, hi, R.fanvel, 1);
-        if (cl & FC_OUTCOPY) lo = hi;
-        if (ch & FC_OUTCOPY) hi = lo;
-        const double vlo = lo, vhi = hi;
-        dmax = fmax(dmax, fabs(lo - v[vl]));
-        v[vl] = lo;
-        if (j == ny - 1) {
-            dmax = fmax(dmax, fabs(hi - v[vh]));
-            v[vh] = hi;
-        }
-        // z faces
-        const int wl = WIX(i, j, k), wh = wl + 1;
-        lo = ws[wl]; hi = ws[wh];
-        if (k >= 1) lo = lo - c0 * ((pc - pzm) * I.cz[k]);
-        if (k + 1 <= nz - 1) hi = hi - c0 * ((pzp - pc) * I.cz[k + 1]);
-        cl = R.fcw[wl]; ch = R.fcw[wh];
-        lo = face_code(cl, lo, R.fanvel, 2);
-        hi = face_code(ch, hi, R.fanvel, 2);
-        if (cl & FC_OUTCOPY) lo = hi;
-        if (ch & FC_OUTCOPY) hi = lo;
-        const double wlo = lo, whi = hi;
-        dmax = fmax(dmax, fabs(lo - w[wl]));
-        w[wl] = lo;
-        if (k == nz - 1) {
-            dmax = fmax(dmax, fabs(hi - w[wh]));
-            w[wh] = hi;
-        }
-        if (isnan(ulo) || isnan(uhi) || isnan(vlo) || isnan(vhi) || isnan(wlo) || isnan(whi)) nan = 1;
-        if (R.ct[c] == CT_FLUID) {
-            const double d = fabs((uhi - ulo) * I.wx[i] + (vhi - vlo) * I.wy[j] + (whi - wlo) * I.wz[k]);
-            divmax = fmax(divmax, d);
+    } else {
+        // Any row length: one cell per work item.  The spacing factors are
+        // formed by division as the reference forms them (the reciprocal
+        // tables measured several times slower in this loop).
+        for (Walk wk(start, stride, ny, nz, R.n); wk.ok(); wk.next()) {
+            const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
+            // the pressure stencil and the old low faces, loaded before any test
+            const double pc = p[c];
+            const double pxm = p[max(c - plane, 0)], pxp = p[min(c + plane, last)];
+            const double pym = p[max(c - nz, 0)], pyp = p[min(c + nz, last)];
+            const double pzm = p[max(c - 1, 0)], pzp = p[min(c + 1, last)];
+            // x faces
+            const int ul = c, uh = c + plane;
+            double lo = us[ul], hi = us[uh];
+            if (i >= 1) lo = lo - c0 * ((pc - pxm) / (0.5 * (R.dxv[i - 1] + R.dxv[i])));
+            if (i + 1 <= nx - 1) hi = hi - c0 * ((pxp - pc) / (0.5 * (R.dxv[i] + R.dxv[i + 1])));
+            uint8_t cl = R.fcu[ul], ch = R.fcu[uh];
+            lo = face_code(cl, lo, R.fanvel, 0);
+            hi = face_code(ch, hi, R.fanvel, 0);
+            if (cl & FC_OUTCOPY) lo = hi;
+            if (ch & FC_OUTCOPY) hi = lo;
+            const double ulo = lo, uhi = hi;
+            dmax = fmax(dmax, fabs(lo - u[ul]));
+            u[ul] = lo;
+            if (i == nx - 1) {
+                dmax = fmax(dmax, fabs(hi - u[uh]));
+                u[uh] = hi;
+            }
+            // y faces
+            const int vl = VIX(i, j, k), vh = vl + nz;
+            lo = vs[vl]; hi = vs[vh];
+            if (j >= 1) lo = lo - c0 * ((pc - pym) / (0.5 * (R.dyv[j - 1] + R.dyv[j])));
+            if (j + 1 <= ny - 1) hi = hi - c0 * ((pyp - pc) / (0.5 * (R.dyv[j] + R.dyv[j + 1])));
+            cl = R.fcv[vl]; ch = R.fcv[vh];
+            lo = face_code(cl, lo, R.fanvel, 1);
+            hi = face_code(ch, hi, R.fanvel, 1);
+            if (cl & FC_OUTCOPY) lo = hi;
+            if (ch & FC_OUTCOPY) hi = lo;
+            const double vlo = lo, vhi = hi;
+            dmax = fmax(dmax, fabs(lo - v[vl]));
+            v[vl] = lo;
+            if (j == ny - 1) {
+                dmax = fmax(dmax, fabs(hi - v[vh]));
+                v[vh] = hi;
+            }
+            // z faces
+            const int wl = WIX(i, j, k), wh = wl + 1;
+            lo = ws[wl]; hi = ws[wh];
+            if (k >= 1) lo = lo - c0 * ((pc - pzm) / (0.5 * (R.dzv[k - 1] + R.dzv[k])));
+            if (k + 1 <= nz - 1) hi = hi - c0 * ((pzp - pc) / (0.5 * (R.dzv[k] + R.dzv[k + 1])));
+            cl = R.fcw[wl]; ch = R.fcw[wh];
+            lo = face_code(cl, lo, R.fanvel, 2);
+            hi = face_code(ch, hi, R.fanvel, 2);
+            if (cl & FC_OUTCOPY) lo = hi;
+            if (ch & FC_OUTCOPY) hi = lo;
+            const double wlo = lo, whi = hi;
+            dmax = fmax(dmax, fabs(lo - w[wl]));
+            w[wl] = lo;
+            if (k == nz - 1) {
+                dmax = fmax(dmax, fabs(hi - w[wh]));
+                w[wh] = hi;
+            }
+            if (isnan(ulo) || isnan(uhi) || isnan(vlo) || isnan(vhi) || isnan(wlo) || isnan(whi)) nan = 1;
+            if (R.ct[c] == CT_FLUID) {
+                const double d = fabs((uhi - ulo) / R.dxv[i] + (vhi - vlo) / R.dyv[j] + (whi - wlo) / R.dzv[k]);
+                divmax = fmax(divmax, d);
+            }
         }
     }
     dmax = block_max(dmax, sh);
@@ -667,6 +702,7 @@ __device__ __forceinline__ void correct_body(const RoomDev &R, const CorrArgs &A
     }
 }
 
+template <bool PAIRS>
 __global__ void __launch_bounds__(256) k_correct(RoomDev R, CorrArgs A, double *__restrict__ u,
                                                  double *__restrict__ v, double *__restrict__ w,
                                                  const double *__restrict__ us,
@@ -675,7 +711,8 @@ __global__ void __launch_bounds__(256) k_correct(RoomDev R, CorrArgs A, double *
                                                  const double *__restrict__ p, StepState *st)
 {
     if (st->halt) return;
-    correct_body(R, A, u, v, w, us, vs, ws, p, st, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+    correct_body<PAIRS>(R, A, u, v, w, us, vs, ws, p, st, blockIdx.x * blockDim.x + threadIdx.x,
+                        gridDim.x * blockDim.x);
 }
 
 // compute_divergence_max (FluidSolver.cpp:470-484) on demand.
@@ -824,58 +861,13 @@ __device__ __forceinline__ void advect_T_body(const RoomDev &R, const ThermArgs 
                                               int start, int stride, int lblock)
 {
     __shared__ double sh[32];
-    const int nx = R.nx, ny = R.ny, nz = R.nz, plane = ny * nz;
+    const int ny = R.ny, nz = R.nz, plane = ny * nz;
     const double *T = st->tpar ? T1 : T0;
     double *Tn = st->tpar ? T0 : T1;
     double sum = 0.0;
     const int last = R.n - 1;
     const InvSpacing I(R);
-    if ((nz & 1) == 0) {
-        // Even rows: the cells (i, j, k0), (i, j, k0 + 1) of a pair, with
-        // 16-byte loads of T and of the x and y faces and 2-byte loads of
-        // the cell types at even indices (a neighbour pair outside the grid
-        // is clamped to a pair inside it and not used); the z face between
-        // the two cells is read once.
-        const int pk = nz >> 1;
-        for (Walk wk(start, stride, ny, pk, nx * ny * pk); wk.ok(); wk.next()) {
-            const int i = wk.i, j = wk.j, k0 = 2 * wk.k;
-            const int c = (i * ny + j) * nz + k0;
-            const uchar2 tcell = *reinterpret_cast<const uchar2 *>(R.ct + c);
-            const double2 tc = *reinterpret_cast<const double2 *>(T + c);
-            const int nb[4] = {max(c - plane, 0), min(c + plane, last - 1), max(c - nz, 0), min(c + nz, last - 1)};
-            uint8_t nct0[6], nct1[6];
-            double nT0[6], nT1[6];
-#pragma unroll
-            for (int a = 0; a < 4; a++) {
-                const uchar2 t2 = *reinterpret_cast<const uchar2 *>(R.ct + nb[a]);
-                const double2 v2 = *reinterpret_cast<const double2 *>(T + nb[a]);
-                nct0[a] = t2.x; nct1[a] = t2.y;
-                nT0[a] = v2.x; nT1[a] = v2.y;
-            }
-            const int zm = max(c - 1, 0), zp = min(c + 2, last);
-            nct0[4] = R.ct[zm]; nT0[4] = T[zm];
-            nct0[5] = tcell.y; nT0[5] = tc.y;
-            nct1[4] = tcell.x; nT1[4] = tc.x;
-            nct1[5] = R.ct[zp]; nT1[5] = T[zp];
-            const double2 ul = *reinterpret_cast<const double2 *>(u + c);
-            const double2 uh = *reinterpret_cast<const double2 *>(u + c + plane);
-            const int vl = VIX(i, j, k0), wl = WIX(i, j, k0);
-            const double2 vlo = *reinterpret_cast<const double2 *>(v + vl);
-            const double2 vhi = *reinterpret_cast<const double2 *>(v + vl + nz);
-            const double w0 = w[wl], w1 = w[wl + 1], w2 = w[wl + 2];
-            double t0 = tc.x, t1 = tc.y;
-            if (tcell.x == CT_FLUID) {
-                t0 = temp_cell<F>(R, A, I, T, i, j, k0, tc.x, nct0, nT0, ul.x, uh.x, vlo.x, vhi.x, w0, w1);
-                sum += t0;
-            }
-            if (tcell.y == CT_FLUID) {
-                t1 = temp_cell<F>(R, A, I, T, i, j, k0 + 1, tc.y, nct1, nT1, ul.y, uh.y, vlo.y, vhi.y, w1, w2);
-                sum += t1;
-            }
-            *reinterpret_cast<double2 *>(Tn + c) = make_double2(t0, t1);
-        }
-    }
-    for (Walk wk(start, stride, ny, nz, (nz & 1) ? R.n : 0); wk.ok(); wk.next()) {
+    for (Walk wk(start, stride, ny, nz, R.n); wk.ok(); wk.next()) {
         const int c = wk.c, i = wk.i, j = wk.j, k = wk.k;
         const uint8_t tcell = R.ct[c];
         const double tc = T[c];
@@ -1095,15 +1087,20 @@ __global__ void __launch_bounds__(256) k_b_predict(const BRoom *rooms, BMap m)
         predict_body<double>(B.R, B.pa, B.u, B.v, B.w, B.T0, B.T1, B.us, B.vs, B.ws, B.st, start, stride);
 }
 
-__global__ void __launch_bounds__(256) k_b_correct(const BRoom *rooms, BMap m)
+__global__ void __launch_bounds__(256, 2) k_b_correct(const BRoom *rooms, BMap m)
 {
     __shared__ __align__(16) BRoom B;
     BPos P;
     const int r = bmap(m, P);
     load_shared(B, rooms + r);
     if (B.st->halt) return;
-    correct_body(B.R, B.co, B.u, B.v, B.w, B.us, B.vs, B.ws, B.p, B.st, P.lb * blockDim.x + threadIdx.x,
-                 P.nb * blockDim.x);
+    // the form the room's own launch takes (bit-identical results)
+    if ((B.R.nz & 1) == 0)
+        correct_body<true>(B.R, B.co, B.u, B.v, B.w, B.us, B.vs, B.ws, B.p, B.st, P.lb * blockDim.x + threadIdx.x,
+                           P.nb * blockDim.x);
+    else
+        correct_body<false>(B.R, B.co, B.u, B.v, B.w, B.us, B.vs, B.ws, B.p, B.st, P.lb * blockDim.x + threadIdx.x,
+                            P.nb * blockDim.x);
 }
 
 __global__ void k_b_opening(const BRoom *rooms, const OpenItem *items, BMap m, int next)
@@ -1520,8 +1517,13 @@ int fluid_enqueue_step(ffr_fluid *s)
     s->prof.end(st, 1);
     CorrArgs co{P.dt / P.rho};
     s->prof.begin(FFR_PROF_CORRECT, st);
-    k_correct<<<s->blocks_cells, kThreads, 0, st>>>(s->R, co, s->u, s->v, s->w, s->us, s->vs, s->ws,
-                                                     s->p, s->st);
+    // rows of even length take the paired form (16-byte loads of two cells)
+    if ((s->R.nz & 1) == 0)
+        k_correct<true><<<s->blocks_cells, kThreads, 0, st>>>(s->R, co, s->u, s->v, s->w, s->us, s->vs, s->ws,
+                                                              s->p, s->st);
+    else
+        k_correct<false><<<s->blocks_cells, kThreads, 0, st>>>(s->R, co, s->u, s->v, s->w, s->us, s->vs, s->ws,
+                                                               s->p, s->st);
     FFR_LAUNCHED(1);
     s->prof.end(st, 1);
     int nthermal = 1;
