@@ -310,8 +310,9 @@ class Server:
     batch_graph (default) each batched step replays one captured CUDA graph
     (recaptured when the membership changes).  batch_cluster (default 16):
     each batched room's whole pressure solve runs on its own thread-block
-    cluster of that size, every room's in one launch, and rooms above
-    Tuner.CLUSTER_MAX_CELLS run beside the batch on their own streams;
+    cluster of that size, every room's in one launch, and rooms the tuner
+    would not solve on a cluster (or above Tuner.CLUSTER_MAX_CELLS) run
+    beside the batch on their own streams with the tuner's schedule;
     batch_cluster=0: every room joins the batch with the one-kernel-per-pass
     solve.  batch_groups (default 1): the batched rooms may be spread over
     that many batches, each with its own stream and chunks."""
@@ -371,9 +372,13 @@ class Server:
                 if pick is None:
                     break
                 req, need = pick
-                small = req.room.n_cells <= Tuner.CLUSTER_MAX_CELLS and req.params.poisson == "mgpcg"
+                # the batch takes the rooms the tuner would solve on one
+                # cluster; the others run beside it with their own schedule
+                sched = self.tuner.schedule(req.room)
+                small = (req.room.n_cells <= Tuner.CLUSTER_MAX_CELLS and req.params.poisson == "mgpcg"
+                         and sched.cluster > 0)
                 if self.batch_cluster and not small:
-                    a = _Active(req, self.tuner.schedule(req.room), now, self.keep_fields, warm_start=self.warm_start)
+                    a = _Active(req, sched, now, self.keep_fields, warm_start=self.warm_start)
                     a.launch()
                     solo.append(a)
                 else:
