@@ -1404,9 +1404,14 @@ size_t fluid_arena_bytes(const HostRoom &room, bool mg, const MGHost &mgh)
            al(sizeof(ffr_step_result) * kRing) + 4 * 256 + (mg ? mg_bytes(room, mgh) : 0);
 }
 
+// Removes a room that is being destroyed from every batch it belongs to
+// (defined with the batch below).
+void fluid_leave_batches(ffr_fluid *s);
+
 struct ffr_fluid {
     HostRoom room;
     ffr_fluid_params prm;
+    std::vector<ffr_batch *> batches;   // the batches this room is a member of
     cudaStream_t stream = nullptr;
     Arena arena;
     RoomTables tab;
@@ -1728,6 +1733,7 @@ int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
 int ffr_fluid_destroy(ffr_fluid *s)
 {
     if (!s) return FFR_OK;
+    fluid_leave_batches(s);
     if (s->stream) cudaStreamSynchronize(s->stream);
     s->prof.destroy();
     if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
@@ -2122,13 +2128,39 @@ struct ffr_batch {
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t body_stream = nullptr;
     unsigned graph_launches = 0;
+    // a member was destroyed: its pointers are still in the device tables,
+    // so nothing is queued until the members are set again
+    bool stale = false;
 };
 
+// A destroyed room leaves every batch: the batch's queued launches may
+// still read the room, and the batch queues nothing more until its members
+// are set again.
+void fluid_leave_batches(ffr_fluid *s)
+{
+    for (ffr_batch *b : s->batches) {
+        if (b->stream) cudaStreamSynchronize(b->stream);
+        b->rooms.erase(std::remove(b->rooms.begin(), b->rooms.end(), s), b->rooms.end());
+        b->stale = true;
+    }
+    s->batches.clear();
+}
+
 namespace {
+
+// Drops b from the membership lists of its rooms.
+void batch_detach_all(ffr_batch *b)
+{
+    for (ffr_fluid *s : b->rooms) {
+        auto &v = s->batches;
+        v.erase(std::remove(v.begin(), v.end(), b), v.end());
+    }
+}
 
 void batch_free(ffr_batch *b)
 {
     if (!b) return;
+    batch_detach_all(b);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
     if (b->graph) cudaGraphDestroy(b->graph);
@@ -2204,7 +2236,10 @@ int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms)
     if (b->graph) cudaGraphDestroy(b->graph);
     b->graph_exec = nullptr;
     b->graph = nullptr;
+    batch_detach_all(b);
     b->rooms.assign(rooms, rooms + nrooms);
+    for (ffr_fluid *s : b->rooms) s->batches.push_back(b);
+    b->stale = false;
     b->cluster_ctas = rooms[0]->cluster_ctas;
     b->any_thermal = false;
     b->max_iter = 0;
@@ -2397,6 +2432,7 @@ int ffr_batch_use_graph(ffr_batch *b, int enable)
 int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge)
 {
     if (!b || nsteps < 0 || nsteps > kRing) return fail(FFR_EINVAL, "bad handle or nsteps (0..1024)");
+    if (b->stale) return fail(FFR_EINVAL, "a member room was destroyed: set the batch's rooms again");
     cudaStream_t st = b->stream;
     for (ffr_fluid *s : b->rooms) {
         if (s->pending) return fail(FFR_EINVAL, "a room has a queued chunk that was not polled");

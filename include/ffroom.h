@@ -242,9 +242,11 @@ int ffr_fluid_set_split(ffr_fluid *s, int mode);
  * ffr_fluid_set_cluster (every room's whole solve runs on its own cluster of
  * that size, all rooms in one launch; results identical to the room solved
  * alone with that cluster size); a room may
- * belong to several batches but only one may run at a time.  A batch keeps
- * pointers to its rooms: after destroying a member, replace the members
- * (ffr_batch_set_rooms) before the next ffr_batch_enqueue. */
+ * belong to several batches but only one may run at a time.  Destroying a
+ * member waits for the batch's queued work and removes the room from the
+ * batch; ffr_batch_enqueue then fails with FFR_EINVAL (queueing nothing)
+ * until ffr_batch_set_rooms replaces the members, since the batch's device
+ * tables still name the destroyed room. */
 typedef struct ffr_batch ffr_batch;
 int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out);
 /* Replaces the member rooms (the batch's device tables are rebuilt in

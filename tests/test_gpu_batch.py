@@ -104,6 +104,29 @@ def test_batch_rejects_rooms_it_cannot_take():
         capi.BatchHandle([h2, h2])
 
 
+def test_destroyed_member_leaves_the_batch():
+    """Destroying a member removes it from its batch: the batch queues
+    nothing (FfrError, before any launch) until its members are set again,
+    and then runs on with the others.  A batch that kept the destroyed
+    room's pointers would launch on freed memory."""
+    from ffrb import capi
+    g = Golden("c1_upwind_10")
+    for graph in (False, True):
+        h1, h2 = _handle(g), _handle(g)
+        b = capi.BatchHandle([h1, h2])
+        if graph:
+            b.use_graph(True)
+        first = b.advance(1)[1][0]["step"]
+        h1.close()
+        with pytest.raises(capi.FfrError):
+            b.enqueue(1)
+        b.set_rooms([h2])
+        (recs,) = b.advance(2)
+        assert [r["step"] for r in recs] == [first + 1, first + 2]
+        b.close()
+        h2.close()
+
+
 def test_batch_graph_matches_host_paced_batch():
     """The batched step captured as one CUDA graph (the solve a WHILE node
     over the count of rooms still iterating) gives exactly the host-paced
