@@ -12,18 +12,15 @@
 // The array is shared by all calls on a device and keeps the contents of
 // the last call; calls that overlap on the GPU (different streams, or
 // different host threads on one device) race on it and must be serialised
-// by the caller.  The first call on a device looks the array's device
-// address up with cudaGetSymbolAddress (set-up, once per device); make that
-// first call before any stream capture.  Each call waits for its stream to
-// finish the solve before it returns (the residual and the iteration count
-// come back through the array).  The stream must belong to the current
-// device, and the cached address lives as long as the process: a caller that
-// resets the device (cudaDeviceReset) must reload the library before calling
-// this again on that device.
+// by the caller.  Every call looks the array's device address up on the
+// current device (cudaGetSymbolAddress; no allocation), so a device reset
+// between calls is harmless.  Each call is synchronous: it copies the
+// spacings in, waits for its stream to finish the solve and copies the
+// residual and the iteration count back, so it cannot be captured into a
+// CUDA graph.  The stream must belong to the current device.
 #include "projection.cuh"
 
 #include <cstring>
-#include <mutex>
 #include <vector>
 
 namespace ffr {
@@ -48,11 +45,6 @@ constexpr size_t kScratchBytes = kOffOut + al256(64);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-namespace {
-std::mutex g_setup_mu;
-unsigned char *g_scratch_dev[256] = {nullptr};
-}  // namespace
-
 }  // namespace ffr
 
 using namespace ffr;
@@ -69,20 +61,12 @@ extern "C" int ffr_poisson_solve_noalloc(int nx, int ny, int nz, const double *d
     if (n > kNoAllocMaxCells || nx > kNoAllocMaxDim || ny > kNoAllocMaxDim || nz > kNoAllocMaxDim)
         return fail(FFR_ERANGE, "room exceeds the no-allocation capacity (FFR_NOALLOC_MAX_CELLS cells, "
                                 "FFR_NOALLOC_MAX_DIM per axis)");
-    int dev = 0;
-    FFR_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 256) return fail(FFR_ERANGE, "device ordinal out of range");
-    unsigned char *base;
+    void *ptr = nullptr;
     {
-        std::lock_guard<std::mutex> lock(g_setup_mu);
-        if (!g_scratch_dev[dev]) {
-            void *ptr = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-            if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
-            g_scratch_dev[dev] = static_cast<unsigned char *>(ptr);
-        }
-        base = g_scratch_dev[dev];
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
     }
+    unsigned char *base = static_cast<unsigned char *>(ptr);
     cudaStream_t st = (cudaStream_t)stream;
     // per-axis stencil scales (PoissonSolver.cpp:33-49), computed on the host
     // exactly as stencil_scales does, copied into the scratch array

@@ -379,13 +379,12 @@ int ffr_poisson_apply(ffr_poisson *s, const double *x, double *ax);
  * FFR_NOALLOC_MAX_DIM cells per axis; larger rooms get FFR_ERANGE.  The
  * caller passes the spacings on the host and the cell types, rhs and
  * pressure on the device; the stream must belong to the current device.
- * The call returns only after the solve has finished on that stream (it
- * reads the residual and iteration count back).  All calls on a device
- * share that array, so calls that overlap on the GPU race; the first call on
- * a device looks the array up (once per device) and should come before any
- * stream capture.  The looked-up address is kept for the life of the
- * process: after cudaDeviceReset the library must be unloaded and loaded
- * again before this entry point is used on that device. */
+ * The call is synchronous: it returns only after the solve has finished
+ * on that stream (it reads the residual and iteration count back), so it
+ * cannot be captured into a CUDA graph.  All calls on a device share that
+ * array, so calls that overlap on the GPU race.  Every call looks the
+ * array's address up on the current device, so a device reset between
+ * calls needs no reload. */
 #define FFR_NOALLOC_MAX_CELLS (64 * 64 * 64)
 #define FFR_NOALLOC_MAX_DIM 4096
 int ffr_poisson_solve_noalloc(int nx, int ny, int nz, const double *dxv, const double *dyv,
