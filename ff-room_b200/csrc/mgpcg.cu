@@ -475,6 +475,12 @@ __device__ void block_vcycle(const PCGArgs &A, int lo)
     for (int l = lo; l < nlev - 1; l++) {
         smooth_color<false>(A, lv, nlev, l, 1, t, nt);
         __syncthreads();
+        for (int sw = 1; sw < level_sweeps(l); sw++) {
+            smooth_color<false>(A, lv, nlev, l, 0, t, nt);
+            __syncthreads();
+            smooth_color<false>(A, lv, nlev, l, 1, t, nt);
+            __syncthreads();
+        }
         restrict_level(A, lv, l, t, nt);
         __syncthreads();
     }
@@ -490,6 +496,12 @@ __device__ void block_vcycle(const PCGArgs &A, int lo)
         __syncthreads();
         smooth_color<false>(A, lv, nlev, l, 0, t, nt);
         __syncthreads();
+        for (int sw = 1; sw < level_sweeps(l); sw++) {
+            smooth_color<false>(A, lv, nlev, l, 1, t, nt);
+            __syncthreads();
+            smooth_color<false>(A, lv, nlev, l, 0, t, nt);
+            __syncthreads();
+        }
     }
     if (smem) {
         const MGLevel &G = M.lv[lo];
@@ -1075,6 +1087,12 @@ __device__ __forceinline__ void pcg_body(const PCGArgs &A)
             for (int l = 0; l < M.nlev_grid && l < M.nlev - 1; l++) {
                 smooth_color<false>(A, M.lv, M.nlev, l, 1, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                for (int sw = 1; sw < level_sweeps(l); sw++) {
+                    smooth_color<false>(A, M.lv, M.nlev, l, 0, t0, nth);
+                    if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                    smooth_color<false>(A, M.lv, M.nlev, l, 1, t0, nth);
+                    if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                }
                 restrict_level(A, M.lv, l, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
             }
@@ -1087,6 +1105,12 @@ __device__ __forceinline__ void pcg_body(const PCGArgs &A)
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
                 smooth_color<false>(A, M.lv, M.nlev, l, 0, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                for (int sw = 1; sw < level_sweeps(l); sw++) {
+                    smooth_color<false>(A, M.lv, M.nlev, l, 1, t0, nth);
+                    if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                    smooth_color<false>(A, M.lv, M.nlev, l, 0, t0, nth);
+                    if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                }
             }
             if (M.nlev_grid >= 1 && M.nlev > 1) {
                 smooth_color<true>(A, M.lv, M.nlev, 0, 1, t0, nth);
@@ -1336,6 +1360,12 @@ __device__ __forceinline__ void sp_mid_body(const PCGArgs &A, int mid)
     for (int l = mid; l < top; l++) {
         smooth_color<false>(A, M.lv, M.nlev, l, 1, t0, nth);
         csync();
+        for (int sw = 1; sw < level_sweeps(l); sw++) {
+            smooth_color<false>(A, M.lv, M.nlev, l, 0, t0, nth);
+            csync();
+            smooth_color<false>(A, M.lv, M.nlev, l, 1, t0, nth);
+            csync();
+        }
         restrict_level(A, M.lv, l, t0, nth);
         csync();
     }
@@ -1347,6 +1377,12 @@ __device__ __forceinline__ void sp_mid_body(const PCGArgs &A, int mid)
         smooth_color<true>(A, M.lv, M.nlev, l, 1, t0, nth);
         csync();
         smooth_color<false>(A, M.lv, M.nlev, l, 0, t0, nth);
+        for (int sw = 1; sw < level_sweeps(l); sw++) {
+            csync();
+            smooth_color<false>(A, M.lv, M.nlev, l, 1, t0, nth);
+            csync();
+            smooth_color<false>(A, M.lv, M.nlev, l, 0, t0, nth);
+        }
         if (l > mid) csync();
     }
 }
@@ -1813,8 +1849,9 @@ unsigned split_body_kernels(const MGDev &M)
     const int top = std::min(M.nlev_grid, M.nlev - 1);
     const int gdown = std::min(M.nlev_mid, top);
     unsigned k = 2u * (unsigned)gdown;                        // grid levels: smooth + restrict
+    for (int l = 1; l < gdown; l++) k += 2u * (level_sweeps(l) - 1);   // their further pre-sweeps
     if (M.nlev_mid < top || M.nlev_grid < M.nlev) k += 1;     // k_sp_mid
-    k += 2u * (unsigned)std::max(0, gdown - 1);               // grid levels gdown-1 .. 1 post-smooth
+    for (int l = 1; l < gdown; l++) k += 2u * level_sweeps(l);         // post-smoothing, levels gdown-1 .. 1
     if (M.nlev_grid >= 1) k += 1;                             // level-0 black post-smooth
     return k + 3;                                             // red post + r.z, direction, residual
 }
@@ -1837,6 +1874,12 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
         for (int l = 0; l < gdown; l++) {
             k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
             chk();
+            for (int sw = 1; sw < level_sweeps(l); sw++) {
+                k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 0);
+                chk();
+                k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
+                chk();
+            }
             k_sp_restrict<<<split_blocks_cells(M, l + 1), 256, 0, bs>>>(a, ss, l);
             chk();
         }
@@ -1862,6 +1905,12 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
             chk();
             k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 0);
             chk();
+            for (int sw = 1; sw < level_sweeps(l); sw++) {
+                k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 1);
+                chk();
+                k_sp_smooth<false><<<split_blocks_pairs(M, l), 256, 0, bs>>>(a, ss, l, 0);
+                chk();
+            }
         }
         if (M.nlev_grid >= 1) {
             k_sp_smooth<true><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 1);
@@ -2161,6 +2210,12 @@ int batch_iteration(BatchSplit &B, cudaStream_t s)
         if (!B.nb_pairs[l]) continue;
         k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 1);
         chk("k_bsp_smooth");
+        for (int sw = 1; sw < level_sweeps(l); sw++) {
+            k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 0);
+            chk("k_bsp_smooth");
+            k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 1);
+            chk("k_bsp_smooth");
+        }
         k_bsp_restrict<<<B.nb_coarse[l], 256, 0, s>>>(B.D, B.coarse[l], l);
         chk("k_bsp_restrict");
     }
@@ -2174,6 +2229,12 @@ int batch_iteration(BatchSplit &B, cudaStream_t s)
         chk("k_bsp_smooth");
         k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 0);
         chk("k_bsp_smooth");
+        for (int sw = 1; sw < level_sweeps(l); sw++) {
+            k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 1);
+            chk("k_bsp_smooth");
+            k_bsp_smooth<false><<<B.nb_pairs[l], 256, 0, s>>>(B.D, B.pairs[l], l, 0);
+            chk("k_bsp_smooth");
+        }
     }
     if (B.nlev >= 1 && B.nb_pairs[0]) {
         k_bsp_smooth<true><<<B.nb_pairs[0], 256, 0, s>>>(B.D, B.pairs[0], 0, 1);

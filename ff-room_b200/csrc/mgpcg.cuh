@@ -13,6 +13,14 @@ constexpr int kBlockLevelCells = 640;
 // one thread-block cluster of kMidThreads-thread blocks.
 constexpr int kMidLevelCells = 32 * 1024;
 constexpr int kMidThreads = 512;
+// Red-black Gauss-Seidel sweeps per visit of a level in the V-cycle, before
+// and after its coarse-grid correction (symmetric, as CG needs): one on
+// level 0, whose red halves are fused into the residual and r.z passes,
+// kCoarseSweeps on every coarser level.  Two on the coarse levels cut the
+// PCG iterations of the 320x256x96 thermal room from 17.2 to 14.8 per step
+// for 10% more time per iteration.
+constexpr int kCoarseSweeps = 2;
+__host__ __device__ constexpr int level_sweeps(int l) { return l == 0 ? 1 : kCoarseSweeps; }
 
 // One coarse level: per cell (T to the x+, y+, z+ neighbour, diagonal), FP32.
 // Inactive cells (no FLUID/INFLOW child) have diagonal 0.
