@@ -1115,6 +1115,13 @@ __device__ __forceinline__ void pcg_body(const PCGArgs &A)
             if (M.nlev_grid >= 1 && M.nlev > 1) {
                 smooth_color<true>(A, M.lv, M.nlev, 0, 1, t0, nth);
                 if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                // the further sweeps; the last red half is the r.z pass's
+                for (int sw = 1; sw < level_sweeps(0); sw++) {
+                    smooth_color<false>(A, M.lv, M.nlev, 0, 0, t0, nth);
+                    if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                    smooth_color<false>(A, M.lv, M.nlev, 0, 1, t0, nth);
+                    if (!G::sync(A)) { flags = FFR_FLAG_TIMEOUT; goto finish; }
+                }
             }
             double acc1[1] = {0.0};
             pass_redpost_dot(A, t0, nth, acc1[0]);
@@ -1849,10 +1856,10 @@ unsigned split_body_kernels(const MGDev &M)
     const int top = std::min(M.nlev_grid, M.nlev - 1);
     const int gdown = std::min(M.nlev_mid, top);
     unsigned k = 2u * (unsigned)gdown;                        // grid levels: smooth + restrict
-    for (int l = 1; l < gdown; l++) k += 2u * (level_sweeps(l) - 1);   // their further pre-sweeps
+    for (int l = 0; l < gdown; l++) k += 2u * (level_sweeps(l) - 1);   // their further pre-sweeps
     if (M.nlev_mid < top || M.nlev_grid < M.nlev) k += 1;     // k_sp_mid
     for (int l = 1; l < gdown; l++) k += 2u * level_sweeps(l);         // post-smoothing, levels gdown-1 .. 1
-    if (M.nlev_grid >= 1) k += 1;                             // level-0 black post-smooth
+    if (M.nlev_grid >= 1) k += 2u * level_sweeps(0) - 1;      // level-0 post-smoothing before the r.z pass
     return k + 3;                                             // red post + r.z, direction, residual
 }
 
@@ -1915,6 +1922,13 @@ int split_iteration(const PCGArgs &a, SplitState *ss, cudaStream_t bs, cudaGraph
         if (M.nlev_grid >= 1) {
             k_sp_smooth<true><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 1);
             chk();
+            // the further sweeps; the last red half is k_sp_redpost's
+            for (int sw = 1; sw < level_sweeps(0); sw++) {
+                k_sp_smooth<false><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 0);
+                chk();
+                k_sp_smooth<false><<<split_blocks_pairs(M, 0), 256, 0, bs>>>(a, ss, 0, 1);
+                chk();
+            }
         }
     }
     k_sp_redpost<<<cb, 256, 0, bs>>>(a, ss);
@@ -2239,6 +2253,13 @@ int batch_iteration(BatchSplit &B, cudaStream_t s)
     if (B.nlev >= 1 && B.nb_pairs[0]) {
         k_bsp_smooth<true><<<B.nb_pairs[0], 256, 0, s>>>(B.D, B.pairs[0], 0, 1);
         chk("k_bsp_smooth");
+        // the further sweeps; the last red half is k_bsp_redpost's
+        for (int sw = 1; sw < level_sweeps(0); sw++) {
+            k_bsp_smooth<false><<<B.nb_pairs[0], 256, 0, s>>>(B.D, B.pairs[0], 0, 0);
+            chk("k_bsp_smooth");
+            k_bsp_smooth<false><<<B.nb_pairs[0], 256, 0, s>>>(B.D, B.pairs[0], 0, 1);
+            chk("k_bsp_smooth");
+        }
     }
     k_bsp_redpost<<<B.nb_cells0, 256, 0, s>>>(B.D, B.cells0);
     chk("k_bsp_redpost");

@@ -14,13 +14,15 @@ constexpr int kBlockLevelCells = 640;
 constexpr int kMidLevelCells = 32 * 1024;
 constexpr int kMidThreads = 512;
 // Red-black Gauss-Seidel sweeps per visit of a level in the V-cycle, before
-// and after its coarse-grid correction (symmetric, as CG needs): one on
-// level 0, whose red halves are fused into the residual and r.z passes,
-// kCoarseSweeps on every coarser level.  Two on the coarse levels cut the
-// PCG iterations of the 320x256x96 thermal room from 17.2 to 14.8 per step
-// for 10% more time per iteration.
-constexpr int kCoarseSweeps = 2;
-__host__ __device__ constexpr int level_sweeps(int l) { return l == 0 ? 1 : kCoarseSweeps; }
+// and after its coarse-grid correction (symmetric, as CG needs).  On level
+// 0 the first sweep's red half before the correction is fused into the
+// residual pass and the last sweep's red half after it into the r.z pass.
+// Measured on the 320x256x96 thermal room: one sweep everywhere 17.2 PCG
+// iterations per step at 388 us each (7.13 ms per step), two on the coarse
+// levels 13.75 at 444 us (6.56 ms), two on every level 9.7 at 571 us
+// (6.01 ms), three on the coarse levels no better than two.
+constexpr int kSmoothSweeps = 2;
+__host__ __device__ constexpr int level_sweeps(int) { return kSmoothSweeps; }
 
 // One coarse level: per cell (T to the x+, y+, z+ neighbour, diagonal), FP32.
 // Inactive cells (no FLUID/INFLOW child) have diagonal 0.
