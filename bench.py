@@ -46,18 +46,21 @@ CG_INIT_B = 50.0       # read u*,v*,w* + code, write r, d, x
 CG_ITER_B = 74.0       # phase A (r, d_old, x, code -> d, Ad, x) + phase B (r, Ad -> r)
 CG_FINAL_B = 24.0      # x += alpha d
 # Multigrid-preconditioned CG, split form (the bench path), per fine cell:
-# the level-0 arrays each pass must move through DRAM, counted once per pass
-# (level 1 and below, 24 MB and less for the large room, stay in L2 and
-# count nothing).  Per iteration: residual update 34 (r read and written, q,
-# code; r32 and z written), black pre-smoothing 14 (z, r32, code read, z
-# written; the colours share DRAM sectors), restriction 11 (z, r32, code;
-# the level-1 rhs), black post-smoothing 14.5 (the same plus the level-1
-# correction), red post-smoothing + r.z 22 (z, r32, code, r; z written),
-# direction + operator 46 (z, d_old, x, code; d, q, x written).  Once per
-# solve: the warm-start extrapolation 40, the set-up 68 (predicted faces,
-# code, the previous pressure; r, two directions, r32, z written) and the
-# final x update 24.
-PCG_ITER_B = 141.5
+# the level-0 arrays each pass reads or writes, counted once per pass
+# (level 1 and below, 24 MB and less for the large room, count nothing).
+# Per iteration (two red-black sweeps per level visit): residual update 34
+# (r read and written, q, code; r32 and z written), pre-smoothing black,
+# red, black 3 x 14 (z, r32, code read, z written; the colours share DRAM
+# sectors), restriction 11 (z, r32, code; the level-1 rhs), post-smoothing
+# black 14.5 (the same plus the level-1 correction), red and black 2 x 14,
+# red + r.z 22 (z, r32, code, r; z written), direction + operator 46 (z,
+# d_old, x, code; d, q, x written).  Once per solve: the warm-start
+# extrapolation 40, the set-up 68 (predicted faces, code, the previous
+# pressure; r, two directions, r32, z written) and the final x update 24.
+# The smoothing passes find z, r32 and the codes (78 MB for the large room)
+# in L2: measured DRAM traffic is 97.6 B per cell and iteration
+# (profiles/traffic.json), so this model counts bytes the L2 serves.
+PCG_ITER_B = 197.5
 PCG_ONCE_B = 132.0
 # LBM step kernel per lattice cell: read and write 19 populations, the
 # flag byte, the cell velocity (FP64 with FP64 populations, else FP32) and
@@ -75,7 +78,10 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed region.  The
+    sampler polls every 200 ms; entering waits (up to 3 s) for its first
+    sample and leaving for one taken after the region ended, so a region
+    shorter than the polling period is still bracketed by two samples."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -84,7 +90,9 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.rows = []
+        self.stamps = []
         self.proc = None
+        self.t_enter = self.t_exit = None
 
     def __enter__(self):
         try:
@@ -93,16 +101,26 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t_end = time.perf_counter() + 3.0
+            while not self.rows and time.perf_counter() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t_enter = time.perf_counter()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
+            self.stamps.append(time.perf_counter())
             self.rows.append([x.strip() for x in line.split(",")])
 
     def __exit__(self, *exc):
+        self.t_exit = time.perf_counter()
         if self.proc:
+            t_end = self.t_exit + 1.0
+            while (not self.stamps or self.stamps[-1] < self.t_exit) and time.perf_counter() < t_end \
+                    and self.proc.poll() is None:
+                time.sleep(0.005)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -121,8 +139,11 @@ class ClockSampler:
             for i, n in enumerate(names):
                 if len(r) > 5 + i and r[5 + i].lower() == "active":
                     reasons.add(n)
+        inside = sum(1 for t in self.stamps if self.t_enter is not None and self.t_exit is not None
+                     and self.t_enter <= t <= self.t_exit)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(self.rows), "samples_inside_region": inside,
+                "sampling": "every 200 ms, plus one sample just before and one just after the region"}
 
 
 def load_traffic(key: str, sub: str = None):
