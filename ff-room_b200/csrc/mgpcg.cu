@@ -10,12 +10,14 @@
 //      non-SOLID rows; the OUTFLOW rows are satisfied exactly by step 2);
 //   2. the OUTFLOW unknowns by one back-substitution of their own rows,
 //      x_o = (b_o + sum_fluid s x_nb) / diag_o;
-//   3. preconditioner: one V-cycle in FP32 on 2x2x2 cell aggregates.  Coarse
-//      face coefficients are half the sum of the fine ones across the coarse
-//      face (the rediscretised volume-scaled Laplacian), restriction sums the
+//   3. preconditioner: one V-cycle in FP32 on 2x2x2 cell aggregates, down to
+//      a level of at most kCoarsestCells cells.  Coarse face coefficients
+//      are half the sum of the fine ones across the coarse face (the
+//      rediscretised volume-scaled Laplacian), restriction sums the
 //      children's residuals, prolongation injects.  Smoothing is red-black
-//      Gauss-Seidel: red then black before the coarse correction, black then
-//      red after it, so the V-cycle is a symmetric operator and CG applies.
+//      Gauss-Seidel, kSmoothSweeps sweeps red then black before the coarse
+//      correction and black then red after it, so the V-cycle is a
+//      symmetric operator and CG applies.
 // The whole solve is one cooperative launch; levels larger than
 // kBlockLevelCells are swept by the whole grid between grid barriers, the
 // remaining small levels by block 0 alone.
@@ -51,7 +53,7 @@ void build_mg_levels(const HostRoom &r, MGHost &out)
     int nx = r.g.nx, ny = r.g.ny, nz = r.g.nz;
     out.nx.push_back(nx); out.ny.push_back(ny); out.nz.push_back(nz);
     const double lx = r.g.lx, ly = r.g.ly, lz = r.g.lz;
-    while ((size_t)nx * ny * nz > 512 && (int)out.nx.size() < kMaxLevels) {
+    while ((size_t)nx * ny * nz > (size_t)kCoarsestCells && (int)out.nx.size() < kMaxLevels) {
         // axes to halve at this level
         const double hx = lx / nx, hy = ly / ny, hz = lz / nz;
         const double hmin = std::min(hx, std::min(hy, hz));
@@ -485,7 +487,7 @@ __device__ void block_vcycle(const PCGArgs &A, int lo)
         __syncthreads();
     }
     const int last = nlev - 1;
-    for (int sweep = 0; sweep < 8; sweep++) {
+    for (int sweep = 0; sweep < kCoarsestSweeps; sweep++) {
         smooth_color<false>(A, lv, nlev, last, 1, t, nt);
         __syncthreads();
         smooth_color<false>(A, lv, nlev, last, 0, t, nt);

@@ -23,6 +23,14 @@ constexpr int kMidThreads = 512;
 // (6.01 ms), three on the coarse levels no better than two.
 constexpr int kSmoothSweeps = 2;
 __host__ __device__ constexpr int level_sweeps(int) { return kSmoothSweeps; }
+// The hierarchy coarsens until a level has at most kCoarsestCells cells,
+// which kCoarsestSweeps red-black sweeps then solve all but exactly.  The
+// coarse solve was the preconditioner's weak point: with levels down to 512
+// cells and 8 sweeps the room above took 9.7 iterations per step, with 16
+// sweeps 8.75, with levels down to 16 cells and 16 sweeps 6.8 (6.01 -> 4.65
+// ms per step); 32 sweeps or levels down to 8 cells gave no fewer.
+constexpr int kCoarsestCells = 16;
+constexpr int kCoarsestSweeps = 16;
 
 // One coarse level: per cell (T to the x+, y+, z+ neighbour, diagonal), FP32.
 // Inactive cells (no FLUID/INFLOW child) have diagonal 0.
