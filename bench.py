@@ -58,7 +58,7 @@ CG_FINAL_B = 24.0      # x += alpha d
 # extrapolation 40, the set-up 68 (predicted faces, code, the previous
 # pressure; r, two directions, r32, z written) and the final x update 24.
 # The smoothing passes find z, r32 and the codes (78 MB for the large room)
-# in L2: measured DRAM traffic is 97.6 B per cell and iteration
+# in L2: measured DRAM traffic is 83.2 B per cell and iteration
 # (profiles/traffic.json), so this model counts bytes the L2 serves.
 PCG_ITER_B = 197.5
 PCG_ONCE_B = 132.0
