@@ -2128,8 +2128,9 @@ struct ffr_batch {
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t body_stream = nullptr;
     unsigned graph_launches = 0;
-    // a member was destroyed: its pointers are still in the device tables,
-    // so nothing is queued until the members are set again
+    // a member was destroyed (its pointers are still in the device tables)
+    // or setting the members failed part-way: nothing is queued until the
+    // members are set again
     bool stale = false;
 };
 
@@ -2239,7 +2240,7 @@ int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms)
     batch_detach_all(b);
     b->rooms.assign(rooms, rooms + nrooms);
     for (ffr_fluid *s : b->rooms) s->batches.push_back(b);
-    b->stale = false;
+    b->stale = true;   // until the tables below are built
     b->cluster_ctas = rooms[0]->cluster_ctas;
     b->any_thermal = false;
     b->max_iter = 0;
@@ -2319,7 +2320,9 @@ int ffr_batch_set_rooms(ffr_batch *b, ffr_fluid *const *rooms, int nrooms)
     b->open = reinterpret_cast<const OpenItem *>(put(oitems.data(), sizeof(OpenItem) * oitems.size()));
     b->heat = reinterpret_cast<const HeatItem *>(put(hitems.data(), sizeof(HeatItem) * hitems.size()));
     FFR_CUDA(cudaMemcpy(b->dev, host.data(), bytes, cudaMemcpyHostToDevice));
-    return batch_split_build(b->split, pa, ss);
+    const int rc = batch_split_build(b->split, pa, ss);
+    if (rc == FFR_OK) b->stale = false;
+    return rc;
 }
 
 int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out)
@@ -2432,7 +2435,9 @@ int ffr_batch_use_graph(ffr_batch *b, int enable)
 int ffr_batch_enqueue(ffr_batch *b, int nsteps, int stop_on_converge)
 {
     if (!b || nsteps < 0 || nsteps > kRing) return fail(FFR_EINVAL, "bad handle or nsteps (0..1024)");
-    if (b->stale) return fail(FFR_EINVAL, "a member room was destroyed: set the batch's rooms again");
+    if (b->stale)
+        return fail(FFR_EINVAL, "the batch has no valid members (a member was destroyed, or setting the "
+                                "members failed): set the batch's rooms again");
     cudaStream_t st = b->stream;
     for (ffr_fluid *s : b->rooms) {
         if (s->pending) return fail(FFR_EINVAL, "a room has a queued chunk that was not polled");

@@ -246,7 +246,8 @@ int ffr_fluid_set_split(ffr_fluid *s, int mode);
  * member waits for the batch's queued work and removes the room from the
  * batch; ffr_batch_enqueue then fails with FFR_EINVAL (queueing nothing)
  * until ffr_batch_set_rooms replaces the members, since the batch's device
- * tables still name the destroyed room. */
+ * tables still name the destroyed room.  The same holds after an
+ * ffr_batch_set_rooms that failed. */
 typedef struct ffr_batch ffr_batch;
 int ffr_batch_create(ffr_fluid *const *rooms, int nrooms, ffr_batch **out);
 /* Replaces the member rooms (the batch's device tables are rebuilt in
