@@ -271,7 +271,7 @@ def run_ours(args, rank: int, world: int, dist):
                 "share_of_step": round(prof.get("pressure", prof.get("pressure_estimate"))[0] / ms, 4),
                 "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}
         if roof["traffic"]:
-            # the same launch judged by the DRAM bytes ncu measured for it
+            # the same launch measured by the DRAM bytes ncu counted for it
             t_launch = (ms_solve / 1e3) if args.graph else (prof["pressure"][0] / 1e3 / launches_cg)
             roof["frac_by_traffic"] = round(roof["traffic"] / t_launch / 1e9 / peak, 4)
         if args.graph:

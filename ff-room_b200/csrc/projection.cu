@@ -1752,7 +1752,7 @@ int ffr_fluid_destroy(ffr_fluid *s)
 
 int ffr_fluid_enqueue(ffr_fluid *s, int nsteps, int stop_on_converge)
 {
-    if (!s || nsteps < 0 || nsteps > kRing) return fail(FFR_EINVAL, "bad handle or nsteps (1..1024)");
+    if (!s || nsteps < 0 || nsteps > kRing) return fail(FFR_EINVAL, "bad handle or nsteps (0..1024)");
     if (s->pending) return fail(FFR_EINVAL, "a queued chunk has not been polled yet");
     k_begin_chunk<<<1, 1, 0, s->stream>>>(s->st, stop_on_converge ? 1 : 0);
     FFR_LAUNCHED(1);

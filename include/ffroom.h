@@ -41,7 +41,9 @@ typedef enum ffr_status {
 #define FFR_FLAG_CG_BREAKDOWN 4  /* |d.Ad| < 1e-30 ended the pressure solve */
 #define FFR_FLAG_TIMEOUT      8  /* a device barrier timed out */
 
-/* Static text for a status code. */
+/* Static text for a status code.  Status codes and the message below take
+ * the place of the reference's C++ exceptions (e.g. Grid.cpp:10-11 throws
+ * std::invalid_argument), which cannot cross a C ABI. */
 const char *ffr_status_string(int status);
 /* Detail of the most recent failure on the calling thread ("" if none). */
 const char *ffr_last_error(void);
@@ -56,9 +58,10 @@ int ffr_set_device_wait_limit(double seconds);
  * in *elapsed_ms; the CUDA context stays usable.  No counterpart in the
  * reference. */
 int ffr_selftest_device_wait(int blocks, double *elapsed_ms);
-/* Library version, e.g. "0.1.0 sm_100a". */
+/* Library version, e.g. "0.1.0 sm_100a" (no counterpart in the reference). */
 const char *ffr_version(void);
-/* Kernels this library has launched since load (all handles). */
+/* Kernels this library has launched since load (all handles; no
+ * counterpart in the reference). */
 unsigned long long ffr_launch_count(void);
 
 /* ------------------------------------------------------------- rooms */
@@ -163,6 +166,8 @@ typedef struct ffr_fluid ffr_fluid;
  * creating rooms never waits for a busy GPU here. */
 int ffr_fluid_create(const ffr_room_desc *room, const ffr_fluid_params *params,
                      const ffr_fields *init, ffr_fluid **out);
+/* Frees the handle (the reference's FluidSolver destructor); waits for its
+ * queued work and leaves every batch it belongs to. */
 int ffr_fluid_destroy(ffr_fluid *s);
 
 /* FluidSolver::step (FluidSolver.cpp:486-550): one projection step; `out`
@@ -187,7 +192,8 @@ int ffr_fluid_enqueue(ffr_fluid *s, int nsteps, int stop_on_converge);
  * results. */
 int ffr_fluid_poll(ffr_fluid *s, ffr_step_result *results, int max_results, int *nresults,
                    int *ready);
-/* Grid size of the cooperative pressure solve (0 = as large as the room can
+/* Schedules and sizes below have no counterpart in the reference.
+ * Grid size of the cooperative pressure solve (0 = as large as the room can
  * use).  Smaller grids let several rooms run side by side. */
 int ffr_fluid_set_blocks(ffr_fluid *s, int blocks);
 /* Runs the multigrid-preconditioned pressure solve of this room in one
@@ -282,7 +288,9 @@ int ffr_fluid_current_step(ffr_fluid *s, int *out);
 int ffr_fluid_get_field(ffr_fluid *s, int field, double *host);
 int ffr_fluid_set_field(ffr_fluid *s, int field, const double *host);
 /* Device pointer of one field (valid until destroy; the solver swaps its
- * buffers between steps, so re-query after every step). */
+ * buffers between steps, so re-query after every step).  This and the two
+ * calls below have no counterpart in the reference, whose fields live in
+ * host memory. */
 int ffr_fluid_field_dev(ffr_fluid *s, int field, double **dev);
 /* Blocks until all queued work of the handle is done. */
 int ffr_fluid_synchronize(ffr_fluid *s);
@@ -353,6 +361,7 @@ typedef struct ffr_poisson ffr_poisson;
  * (cpp/src/core/PoissonSolver.hpp:20-38); allocates its CG scratch. */
 int ffr_poisson_create(const ffr_room_desc *room, int max_iter, double tol,
                        ffr_poisson **out);
+/* Frees the handle and its CG scratch. */
 int ffr_poisson_destroy(ffr_poisson *s);
 
 /* PoissonSolver::solve (PoissonSolver.cpp:93-158) on device buffers: CG
@@ -402,6 +411,7 @@ typedef struct ffr_lbm ffr_lbm;
 int ffr_lbm_create(const ffr_room_desc *room, double tau, int max_steps,
                    double convergence_tol, double dt, int storage,
                    const ffr_fields *init, ffr_lbm **out);
+/* Frees the handle (the reference's LBMSolver destructor). */
 int ffr_lbm_destroy(ffr_lbm *s);
 /* LBMSolver::step (LBMSolver.cpp:402-440). */
 int ffr_lbm_step(ffr_lbm *s, ffr_step_result *out);
@@ -410,13 +420,15 @@ int ffr_lbm_advance(ffr_lbm *s, int nsteps, int stop_on_converge,
                     ffr_step_result *results, int *steps_done);
 /* LBMSolver::compute_divergence_max (LBMSolver.cpp:382-396). */
 int ffr_lbm_divergence_max(ffr_lbm *s, double *out);
+/* LBMSolver::current_step (LBMSolver.hpp:38). */
 int ffr_lbm_current_step(ffr_lbm *s, int *out);
 /* Fields as the reference writes them into the Grid each step
  * (extract_macroscopic, LBMSolver.cpp:288-376): u, v, w faces and p. */
 int ffr_lbm_get_field(ffr_lbm *s, int field, double *host);
 int ffr_lbm_set_field(ffr_lbm *s, int field, const double *host);
 /* Device pointer of the u, v, w or p field (valid until destroy; written in
- * place by every step, so read it in stream order). */
+ * place by every step, so read it in stream order), a wait for the handle's
+ * queued work, and its cudaStream_t; no counterpart in the reference. */
 int ffr_lbm_field_dev(ffr_lbm *s, int field, double **dev);
 int ffr_lbm_synchronize(ffr_lbm *s);
 int ffr_lbm_stream(ffr_lbm *s, void **stream);
