@@ -7,8 +7,8 @@ loop only polls (``ffr_fluid_poll``), so every active room's kernels are in
 flight together and their work overlaps on the GPU.  A room leaves at the
 chunk boundary where it converged (max|du|/dt < tol) or reached its step
 cap; a waiting room is admitted as soon as a slot and enough device memory
-are free (admission by footprint: each room is charged its estimated
-device bytes against the budget until it leaves).  Per request the server records arrival,
+are free (admission by footprint: each room is charged the library's
+figure for its device bytes against the budget until it leaves).  Per request the server records arrival,
 admission and completion times; the report gives p50/p99 time-to-converged,
 room-solves/s and cell-steps/s.
 
@@ -29,17 +29,16 @@ from . import capi
 from .params import FluidParams
 from .scene import RoomSpec, SceneConfig, build_room
 
-# device bytes per cell of a projection solver (8-byte fields u, v, w and
-# their predicted copies, p, two T buffers, four Krylov vectors, codes) and
-# the multigrid extra (FP32 z and residual, coarse levels, about 1/7 of the
-# fine level at 24 bytes per cell)
-BYTES_PER_CELL = 6 * 8 + 3 * 8 + 4 * 8 + 2 + 3 + 1
-MG_BYTES_PER_CELL = 8 + 4
+_library_estimate = capi.estimate_bytes
 
 
 def estimate_bytes(room: RoomSpec, params: FluidParams) -> int:
-    per = BYTES_PER_CELL + (MG_BYTES_PER_CELL if params.poisson == "mgpcg" else 0)
-    return int(room.n_cells * per * 1.05) + (4 << 20)
+    """Device bytes a handle of this room takes: the library's own figure
+    (ffr_fluid_estimate_bytes: the handle's allocation plus the transient
+    scratch of its multigrid set-up; host arithmetic only, no GPU needed),
+    the same figure the native server charges.  Admission charges it
+    against the budget while the room is in flight."""
+    return _library_estimate(room, params)
 
 
 def size_class(cells: int) -> int:
