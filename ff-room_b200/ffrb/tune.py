@@ -1,12 +1,13 @@
 """Autotuning of the per-room schedules on the GPU at hand.
 
 The streams engine of the server runs every room with a Schedule chosen by
-its size class (log2 of the cell count): the pressure solve on the whole GPU
-(persistent or one kernel per pass), on a fraction of the co-resident
-blocks, or on one thread-block cluster of 4, 8 or 16 blocks per room; steps
-replayed from a CUDA graph or launched one by one.  ``Tuner.tune`` times the
-candidates on rooms of each class running side by side and keeps the
-fastest by aggregate cell-steps/s.  This module runs it on samples of the
+its size class (log2 of the cell count).  The candidates
+(``Tuner.CANDIDATES``) are the pressure solve one kernel per pass on the
+whole GPU, or on one thread-block cluster of 4, 8 or 16 blocks per room,
+each step replayed from a CUDA graph (the persistent cooperative solve is
+left out: beside other rooms' kernels its grid is not co-resident).
+``Tuner.tune`` times the candidates on rooms of each class running side by
+side and keeps the fastest by aggregate cell-steps/s.  This module runs it on samples of the
 serving stream and of the batch of uneven rooms and stores the table, so
 that servers (and the benchmark) start from a tuned table instead of the
 built-in defaults:
