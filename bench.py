@@ -327,6 +327,21 @@ def run_e2e(args, kind, room, params):
 
 # ------------------------------------------------- CPU reference timing
 
+def host_threads() -> int:
+    """Threads the reference's OpenMP loops run on: OMP_NUM_THREADS when it
+    is set, else every core this process may run on (its affinity mask)."""
+    try:
+        n = int(os.environ.get("OMP_NUM_THREADS", "").split(",")[0])
+        if n > 0:
+            return n
+    except ValueError:
+        pass
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_reference(kind, room, params, nsteps=20, budget_s=15.0, single_thread=True):
     """The reference solver (oracle/_ref driver) on a bounded sample of the
     workload: the first steps of the room from rest, stopping at the first
@@ -334,7 +349,7 @@ def cpu_reference(kind, room, params, nsteps=20, budget_s=15.0, single_thread=Tr
     cells divided by the median wall time of one step() call.  With
     single_thread, a one-thread estimate is added beside it."""
     import oracle as orc
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     cells = room.n_cells
     if not orc.ref_available():
