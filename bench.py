@@ -360,7 +360,8 @@ def cpu_reference(kind, room, params, nsteps=20, budget_s=15.0, single_thread=Tr
         t = statistics.median(r.seconds for r in recs)
         return {"value": cells / t, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
                 "sample": f"{len(recs)} LBM steps of the {room.nx}x{room.ny}x{room.nz} lattice, median step() "
-                          "time (the reference LBM has no OpenMP)"}
+                          "time (the reference LBM has no OpenMP)",
+                "steps_timed": len(recs), "seconds_stepping": round(sum(r.seconds for r in recs), 2)}
     # the reference has one pressure method: plain FP64 CG, to the same
     # tolerance and iteration cap
     p = params.with_(precision="fp64", poisson="cg")
