@@ -264,6 +264,9 @@ class RefDriver:
         self.lib.ffref_lbm_run.argtypes = [C.POINTER(_RefRoom), C.c_double, C.c_double, C.c_double,
                                            C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.POINTER(_RefResult)]
         self.lib.ffref_lbm_run.restype = C.c_int
+        self.lib.ffref_poisson_solve.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                                 _u8p, _dp, C.c_int, C.c_double, _dp, _ip]
+        self.lib.ffref_poisson_solve.restype = C.c_double
 
     @staticmethod
     def room(room):
@@ -319,6 +322,17 @@ class RefDriver:
                                      _ptr(ct, _u8p), _ptr(fl["u"]), _ptr(fl["v"]), _ptr(fl["w"]),
                                      _ptr(fl["p"]), _ptr(fl["T"]), res)
         return fl, ct, _records(res, n)
+
+    def poisson_solve(self, room, rhs, max_iter, tol):
+        """The reference PoissonSolver on the room's cell types as given
+        (no BoundaryManager replay): returns (p, residual, iterations)."""
+        ct = np.ascontiguousarray(room.cell_type, dtype=np.uint8)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        p = np.zeros(room.n_cells)
+        it = C.c_int(0)
+        res = self.lib.ffref_poisson_solve(room.nx, room.ny, room.nz, room.lx, room.ly, room.lz, _ptr(ct, _u8p),
+                                           _ptr(rhs), max_iter, tol, _ptr(p), C.byref(it))
+        return p, res, it.value
 
     def lbm_run(self, room, tau, dt, tol, nsteps, stop_on_converge=False):
         r, keep = self.room(room)

@@ -198,4 +198,24 @@ int ffref_lbm_run(const ffref_room *d, double tau, double dt, double tol, int ns
     return done;
 }
 
+// PoissonSolver::solve (PoissonSolver.cpp:93-158) on a grid whose cell
+// types are given cell by cell, as the reference's own Poisson test sets
+// them (a room no BoundaryManager call can build).  Writes the pressure and
+// the iteration count; returns the relative residual.
+double ffref_poisson_solve(int nx, int ny, int nz, double lx, double ly, double lz,
+                           const uint8_t *cell_type, const double *rhs, int max_iter, double tol,
+                           double *p, int *iterations)
+{
+    Grid g(nx, ny, nz, lx, ly, lz);
+    for (size_t c = 0; c < g.cell_type.size(); c++) g.cell_type[c] = static_cast<CellType>(cell_type[c]);
+    PoissonSolverParams prm;
+    prm.max_iter = max_iter;
+    prm.tol = tol;
+    PoissonSolver s(prm);
+    const double res = s.solve(g, std::vector<double>(rhs, rhs + g.p.size()));
+    put(g.p, p);
+    if (iterations) *iterations = s.last_iterations();
+    return res;
+}
+
 }  // extern "C"
