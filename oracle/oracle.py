@@ -264,9 +264,10 @@ class RefDriver:
         self.lib.ffref_lbm_run.argtypes = [C.POINTER(_RefRoom), C.c_double, C.c_double, C.c_double,
                                            C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.POINTER(_RefResult)]
         self.lib.ffref_lbm_run.restype = C.c_int
-        self.lib.ffref_poisson_solve.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
-                                                 _u8p, _dp, C.c_int, C.c_double, _dp, _ip]
-        self.lib.ffref_poisson_solve.restype = C.c_double
+        if hasattr(self.lib, "ffref_poisson_solve"):     # absent from drivers built before it was added
+            self.lib.ffref_poisson_solve.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                                     C.c_double, _u8p, _dp, C.c_int, C.c_double, _dp, _ip]
+            self.lib.ffref_poisson_solve.restype = C.c_double
 
     @staticmethod
     def room(room):
