@@ -196,7 +196,7 @@ def make_workload(name: str, precision: str, grid=None):
 
 # ---------------------------------------------------------- our arm
 
-def run_ours(args, rank: int, world: int, dist):
+def run_ours(args, rank: int, world: int, dist, with_e2e: bool = True):
     import torch
     from ffrb import capi
     kind, cfg, room, params = make_workload(args.workload, args.precision, args.grid)
@@ -289,9 +289,30 @@ def run_ours(args, rank: int, world: int, dist):
                 "groups_ms": {g: round(v[0], 3) for g, v in prof.items()}}
         extra = {"storage": params["storage"]}
     h.close()
-    e2e = run_e2e(args, kind, room, params) if rank == 0 else None
+    e2e = run_e2e(args, kind, room, params) if (rank == 0 and with_e2e) else None
     return {"value": value, "ms": ms, "steps": steps_done, "launches": launches, "roofline": roof,
             "clocks": clk.summary(), "extra": extra, "e2e": e2e, "cells": cells, "kind": kind}
+
+
+def run_plain_fp64(args):
+    """The reference's method on this GPU, on the same room: plain FP64 CG
+    from a zero pressure (FFR_PREC_FP64, FFR_POISSON_CG), 2 timed steps
+    after 1 warm-up step from rest, each step replayed from a CUDA graph.
+    The like-for-like comparison beside the headline value, which adds the
+    mixed-precision multigrid method.  A failure here is reported in the
+    block and leaves the rest of the line intact."""
+    import copy
+    a = copy.copy(args)
+    a.precision, a.steps, a.warmup = "fp64", 2, 1
+    try:
+        r = run_ours(a, 0, 1, None, with_e2e=False)
+    except Exception as e:  # noqa: BLE001 - reported, not raised
+        return {"error": f"{type(e).__name__}: {e}"}
+    return {"value": r["value"], "unit": "cell-steps/s", "steps": r["steps"], "warmup": 1,
+            "ms_per_step": r["ms"] / max(1, r["steps"]), "cg_iterations_mean": r["extra"]["cg_iterations_mean"],
+            "method": "plain FP64 CG from a zero pressure (the reference's method) on this GPU, same room, "
+                      "steps 2-3 from rest",
+            "roofline": r["roofline"], "gpu_launches": r["launches"], "clocks": r["clocks"]}
 
 
 def run_e2e(args, kind, room, params):
@@ -733,7 +754,7 @@ def main():
     ap.add_argument("--max-cells", type=int, default=600_000, help="serving/batch: largest room in the sample")
     ap.add_argument("--max-steps", type=int, default=40, help="serving/batch: step cap per room")
     ap.add_argument("--no-serving", action="store_true",
-                    help="default run: skip the serving, batch and lattice samples")
+                    help="default run: skip the plain FP64 comparison and the serving, batch and lattice samples")
     ap.add_argument("--tol", type=float, default=1e-4, help="serving_c5: the stop rule's max|du|/dt")
     ap.add_argument("--batched", type=int, default=0,
                     help="serving/batch: 1 = one launch per stage for all active rooms, 0 = one stream per room")
@@ -791,6 +812,11 @@ def main():
         extra_blocks = {}
         if not args.no_serving and args.workload == "large_thermal" and world == 1:
             # the other benchmark configurations, each a bounded sample
+            if kind == "fluid" and args.precision != "fp64":
+                pf = run_plain_fp64(args)
+                if "value" in pf:
+                    pf["headline_over_plain_fp64"] = res["value"] / pf["value"]
+                extra_blocks["plain_fp64_same_room"] = pf
             extra_blocks["serving"] = run_serving_c5(96, 200, 1e-4)
             extra_blocks["serving_reference_tol"] = run_serving_c5(48, 2000, 1.0, max_cells=600_000,
                                                                    engines=("streams",))
