@@ -69,3 +69,33 @@ def test_host_threads_follow_the_openmp_setting(monkeypatch):
     assert bench.host_threads() == 5
     monkeypatch.delenv("OMP_NUM_THREADS")
     assert bench.host_threads() == len(os.sched_getaffinity(0))
+
+
+def test_clock_summary_names_the_throttle_reasons():
+    """The clocks block of the line: median SM clock under load, the
+    maximum, and every throttle reason seen active (nvidia-smi columns in
+    the order ClockSampler.Q asks for them)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.ClockSampler(0)
+    na = "Not Active"
+    c.rows = [["0", "1965", "1965", "700.1", "0x0", na, na, na, na],
+              ["0", "1800", "1965", "990.0", "0x4", na, na, na, "Active"],
+              ["0", "1410", "1965", "990.0", "0x8", na, na, "Active", "Active"]]
+    c.stamps = [1.0, 2.0, 3.0]
+    c.t_enter, c.t_exit = 1.5, 3.5
+    s = c.summary()
+    assert s["sm_mhz"] == 1800.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap", "sw_thermal_slowdown"]
+    assert s["samples"] == 3 and s["samples_inside_region"] == 2
+    assert bench.ClockSampler(0).summary()["reasons"] == ["unsampled"]
+
+
+def test_solve_traffic_scales_the_measured_figures():
+    sys.path.insert(0, ROOT)
+    import bench
+    it = bench.load_traffic("pcg_split_bytes_per_cell_iter")
+    once = bench.load_traffic("pcg_split_bytes_per_cell_once")
+    assert it > 0 and once > 0
+    assert bench.solve_traffic(True, 1000, 7.0) == pytest.approx(1000 * (once + 7.0 * it))
+    assert bench.solve_traffic(False, 1000, 10.0) == pytest.approx(1000 * 10.0 * bench.load_traffic("cg_bytes_per_cell_iter"))
